@@ -1,0 +1,343 @@
+/*
+ * slosh_cuda.h -- C ABI of the B200-native Slosh FLIP/APIC substep.
+ *
+ * The types mirror the plain-data simulation types of the Slosh Unreal plugin
+ * (PLUG = SloshDemo/Plugins/Slosh):
+ *   slosh_settings_t        <- FSloshSolverSettings   PLUG/Source/SloshCore/Public/SloshTypes.h:113-160
+ *   slosh_particle_t        <- FSloshParticleGPU      SloshTypes.h:84-91 (48 bytes, C as 9 halves)
+ *   slosh_collider_t        <- FSloshColliderGPU      SloshTypes.h:32-44 (80 bytes)
+ *   slosh_manipulator_t     <- FSloshManipulatorGPU   SloshTypes.h:66-80 (80 bytes)
+ *   slosh_emit_request_t    <- FSloshEmitRequest      SloshTypes.h:169-181
+ *   slosh_frame_input_t     <- FSloshFrameInput       SloshTypes.h:184-194
+ *   slosh_results_t         <- FSloshResults          SloshTypes.h:208-231
+ *
+ * The functions replace the public surface of FSloshProxy
+ * (PLUG/Source/SloshCore/Public/SloshProxy.h:23-147); each declaration names the
+ * member it stands in for. All calls are synchronous with respect to the host
+ * unless stated; device work is issued on the context's CUDA stream.
+ *
+ * Ownership: the library owns all device memory. Host arrays passed in are
+ * copied during the call. Device pointers handed out stay valid until the next
+ * step call or slosh_destroy.
+ *
+ * Threading: one context per host thread at a time; no internal threads.
+ */
+#ifndef SLOSH_CUDA_H
+#define SLOSH_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(_WIN32)
+#define SLOSH_API __declspec(dllexport)
+#else
+#define SLOSH_API __attribute__((visibility("default")))
+#endif
+
+#define SLOSH_ABI_VERSION 1u
+
+/* Limits, SloshTypes.h:93-110. The particle cap is raised above the reference's 16,777,216. */
+#define SLOSH_MAX_COLLIDERS 64u
+#define SLOSH_MAX_MANIPULATORS 32u
+#define SLOSH_COUPLING_STRIDE 16u
+#define SLOSH_NUM_STATS 16u
+#define SLOSH_MAX_MG_LEVELS 8u
+
+/* Status codes. The reference has none (values are clamped silently,
+ * SloshProxy.cpp:345-347); every entry point here returns one. */
+typedef enum slosh_status {
+    SLOSH_OK = 0,
+    SLOSH_ERR_INVALID_ARG = 1,
+    SLOSH_ERR_OUT_OF_MEMORY = 2,
+    SLOSH_WARN_POOL_OVERFLOW = 3, /* warning: bricks found the pool full (ballistic fallback ran) */
+    SLOSH_ERR_NOT_CONVERGED = 4,  /* warning: a solve hit max_iterations above its tolerance */
+    SLOSH_ERR_DEVICE_TIMEOUT = 5, /* a bounded device-side wait gave up */
+    SLOSH_ERR_CUDA = 6,
+    SLOSH_ERR_NO_DEVICE = 7,
+    SLOSH_ERR_CAPACITY = 8        /* particle capacity exceeded */
+} slosh_status;
+
+/* ESloshTransferMode, SloshTypes.h:10-14 */
+enum { SLOSH_TRANSFER_FLIP = 0, SLOSH_TRANSFER_APIC = 1 };
+/* ESloshPressureSolver, SloshTypes.h:16-22 */
+enum { SLOSH_SOLVER_RBGS = 0, SLOSH_SOLVER_MGPCG = 1 };
+/* ESloshColliderShape, SloshTypes.h:24-29 */
+enum { SLOSH_COLLIDER_SPHERE = 0, SLOSH_COLLIDER_BOX = 1, SLOSH_COLLIDER_CAPSULE = 2 };
+/* ESloshEmitShape, SloshTypes.h:162-167 */
+enum { SLOSH_EMIT_FILL_CELLS = 0, SLOSH_EMIT_SPHERE = 1, SLOSH_EMIT_BOX = 2 };
+/* Storage precision of the multigrid preconditioner (extension, no reference counterpart). */
+enum { SLOSH_PRECISION_FP32 = 0, SLOSH_PRECISION_FP16_STORAGE = 1, SLOSH_PRECISION_BF16_STORAGE = 2 };
+/* Pressure warm start (extension). PREVIOUS is the reference behaviour (MarkCellsCS rescale). */
+enum { SLOSH_WARM_START_ZERO = 0, SLOSH_WARM_START_PREVIOUS = 1, SLOSH_WARM_START_LEARNED = 2 };
+
+/* FSloshSolverSettings, field for field (SloshTypes.h:113-160), then extensions. */
+typedef struct slosh_settings_t {
+    int32_t grid_dim[3];                 /* GridDim                     */
+    float cell_size;                     /* CellSize (m)                */
+    uint32_t particle_capacity;          /* ParticleCapacity            */
+    uint32_t transfer_mode;              /* TransferMode                */
+    float flip_ratio;                    /* FlipRatio                   */
+    float density;                       /* Density (kg/m^3)            */
+    float kinematic_viscosity;           /* KinematicViscosity          */
+    float boundary_friction;             /* BoundaryFriction            */
+    float adhesion;                      /* Adhesion                    */
+    float adhesion_distance;             /* AdhesionDistance            */
+    float density_correction;            /* DensityCorrection           */
+    float density_deadband;              /* DensityDeadband             */
+    uint32_t two_sided_density_projection; /* bTwoSidedDensityProjection */
+    float density_relaxation;            /* DensityRelaxation           */
+    int32_t density_projection_iterations; /* DensityProjectionIterations */
+    int32_t density_projection_interval; /* DensityProjectionInterval   */
+    uint32_t sparse_bricks;              /* bSparseBricks               */
+    float sparse_max_active_fraction;    /* SparseMaxActiveFraction     */
+    float sparse_storage_budget;         /* SparseStorageBudget         */
+    float particle_radius_cells;         /* ParticleRadiusCells         */
+    float gravity[3];                    /* Gravity                     */
+    uint32_t pressure_solver;            /* PressureSolver              */
+    int32_t pressure_iterations;         /* PressureIterations (RBGS)   */
+    float sor_weight;                    /* SORWeight                   */
+    int32_t pcg_iterations;              /* PCGIterations               */
+    int32_t mg_coarse_iterations;        /* MGCoarseIterations          */
+    int32_t sort_interval;               /* SortInterval                */
+    uint32_t smooth_coupling_force;      /* bSmoothCouplingForce        */
+    uint32_t ghost_fluid;                /* bGhostFluid                 */
+    int32_t viscosity_iterations;        /* ViscosityIterations         */
+    int32_t extrapolation_layers;        /* ExtrapolationLayers         */
+    int32_t min_substeps;                /* MinSubsteps                 */
+    int32_t max_substeps;                /* MaxSubsteps                 */
+    float max_frame_dt;                  /* MaxFrameDt                  */
+    float cfl;                           /* CFL                         */
+    float max_speed;                     /* MaxSpeed                    */
+    /* ---- extensions (no reference counterpart) ---- */
+    float tolerance;        /* > 0: MGPCG iterates until ||r||/||b|| <= tolerance (or max_iterations);
+                               <= 0: the reference's fixed pcg_iterations */
+    int32_t max_iterations; /* iteration cap when tolerance > 0 */
+    uint32_t precision_mode;/* SLOSH_PRECISION_* of the V-cycle storage */
+    uint32_t warm_start;    /* SLOSH_WARM_START_* */
+} slosh_settings_t;
+
+/* FSloshParticleGPU (SloshTypes.h:84-91): Pos, Age (negative or NaN = dead), Vel,
+ * C = APIC affine rows Cx, Cy, Cz as 9 halves in 5 words (SloshCommon.ush:63-105). */
+typedef struct slosh_particle_t {
+    float pos[3];
+    float age;
+    float vel[3];
+    uint32_t c[5];
+} slosh_particle_t;
+
+/* FSloshColliderGPU (SloshTypes.h:32-44). */
+typedef struct slosh_collider_t {
+    float center[3];
+    uint32_t type;
+    float rotation[4]; /* quaternion x, y, z, w; local -> sim */
+    float extent[3];
+    uint32_t flags;
+    float linear_velocity[3];
+    float pad0;
+    float angular_velocity[3];
+    float pad1;
+} slosh_collider_t;
+
+/* FSloshManipulatorGPU (SloshTypes.h:66-80). */
+typedef struct slosh_manipulator_t {
+    float center[3];
+    uint32_t kind;
+    float rotation[4];
+    float extent[3];
+    uint32_t shape;
+    float axis[3];
+    float strength;
+    float falloff;
+    float param0;
+    float param1;
+    uint32_t pad;
+} slosh_manipulator_t;
+
+/* FSloshEmitRequest (SloshTypes.h:169-181) plus fill_jitter. */
+typedef struct slosh_emit_request_t {
+    uint32_t shape;           /* SLOSH_EMIT_* */
+    float center[3];
+    float extent[3];
+    float velocity[3];
+    float rotation[4];
+    float velocity_spread;
+    float speed_jitter;
+    int32_t cell_min[3];      /* FillCells only */
+    int32_t cell_dims[3];
+    uint32_t count;           /* Sphere / Box */
+    float fill_jitter;        /* extension: FillCells jitter amplitude in half-cells; the reference
+                                 hard-codes 0.8 (Slosh.usf:310); 1.0 gives +-0.25 cell */
+} slosh_emit_request_t;
+
+/* FSloshFrameInput (SloshTypes.h:184-194) with POD arrays; SimToWorld is a rendering
+ * concern and is not carried. */
+typedef struct slosh_frame_input_t {
+    slosh_settings_t settings;
+    const slosh_collider_t* colliders;
+    uint32_t num_colliders;
+    const slosh_emit_request_t* emits;
+    uint32_t num_emits;
+    const slosh_manipulator_t* manipulators;
+    uint32_t num_manipulators;
+    float delta_time;
+    uint32_t reset;
+    uint32_t paused;
+} slosh_frame_input_t;
+
+/* FSloshColliderFeedback (SloshTypes.h:197-206). */
+typedef struct slosh_collider_feedback_t {
+    float pressure_force[3];
+    float pressure_torque[3];
+    float mean_fluid_velocity[3];
+    float submerged_centroid_offset[3];
+    int32_t wetted_faces;
+    int32_t submerged_cells;
+    int32_t solid_cells;
+} slosh_collider_feedback_t;
+
+/* FSloshResults (SloshTypes.h:208-231) decoded synchronously (the reference reads back
+ * 2-4 frames late, SloshProxy.cpp:739-805), plus solver statistics. */
+typedef struct slosh_results_t {
+    float max_particle_speed;
+    int32_t fluid_cells;
+    float max_divergence;
+    float mean_divergence;
+    float mean_interior_density;
+    int32_t interior_cells;
+    float active_brick_fraction;
+    float pool_usage;
+    int32_t pool_overflow_bricks;
+    int32_t clamped_particles;
+    int32_t clamped_in_solid;
+    float clamped_centroid[3];
+    float grid_memory_mb;
+    float particle_memory_mb;
+    int32_t allocated_particle_capacity;
+    int32_t live_particles;
+    int64_t drained_particles;
+    int32_t substeps;
+    uint64_t sim_frame;
+    uint32_t num_colliders;
+    slosh_collider_feedback_t colliders[SLOSH_MAX_COLLIDERS];
+    /* extensions */
+    int32_t last_solve_iterations;     /* PCG iterations of the last pressure solve */
+    float last_solve_rel_residual;     /* recursive ||r||/||b|| at its end */
+    float last_solve_true_rel_residual;/* ||b - A p||/||b|| recomputed at its end */
+    uint32_t raw_stats[SLOSH_NUM_STATS];
+} slosh_results_t;
+
+/* Grid and pool layout (SloshProxy.cpp:185-306), for parity tools. */
+typedef struct slosh_layout_t {
+    int32_t grid_dim[3];
+    int32_t brick_dim[3];
+    uint32_t num_bricks;
+    uint32_t num_pool_bricks;   /* pool slots including the null slot 0 */
+    uint32_t pool_cells;        /* num_pool_bricks * 512 */
+    uint32_t total_faces;       /* 3 * pool_cells */
+    int32_t sort_brick_dim[3];
+    uint32_t num_sort_keys;
+    uint32_t num_mg_levels;
+    int32_t mg_dim[SLOSH_MAX_MG_LEVELS][3];
+    uint32_t num_particles;     /* particle slots in use (dispatch bound) */
+    uint32_t particle_capacity;
+    uint32_t current_vel;       /* which face-velocity buffer holds the post-step field */
+} slosh_layout_t;
+
+/* Buffer identifiers for slosh_read_buffer / slosh_write_buffer (state export/import
+ * for parity tests and checkpoints). Element types: u32 unless noted. */
+typedef enum slosh_buffer_id {
+    SLOSH_BUF_PARTICLES = 0,    /* slosh_particle_t[num_particles] */
+    SLOSH_BUF_VEL = 1,          /* f32[total_faces], the current face-velocity field */
+    SLOSH_BUF_VEL_OLD = 2,      /* f32[total_faces] */
+    SLOSH_BUF_FACE_FLAGS = 3,   /* u32[total_faces] */
+    SLOSH_BUF_FACE_WEIGHT = 4,  /* f32[total_faces] */
+    SLOSH_BUF_CELL_TYPE = 5,    /* u32[pool_cells] */
+    SLOSH_BUF_CELL_COUNT = 6,   /* i32[pool_cells] */
+    SLOSH_BUF_PRESSURE = 7,     /* f32[pool_cells] */
+    SLOSH_BUF_DIVERGENCE = 8,   /* f32[pool_cells] */
+    SLOSH_BUF_CELL_DIAG = 9,    /* f32[pool_cells] */
+    SLOSH_BUF_DENSITY_Q = 10,   /* f32[pool_cells] */
+    SLOSH_BUF_DENSITY_RHS = 11, /* f32[pool_cells] */
+    SLOSH_BUF_BRICK_TABLE = 12, /* u32[num_bricks] */
+    SLOSH_BUF_SLOT_BRICK = 13,  /* u32[num_pool_bricks] */
+    SLOSH_BUF_FREE_SLOTS = 14,  /* u32[num_pool_bricks] */
+    SLOSH_BUF_ACTIVE_BRICKS = 15, /* u32[num_bricks + 1] */
+    SLOSH_BUF_NEW_SLOTS = 16,   /* u32[num_pool_bricks + 1] */
+    SLOSH_BUF_BRICK_TOUCH = 17, /* u32[num_bricks] */
+    SLOSH_BUF_STATS = 18,       /* u32[16] */
+    SLOSH_BUF_SORT_COUNTS = 19, /* u32[num_sort_keys] */
+    SLOSH_BUF_SORT_OFFSETS = 20,/* u32[num_sort_keys], global exclusive offsets */
+    SLOSH_BUF_SORT_PERM = 21,   /* u32[num_particles]: source slot of each sorted particle (last sort) */
+    SLOSH_BUF_PARTICLE_COUNT = 22, /* u32[4] */
+    SLOSH_BUF_ACCUM = 23,       /* i32[2 * total_faces] */
+    SLOSH_BUF_VEL_EXTRAP = 24,  /* f32[total_faces]: displacement / scratch velocity buffer of the last G2P */
+    SLOSH_BUF_COUNT_
+} slosh_buffer_id;
+
+/* ---- library ---- */
+SLOSH_API uint32_t slosh_abi_version(void);
+/* Reference defaults of FSloshSolverSettings (SloshTypes.h:113-160) and extension defaults. */
+SLOSH_API void slosh_settings_default(slosh_settings_t* out);
+/* Thread-local text of the last error of any call on this thread. */
+SLOSH_API const char* slosh_last_error_string(void);
+
+/* ---- lifecycle: replaces FSloshProxy construction / ReleaseOnRenderThread (SloshProxy.h:26-33)
+ * and Allocate (SloshProxy.cpp:185-306). device < 0 uses the current device. */
+SLOSH_API slosh_status slosh_create(const slosh_settings_t* settings, int32_t device, void** out_ctx);
+SLOSH_API void slosh_destroy(void* ctx);
+/* Issue device work on an external stream (cudaStream_t); NULL restores the context's own stream. */
+SLOSH_API slosh_status slosh_set_stream(void* ctx, void* cuda_stream);
+SLOSH_API slosh_status slosh_synchronize(void* ctx);
+
+/* ---- frame: replaces SubmitFrame_GameThread + Step_RenderThread (SloshProxy.cpp:146-161, 339-737).
+ * Emission, the periodic spatial sort, CFL substep count and all substeps of one frame. */
+SLOSH_API slosh_status slosh_step_frame(void* ctx, const slosh_frame_input_t* input);
+/* Split form of slosh_step_frame for per-substep harnesses: begin_frame does the frame prologue
+ * (settings, emission, sort) and returns the substep count and dt; substep(i) runs one substep. */
+SLOSH_API slosh_status slosh_begin_frame(void* ctx, const slosh_frame_input_t* input,
+                                         int32_t* out_substeps, float* out_dt);
+SLOSH_API slosh_status slosh_substep(void* ctx, int32_t step_index);
+SLOSH_API slosh_status slosh_end_frame(void* ctx);
+
+/* ---- individual phases (harness control; SloshProxy.cpp:1022-1087, 582-592) ---- */
+/* Spatial sort + compaction of the particle buffer (AddSpatialSort). */
+SLOSH_API slosh_status slosh_sort_particles(void* ctx);
+/* One emission request (EmitReserveCS + EmitParticlesCS, Slosh.usf:272-358). */
+SLOSH_API slosh_status slosh_emit(void* ctx, const slosh_emit_request_t* request);
+/* Sets the proxy's emission seed counter (FSloshProxy::EmitSeed, SloshProxy.h:80; starts at 1
+ * and increments once per emission, SloshProxy.cpp:529). */
+SLOSH_API slosh_status slosh_set_emit_seed(void* ctx, uint32_t seed);
+
+/* ---- particle data: replaces GetParticleBuffer_RenderThread / GetNumParticles_RenderThread
+ * (SloshProxy.h:41-42). The reference has no upload; it is added for seeded scenes. */
+SLOSH_API slosh_status slosh_upload_particles(void* ctx, const slosh_particle_t* particles, uint32_t count);
+SLOSH_API slosh_status slosh_download_particles(void* ctx, slosh_particle_t* out, uint32_t capacity, uint32_t* out_count);
+SLOSH_API slosh_status slosh_particle_device_ptr(void* ctx, void** out_ptr, uint32_t* out_count);
+
+/* ---- results: replaces GetResults (SloshProxy.cpp:177-183) + PollReadbacks decode (:739-805) ---- */
+SLOSH_API slosh_status slosh_get_results(void* ctx, slosh_results_t* out);
+SLOSH_API slosh_status slosh_get_layout(void* ctx, slosh_layout_t* out);
+
+/* ---- state export / import (checkpoint and parity; the reference has none) ---- */
+SLOSH_API slosh_status slosh_buffer_bytes(void* ctx, int32_t buffer_id, size_t* out_bytes);
+SLOSH_API slosh_status slosh_read_buffer(void* ctx, int32_t buffer_id, void* host_dst, size_t bytes);
+SLOSH_API slosh_status slosh_write_buffer(void* ctx, int32_t buffer_id, const void* host_src, size_t bytes);
+
+/* ---- timing (CUDA events on the context's stream): per-phase device milliseconds of the
+ * last frame, summed over substeps. Phases: 0 sort, 1 pool, 2 p2g, 3 grid (mark, normalize,
+ * divergence), 4 pressure, 5 project+residual, 6 density projection, 7 extrapolate, 8 g2p. */
+#define SLOSH_NUM_PHASES 9
+SLOSH_API slosh_status slosh_enable_phase_timing(void* ctx, int32_t enable);
+SLOSH_API slosh_status slosh_get_phase_ms(void* ctx, float* out_ms, int32_t n);
+/* Number of kernel launches this library issued since creation. */
+SLOSH_API uint64_t slosh_launch_count(void* ctx);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* SLOSH_CUDA_H */

@@ -1,0 +1,1117 @@
+// Host driver and C ABI of the B200-native Slosh substep.
+//
+// Replaces FSloshProxy (PLUG/Source/SloshCore/Public/SloshProxy.h:23-147,
+// PLUG/Source/SloshCore/Private/SloshProxy.cpp): Allocate (:185-306), EnsureParticleCapacity
+// (:308-337), Step_RenderThread (:339-737), PollReadbacks_RenderThread's decode (:739-805),
+// AddPressureSolveMGPCG (:807-1020) and AddSpatialSort (:1022-1087). Device work is issued on one CUDA
+// stream; kernels read counts (active bricks, new slots, particle count) on the device, so a substep
+// enqueues without host round trips except for the optional relative-residual test of MGPCG.
+//
+// Differences from the reference's host code, by design:
+//   * results are read back synchronously at the end of each frame (the reference polls a 4-slot ring
+//     2-4 frames late); the substep count therefore uses the previous frame's exact max speed;
+//   * particle storage is sized to particle_capacity when the layout is allocated, and grows if the
+//     capacity is raised;
+//   * the three face-velocity buffers rotate roles instead of copying the final field into buffer 0
+//     (SloshProxy.cpp:709-712); slosh_read_buffer(SLOSH_BUF_VEL) returns the current field;
+//   * the grid and particle caps are raised (2048 cells per axis, 2^28 particles).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "kernels.h"
+
+namespace slosh {
+namespace {
+
+thread_local std::string g_error;
+
+struct CudaError {
+    cudaError_t code;
+    const char* what;
+};
+#define CK(call)                                                      \
+    do {                                                              \
+        cudaError_t e_ = (call);                                      \
+        if (e_ != cudaSuccess) throw CudaError{e_, #call};            \
+    } while (0)
+
+struct StatusError {
+    slosh_status code;
+    std::string what;
+};
+
+constexpr uint32_t MG_COARSEST_MAX_CELLS = 512u;
+constexpr int MG_MAX_LEVELS = 8;
+constexpr int NUM_PHASES = SLOSH_NUM_PHASES;
+
+slosh_settings_t defaults() {
+    slosh_settings_t s;
+    std::memset(&s, 0, sizeof(s));
+    s.grid_dim[0] = 64; s.grid_dim[1] = 64; s.grid_dim[2] = 48;
+    s.cell_size = 0.05f;
+    s.particle_capacity = 262144u;
+    s.transfer_mode = SLOSH_TRANSFER_APIC;
+    s.flip_ratio = 0.95f;
+    s.density = 1000.0f;
+    s.adhesion_distance = 0.025f;
+    s.density_correction = 0.15f;
+    s.density_deadband = 0.05f;
+    s.two_sided_density_projection = 1u;
+    s.density_relaxation = 0.5f;
+    s.density_projection_iterations = 30;
+    s.density_projection_interval = 1;
+    s.sparse_bricks = 1u;
+    s.sparse_max_active_fraction = 0.5f;
+    s.sparse_storage_budget = 1.0f;
+    s.particle_radius_cells = 0.25f;
+    s.gravity[2] = -9.81f;
+    s.pressure_solver = SLOSH_SOLVER_MGPCG;
+    s.pressure_iterations = 60;
+    s.sor_weight = 1.7f;
+    s.pcg_iterations = 8;
+    s.mg_coarse_iterations = 16;
+    s.sort_interval = 4;
+    s.smooth_coupling_force = 1u;
+    s.ghost_fluid = 1u;
+    s.viscosity_iterations = 12;
+    s.extrapolation_layers = 2;
+    s.min_substeps = 1;
+    s.max_substeps = 4;
+    s.max_frame_dt = 1.0f / 30.0f;
+    s.cfl = 2.0f;
+    s.max_speed = 20.0f;
+    s.tolerance = 0.0f;
+    s.max_iterations = 200;
+    s.precision_mode = SLOSH_PRECISION_FP32;
+    s.warm_start = SLOSH_WARM_START_PREVIOUS;
+    return s;
+}
+
+inline float clampf_h(float v, float lo, float hi) { return std::fmin(std::fmax(v, lo), hi); }
+inline int clampi_h(int v, int lo, int hi) { return std::min(std::max(v, lo), hi); }
+
+slosh_settings_t clamp_settings(slosh_settings_t s) {  // SloshProxy.cpp:344-347 (caps raised)
+    for (int a = 0; a < 3; ++a) s.grid_dim[a] = clampi_h(s.grid_dim[a], 4, 2048);
+    s.particle_capacity = std::min(std::max(s.particle_capacity, 1024u), 1u << 28);
+    s.cell_size = std::max(s.cell_size, 1e-3f);
+    return s;
+}
+bool layout_equals(const slosh_settings_t& a, const slosh_settings_t& b) {
+    return a.grid_dim[0] == b.grid_dim[0] && a.grid_dim[1] == b.grid_dim[1] && a.grid_dim[2] == b.grid_dim[2] &&
+           a.sparse_storage_budget == b.sparse_storage_budget;
+}
+
+struct Ctx {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    slosh_settings_t S{};
+    bool allocated = false;
+
+    // layout
+    int3 grid{}, brick_dim{}, sort_dim{};
+    uint32_t num_cells = 0, num_bricks = 0, num_pool_bricks = 0, pool_cells = 0, total_faces = 0, num_sort_keys = 0;
+    int num_levels = 0;
+    int3 level_dim[MG_MAX_LEVELS]{};
+    uint32_t level_cells[MG_MAX_LEVELS]{};
+
+    // device memory
+    std::vector<void*> grid_allocs;
+    std::vector<void*> particle_allocs;
+    uint64_t grid_bytes = 0, particle_bytes = 0;
+    slosh_particle_t* particles[2] = {nullptr, nullptr};
+    int pbuf = 0;
+    uint32_t capacity = 0;
+    float* vel[3] = {nullptr, nullptr, nullptr};
+    int vmap[3] = {0, 1, 2};
+    int disp_phys = 2;
+    float* vel_old = nullptr;
+    int32_t* accum = nullptr;
+    uint32_t* face_flags = nullptr;
+    float* face_weight = nullptr;
+    uint32_t* cell_type = nullptr;
+    int32_t* cell_count = nullptr;
+    float *pressure = nullptr, *divergence = nullptr, *cell_diag = nullptr, *density_q = nullptr, *density_rhs = nullptr;
+    uint32_t *brick_table = nullptr, *slot_brick = nullptr, *free_slots = nullptr, *brick_touch = nullptr;
+    uint32_t *brick_want = nullptr, *new_slots = nullptr, *active_bricks = nullptr;
+    uint32_t* stats = nullptr;
+    int32_t* coupling = nullptr;
+    slosh_collider_t* colliders_d = nullptr;
+    slosh_manipulator_t* manipulators_d = nullptr;
+    uint32_t* particle_count = nullptr;
+    SortBuffers sortb{};
+    MGState mg{};
+
+    // pinned host staging
+    slosh_collider_t* h_colliders = nullptr;
+    slosh_manipulator_t* h_manipulators = nullptr;
+    uint32_t* h_stats = nullptr;     // [0..15] stats, [16..19] particle count
+    double* h_scalars = nullptr;     // [0..7] device scalars, [8..9] ||b||^2, ||r||^2 of the last pressure solve
+    int32_t* h_coupling = nullptr;
+
+    // simulation state on the host
+    uint32_t num_particles = 0;
+    uint64_t total_emitted = 0, sim_frame = 0;
+    uint32_t emit_seed = 1;
+    float prev_dt = 0.0f, last_max_speed = 0.0f;
+    Pass P{};
+    Shape shape{};
+    uint32_t num_colliders = 0, num_manipulators = 0;
+    int substeps = 0;
+    float dt = 0.0f;
+    bool density_frame = false;
+    int last_iterations = 0;
+    float last_rel = 0.0f, last_true_rel = 0.0f;
+    bool last_converged = true;
+    bool pool_overflow_seen = false;
+    bool rel_pending = false;
+
+    // timing
+    bool timing = false;
+    std::vector<cudaEvent_t> event_pool;
+    size_t event_next = 0;
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> phase_events;
+    float phase_ms[NUM_PHASES] = {};
+    uint64_t launches = 0;
+
+    // ---------------------------------------------------------------------------------------------
+    template <class T>
+    T* dalloc(size_t count, bool particle, uint64_t* bytes_out = nullptr) {
+        void* p = nullptr;
+        const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+        cudaError_t e = cudaMalloc(&p, bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            throw StatusError{SLOSH_ERR_OUT_OF_MEMORY, "cudaMalloc of " + std::to_string(bytes) + " bytes failed"};
+        }
+        (particle ? particle_allocs : grid_allocs).push_back(p);
+        (particle ? particle_bytes : grid_bytes) += bytes;
+        (void)bytes_out;
+        return static_cast<T*>(p);
+    }
+    void free_list(std::vector<void*>& v) {
+        for (void* p : v) cudaFree(p);
+        v.clear();
+    }
+    void release() {
+        if (stream) cudaStreamSynchronize(stream);
+        free_list(grid_allocs);
+        free_list(particle_allocs);
+        grid_bytes = particle_bytes = 0;
+        allocated = false;
+    }
+
+    void compute_layout(const slosh_settings_t& s) {
+        grid = make_int3(s.grid_dim[0], s.grid_dim[1], s.grid_dim[2]);
+        num_cells = uint32_t(grid.x) * uint32_t(grid.y) * uint32_t(grid.z);
+        brick_dim = make_int3((grid.x + 7) / 8, (grid.y + 7) / 8, (grid.z + 7) / 8);
+        num_bricks = uint32_t(brick_dim.x) * uint32_t(brick_dim.y) * uint32_t(brick_dim.z);
+        const double budget = double(clampf_h(s.sparse_storage_budget, 0.0f, 1.0f));
+        uint32_t slots = uint32_t(std::ceil(budget * double(num_bricks)));
+        slots = std::min(std::max(slots, 1u), num_bricks);
+        num_pool_bricks = slots + 1u;
+        pool_cells = num_pool_bricks * BRICK_CELLS;
+        total_faces = 3u * pool_cells;
+        sort_dim = sort_brick_dim(grid);
+        num_sort_keys = uint32_t(sort_dim.x) * uint32_t(sort_dim.y) * uint32_t(sort_dim.z) + 1u;
+        num_levels = 1;
+        level_dim[0] = grid;
+        level_cells[0] = num_cells;
+        while (level_cells[num_levels - 1] > MG_COARSEST_MAX_CELLS && num_levels < MG_MAX_LEVELS) {
+            const int3 p = level_dim[num_levels - 1];
+            const int3 dd = make_int3((p.x + 1) / 2, (p.y + 1) / 2, (p.z + 1) / 2);
+            level_dim[num_levels] = dd;
+            level_cells[num_levels] = uint32_t(dd.x) * uint32_t(dd.y) * uint32_t(dd.z);
+            ++num_levels;
+        }
+    }
+
+    void alloc_particles(uint32_t cap) {
+        free_list(particle_allocs);
+        particle_bytes = 0;
+        capacity = cap;
+        particles[0] = dalloc<slosh_particle_t>(cap, true);
+        particles[1] = dalloc<slosh_particle_t>(cap, true);
+        sortb.keys[0] = dalloc<uint32_t>(cap, true);
+        sortb.keys[1] = dalloc<uint32_t>(cap, true);
+        sortb.vals[0] = dalloc<uint32_t>(cap, true);
+        sortb.vals[1] = dalloc<uint32_t>(cap, true);
+        sortb.perm = dalloc<uint32_t>(cap, true);
+        sortb.tile_hist_capacity = sort_tile_hist_size(cap);
+        sortb.tile_hist = dalloc<uint32_t>(sortb.tile_hist_capacity, true);
+        sortb.scan_tmp_capacity = sort_scan_tmp_size(cap, num_sort_keys);
+        sortb.scan_tmp = dalloc<uint32_t>(sortb.scan_tmp_capacity, true);
+        pbuf = 0;
+    }
+
+    // Allocate (SloshProxy.cpp:185-306).
+    void allocate(const slosh_settings_t& s) {
+        release();
+        S = s;
+        compute_layout(s);
+        alloc_particles(s.particle_capacity);
+        num_particles = 0;
+        const size_t tf = total_faces, pc = pool_cells;
+        for (int i = 0; i < 3; ++i) vel[i] = dalloc<float>(tf, false);
+        vmap[0] = 0; vmap[1] = 1; vmap[2] = 2;
+        disp_phys = 2;
+        vel_old = dalloc<float>(tf, false);
+        accum = dalloc<int32_t>(2 * tf, false);
+        face_flags = dalloc<uint32_t>(tf, false);
+        face_weight = dalloc<float>(tf, false);
+        cell_type = dalloc<uint32_t>(pc, false);
+        cell_count = dalloc<int32_t>(pc, false);
+        pressure = dalloc<float>(pc, false);
+        divergence = dalloc<float>(pc, false);
+        cell_diag = dalloc<float>(pc, false);
+        density_q = dalloc<float>(pc, false);
+        density_rhs = dalloc<float>(pc, false);
+        coupling = dalloc<int32_t>(SLOSH_MAX_COLLIDERS * SLOSH_COUPLING_STRIDE, false);
+        stats = dalloc<uint32_t>(SLOSH_NUM_STATS, false);
+        particle_count = dalloc<uint32_t>(4, false);
+        active_bricks = dalloc<uint32_t>(num_bricks + 1u, false);
+        brick_table = dalloc<uint32_t>(num_bricks, false);
+        brick_touch = dalloc<uint32_t>(num_bricks, false);
+        brick_want = dalloc<uint32_t>(num_bricks, false);
+        new_slots = dalloc<uint32_t>(num_pool_bricks + 1u, false);
+        slot_brick = dalloc<uint32_t>(num_pool_bricks, false);
+        free_slots = dalloc<uint32_t>(num_pool_bricks, false);
+        colliders_d = dalloc<slosh_collider_t>(SLOSH_MAX_COLLIDERS, false);
+        manipulators_d = dalloc<slosh_manipulator_t>(SLOSH_MAX_MANIPULATORS, false);
+        sortb.counts = dalloc<uint32_t>(num_sort_keys, false);
+        sortb.offsets = dalloc<uint32_t>(num_sort_keys, false);
+        sortb.particle_count = particle_count;
+        mg.num_levels = num_levels;
+        for (int l = 0; l < num_levels; ++l) {
+            mg.lv[l].dim = level_dim[l];
+            mg.lv[l].cells = level_cells[l];
+            if (l > 0) {
+                mg.lv[l].type = dalloc<uint32_t>(level_cells[l], false);
+                mg.lv[l].x = dalloc<float>(level_cells[l], false);
+                mg.lv[l].b = dalloc<float>(level_cells[l], false);
+            } else {
+                mg.lv[l].type = nullptr; mg.lv[l].x = nullptr; mg.lv[l].b = nullptr;
+            }
+        }
+        mg.r = dalloc<float>(pc, false);
+        mg.z = dalloc<float>(pc, false);
+        mg.dvec = dalloc<float>(pc, false);
+        mg.q = dalloc<float>(pc, false);
+        mg.partials = dalloc<double>(2 * size_t(num_pool_bricks), false);
+        mg.scalars = dalloc<double>(8, false);
+        mg.counters = dalloc<uint32_t>(8, false);
+        // zero everything (AddClearUAVPass of every buffer), then the free stack and the slot table
+        zero_all();
+        std::vector<uint32_t> free_init(num_pool_bricks);
+        const uint32_t pool_slots = num_pool_bricks - 1u;
+        free_init[0] = pool_slots;
+        for (uint32_t sl = 1; sl <= pool_slots; ++sl) free_init[sl] = sl;
+        CK(cudaMemcpy(free_slots, free_init.data(), sizeof(uint32_t) * num_pool_bricks, cudaMemcpyHostToDevice));
+        CK(cudaMemset(slot_brick, 0xFF, sizeof(uint32_t) * num_pool_bricks));
+        total_emitted = 0;
+        prev_dt = 0.0f;
+        last_max_speed = 0.0f;
+        int brick_ctas = std::max(1, std::min<int>(int(num_pool_bricks - 1u), num_sms * 8));
+        shape.brick_ctas = brick_ctas;
+        shape.num_sms = num_sms;
+        allocated = true;
+    }
+    void zero_all() {
+        const size_t tf = total_faces, pc = pool_cells;
+        for (int i = 0; i < 3; ++i) CK(cudaMemset(vel[i], 0, tf * 4));
+        CK(cudaMemset(vel_old, 0, tf * 4));
+        CK(cudaMemset(accum, 0, 2 * tf * 4));
+        CK(cudaMemset(face_flags, 0, tf * 4));
+        CK(cudaMemset(face_weight, 0, tf * 4));
+        for (void* p : {(void*)cell_type, (void*)cell_count, (void*)pressure, (void*)divergence, (void*)cell_diag, (void*)density_q,
+                        (void*)density_rhs, (void*)mg.r, (void*)mg.z, (void*)mg.dvec, (void*)mg.q})
+            CK(cudaMemset(p, 0, pc * 4));
+        CK(cudaMemset(coupling, 0, SLOSH_MAX_COLLIDERS * SLOSH_COUPLING_STRIDE * 4));
+        CK(cudaMemset(stats, 0, SLOSH_NUM_STATS * 4));
+        CK(cudaMemset(particle_count, 0, 16));
+        CK(cudaMemset(active_bricks, 0, (num_bricks + 1) * 4));
+        CK(cudaMemset(brick_table, 0, num_bricks * 4));
+        CK(cudaMemset(brick_touch, 0, num_bricks * 4));
+        CK(cudaMemset(brick_want, 0, num_bricks * 4));
+        CK(cudaMemset(new_slots, 0, (num_pool_bricks + 1) * 4));
+        CK(cudaMemset(sortb.counts, 0, num_sort_keys * 4));
+        CK(cudaMemset(sortb.offsets, 0, num_sort_keys * 4));
+        for (int l = 1; l < num_levels; ++l) {
+            CK(cudaMemset(mg.lv[l].type, 0, level_cells[l] * 4));
+            CK(cudaMemset(mg.lv[l].x, 0, level_cells[l] * 4));
+            CK(cudaMemset(mg.lv[l].b, 0, level_cells[l] * 4));
+        }
+        CK(cudaMemset(mg.scalars, 0, 8 * sizeof(double)));
+        CK(cudaMemset(mg.counters, 0, 8 * 4));
+        CK(cudaMemset(particles[0], 0, size_t(capacity) * sizeof(slosh_particle_t)));
+    }
+
+    // EnsureParticleCapacity (SloshProxy.cpp:308-337): grow, keeping the particles in use.
+    void ensure_capacity(uint32_t cap) {
+        if (cap <= capacity) return;
+        CK(cudaStreamSynchronize(stream));
+        std::vector<slosh_particle_t> keep(num_particles);
+        if (num_particles)
+            CK(cudaMemcpy(keep.data(), particles[pbuf], sizeof(slosh_particle_t) * num_particles, cudaMemcpyDeviceToHost));
+        alloc_particles(cap);
+        CK(cudaMemset(particles[0], 0, size_t(cap) * sizeof(slosh_particle_t)));
+        if (num_particles)
+            CK(cudaMemcpy(particles[0], keep.data(), sizeof(slosh_particle_t) * num_particles, cudaMemcpyHostToDevice));
+    }
+
+    Dev dev() const {
+        Dev d;
+        d.grid = grid;
+        d.brick_dim = brick_dim;
+        d.num_bricks = num_bricks;
+        d.num_pool_bricks = num_pool_bricks;
+        d.pool_cells = pool_cells;
+        d.total_faces = total_faces;
+        d.h = S.cell_size;
+        d.inv_h = 1.0f / S.cell_size;
+        d.brick_table = brick_table;
+        d.brick_table_w = brick_table;
+        d.slot_brick = slot_brick;
+        d.free_slots = free_slots;
+        d.brick_touch = brick_touch;
+        d.brick_want = brick_want;
+        d.new_slots = new_slots;
+        d.active_bricks = active_bricks;
+        d.cell_type = cell_type;
+        d.cell_count = cell_count;
+        d.pressure = pressure;
+        d.divergence = divergence;
+        d.cell_diag = cell_diag;
+        d.density_q = density_q;
+        d.density_rhs = density_rhs;
+        d.accum = accum;
+        d.face_flags = face_flags;
+        d.face_weight = face_weight;
+        d.vel_old = vel_old;
+        d.stats = stats;
+        d.coupling = coupling;
+        d.colliders = colliders_d;
+        d.manipulators = manipulators_d;
+        return d;
+    }
+
+    // ---- timing ----
+    cudaEvent_t next_event() {
+        if (event_next == event_pool.size()) {
+            cudaEvent_t e;
+            CK(cudaEventCreate(&e));
+            event_pool.push_back(e);
+        }
+        return event_pool[event_next++];
+    }
+    struct PhaseScope {
+        Ctx* c;
+        int phase;
+        cudaEvent_t end;
+        PhaseScope(Ctx* ctx, int ph) : c(ctx), phase(ph), end(nullptr) {
+            if (!c->timing) return;
+            cudaEvent_t s = c->next_event();
+            end = c->next_event();
+            CK(cudaEventRecord(s, c->stream));
+            c->phase_events.push_back({phase, {s, end}});
+        }
+        ~PhaseScope() {
+            if (end) cudaEventRecord(end, c->stream);
+        }
+    };
+    void count(int n) { launches += uint64_t(n); }
+
+    // ---- pass parameters (Step_RenderThread, SloshProxy.cpp:400-483) ----
+    void set_pass_params(const slosh_frame_input_t& in) {
+        const slosh_settings_t& s = S;
+        num_colliders = std::min<uint32_t>(in.num_colliders, SLOSH_MAX_COLLIDERS);
+        num_manipulators = std::min<uint32_t>(in.num_manipulators, SLOSH_MAX_MANIPULATORS);
+        if (num_colliders && !in.colliders) throw StatusError{SLOSH_ERR_INVALID_ARG, "colliders is NULL"};
+        if (num_manipulators && !in.manipulators) throw StatusError{SLOSH_ERR_INVALID_ARG, "manipulators is NULL"};
+        if (num_colliders) {
+            std::memcpy(h_colliders, in.colliders, sizeof(slosh_collider_t) * num_colliders);
+            CK(cudaMemcpyAsync(colliders_d, h_colliders, sizeof(slosh_collider_t) * num_colliders, cudaMemcpyHostToDevice, stream));
+        }
+        if (num_manipulators) {
+            std::memcpy(h_manipulators, in.manipulators, sizeof(slosh_manipulator_t) * num_manipulators);
+            CK(cudaMemcpyAsync(manipulators_d, h_manipulators, sizeof(slosh_manipulator_t) * num_manipulators, cudaMemcpyHostToDevice,
+                               stream));
+        }
+        const float h = s.cell_size;
+        P.num_colliders = num_colliders;
+        P.num_manipulators = num_manipulators;
+        for (int a = 0; a < 3; ++a) P.gravity[a] = s.gravity[a];
+        P.flip_ratio = clampf_h(s.flip_ratio, 0.0f, 1.0f);
+        P.use_apic = s.transfer_mode == SLOSH_TRANSFER_APIC ? 1u : 0u;
+        P.max_speed = std::max(s.max_speed, 0.1f);
+        P.friction = clampf_h(s.boundary_friction, 0.0f, 1.0f);
+        const float gmag = std::sqrt(s.gravity[0] * s.gravity[0] + s.gravity[1] * s.gravity[1] + s.gravity[2] * s.gravity[2]);
+        P.adhesion_accel = std::max(s.adhesion, 0.0f) * 1.5f * gmag;
+        P.adhesion_range = std::max(s.adhesion_distance, 1e-4f);
+        P.particle_radius = s.particle_radius_cells * h;
+        P.density_correction = s.two_sided_density_projection ? 0.0f : std::max(s.density_correction, 0.0f);
+        P.target_ppc = 8.0f;
+        P.density_deadband = std::max(s.density_deadband, 0.0f);
+        P.warm_start_scale = 1.0f;
+        P.ghost_fluid = s.ghost_fluid ? 1u : 0u;
+        const int interval = clampi_h(s.density_projection_interval, 1, 8);
+        P.density_relaxation = 1.0f - std::pow(1.0f - clampf_h(s.density_relaxation, 0.0f, 1.0f), float(interval));
+    }
+
+    // ---- emission (Step_RenderThread :485-541) ----
+    void emit(const slosh_emit_request_t& em) {
+        uint64_t cnt = em.count;
+        if (em.shape == SLOSH_EMIT_FILL_CELLS)
+            cnt = uint64_t(std::max(em.cell_dims[0], 0)) * uint64_t(std::max(em.cell_dims[1], 0)) * uint64_t(std::max(em.cell_dims[2], 0)) * 8ull;
+        cnt = std::min<uint64_t>(cnt, uint64_t(capacity) - std::min(num_particles, capacity));
+        if (cnt == 0) return;
+        const uint32_t bound = num_particles;
+        const Dev d = dev();
+        count(launch_emit_reserve(particle_count, uint32_t(cnt), stream));
+        count(launch_emit(d, particles[pbuf], particle_count, em, uint32_t(cnt), bound, capacity, emit_seed++, stream));
+        total_emitted += cnt;
+        num_particles += uint32_t(cnt);
+    }
+
+    void sort_particles() {
+        PhaseScope ps(this, 0);
+        count(launch_sort(dev(), sortb, particles[pbuf], particles[pbuf ^ 1], num_particles, num_sort_keys, sort_dim, stream));
+        pbuf ^= 1;
+    }
+
+    // ---- MGPCG driver (AddPressureSolveMGPCG, SloshProxy.cpp:807-1020) ----
+    void vcycle(const Dev& d, int coarse_iterations) {
+        const int nl = num_levels;
+        if (nl == 1) {
+            count(launch_mg_coarse_solve(d, mg, 0, coarse_iterations, stream));
+            count(launch_mg_smooth(d, mg, 0, 0u, true, shape, stream));
+            return;
+        }
+        count(launch_mg_smooth(d, mg, 0, 1u, false, shape, stream));
+        for (int l = 0; l < nl - 1; ++l) {
+            count(launch_mg_restrict(d, mg, l, shape, stream));
+            if (l + 1 < nl - 1) count(launch_mg_smooth(d, mg, l + 1, 1u, false, shape, stream));
+        }
+        count(launch_mg_coarse_solve(d, mg, nl - 1, coarse_iterations, stream));
+        for (int l = nl - 2; l >= 0; --l) {
+            count(launch_mg_prolong(d, mg, l, shape, stream));
+            count(launch_mg_smooth(d, mg, l, 1u, false, shape, stream));
+            count(launch_mg_smooth(d, mg, l, 0u, l == 0, shape, stream));
+        }
+    }
+    double read_rel_residual() {
+        CK(cudaMemcpyAsync(h_scalars + 4, mg.scalars + 4, 2 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+        CK(cudaStreamSynchronize(stream));
+        const double bb = h_scalars[4], rr = h_scalars[5];
+        return bb > 0.0 ? std::sqrt(rr / bb) : 0.0;
+    }
+    int mgpcg(float* p, const float* div, int fixed_iterations, float tolerance, int max_iterations, int coarse_iterations,
+              bool record) {
+        const Dev d = dev();
+        for (int l = 0; l < num_levels - 1; ++l) count(launch_mg_build_type(d, mg, l, stream));
+        count(launch_pcg_init(d, mg, p, div, shape, stream));
+        const bool tol_mode = fixed_iterations <= 0;
+        const int iterations = tol_mode ? std::max(max_iterations, 1) : std::min(std::max(fixed_iterations, 1), 100);
+        double rel = 0.0;
+        if (tol_mode) {
+            rel = read_rel_residual();
+            if (rel <= double(tolerance)) {
+                if (record) { last_iterations = 0; last_rel = float(rel); last_converged = true; }
+                return 0;
+            }
+        }
+        vcycle(d, coarse_iterations);
+        count(launch_pcg_update_d(d, mg, true, shape, stream));
+        int done = 0;
+        for (int it = 0; it < iterations; ++it) {
+            count(launch_pcg_apply_a(d, mg, shape, stream));
+            count(launch_pcg_update_pr(d, mg, p, shape, stream));
+            done = it + 1;
+            if (tol_mode) {
+                rel = read_rel_residual();
+                if (rel <= double(tolerance)) break;
+            }
+            if (it + 1 < iterations) {
+                vcycle(d, coarse_iterations);
+                count(launch_pcg_update_d(d, mg, false, shape, stream));
+            }
+        }
+        if (record) {
+            last_iterations = done;
+            last_converged = !tol_mode || rel <= double(tolerance);
+            if (tol_mode) {
+                last_rel = float(rel);
+                rel_pending = false;
+            } else {  // read at the end of the frame, without a sync here
+                CK(cudaMemcpyAsync(h_scalars + 8, mg.scalars + 4, 2 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+                rel_pending = true;
+            }
+        }
+        return done;
+    }
+
+    // ---- frame prologue (Step_RenderThread :339-562) ----
+    int begin_frame(const slosh_frame_input_t& in) {
+        const slosh_settings_t s = clamp_settings(in.settings);
+        if (in.reset || !allocated || !layout_equals(s, S)) allocate(s);
+        ensure_capacity(s.particle_capacity);
+        S = s;
+        ++sim_frame;
+        event_next = 0;
+        phase_events.clear();
+        set_pass_params(in);
+        bool has_drain = false;
+        for (uint32_t m = 0; m < num_manipulators; ++m) has_drain = has_drain || in.manipulators[m].kind == 0u;
+        CK(cudaMemsetAsync(coupling, 0, SLOSH_MAX_COLLIDERS * SLOSH_COUPLING_STRIDE * 4, stream));
+        CK(cudaMemsetAsync(stats, 0, SLOSH_NUM_STATS * 4, stream));
+        if (in.num_emits && !in.emits) throw StatusError{SLOSH_ERR_INVALID_ARG, "emits is NULL"};
+        for (uint32_t e = 0; e < in.num_emits; ++e) emit(in.emits[e]);
+        if (num_particles > 0 &&
+            ((s.sort_interval > 0 && (sim_frame % uint64_t(s.sort_interval)) == 0) || (has_drain && (sim_frame % 8ull) == 0)))
+            sort_particles();
+        substeps = 0;
+        density_frame = false;
+        if (!in.paused && num_particles > 0) {
+            const float frame_dt = clampf_h(in.delta_time, 1e-4f, clampf_h(s.max_frame_dt, 1.0f / 240.0f, 1.0f / 10.0f));
+            const float gmag = std::sqrt(s.gravity[0] * s.gravity[0] + s.gravity[1] * s.gravity[1] + s.gravity[2] * s.gravity[2]);
+            const float speed_estimate = std::max(last_max_speed, 1.0f) + gmag * frame_dt;
+            substeps = clampi_h(int(std::ceil(speed_estimate * frame_dt / (std::max(s.cfl, 0.1f) * s.cell_size))),
+                                std::max(s.min_substeps, 1), std::max(s.max_substeps, 1));
+            dt = frame_dt / float(substeps);
+            P.dt = dt;
+            P.viscosity_alpha = s.kinematic_viscosity * dt / (s.cell_size * s.cell_size);
+            P.pressure_to_pascal = s.density * s.cell_size / dt;
+            const int interval = clampi_h(s.density_projection_interval, 1, 8);
+            density_frame = s.two_sided_density_projection && P.density_relaxation > 0.0f && (sim_frame % uint64_t(interval)) == 0;
+        }
+        return substeps;
+    }
+
+    // ---- one substep (Step_RenderThread :564-713) ----
+    void substep(int step) {
+        const bool last = step == substeps - 1;
+        P.warm_start_scale = prev_dt > 0.0f ? P.dt / prev_dt : 1.0f;
+        prev_dt = P.dt;
+        P.frame_seed = uint32_t(sim_frame * 16ull + uint64_t(step));
+        const Dev d = dev();
+        {
+            PhaseScope ps(this, 1);
+            count(launch_pool_update(d, stream));
+            count(launch_clear_new_slots(d, shape, stream));
+        }
+        float* V[3] = {vel[vmap[0]], vel[vmap[1]], vel[vmap[2]]};
+        {
+            PhaseScope ps(this, 2);
+            count(launch_p2g(d, P, particles[pbuf], num_particles, stream));
+        }
+        int c = 0;
+        {
+            PhaseScope ps(this, 3);
+            count(launch_mark_cells(d, P, shape, stream));
+            count(launch_normalize_faces(d, P, V[0], shape, stream));
+            if (P.viscosity_alpha > 0.0f && S.viscosity_iterations > 0) {
+                CK(cudaMemcpyAsync(V[1], V[0], size_t(total_faces) * 4, cudaMemcpyDeviceToDevice, stream));
+                int src = 1;
+                for (int it = 0; it < S.viscosity_iterations; ++it) {
+                    const int dst = src == 1 ? 2 : 1;
+                    count(launch_viscosity(d, P, V[0], V[src], V[dst], shape, stream));
+                    src = dst;
+                }
+                c = src;
+            }
+            count(launch_divergence(d, P, V[c], shape, stream));
+        }
+        {
+            PhaseScope ps(this, 4);
+            if (S.pressure_solver == SLOSH_SOLVER_MGPCG) {
+                const int coarse = clampi_h(S.mg_coarse_iterations, 1, 200);
+                if (S.tolerance > 0.0f) mgpcg(pressure, divergence, 0, S.tolerance, S.max_iterations, coarse, true);
+                else mgpcg(pressure, divergence, S.pcg_iterations, 0.0f, 0, coarse, true);
+            } else {
+                const float omega = clampf_h(S.sor_weight, 0.5f, 1.95f);
+                for (int it = 0; it < S.pressure_iterations; ++it)
+                    for (uint32_t colour = 0; colour < 2u; ++colour) count(launch_rbgs(d, pressure, divergence, colour, omega, shape, stream));
+                last_iterations = S.pressure_iterations;
+                last_converged = true;
+            }
+            if (last) count(launch_true_residual(d, mg, pressure, divergence, shape, stream));
+        }
+        {
+            PhaseScope ps(this, 5);
+            count(launch_project(d, P, V[c], shape, stream));
+            if (last) count(launch_residual(d, P, V[c], shape, stream));
+        }
+        const bool density = density_frame && last;
+        if (density) {
+            PhaseScope ps(this, 6);
+            count(launch_density_rhs(d, P, shape, stream));
+            if (S.pressure_solver == SLOSH_SOLVER_MGPCG) {
+                mgpcg(density_q, density_rhs, 2, 0.0f, 0, clampi_h(S.mg_coarse_iterations, 1, 200), false);
+            } else {
+                for (int it = 0; it < std::max(S.density_projection_iterations, 1); ++it)
+                    for (uint32_t colour = 0; colour < 2u; ++colour)
+                        count(launch_rbgs(d, density_q, density_rhs, colour, 1.7f, shape, stream));
+            }
+        }
+        {
+            PhaseScope ps(this, 7);
+            for (int it = 0; it < S.extrapolation_layers; ++it) {
+                const int dst = (c + 1) % 3;
+                count(launch_extrapolate(d, V[c], V[dst], uint32_t(it), shape, stream));
+                c = dst;
+            }
+            if (density) count(launch_density_displacement(d, V[(c + 2) % 3], shape, stream));
+        }
+        {
+            PhaseScope ps(this, 8);
+            count(launch_g2p(d, P, particles[pbuf], num_particles, V[c], V[(c + 2) % 3], density, stream));
+        }
+        // The field of logical buffer c becomes logical buffer 0 for the next substep.
+        const int nm[3] = {vmap[c], vmap[(c + 1) % 3], vmap[(c + 2) % 3]};
+        disp_phys = vmap[(c + 2) % 3];
+        vmap[0] = nm[0]; vmap[1] = nm[1]; vmap[2] = nm[2];
+        CK(cudaGetLastError());
+    }
+
+    // ---- frame epilogue: AccumulateStatsCS + the readback decode ----
+    void end_frame();
+};
+
+__global__ void k_accumulate_stats(uint32_t* stats, uint32_t* pc) {  // AccumulateStatsCS (Slosh.usf:264-270)
+    pc[2] += stats[15];
+    stats[14] = pc[0];
+    stats[15] = pc[2];
+}
+
+void Ctx::end_frame() {
+    k_accumulate_stats<<<1, 1, 0, stream>>>(stats, particle_count);
+    count(1);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(h_stats, stats, SLOSH_NUM_STATS * 4, cudaMemcpyDeviceToHost, stream));
+    CK(cudaMemcpyAsync(h_stats + SLOSH_NUM_STATS, particle_count, 16, cudaMemcpyDeviceToHost, stream));
+    CK(cudaMemcpyAsync(h_scalars, mg.scalars, 8 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    CK(cudaMemcpyAsync(h_coupling, coupling, SLOSH_MAX_COLLIDERS * SLOSH_COUPLING_STRIDE * 4, cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    if (substeps > 0) {
+        float ms;
+        std::memcpy(&ms, &h_stats[0], 4);
+        last_max_speed = std::isfinite(ms) ? ms : 0.0f;
+        const double num = h_scalars[6], den = h_scalars[7];
+        last_true_rel = float(den > 0.0 ? std::sqrt(num / den) : 0.0);
+        if (S.pressure_solver != SLOSH_SOLVER_MGPCG) last_rel = last_true_rel;
+    }
+    if (rel_pending) {
+        last_rel = float(h_scalars[8] > 0.0 ? std::sqrt(h_scalars[9] / h_scalars[8]) : 0.0);
+        rel_pending = false;
+    }
+    num_particles = std::min(num_particles, h_stats[SLOSH_NUM_STATS + 0]);
+    pool_overflow_seen = h_stats[8] != 0u;
+    if (timing) {
+        std::fill(phase_ms, phase_ms + NUM_PHASES, 0.0f);
+        for (auto& pe : phase_events) {
+            float ms = 0.0f;
+            if (cudaEventElapsedTime(&ms, pe.second.first, pe.second.second) == cudaSuccess) phase_ms[pe.first] += ms;
+        }
+    }
+}
+
+void decode_results(const Ctx& c, slosh_results_t* out) {
+    std::memset(out, 0, sizeof(*out));
+    const uint32_t* st = c.h_stats;
+    const float inv_sub = 1.0f / float(std::max(c.substeps, 1));
+    const float inv_scale = 1.0f / 1024.0f;
+    out->num_colliders = c.num_colliders;
+    for (uint32_t k = 0; k < c.num_colliders; ++k) {
+        const int32_t* cc = c.h_coupling + k * SLOSH_COUPLING_STRIDE;
+        slosh_collider_feedback_t& o = out->colliders[k];
+        for (int a = 0; a < 3; ++a) {
+            o.pressure_force[a] = float(cc[a]) * (inv_scale * inv_sub);
+            o.pressure_torque[a] = float(cc[3 + a]) * (inv_scale * inv_sub);
+            o.submerged_centroid_offset[a] = cc[7] > 0 ? float(cc[12 + a]) * (inv_scale / float(cc[7])) : 0.0f;
+            o.mean_fluid_velocity[a] = cc[6] > 0 ? float(cc[8 + a]) * (inv_scale / float(cc[6])) : 0.0f;
+        }
+        o.wetted_faces = int32_t(std::lround(double(cc[6]) * inv_sub));
+        o.submerged_cells = cc[7];
+        o.solid_cells = cc[11];
+    }
+    float ms;
+    std::memcpy(&ms, &st[0], 4);
+    out->max_particle_speed = std::isfinite(ms) ? ms : 0.0f;
+    out->fluid_cells = int32_t(std::lround(double(st[1]) * inv_sub));
+    std::memcpy(&out->max_divergence, &st[2], 4);
+    out->mean_divergence = st[4] > 0 ? float(double(st[3]) * 1e-3 / double(st[4])) : 0.0f;
+    out->mean_interior_density = st[6] > 0 ? float(1.0 + double(int32_t(st[5])) * 1e-4 / double(st[6])) : 0.0f;
+    out->interior_cells = int32_t(st[6]);
+    out->active_brick_fraction = c.num_bricks > 0 ? float(st[7]) / float(c.num_bricks) : -1.0f;
+    out->pool_usage = c.num_pool_bricks > 1 ? float(st[7]) / float(c.num_pool_bricks - 1) : -1.0f;
+    out->pool_overflow_bricks = int32_t(st[8]);
+    out->clamped_particles = int32_t(st[9]);
+    out->clamped_in_solid = int32_t(st[13]);
+    for (int a = 0; a < 3; ++a) out->clamped_centroid[a] = st[9] > 0 ? float(st[10 + a]) * (0.01f / float(st[9])) : 0.0f;
+    out->grid_memory_mb = float(double(c.grid_bytes) / (1024.0 * 1024.0));
+    out->particle_memory_mb = float(double(c.particle_bytes) / (1024.0 * 1024.0));
+    out->allocated_particle_capacity = int32_t(c.capacity);
+    out->live_particles = int32_t(st[14]);
+    out->drained_particles = int64_t(st[15]);
+    out->substeps = c.substeps;
+    out->sim_frame = c.sim_frame;
+    out->last_solve_iterations = c.last_iterations;
+    out->last_solve_rel_residual = c.last_rel;
+    out->last_solve_true_rel_residual = c.last_true_rel;
+    std::memcpy(out->raw_stats, st, sizeof(out->raw_stats));
+}
+
+// Buffer export/import map.
+struct BufView {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+};
+BufView buffer_view(Ctx& c, int id) {
+    BufView v;
+    const size_t tf = c.total_faces, pc = c.pool_cells;
+    switch (id) {
+        case SLOSH_BUF_PARTICLES: v = {c.particles[c.pbuf], size_t(c.num_particles) * sizeof(slosh_particle_t)}; break;
+        case SLOSH_BUF_VEL: v = {c.vel[c.vmap[0]], tf * 4}; break;
+        case SLOSH_BUF_VEL_OLD: v = {c.vel_old, tf * 4}; break;
+        case SLOSH_BUF_FACE_FLAGS: v = {c.face_flags, tf * 4}; break;
+        case SLOSH_BUF_FACE_WEIGHT: v = {c.face_weight, tf * 4}; break;
+        case SLOSH_BUF_CELL_TYPE: v = {c.cell_type, pc * 4}; break;
+        case SLOSH_BUF_CELL_COUNT: v = {c.cell_count, pc * 4}; break;
+        case SLOSH_BUF_PRESSURE: v = {c.pressure, pc * 4}; break;
+        case SLOSH_BUF_DIVERGENCE: v = {c.divergence, pc * 4}; break;
+        case SLOSH_BUF_CELL_DIAG: v = {c.cell_diag, pc * 4}; break;
+        case SLOSH_BUF_DENSITY_Q: v = {c.density_q, pc * 4}; break;
+        case SLOSH_BUF_DENSITY_RHS: v = {c.density_rhs, pc * 4}; break;
+        case SLOSH_BUF_BRICK_TABLE: v = {c.brick_table, size_t(c.num_bricks) * 4}; break;
+        case SLOSH_BUF_SLOT_BRICK: v = {c.slot_brick, size_t(c.num_pool_bricks) * 4}; break;
+        case SLOSH_BUF_FREE_SLOTS: v = {c.free_slots, size_t(c.num_pool_bricks) * 4}; break;
+        case SLOSH_BUF_ACTIVE_BRICKS: v = {c.active_bricks, size_t(c.num_bricks + 1) * 4}; break;
+        case SLOSH_BUF_NEW_SLOTS: v = {c.new_slots, size_t(c.num_pool_bricks + 1) * 4}; break;
+        case SLOSH_BUF_BRICK_TOUCH: v = {c.brick_touch, size_t(c.num_bricks) * 4}; break;
+        case SLOSH_BUF_STATS: v = {c.stats, SLOSH_NUM_STATS * 4}; break;
+        case SLOSH_BUF_SORT_COUNTS: v = {c.sortb.counts, size_t(c.num_sort_keys) * 4}; break;
+        case SLOSH_BUF_SORT_OFFSETS: v = {c.sortb.offsets, size_t(c.num_sort_keys) * 4}; break;
+        case SLOSH_BUF_SORT_PERM: v = {c.sortb.perm, size_t(c.num_particles) * 4}; break;
+        case SLOSH_BUF_PARTICLE_COUNT: v = {c.particle_count, 16}; break;
+        case SLOSH_BUF_ACCUM: v = {c.accum, 2 * tf * 4}; break;
+        case SLOSH_BUF_VEL_EXTRAP: v = {c.vel[c.disp_phys], tf * 4}; break;
+        default: break;
+    }
+    return v;
+}
+
+template <class Fn>
+slosh_status guarded(Fn fn) {
+    try {
+        return fn();
+    } catch (const CudaError& e) {
+        g_error = std::string(e.what) + ": " + cudaGetErrorString(e.code);
+        return SLOSH_ERR_CUDA;
+    } catch (const StatusError& e) {
+        g_error = e.what;
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        g_error = "host allocation failed";
+        return SLOSH_ERR_OUT_OF_MEMORY;
+    } catch (...) {
+        g_error = "unknown error";
+        return SLOSH_ERR_CUDA;
+    }
+}
+
+Ctx* as_ctx(void* p) {
+    if (!p) throw StatusError{SLOSH_ERR_INVALID_ARG, "context is NULL"};
+    Ctx* c = static_cast<Ctx*>(p);
+    CK(cudaSetDevice(c->device));
+    return c;
+}
+
+}  // namespace
+}  // namespace slosh
+
+using namespace slosh;
+
+extern "C" {
+
+SLOSH_API uint32_t slosh_abi_version(void) { return SLOSH_ABI_VERSION; }
+SLOSH_API void slosh_settings_default(slosh_settings_t* out) {
+    if (out) *out = defaults();
+}
+SLOSH_API const char* slosh_last_error_string(void) { return g_error.c_str(); }
+
+SLOSH_API slosh_status slosh_create(const slosh_settings_t* settings, int32_t device, void** out_ctx) {
+    return guarded([&]() -> slosh_status {
+        if (!settings || !out_ctx) throw StatusError{SLOSH_ERR_INVALID_ARG, "settings or out_ctx is NULL"};
+        *out_ctx = nullptr;
+        int count = 0;
+        if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+            cudaGetLastError();
+            throw StatusError{SLOSH_ERR_NO_DEVICE, "no CUDA device: the Slosh substep runs only on the GPU"};
+        }
+        int dev = device;
+        if (dev < 0) CK(cudaGetDevice(&dev));
+        if (dev >= count) throw StatusError{SLOSH_ERR_INVALID_ARG, "device index out of range"};
+        CK(cudaSetDevice(dev));
+        cudaDeviceProp prop;
+        CK(cudaGetDeviceProperties(&prop, dev));
+        if (prop.major < 10) throw StatusError{SLOSH_ERR_NO_DEVICE, "this library is built for sm_100a (B200)"};
+        Ctx* c = new Ctx();
+        c->device = dev;
+        c->num_sms = prop.multiProcessorCount;
+        try {
+            CK(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
+            c->stream = c->own_stream;
+            CK(cudaMallocHost(&c->h_colliders, sizeof(slosh_collider_t) * SLOSH_MAX_COLLIDERS));
+            CK(cudaMallocHost(&c->h_manipulators, sizeof(slosh_manipulator_t) * SLOSH_MAX_MANIPULATORS));
+            CK(cudaMallocHost(&c->h_stats, 4 * (SLOSH_NUM_STATS + 4)));
+            CK(cudaMallocHost(&c->h_scalars, 16 * sizeof(double)));
+            CK(cudaMallocHost(&c->h_coupling, 4 * SLOSH_MAX_COLLIDERS * SLOSH_COUPLING_STRIDE));
+            std::memset(c->h_stats, 0, 4 * (SLOSH_NUM_STATS + 4));
+            std::memset(c->h_scalars, 0, 16 * sizeof(double));
+            std::memset(c->h_coupling, 0, 4 * SLOSH_MAX_COLLIDERS * SLOSH_COUPLING_STRIDE);
+            c->allocate(clamp_settings(*settings));
+            CK(cudaDeviceSynchronize());
+        } catch (...) {
+            slosh_destroy(c);
+            throw;
+        }
+        *out_ctx = c;
+        return SLOSH_OK;
+    });
+}
+
+SLOSH_API void slosh_destroy(void* ctx) {
+    if (!ctx) return;
+    Ctx* c = static_cast<Ctx*>(ctx);
+    cudaSetDevice(c->device);
+    c->release();
+    for (cudaEvent_t e : c->event_pool) cudaEventDestroy(e);
+    if (c->h_colliders) cudaFreeHost(c->h_colliders);
+    if (c->h_manipulators) cudaFreeHost(c->h_manipulators);
+    if (c->h_stats) cudaFreeHost(c->h_stats);
+    if (c->h_scalars) cudaFreeHost(c->h_scalars);
+    if (c->h_coupling) cudaFreeHost(c->h_coupling);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    delete c;
+}
+
+SLOSH_API slosh_status slosh_set_stream(void* ctx, void* cuda_stream) {
+    return guarded([&]() -> slosh_status {
+        Ctx* c = as_ctx(ctx);
+        CK(cudaStreamSynchronize(c->stream));
+        c->stream = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : c->own_stream;
+        return SLOSH_OK;
+    });
+}
+SLOSH_API slosh_status slosh_synchronize(void* ctx) {
+    return guarded([&]() -> slosh_status {
+        CK(cudaStreamSynchronize(as_ctx(ctx)->stream));
+        return SLOSH_OK;
+    });
+}
+
+static slosh_status frame_status(const Ctx* c) {
+    if (c->pool_overflow_seen) return SLOSH_WARN_POOL_OVERFLOW;
+    if (!c->last_converged) return SLOSH_ERR_NOT_CONVERGED;
+    return SLOSH_OK;
+}
+
+SLOSH_API slosh_status slosh_begin_frame(void* ctx, const slosh_frame_input_t* input, int32_t* out_substeps, float* out_dt) {
+    return guarded([&]() -> slosh_status {
+        Ctx* c = as_ctx(ctx);
+        if (!input) throw StatusError{SLOSH_ERR_INVALID_ARG, "input is NULL"};
+        const int n = c->begin_frame(*input);
+        if (out_substeps) *out_substeps = n;
+        if (out_dt) *out_dt = c->dt;
+        CK(cudaGetLastError());
+        return SLOSH_OK;
+    });
+}
+SLOSH_API slosh_status slosh_substep(void* ctx, int32_t step_index) {
+    return guarded([&]() -> slosh_status {
+        Ctx* c = as_ctx(ctx);
+        if (step_index < 0 || step_index >= c->substeps) throw StatusError{SLOSH_ERR_INVALID_ARG, "substep index out of range"};
+        c->substep(step_index);
+        return c->last_converged ? SLOSH_OK : SLOSH_ERR_NOT_CONVERGED;
+    });
+}
+SLOSH_API slosh_status slosh_end_frame(void* ctx) {
+    return guarded([&]() -> slosh_status {
+        Ctx* c = as_ctx(ctx);
+        c->end_frame();
+        return frame_status(c);
+    });
+}
+SLOSH_API slosh_status slosh_step_frame(void* ctx, const slosh_frame_input_t* input) {
+    return guarded([&]() -> slosh_status {
+        Ctx* c = as_ctx(ctx);
+        if (!input) throw StatusError{SLOSH_ERR_INVALID_ARG, "input is NULL"};
+        const int n = c->begin_frame(*input);
+        bool converged = true;
+        for (int s = 0; s < n; ++s) {
+            c->substep(s);
+            converged = converged && c->last_converged;
+        }
+        c->end_frame();
+        c->last_converged = converged;
+        return frame_status(c);
+    });
+}
+
+SLOSH_API slosh_status slosh_sort_particles(void* ctx) {
+    return guarded([&]() -> slosh_status {
+        Ctx* c = as_ctx(ctx);
+        c->sort_particles();
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(c->stream));
+        return SLOSH_OK;
+    });
+}
+SLOSH_API slosh_status slosh_emit(void* ctx, const slosh_emit_request_t* request) {
+    return guarded([&]() -> slosh_status {
+        Ctx* c = as_ctx(ctx);
+        if (!request) throw StatusError{SLOSH_ERR_INVALID_ARG, "request is NULL"};
+        c->emit(*request);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(c->stream));
+        return SLOSH_OK;
+    });
+}
+SLOSH_API slosh_status slosh_set_emit_seed(void* ctx, uint32_t seed) {
+    return guarded([&]() -> slosh_status {
+        as_ctx(ctx)->emit_seed = seed;
+        return SLOSH_OK;
+    });
+}
+
+SLOSH_API slosh_status slosh_upload_particles(void* ctx, const slosh_particle_t* particles, uint32_t count) {
+    return guarded([&]() -> slosh_status {
+        Ctx* c = as_ctx(ctx);
+        if (!particles && count) throw StatusError{SLOSH_ERR_INVALID_ARG, "particles is NULL"};
+        if (count > c->capacity) throw StatusError{SLOSH_ERR_CAPACITY, "more particles than particle_capacity"};
+        if (count)
+            CK(cudaMemcpyAsync(c->particles[c->pbuf], particles, sizeof(slosh_particle_t) * count, cudaMemcpyHostToDevice, c->stream));
+        c->num_particles = count;
+        uint32_t pcv[2] = {count, 0u};
+        CK(cudaMemcpyAsync(c->particle_count, pcv, 8, cudaMemcpyHostToDevice, c->stream));
+        c->count(launch_touch_particles(c->dev(), c->particles[c->pbuf], count, c->stream));
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(c->stream));
+        return SLOSH_OK;
+    });
+}
+SLOSH_API slosh_status slosh_download_particles(void* ctx, slosh_particle_t* out, uint32_t capacity, uint32_t* out_count) {
+    return guarded([&]() -> slosh_status {
+        Ctx* c = as_ctx(ctx);
+        if (out_count) *out_count = c->num_particles;
+        if (!out) return SLOSH_OK;
+        const uint32_t n = std::min(capacity, c->num_particles);
+        if (n) CK(cudaMemcpyAsync(out, c->particles[c->pbuf], sizeof(slosh_particle_t) * n, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        return SLOSH_OK;
+    });
+}
+SLOSH_API slosh_status slosh_particle_device_ptr(void* ctx, void** out_ptr, uint32_t* out_count) {
+    return guarded([&]() -> slosh_status {
+        Ctx* c = as_ctx(ctx);
+        if (out_ptr) *out_ptr = c->particles[c->pbuf];
+        if (out_count) *out_count = c->num_particles;
+        return SLOSH_OK;
+    });
+}
+
+SLOSH_API slosh_status slosh_get_results(void* ctx, slosh_results_t* out) {
+    return guarded([&]() -> slosh_status {
+        Ctx* c = as_ctx(ctx);
+        if (!out) throw StatusError{SLOSH_ERR_INVALID_ARG, "out is NULL"};
+        decode_results(*c, out);
+        return SLOSH_OK;
+    });
+}
+SLOSH_API slosh_status slosh_get_layout(void* ctx, slosh_layout_t* out) {
+    return guarded([&]() -> slosh_status {
+        Ctx* c = as_ctx(ctx);
+        if (!out) throw StatusError{SLOSH_ERR_INVALID_ARG, "out is NULL"};
+        std::memset(out, 0, sizeof(*out));
+        out->grid_dim[0] = c->grid.x; out->grid_dim[1] = c->grid.y; out->grid_dim[2] = c->grid.z;
+        out->brick_dim[0] = c->brick_dim.x; out->brick_dim[1] = c->brick_dim.y; out->brick_dim[2] = c->brick_dim.z;
+        out->num_bricks = c->num_bricks;
+        out->num_pool_bricks = c->num_pool_bricks;
+        out->pool_cells = c->pool_cells;
+        out->total_faces = c->total_faces;
+        out->sort_brick_dim[0] = c->sort_dim.x; out->sort_brick_dim[1] = c->sort_dim.y; out->sort_brick_dim[2] = c->sort_dim.z;
+        out->num_sort_keys = c->num_sort_keys;
+        out->num_mg_levels = uint32_t(c->num_levels);
+        for (int l = 0; l < c->num_levels; ++l) {
+            out->mg_dim[l][0] = c->level_dim[l].x; out->mg_dim[l][1] = c->level_dim[l].y; out->mg_dim[l][2] = c->level_dim[l].z;
+        }
+        out->num_particles = c->num_particles;
+        out->particle_capacity = c->capacity;
+        out->current_vel = uint32_t(c->vmap[0]);
+        return SLOSH_OK;
+    });
+}
+
+SLOSH_API slosh_status slosh_buffer_bytes(void* ctx, int32_t buffer_id, size_t* out_bytes) {
+    return guarded([&]() -> slosh_status {
+        Ctx* c = as_ctx(ctx);
+        if (!out_bytes || buffer_id < 0 || buffer_id >= SLOSH_BUF_COUNT_) throw StatusError{SLOSH_ERR_INVALID_ARG, "bad buffer id"};
+        *out_bytes = buffer_view(*c, buffer_id).bytes;
+        return SLOSH_OK;
+    });
+}
+SLOSH_API slosh_status slosh_read_buffer(void* ctx, int32_t buffer_id, void* host_dst, size_t bytes) {
+    return guarded([&]() -> slosh_status {
+        Ctx* c = as_ctx(ctx);
+        if (buffer_id < 0 || buffer_id >= SLOSH_BUF_COUNT_) throw StatusError{SLOSH_ERR_INVALID_ARG, "bad buffer id"};
+        const BufView v = buffer_view(*c, buffer_id);
+        if (bytes < v.bytes || (!host_dst && v.bytes)) throw StatusError{SLOSH_ERR_INVALID_ARG, "destination too small"};
+        CK(cudaStreamSynchronize(c->stream));
+        if (v.bytes) CK(cudaMemcpy(host_dst, v.ptr, v.bytes, cudaMemcpyDeviceToHost));
+        return SLOSH_OK;
+    });
+}
+SLOSH_API slosh_status slosh_write_buffer(void* ctx, int32_t buffer_id, const void* host_src, size_t bytes) {
+    return guarded([&]() -> slosh_status {
+        Ctx* c = as_ctx(ctx);
+        if (buffer_id < 0 || buffer_id >= SLOSH_BUF_COUNT_) throw StatusError{SLOSH_ERR_INVALID_ARG, "bad buffer id"};
+        CK(cudaStreamSynchronize(c->stream));
+        if (buffer_id == SLOSH_BUF_PARTICLES) {
+            const size_t n = bytes / sizeof(slosh_particle_t);
+            if (n > c->capacity) throw StatusError{SLOSH_ERR_CAPACITY, "more particles than particle_capacity"};
+            if (n) CK(cudaMemcpy(c->particles[c->pbuf], host_src, n * sizeof(slosh_particle_t), cudaMemcpyHostToDevice));
+            c->num_particles = uint32_t(n);
+            return SLOSH_OK;
+        }
+        const BufView v = buffer_view(*c, buffer_id);
+        if (bytes != v.bytes || (!host_src && v.bytes)) throw StatusError{SLOSH_ERR_INVALID_ARG, "size mismatch"};
+        if (v.bytes) CK(cudaMemcpy(v.ptr, host_src, v.bytes, cudaMemcpyHostToDevice));
+        return SLOSH_OK;
+    });
+}
+
+SLOSH_API slosh_status slosh_enable_phase_timing(void* ctx, int32_t enable) {
+    return guarded([&]() -> slosh_status {
+        as_ctx(ctx)->timing = enable != 0;
+        return SLOSH_OK;
+    });
+}
+SLOSH_API slosh_status slosh_get_phase_ms(void* ctx, float* out_ms, int32_t n) {
+    return guarded([&]() -> slosh_status {
+        Ctx* c = as_ctx(ctx);
+        if (!out_ms) throw StatusError{SLOSH_ERR_INVALID_ARG, "out_ms is NULL"};
+        for (int i = 0; i < std::min<int>(n, NUM_PHASES); ++i) out_ms[i] = c->phase_ms[i];
+        return SLOSH_OK;
+    });
+}
+SLOSH_API uint64_t slosh_launch_count(void* ctx) { return ctx ? static_cast<Ctx*>(ctx)->launches : 0; }
+
+}  // extern "C"

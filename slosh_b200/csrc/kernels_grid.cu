@@ -1,0 +1,536 @@
+// Brick-pool allocator and per-cell grid passes of the Slosh substep (sm_100a).
+//
+// Reference kernels (PLUG/Shaders/Private/Slosh.usf): BrickFreeCS / BrickAllocCS / PoolArgsCS
+// (:1719-1817), ClearNewSlotsCS (:1819-1831), BuildSolidCS (:365-395) fused into MarkCellsCS
+// (:569-598), NormalizeFace (:604-651), ViscosityJacobiFace (:657-686), DivergenceCS (:692-741),
+// DensityProjectionRhsCS (:775-805), DensityDisplacementFace (:808-828), PressureRBGSCS (:860-892),
+// ProjectFace (:995-1052), ResidualCS (:1222-1257), ExtrapolateFace (:1263-1310).
+//
+// Every brick pass is a grid-stride loop of 256-thread CTAs over the active-brick list; thread t of a
+// CTA owns cells t and t + 256 of the current brick, so each warp touches 32 consecutive cells of a
+// 512-cell slot (fully coalesced 128-byte lines). The pass is HBM-bound; the launch shape is fixed
+// (a multiple of the SM count) and the active count is read on the device, so no host round trip
+// and a capturable stream.
+#include "kernels.h"
+
+namespace slosh {
+
+namespace {
+
+// In-grid neighbour n of cell (c, index); out-of-grid neighbours resolve into the null brick.
+__device__ __forceinline__ uint32_t nidx(const Dev& d, uint32_t index, int3 c, int n) {
+    const int3 nb = add3(c, nbr_off(n));
+    if (!in_grid(d, nb)) return local_index_of(nb);
+    return nbr_index(d, index, c, n);
+}
+__device__ __forceinline__ uint32_t ntype(const Dev& d, uint32_t index, int3 c, int n) {
+    const int3 nb = add3(c, nbr_off(n));
+    if (!in_grid(d, nb)) return CELL_SOLID;
+    return d.cell_type[nbr_index(d, index, c, n)];
+}
+
+// CellDensity (Slosh.usf:211-224).
+__device__ float cell_density(const Dev& d, const Pass& p, int3 c) {
+    if (!in_grid(d, c)) return 0.0f;
+    float ws = 0.0f;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+        ws = ws + (d.face_weight[face_index(d, a, c)] + d.face_weight[face_index(d, a, add3(c, axis_off(a)))]);
+    return ws / (6.0f * p.target_ppc);
+}
+// AirFaceWeight (Slosh.usf:227-230).
+__device__ __forceinline__ float air_face_weight(const Dev& d, const Pass& p, float rho_fluid, int3 air) {
+    return p.ghost_fluid != 0u ? 1.0f / ghost_theta(rho_fluid, cell_density(d, p, air)) : 1.0f;
+}
+// CellDensityInterior (Slosh.usf:753-773).
+__device__ float cell_density_interior(const Dev& d, const Pass& p, uint32_t index, int3 c) {
+    float ws = 0.0f, faces = 0.0f;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        if (type_of(ntype(d, index, c, 2 * a)) != CELL_SOLID) {
+            ws = ws + d.face_weight[uint32_t(a) * d.pool_cells + index];
+            faces = faces + 1.0f;
+        }
+        if (type_of(ntype(d, index, c, 2 * a + 1)) != CELL_SOLID) {
+            ws = ws + d.face_weight[uint32_t(a) * d.pool_cells + nidx(d, index, c, 2 * a + 1)];
+            faces = faces + 1.0f;
+        }
+    }
+    return faces > 0.0f ? ws / (faces * p.target_ppc) : 1.0f;
+}
+__device__ __forceinline__ bool touches_air(const Dev& d, uint32_t index, int3 c) {
+    bool t = false;
+#pragma unroll
+    for (int n = 0; n < 6; ++n) t = t || type_of(ntype(d, index, c, n)) == CELL_AIR;
+    return t;
+}
+
+// Visits the in-grid cells of the active bricks: fn(index, c). fn must not contain CTA barriers.
+template <class Fn>
+__device__ __forceinline__ void for_active_cells(const Dev& d, Fn fn) {
+    const uint32_t active = d.active_bricks[0];
+    for (uint32_t e = blockIdx.x; e < active; e += gridDim.x) {
+        const uint32_t brick = d.active_bricks[1u + e];
+        const uint32_t slot = __ldg(d.brick_table + brick);
+        const int3 bc = brick_coord_of(d, brick);
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const uint32_t l = threadIdx.x + uint32_t(k) * 256u;
+            const int3 lc = local_coord_of(l);
+            const int3 c = make_int3(bc.x * 8 + lc.x, bc.y * 8 + lc.y, bc.z * 8 + lc.z);
+            if (in_grid(d, c)) fn(slot * BRICK_CELLS + l, c);
+        }
+    }
+}
+
+// Block-wide exclusive scan of one value per thread (1024 threads). Returns the exclusive prefix;
+// *total receives the sum.
+__device__ uint32_t block_scan_1024(uint32_t v, uint32_t* s_warp, uint32_t* total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, off);
+        if (lane >= off) x += y;
+    }
+    if (lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = s_warp[lane];
+        uint32_t ws = w;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, ws, off);
+            if (lane >= off) ws += y;
+        }
+        s_warp[lane] = ws - w;  // exclusive prefix of warp totals
+        if (lane == 31) s_warp[32] = ws;
+    }
+    __syncthreads();
+    const uint32_t excl = s_warp[warp] + x - v;
+    *total = s_warp[32];
+    __syncthreads();
+    return excl;
+}
+
+// ---- brick pool: BrickFreeCS + BrickAllocCS + PoolArgsCS in one CTA ------------------------------
+// The reference pushes and pops the free stack with atomics, so slot assignment depends on thread
+// timing. Here the same stack discipline runs in ascending brick order through block scans: freed
+// slots are pushed in brick order, the j-th brick needing storage pops entry (free count - j), and
+// the active and new-slot lists come out in brick order. This is the serial (canonical) result.
+__global__ void __launch_bounds__(1024) k_pool_update(Dev d) {
+    __shared__ uint32_t s_warp[33];
+    const uint32_t nb = d.num_bricks;
+    const uint32_t per = (nb + blockDim.x - 1u) / blockDim.x;
+    const uint32_t b0 = min(threadIdx.x * per, nb);
+    const uint32_t b1 = min(b0 + per, nb);
+    const int f0 = int(d.free_slots[0]);
+    const int bx = d.brick_dim.x, by = d.brick_dim.y, bz = d.brick_dim.z;
+
+    // Phase 1: wanted = touched within one brick; unwanted bricks with storage free their slot.
+    uint32_t nfree = 0;
+    for (uint32_t b = b0; b < b1; ++b) {
+        const int3 c = brick_coord_of(d, b);
+        bool wanted = false;
+        for (int z = max(c.z - 1, 0); z <= min(c.z + 1, bz - 1) && !wanted; ++z)
+            for (int y = max(c.y - 1, 0); y <= min(c.y + 1, by - 1) && !wanted; ++y)
+                for (int x = max(c.x - 1, 0); x <= min(c.x + 1, bx - 1); ++x)
+                    if (d.brick_touch[uint32_t(x + bx * (y + by * z))] != 0u) { wanted = true; break; }
+        d.brick_want[b] = wanted ? 1u : 0u;
+        if (!wanted && d.brick_table_w[b] != 0u) ++nfree;
+    }
+    uint32_t total_free;
+    uint32_t k = block_scan_1024(nfree, s_warp, &total_free);
+    for (uint32_t b = b0; b < b1; ++b) {
+        if (d.brick_want[b] == 0u) {
+            const uint32_t slot = d.brick_table_w[b];
+            if (slot != 0u) {
+                d.free_slots[1u + uint32_t(f0) + k] = slot;
+                ++k;
+                d.slot_brick[slot] = NO_BRICK;
+                d.brick_table_w[b] = 0u;
+            }
+        }
+    }
+    const int f = f0 + int(total_free);
+    __syncthreads();
+
+    // Phase 2: wanted bricks without storage pop slots in brick order.
+    uint32_t nneed = 0;
+    for (uint32_t b = b0; b < b1; ++b)
+        if (d.brick_want[b] != 0u && d.brick_table_w[b] == 0u) ++nneed;
+    uint32_t total_need;
+    uint32_t j = block_scan_1024(nneed, s_warp, &total_need);
+    for (uint32_t b = b0; b < b1; ++b) {
+        if (d.brick_want[b] != 0u && d.brick_table_w[b] == 0u) {
+            const int count = f - int(j);
+            if (count > 0) {
+                const uint32_t slot = d.free_slots[count];
+                d.brick_table_w[b] = slot;
+                d.slot_brick[slot] = b;
+                d.new_slots[1u + j] = slot;
+            }
+            ++j;
+        }
+    }
+    __syncthreads();
+
+    // Phase 3: active list in brick order; touch flags consumed.
+    uint32_t nact = 0;
+    for (uint32_t b = b0; b < b1; ++b)
+        if (d.brick_want[b] != 0u && d.brick_table_w[b] != 0u) ++nact;
+    uint32_t total_act;
+    uint32_t a = block_scan_1024(nact, s_warp, &total_act);
+    for (uint32_t b = b0; b < b1; ++b) {
+        d.brick_touch[b] = 0u;
+        if (d.brick_want[b] != 0u && d.brick_table_w[b] != 0u) d.active_bricks[1u + a++] = b;
+    }
+    if (threadIdx.x == 0) {
+        const uint32_t ok = uint32_t(min(int(total_need), max(f, 0)));
+        d.new_slots[0] = ok;
+        d.free_slots[0] = uint32_t(max(f - int(total_need), 0));
+        d.active_bricks[0] = total_act;
+        d.stats[8] += total_need - ok;
+        d.stats[7] = max(d.stats[7], total_act);
+    }
+}
+
+__global__ void k_clear_new_slots(Dev d) {  // ClearNewSlotsCS
+    const uint32_t n = d.new_slots[0];
+    for (uint32_t e = blockIdx.x; e < n; e += gridDim.x) {
+        const uint32_t base = d.new_slots[1u + e] * BRICK_CELLS;
+        for (uint32_t l = threadIdx.x; l < BRICK_CELLS; l += blockDim.x) {
+            d.pressure[base + l] = 0.0f;
+            d.cell_count[base + l] = 0;
+            d.density_q[base + l] = 0.0f;
+        }
+    }
+}
+
+// ---- BuildSolidCS fused into MarkCellsCS -------------------------------------------------------------
+// BuildSolid runs before P2G in the reference but P2G never reads CellType, so classifying solids here,
+// just before the count-based fluid marking, gives the same types in one pass over the cells.
+__global__ void __launch_bounds__(GRID_THREADS) k_mark_cells(Dev d, Pass p) {
+    uint32_t fluid = 0;
+    for_active_cells(d, [&](uint32_t index, int3 c) {
+        uint32_t packed = CELL_AIR;
+        if (c.x == 0 || c.y == 0 || c.z == 0 || c.x == d.grid.x - 1 || c.y == d.grid.y - 1 || c.z == d.grid.z - 1) {
+            packed = CELL_SOLID;
+        } else {
+            const float3 x = make_float3((float(c.x) + 0.5f) * d.h, (float(c.y) + 0.5f) * d.h, (float(c.z) + 0.5f) * d.h);
+            float best = 0.0f;
+            for (uint32_t k = 0; k < p.num_colliders; ++k) {
+                const float s = collider_sdf(d.colliders[k], x);
+                if (s < best) { best = s; packed = CELL_SOLID | ((k + 1u) << CELL_COLLIDER_SHIFT); }
+            }
+        }
+        if (type_of(packed) != CELL_SOLID) {
+            const int count = d.cell_count[index];
+            packed = count > 0 ? CELL_FLUID : CELL_AIR;
+            if (float(count) >= 0.5f * p.target_ppc) packed |= CELL_DENSE_FLAG;
+        }
+        d.cell_type[index] = packed;
+        if (type_of(packed) == CELL_FLUID) {
+            d.pressure[index] = d.pressure[index] * p.warm_start_scale;
+            ++fluid;
+        } else {
+            d.pressure[index] = 0.0f;
+        }
+    });
+    fluid = __reduce_add_sync(0xFFFFFFFFu, fluid);
+    if ((threadIdx.x & 31) == 0 && fluid) atomicAdd(d.stats + 1, fluid);
+}
+
+// ---- NormalizeFace ------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(GRID_THREADS) k_normalize(Dev d, Pass p, float* __restrict__ vel) {
+    const uint32_t tf = d.total_faces;
+    for_active_cells(d, [&](uint32_t index, int3 c) {
+        const uint32_t b = d.cell_type[index];
+#pragma unroll
+        for (int axis = 0; axis < 3; ++axis) {
+            const uint32_t f = uint32_t(axis) * d.pool_cells + index;
+            const int mom = d.accum[f], wt = d.accum[tf + f];
+            if (mom != 0 || wt != 0) { d.accum[f] = 0; d.accum[tf + f] = 0; }
+            float u = wt > 0 ? float(mom) / float(wt) : 0.0f;
+            d.face_weight[f] = float(wt) * P2G_FIXED_INV;
+            uint32_t flags = wt > 0 ? FACE_HAS_WEIGHT : 0u;
+            if (p.use_apic == 0u) d.vel_old[f] = u;
+            const uint32_t a = ntype(d, index, c, 2 * axis);
+            if (type_of(a) == CELL_SOLID || type_of(b) == CELL_SOLID) {
+                const uint32_t solid = type_of(b) == CELL_SOLID ? b : a;
+                const uint32_t id = collider_of(solid);
+                if (id == 0u) {
+                    u = 0.0f;
+                } else {
+                    const float3 x = make_float3((float(c.x) + (axis == 0 ? 0.0f : 0.5f)) * d.h,
+                                                 (float(c.y) + (axis == 1 ? 0.0f : 0.5f)) * d.h,
+                                                 (float(c.z) + (axis == 2 ? 0.0f : 0.5f)) * d.h);
+                    const float3 v = collider_velocity_at(d.colliders[id - 1u], x);
+                    const float3 e = make_float3(axis == 0 ? 1.0f : 0.0f, axis == 1 ? 1.0f : 0.0f, axis == 2 ? 1.0f : 0.0f);
+                    u = dot3(v, e);
+                }
+                if (!(type_of(a) == CELL_SOLID && type_of(b) == CELL_SOLID)) flags |= FACE_VALID | FACE_SOLID;
+            } else if (type_of(a) == CELL_FLUID || type_of(b) == CELL_FLUID) {
+                u = u + p.gravity[axis] * p.dt;
+                flags |= FACE_VALID;
+            } else {
+                u = 0.0f;
+            }
+            vel[f] = u;
+            d.face_flags[f] = flags;
+        }
+    });
+}
+
+// ---- ViscosityJacobiFace -----------------------------------------------------------------------------
+__global__ void __launch_bounds__(GRID_THREADS) k_viscosity(Dev d, Pass p, const float* __restrict__ ustar,
+                                                            const float* __restrict__ src, float* __restrict__ dst) {
+    const float alpha = p.viscosity_alpha;
+    for_active_cells(d, [&](uint32_t index, int3 c) {
+#pragma unroll
+        for (int axis = 0; axis < 3; ++axis) {
+            const uint32_t f = uint32_t(axis) * d.pool_cells + index;
+            const uint32_t flags = d.face_flags[f];
+            const float center = src[f];
+            if ((flags & FACE_VALID) == 0u || (flags & FACE_SOLID) != 0u) { dst[f] = center; continue; }
+            float sum = 0.0f;
+            for (int n = 0; n < 6; ++n) {
+                float value = center;
+                if (in_grid(d, add3(c, nbr_off(n)))) {
+                    const uint32_t ni = uint32_t(axis) * d.pool_cells + nbr_index(d, index, c, n);
+                    if ((d.face_flags[ni] & FACE_VALID) != 0u) value = src[ni];
+                }
+                sum = sum + value;
+            }
+            dst[f] = (ustar[f] + alpha * sum) / (1.0f + 6.0f * alpha);
+        }
+    });
+}
+
+// ---- DivergenceCS --------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(GRID_THREADS) k_divergence(Dev d, Pass p, const float* __restrict__ vel) {
+    for_active_cells(d, [&](uint32_t index, int3 c) {
+        d.cell_count[index] = 0;
+        if (type_of(d.cell_type[index]) != CELL_FLUID) {
+            d.divergence[index] = 0.0f;
+            d.cell_diag[index] = 0.0f;
+            return;
+        }
+        float div = 0.0f;
+        float ws = 0.0f;
+        uint32_t plus[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) plus[a] = nidx(d, index, c, 2 * a + 1);
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+            div = div + (vel[uint32_t(a) * d.pool_cells + plus[a]] - vel[uint32_t(a) * d.pool_cells + index]);
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+            ws = ws + (d.face_weight[uint32_t(a) * d.pool_cells + index] + d.face_weight[uint32_t(a) * d.pool_cells + plus[a]]);
+        const float rho = ws / (6.0f * p.target_ppc);
+        const float excess = fmaxf(rho - (1.0f + p.density_deadband), 0.0f);
+        const float target = fminf(p.density_correction * excess, 0.5f) * d.h / p.dt;
+        d.divergence[index] = div - target;
+        float diag = 0.0f;
+#pragma unroll
+        for (int n = 0; n < 6; ++n) {
+            const uint32_t nt = type_of(ntype(d, index, c, n));
+            diag = diag + (nt == CELL_FLUID ? 1.0f : (nt == CELL_AIR ? air_face_weight(d, p, rho, add3(c, nbr_off(n))) : 0.0f));
+        }
+        d.cell_diag[index] = diag;
+    });
+}
+
+// ---- PressureRBGSCS: one SOR colour sweep ----------------------------------------------------------------
+__global__ void __launch_bounds__(GRID_THREADS) k_rbgs(Dev d, float* __restrict__ pres, const float* __restrict__ rhs,
+                                                       uint32_t parity, float omega) {
+    for_active_cells(d, [&](uint32_t index, int3 c) {
+        if (type_of(d.cell_type[index]) != CELL_FLUID) return;
+        if ((uint32_t(c.x + c.y + c.z) & 1u) != parity) return;
+        float sum = 0.0f;
+        const float diag = d.cell_diag[index];
+#pragma unroll
+        for (int n = 0; n < 6; ++n) {
+            const int3 nb = add3(c, nbr_off(n));
+            if (!in_grid(d, nb)) continue;
+            const uint32_t ni = nbr_index(d, index, c, n);
+            if (type_of(d.cell_type[ni]) == CELL_FLUID) sum = sum + pres[ni];
+        }
+        if (diag > 0.0f) {
+            const float gs = (sum - rhs[index]) / diag;
+            const float old = pres[index];
+            pres[index] = old + omega * (gs - old);
+        }
+    });
+}
+
+// ---- ProjectFace (the two-way coupling accumulation is not part of this pass) -----------------------------
+__global__ void __launch_bounds__(GRID_THREADS) k_project(Dev d, Pass p, float* __restrict__ vel) {
+    for_active_cells(d, [&](uint32_t index, int3 c) {
+        const uint32_t b = d.cell_type[index];
+#pragma unroll
+        for (int axis = 0; axis < 3; ++axis) {
+            const uint32_t f = uint32_t(axis) * d.pool_cells + index;
+            const uint32_t a = ntype(d, index, c, 2 * axis);
+            uint32_t flags = d.face_flags[f] & FACE_HAS_WEIGHT;
+            if (type_of(a) == CELL_SOLID && type_of(b) == CELL_SOLID) {
+            } else if (type_of(a) == CELL_SOLID || type_of(b) == CELL_SOLID) {
+                flags |= FACE_VALID | FACE_SOLID;
+            } else if (type_of(a) == CELL_FLUID || type_of(b) == CELL_FLUID) {
+                const int3 ca = add3(c, nbr_off(2 * axis));
+                float pa, pb;
+                if (type_of(a) == CELL_FLUID && type_of(b) == CELL_FLUID) {
+                    pa = d.pressure[nbr_index(d, index, c, 2 * axis)];
+                    pb = d.pressure[index];
+                } else if (type_of(a) == CELL_FLUID) {
+                    pa = d.pressure[nbr_index(d, index, c, 2 * axis)];
+                    pb = pa - pa * air_face_weight(d, p, cell_density(d, p, ca), c);
+                } else {
+                    pb = d.pressure[index];
+                    pa = pb - pb * air_face_weight(d, p, cell_density(d, p, c), ca);
+                }
+                vel[f] = vel[f] - (pb - pa);
+                flags |= FACE_VALID;
+            }
+            d.face_flags[f] = flags;
+        }
+    });
+}
+
+// ---- ResidualCS ------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(GRID_THREADS) k_residual(Dev d, Pass p, const float* __restrict__ vel) {
+    for_active_cells(d, [&](uint32_t index, int3 c) {
+        if (type_of(d.cell_type[index]) != CELL_FLUID) return;
+        float div = 0.0f;
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+            div = div + (vel[uint32_t(a) * d.pool_cells + nidx(d, index, c, 2 * a + 1)] - vel[uint32_t(a) * d.pool_cells + index]);
+        const float rate = fabsf(div) * d.inv_h;
+        atomicMax(d.stats + 2, __float_as_uint(rate));
+        atomicAdd(d.stats + 3, __float2uint_rz(fminf(rate, 1.0e5f) * 1000.0f));
+        atomicAdd(d.stats + 4, 1u);
+        if (!touches_air(d, index, c)) {
+            const float dens = clampf(cell_density_interior(d, p, index, c), 0.0f, 4.0f);
+            atomicAdd(d.stats + 5, uint32_t(__float2int_rn((dens - 1.0f) * 10000.0f)));
+            atomicAdd(d.stats + 6, 1u);
+        }
+    });
+}
+
+// ---- DensityProjectionRhsCS -------------------------------------------------------------------------------
+__global__ void __launch_bounds__(GRID_THREADS) k_density_rhs(Dev d, Pass p) {
+    for_active_cells(d, [&](uint32_t index, int3 c) {
+        d.density_q[index] = 0.0f;
+        if (type_of(d.cell_type[index]) != CELL_FLUID) { d.density_rhs[index] = 0.0f; return; }
+        float dev = cell_density_interior(d, p, index, c) - 1.0f;
+        if (touches_air(d, index, c)) dev = fmaxf(dev, 0.0f);
+        d.density_rhs[index] = -p.density_relaxation * clampf(dev, -0.5f, 0.5f);
+    });
+}
+
+// ---- DensityDisplacementFace -----------------------------------------------------------------------------
+__global__ void __launch_bounds__(GRID_THREADS) k_density_displacement(Dev d, float* __restrict__ dst) {
+    for_active_cells(d, [&](uint32_t index, int3 c) {
+        const uint32_t b = d.cell_type[index];
+#pragma unroll
+        for (int axis = 0; axis < 3; ++axis) {
+            const uint32_t f = uint32_t(axis) * d.pool_cells + index;
+            const uint32_t a = ntype(d, index, c, 2 * axis);
+            float value;
+            if (type_of(a) == CELL_SOLID || type_of(b) == CELL_SOLID) {
+                value = 0.0f;
+            } else {
+                const float qa = type_of(a) == CELL_FLUID ? d.density_q[nbr_index(d, index, c, 2 * axis)] : 0.0f;
+                const float qb = type_of(b) == CELL_FLUID ? d.density_q[index] : 0.0f;
+                value = -(qb - qa);
+            }
+            dst[f] = value;
+        }
+    });
+}
+
+// ---- ExtrapolateFace ---------------------------------------------------------------------------------------
+// A face's own new bit is written while neighbours read its flags; readers only test bits set by
+// earlier layers, so the result does not depend on the interleaving.
+__global__ void __launch_bounds__(GRID_THREADS) k_extrapolate(Dev d, const float* __restrict__ src, float* __restrict__ dst,
+                                                              uint32_t iteration) {
+    uint32_t known = FACE_VALID;
+    for (uint32_t it = 0; it < iteration; ++it) known |= 1u << (FACE_EXTRAP_SHIFT + it);
+    const uint32_t new_bit = 1u << (FACE_EXTRAP_SHIFT + iteration);
+    for_active_cells(d, [&](uint32_t index, int3 c) {
+#pragma unroll
+        for (int axis = 0; axis < 3; ++axis) {
+            const uint32_t f = uint32_t(axis) * d.pool_cells + index;
+            const uint32_t flags = d.face_flags[f];
+            const float center = src[f];
+            if ((flags & known) != 0u) { dst[f] = center; continue; }
+            float sum = 0.0f, count = 0.0f;
+#pragma unroll
+            for (int n = 0; n < 6; ++n) {
+                if (!in_grid(d, add3(c, nbr_off(n)))) continue;
+                const uint32_t ni = uint32_t(axis) * d.pool_cells + nbr_index(d, index, c, n);
+                const uint32_t nf = d.face_flags[ni];
+                if ((nf & known) != 0u && (nf & FACE_SOLID) == 0u) { sum = sum + src[ni]; count = count + 1.0f; }
+            }
+            if (count > 0.0f) {
+                dst[f] = sum / count;
+                d.face_flags[f] = flags | new_bit;
+            } else {
+                dst[f] = 0.0f;
+            }
+        }
+    });
+}
+
+}  // namespace
+
+int launch_pool_update(const Dev& d, cudaStream_t s) {
+    k_pool_update<<<1, 1024, 0, s>>>(d);
+    return 1;
+}
+int launch_clear_new_slots(const Dev& d, const Shape& sh, cudaStream_t s) {
+    k_clear_new_slots<<<sh.brick_ctas, 256, 0, s>>>(d);
+    return 1;
+}
+int launch_mark_cells(const Dev& d, const Pass& p, const Shape& sh, cudaStream_t s) {
+    k_mark_cells<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, p);
+    return 1;
+}
+int launch_normalize_faces(const Dev& d, const Pass& p, float* vel, const Shape& sh, cudaStream_t s) {
+    k_normalize<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, p, vel);
+    return 1;
+}
+int launch_viscosity(const Dev& d, const Pass& p, const float* ustar, const float* src, float* dst, const Shape& sh, cudaStream_t s) {
+    k_viscosity<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, p, ustar, src, dst);
+    return 1;
+}
+int launch_divergence(const Dev& d, const Pass& p, const float* vel, const Shape& sh, cudaStream_t s) {
+    k_divergence<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, p, vel);
+    return 1;
+}
+int launch_rbgs(const Dev& d, float* pres, const float* rhs, uint32_t parity, float omega, const Shape& sh, cudaStream_t s) {
+    k_rbgs<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, pres, rhs, parity, omega);
+    return 1;
+}
+int launch_project(const Dev& d, const Pass& p, float* vel, const Shape& sh, cudaStream_t s) {
+    k_project<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, p, vel);
+    return 1;
+}
+int launch_residual(const Dev& d, const Pass& p, const float* vel, const Shape& sh, cudaStream_t s) {
+    k_residual<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, p, vel);
+    return 1;
+}
+int launch_density_rhs(const Dev& d, const Pass& p, const Shape& sh, cudaStream_t s) {
+    k_density_rhs<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, p);
+    return 1;
+}
+int launch_density_displacement(const Dev& d, float* dst, const Shape& sh, cudaStream_t s) {
+    k_density_displacement<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, dst);
+    return 1;
+}
+int launch_extrapolate(const Dev& d, const float* src, float* dst, uint32_t iteration, const Shape& sh, cudaStream_t s) {
+    k_extrapolate<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, src, dst, iteration);
+    return 1;
+}
+
+}  // namespace slosh

@@ -1,0 +1,521 @@
+// Particle kernels of the Slosh substep (sm_100a): emission, P2G, G2P + advection.
+//
+// Reference (PLUG/Shaders/Private/Slosh.usf): EmitReserveCS / EmitParticlesCS (:272-358), P2GCS with
+// ScatterComponentTiled (:448-563), GatherComponent / SampleVelocityComponent / AdvectParticle /
+// G2PAdvectCS (:1376-1678).
+//
+// Particles are 48-byte records read and written as three 16-byte vectors per thread. P2G accumulates
+// APIC momentum and weight as 2^20 fixed-point int32 (SloshCommon.ush:46-48), so the sums are exact
+// and independent of the order in which particles add them.
+#include "kernels.h"
+
+namespace slosh {
+
+namespace {
+
+// ---- EmitReserveCS: base = count; count += n ---------------------------------------------------------
+__global__ void k_emit_reserve(uint32_t* pc, uint32_t count) {
+    const uint32_t base = pc[0];
+    pc[1] = base;
+    pc[0] = base + count;
+}
+
+// ---- EmitParticlesCS -----------------------------------------------------------------------------------
+__global__ void k_emit(Dev d, slosh_particle_t* __restrict__ particles, const uint32_t* __restrict__ pc,
+                       slosh_emit_request_t em, uint32_t count, uint32_t bound, uint32_t capacity, uint32_t seed) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const uint32_t base = pc[1];
+    const uint32_t fill = bound + i;
+    if (fill >= base + count && fill < capacity) store_dead(particles, fill);
+    const uint32_t h0 = pcg_hash(i * 3u + seed * 7919u);
+    const uint32_t h1 = pcg_hash(h0);
+    const uint32_t h2 = pcg_hash(h1);
+    const float3 rnd = make_float3(hash_to_unit(h0), hash_to_unit(h1), hash_to_unit(h2));
+    const float h = d.h;
+    float3 pos;
+    if (em.shape == SLOSH_EMIT_FILL_CELLS) {
+        const uint32_t cell_linear = i / 8u, sub = i % 8u;
+        const int lx = int(cell_linear % uint32_t(em.cell_dims[0]));
+        const int ly = int((cell_linear / uint32_t(em.cell_dims[0])) % uint32_t(em.cell_dims[1]));
+        const int lz = int(cell_linear / uint32_t(em.cell_dims[0] * em.cell_dims[1]));
+        const float sx = float(sub & 1u), sy = float((sub >> 1u) & 1u), sz = float((sub >> 2u) & 1u);
+        const float j = em.fill_jitter;
+        pos.x = (float(em.cell_min[0] + lx) + ((sx + 0.5f) + j * (rnd.x - 0.5f)) * 0.5f) * h;
+        pos.y = (float(em.cell_min[1] + ly) + ((sy + 0.5f) + j * (rnd.y - 0.5f)) * 0.5f) * h;
+        pos.z = (float(em.cell_min[2] + lz) + ((sz + 0.5f) + j * (rnd.z - 0.5f)) * 0.5f) * h;
+    } else if (em.shape == SLOSH_EMIT_SPHERE) {
+        const uint32_t h3 = pcg_hash(h2);
+        const float cos_t = 2.0f * rnd.x - 1.0f;
+        const float sin_t = sqrtf(saturatef(1.0f - cos_t * cos_t));
+        const float phi = 6.28318530718f * rnd.y;
+        const float r = em.extent[0] * powf(fmaxf(hash_to_unit(h3), 1e-6f), 1.0f / 3.0f);
+        pos = addf3(ld3(em.center), scale3(r, make_float3(sin_t * cosf(phi), sin_t * sinf(phi), cos_t)));
+    } else {
+        const float3 q = make_float3((2.0f * rnd.x - 1.0f) * em.extent[0], (2.0f * rnd.y - 1.0f) * em.extent[1],
+                                     (2.0f * rnd.z - 1.0f) * em.extent[2]);
+        pos = addf3(ld3(em.center), quat_rotate(make_float4(em.rotation[0], em.rotation[1], em.rotation[2], em.rotation[3]), q));
+    }
+    const float lo = h * 1.01f;
+    const float3 hi = make_float3((float(d.grid.x) - 1.01f) * h, (float(d.grid.y) - 1.01f) * h, (float(d.grid.z) - 1.01f) * h);
+    float3 velocity = ld3(em.velocity);
+    const float speed = len3(velocity);
+    if (speed > 1e-6f && (em.velocity_spread > 0.0f || em.speed_jitter > 0.0f)) {
+        const uint32_t h4 = pcg_hash(h2 ^ 0x9E3779B9u), h5 = pcg_hash(h4), h6 = pcg_hash(h5);
+        float3 dir = make_float3(velocity.x / speed, velocity.y / speed, velocity.z / speed);
+        const float3 ref = fabsf(dir.z) < 0.9f ? make_float3(0.0f, 0.0f, 1.0f) : make_float3(1.0f, 0.0f, 0.0f);
+        float3 t0 = cross3(dir, ref);
+        const float t0l = len3(t0);
+        t0 = make_float3(t0.x / t0l, t0.y / t0l, t0.z / t0l);
+        const float3 t1 = cross3(dir, t0);
+        const float cos_a = 1.0f + hash_to_unit(h4) * (cosf(em.velocity_spread) - 1.0f);
+        const float sin_a = sqrtf(saturatef(1.0f - cos_a * cos_a));
+        const float phi = 6.28318530718f * hash_to_unit(h5);
+        dir = addf3(scale3(cos_a, dir), scale3(sin_a, addf3(scale3(cosf(phi), t0), scale3(sinf(phi), t1))));
+        velocity = mul3s(mul3s(dir, speed), fmaxf(1.0f + em.speed_jitter * (2.0f * hash_to_unit(h6) - 1.0f), 0.0f));
+    }
+    ParticleF p;
+    p.pos = make_float3(clampf(pos.x, lo, hi.x), clampf(pos.y, lo, hi.y), clampf(pos.z, lo, hi.z));
+    p.vel = velocity;
+    p.cx = p.cy = p.cz = make_float3(0.0f, 0.0f, 0.0f);
+    p.age = 0.0f;
+    store_particle(particles, base + i, p);
+    const int3 c = make_int3(clampi(int(floorf(p.pos.x * d.inv_h)), 0, d.grid.x - 1),
+                             clampi(int(floorf(p.pos.y * d.inv_h)), 0, d.grid.y - 1),
+                             clampi(int(floorf(p.pos.z * d.inv_h)), 0, d.grid.z - 1));
+    d.brick_touch[brick_index_of(d, make_int3(c.x >> 3, c.y >> 3, c.z >> 3))] = 1u;
+}
+
+// Touch flags of uploaded particles (what EmitParticlesCS does for the particles it writes).
+__global__ void k_touch(Dev d, const slosh_particle_t* __restrict__ particles, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 a = __ldg(reinterpret_cast<const float4*>(particles + i));
+    if (is_dead_age(a.w)) return;
+    const int3 c = make_int3(clampi(int(floorf(a.x * d.inv_h)), 0, d.grid.x - 1), clampi(int(floorf(a.y * d.inv_h)), 0, d.grid.y - 1),
+                             clampi(int(floorf(a.z * d.inv_h)), 0, d.grid.z - 1));
+    d.brick_touch[brick_index_of(d, make_int3(c.x >> 3, c.y >> 3, c.z >> 3))] = 1u;
+}
+
+// ---- P2G --------------------------------------------------------------------------------------------------
+// One CTA takes 256 consecutive (spatially sorted) particles, finds the bounding box of their cells and,
+// when the box plus its one-node halo fits, accumulates the 6 fixed-point quantities (momentum and weight
+// of the three MAC components) and the per-cell counts in shared memory with integer atomics; it then
+// adds each non-zero tile entry to global memory once. A CTA whose box does not fit adds directly to
+// global memory. Integer sums make both paths give identical results.
+constexpr int P2G_THREADS = 256;
+constexpr int P2G_TILE_NODES = 2048;  // nodes per quantity (6 quantities) = 48 KB
+constexpr int P2G_TILE_CELLS = 1024;  // counted cells = 4 KB
+
+__global__ void __launch_bounds__(P2G_THREADS) k_p2g(Dev d, Pass p, const slosh_particle_t* __restrict__ particles, uint32_t n) {
+    extern __shared__ int smem[];
+    int* tile = smem;                          // [6][P2G_TILE_NODES]
+    int* ctile = smem + 6 * P2G_TILE_NODES;    // [P2G_TILE_CELLS]
+    __shared__ int s_box[6];
+    const uint32_t i = blockIdx.x * P2G_THREADS + threadIdx.x;
+    if (threadIdx.x < 3) { s_box[threadIdx.x] = 0x7FFFFFFF; s_box[3 + threadIdx.x] = -0x7FFFFFFF; }
+
+    bool valid = i < n;
+    ParticleF part;
+    if (valid) {
+        float4 a, b;
+        uint4 c;
+        load_particle_raw(particles, i, a, b, c);
+        part = unpack_particle(a, b, c);
+        valid = !is_dead_age(part.age);
+    }
+    int3 cell = make_int3(0, 0, 0);
+    if (valid)
+        cell = make_int3(clampi(int(floorf(part.pos.x * d.inv_h)), 0, d.grid.x - 1),
+                         clampi(int(floorf(part.pos.y * d.inv_h)), 0, d.grid.y - 1),
+                         clampi(int(floorf(part.pos.z * d.inv_h)), 0, d.grid.z - 1));
+    __syncthreads();
+    {
+        const int big = 0x7FFFFFFF;
+        const int mnx = __reduce_min_sync(0xFFFFFFFFu, valid ? cell.x : big);
+        const int mny = __reduce_min_sync(0xFFFFFFFFu, valid ? cell.y : big);
+        const int mnz = __reduce_min_sync(0xFFFFFFFFu, valid ? cell.z : big);
+        const int mxx = __reduce_max_sync(0xFFFFFFFFu, valid ? cell.x : -big);
+        const int mxy = __reduce_max_sync(0xFFFFFFFFu, valid ? cell.y : -big);
+        const int mxz = __reduce_max_sync(0xFFFFFFFFu, valid ? cell.z : -big);
+        if ((threadIdx.x & 31) == 0) {
+            atomicMin(s_box + 0, mnx); atomicMin(s_box + 1, mny); atomicMin(s_box + 2, mnz);
+            atomicMax(s_box + 3, mxx); atomicMax(s_box + 4, mxy); atomicMax(s_box + 5, mxz);
+        }
+    }
+    __syncthreads();
+    if (s_box[0] == 0x7FFFFFFF) return;  // no live particle in this CTA (uniform)
+    const int3 mn = make_int3(s_box[0], s_box[1], s_box[2]);
+    const int3 cdim = make_int3(s_box[3] - mn.x + 1, s_box[4] - mn.y + 1, s_box[5] - mn.z + 1);
+    const int3 origin = make_int3(mn.x - 1, mn.y - 1, mn.z - 1);
+    const int3 ndim = make_int3(cdim.x + 2, cdim.y + 2, cdim.z + 2);
+    const long long nodes_ll = (long long)ndim.x * ndim.y * ndim.z;
+    const long long cells_ll = (long long)cdim.x * cdim.y * cdim.z;
+    const bool tiled = nodes_ll <= P2G_TILE_NODES && cells_ll <= P2G_TILE_CELLS;
+    const int nodes = tiled ? int(nodes_ll) : 0;
+    const int ncells = tiled ? int(cells_ll) : 0;
+    if (tiled) {
+        for (int t = threadIdx.x; t < 6 * nodes; t += P2G_THREADS) tile[(t / nodes) * P2G_TILE_NODES + (t % nodes)] = 0;
+        for (int t = threadIdx.x; t < ncells; t += P2G_THREADS) ctile[t] = 0;
+    }
+    __syncthreads();
+
+    if (valid) {
+        const float inv_h = d.inv_h, h = d.h;
+        const uint32_t tf = d.total_faces;
+#pragma unroll
+        for (int axis = 0; axis < 3; ++axis) {
+            const float3 cp = p.use_apic ? (axis == 0 ? part.cx : (axis == 1 ? part.cy : part.cz)) : make_float3(0.0f, 0.0f, 0.0f);
+            const float up = compf(part.vel, axis);
+            const float ox = axis == 0 ? 0.0f : 0.5f, oy = axis == 1 ? 0.0f : 0.5f, oz = axis == 2 ? 0.0f : 0.5f;
+            const float gx = part.pos.x * inv_h - ox, gy = part.pos.y * inv_h - oy, gz = part.pos.z * inv_h - oz;
+            const int3 base = make_int3(int(floorf(gx)), int(floorf(gy)), int(floorf(gz)));
+            const float fx = gx - float(base.x), fy = gy - float(base.y), fz = gz - float(base.z);
+#pragma unroll
+            for (int o = 0; o < 8; ++o) {
+                const int oix = o & 1, oiy = (o >> 1) & 1, oiz = (o >> 2) & 1;
+                const int3 node = make_int3(base.x + oix, base.y + oiy, base.z + oiz);
+                if (!in_grid(d, node)) continue;
+                const float w3x = oix ? fx : 1.0f - fx, w3y = oiy ? fy : 1.0f - fy, w3z = oiz ? fz : 1.0f - fz;
+                const float w = w3x * w3y * w3z;
+                if (w <= 0.0f) continue;
+                const float3 xn = make_float3((float(node.x) + ox) * h, (float(node.y) + oy) * h, (float(node.z) + oz) * h);
+                const int mom = __float2int_rn(w * (up + dot3(cp, sub3(xn, part.pos))) * P2G_FIXED_SCALE);
+                const int wt = __float2int_rn(w * P2G_FIXED_SCALE);
+                if (tiled) {
+                    const int t = (node.x - origin.x) + ndim.x * ((node.y - origin.y) + ndim.y * (node.z - origin.z));
+                    atomicAdd(tile + (2 * axis) * P2G_TILE_NODES + t, mom);
+                    atomicAdd(tile + (2 * axis + 1) * P2G_TILE_NODES + t, wt);
+                } else {
+                    const uint32_t ci = cell_index(d, node);
+                    if (!is_null_cell(ci)) {
+                        const uint32_t f = uint32_t(axis) * d.pool_cells + ci;
+                        atomicAdd(d.accum + f, mom);
+                        atomicAdd(d.accum + tf + f, wt);
+                    }
+                }
+            }
+        }
+        if (tiled) {
+            atomicAdd(ctile + (cell.x - mn.x) + cdim.x * ((cell.y - mn.y) + cdim.y * (cell.z - mn.z)), 1);
+        } else {
+            const uint32_t ci = cell_index(d, cell);
+            if (!is_null_cell(ci)) atomicAdd(d.cell_count + ci, 1);
+        }
+    }
+    if (!tiled) return;  // uniform
+    __syncthreads();
+    // Flush: one global add per non-zero tile entry.
+    for (int t = threadIdx.x; t < 6 * nodes; t += P2G_THREADS) {
+        const int q = t / nodes, l = t - q * nodes;
+        const int v = tile[q * P2G_TILE_NODES + l];
+        if (v == 0) continue;
+        const int lx = l % ndim.x, ly = (l / ndim.x) % ndim.y, lz = l / (ndim.x * ndim.y);
+        const int3 node = make_int3(origin.x + lx, origin.y + ly, origin.z + lz);
+        if (!in_grid(d, node)) continue;
+        const uint32_t ci = cell_index(d, node);
+        if (is_null_cell(ci)) continue;
+        const int axis = q >> 1;
+        atomicAdd(d.accum + (q & 1) * d.total_faces + uint32_t(axis) * d.pool_cells + ci, v);
+    }
+    for (int t = threadIdx.x; t < ncells; t += P2G_THREADS) {
+        const int v = ctile[t];
+        if (v == 0) continue;
+        const int lx = t % cdim.x, ly = (t / cdim.x) % cdim.y, lz = t / (cdim.x * cdim.y);
+        const uint32_t ci = cell_index(d, make_int3(mn.x + lx, mn.y + ly, mn.z + lz));
+        if (!is_null_cell(ci)) atomicAdd(d.cell_count + ci, v);
+    }
+}
+
+// ---- G2P + advection ---------------------------------------------------------------------------------
+struct Stencil {
+    int3 base;
+    float fx, fy, fz;
+};
+__device__ __forceinline__ Stencil stencil_of(const Dev& d, float3 x, int axis) {
+    const float ox = axis == 0 ? 0.0f : 0.5f, oy = axis == 1 ? 0.0f : 0.5f, oz = axis == 2 ? 0.0f : 0.5f;
+    const float gx = x.x * d.inv_h - ox, gy = x.y * d.inv_h - oy, gz = x.z * d.inv_h - oz;
+    Stencil s;
+    s.base = make_int3(int(floorf(gx)), int(floorf(gy)), int(floorf(gz)));
+    s.fx = gx - float(s.base.x);
+    s.fy = gy - float(s.base.y);
+    s.fz = gz - float(s.base.z);
+    return s;
+}
+__device__ __forceinline__ int3 stencil_node(const Dev& d, const Stencil& s, int o) {
+    return make_int3(clampi(s.base.x + (o & 1), 0, d.grid.x - 1), clampi(s.base.y + ((o >> 1) & 1), 0, d.grid.y - 1),
+                     clampi(s.base.z + ((o >> 2) & 1), 0, d.grid.z - 1));
+}
+
+// GatherComponent (Slosh.usf:1376-1410).
+__device__ __forceinline__ void gather_component(const Dev& d, const Pass& p, int axis, float3 xp, const float* __restrict__ vel,
+                                                 float& unew, float& dsum, float& dw, float3& grad) {
+    const Stencil s = stencil_of(d, xp, axis);
+    unew = 0.0f; dsum = 0.0f; dw = 0.0f;
+    grad = make_float3(0.0f, 0.0f, 0.0f);
+#pragma unroll
+    for (int o = 0; o < 8; ++o) {
+        const int oix = o & 1, oiy = (o >> 1) & 1, oiz = (o >> 2) & 1;
+        const int3 node = stencil_node(d, s, o);
+        const float w3x = oix ? s.fx : 1.0f - s.fx, w3y = oiy ? s.fy : 1.0f - s.fy, w3z = oiz ? s.fz : 1.0f - s.fz;
+        const float w = w3x * w3y * w3z;
+        const float sx = oix ? 1.0f : -1.0f, sy = oiy ? 1.0f : -1.0f, sz = oiz ? 1.0f : -1.0f;
+        const uint32_t f = face_index(d, axis, node);
+        const float u = vel[f];
+        unew = unew + w * u;
+        if (p.use_apic != 0u) {
+            grad.x = grad.x + sx * (w3y * w3z) * d.inv_h * u;
+            grad.y = grad.y + sy * (w3x * w3z) * d.inv_h * u;
+            grad.z = grad.z + sz * (w3x * w3y) * d.inv_h * u;
+        } else if ((d.face_flags[f] & FACE_HAS_WEIGHT) != 0u) {
+            dsum = dsum + w * (u - d.vel_old[f]);
+            dw = dw + w;
+        }
+    }
+}
+// SampleVelocityComponent (Slosh.usf:1417-1443).
+__device__ __forceinline__ float sample_component(const Dev& d, int axis, float3 xp, float fallback, bool check,
+                                                  const float* __restrict__ vel) {
+    const uint32_t known = FACE_VALID | (0xFFFFFFFFu << FACE_EXTRAP_SHIFT);
+    const Stencil s = stencil_of(d, xp, axis);
+    float u = 0.0f;
+#pragma unroll
+    for (int o = 0; o < 8; ++o) {
+        const int oix = o & 1, oiy = (o >> 1) & 1, oiz = (o >> 2) & 1;
+        const int3 node = stencil_node(d, s, o);
+        const float w3x = oix ? s.fx : 1.0f - s.fx, w3y = oiy ? s.fy : 1.0f - s.fy, w3z = oiz ? s.fz : 1.0f - s.fz;
+        const uint32_t f = face_index(d, axis, node);
+        float uf = vel[f];
+        if (check && (d.face_flags[f] & known) == 0u) uf = fallback;
+        u = u + w3x * w3y * w3z * uf;
+    }
+    return u;
+}
+// SampleDensityDisplacement (Slosh.usf:830-854).
+__device__ __forceinline__ float3 sample_displacement(const Dev& d, float3 xp, const float* __restrict__ disp) {
+    float out[3];
+#pragma unroll
+    for (int axis = 0; axis < 3; ++axis) {
+        const Stencil s = stencil_of(d, xp, axis);
+        float value = 0.0f;
+#pragma unroll
+        for (int o = 0; o < 8; ++o) {
+            const int oix = o & 1, oiy = (o >> 1) & 1, oiz = (o >> 2) & 1;
+            const int3 node = stencil_node(d, s, o);
+            const float w3x = oix ? s.fx : 1.0f - s.fx, w3y = oiy ? s.fy : 1.0f - s.fy, w3z = oiz ? s.fz : 1.0f - s.fz;
+            value = value + w3x * w3y * w3z * disp[face_index(d, axis, node)];
+        }
+        out[axis] = value;
+    }
+    const float3 v = make_float3(out[0], out[1], out[2]);
+    const float len = len3(v);
+    const float3 dd = len > 0.5f ? mul3s(v, 0.5f / len) : v;
+    return mul3s(dd, d.h);
+}
+
+constexpr int G2P_THREADS = 256;
+
+// AdvectParticle + G2PAdvectCS (Slosh.usf:1452-1678).
+__global__ void __launch_bounds__(G2P_THREADS) k_g2p(Dev d, Pass p, slosh_particle_t* __restrict__ particles, uint32_t n,
+                                                     const float* __restrict__ vel, const float* __restrict__ disp,
+                                                     uint32_t apply_density) {
+    const uint32_t i = blockIdx.x * G2P_THREADS + threadIdx.x;
+    uint32_t brick = NO_BRICK;
+    uint32_t speed_bits = 0u;
+    if (i < n) {
+        float4 ra, rb;
+        uint4 rc;
+        load_particle_raw(particles, i, ra, rb, rc);
+        ParticleF P = unpack_particle(ra, rb, rc);
+        if (!is_dead_age(P.age)) {
+            const float h = d.h, inv_h = d.inv_h, dt = p.dt;
+            const float lo = h * 1.01f;
+            const float3 hi = make_float3((float(d.grid.x) - 1.01f) * h, (float(d.grid.y) - 1.01f) * h, (float(d.grid.z) - 1.01f) * h);
+            float3 pic, delta, dw, gx, gy, gz;
+            gather_component(d, p, 0, P.pos, vel, pic.x, delta.x, dw.x, gx);
+            gather_component(d, p, 1, P.pos, vel, pic.y, delta.y, dw.y, gy);
+            gather_component(d, p, 2, P.pos, vel, pic.z, delta.z, dw.z, gz);
+            float3 nv;
+            if (p.use_apic) {
+                nv = pic;
+                P.cx = gx; P.cy = gy; P.cz = gz;
+            } else {
+                const float fdx = dw.x > 1e-4f ? delta.x / dw.x : pic.x - P.vel.x;
+                const float fdy = dw.y > 1e-4f ? delta.y / dw.y : pic.y - P.vel.y;
+                const float fdz = dw.z > 1e-4f ? delta.z / dw.z : pic.z - P.vel.z;
+                const float3 target = make_float3(P.vel.x + fdx, P.vel.y + fdy, P.vel.z + fdz);
+                nv = make_float3(pic.x + p.flip_ratio * (target.x - pic.x), pic.y + p.flip_ratio * (target.y - pic.y),
+                                 pic.z + p.flip_ratio * (target.z - pic.z));
+                P.cx = P.cy = P.cz = make_float3(0.0f, 0.0f, 0.0f);
+            }
+            // RK2 midpoint with the Euler blend.
+            const float3 v1 = pic;
+            const float half_dt = 0.5f * dt;
+            float3 mid = addf3(P.pos, scale3(half_dt, v1));
+            mid = make_float3(clampf(mid.x, lo, hi.x), clampf(mid.y, lo, hi.y), clampf(mid.z, lo, hi.z));
+            const float mid_cells = half_dt * len3(v1) * inv_h;
+            float3 v2 = v1;
+            if (mid_cells < 2.0f) {
+                const bool check = mid_cells > 1.0f;
+                const float3 sv = make_float3(sample_component(d, 0, mid, v1.x, check, vel), sample_component(d, 1, mid, v1.y, check, vel),
+                                              sample_component(d, 2, mid, v1.z, check, vel));
+                const float t = saturatef(mid_cells - 1.0f);
+                v2 = make_float3(sv.x + t * (v1.x - sv.x), sv.y + t * (v1.y - sv.y), sv.z + t * (v1.z - sv.z));
+            }
+            float3 x = addf3(P.pos, scale3(dt, v2));
+            if (apply_density) {
+                const float3 cpos = make_float3(clampf(P.pos.x, lo, hi.x), clampf(P.pos.y, lo, hi.y), clampf(P.pos.z, lo, hi.z));
+                x = addf3(x, sample_displacement(d, cpos, disp));
+            }
+            // Pool exhausted: ballistic.
+            const int3 pcell = make_int3(clampi(int(floorf(P.pos.x * inv_h)), 0, d.grid.x - 1),
+                                         clampi(int(floorf(P.pos.y * inv_h)), 0, d.grid.y - 1),
+                                         clampi(int(floorf(P.pos.z * inv_h)), 0, d.grid.z - 1));
+            if (is_null_cell(cell_index(d, pcell))) {
+                const float3 g = make_float3(p.gravity[0], p.gravity[1], p.gravity[2]);
+                nv = addf3(P.vel, mul3s(g, dt));
+                x = addf3(P.pos, scale3(dt, nv));
+                P.cx = P.cy = P.cz = make_float3(0.0f, 0.0f, 0.0f);
+            }
+            // Force-field manipulators.
+            for (uint32_t m = 0; m < p.num_manipulators; ++m) {
+                const slosh_manipulator_t& f = d.manipulators[m];
+                if (f.kind == MANIP_DRAIN) continue;
+                const float w = manipulator_weight(f, x);
+                if (w <= 0.0f) continue;
+                const float3 r = sub3(x, ld3(f.center));
+                const float3 ax = ld3(f.axis);
+                if (f.kind == MANIP_DIRECTIONAL) {
+                    nv = addf3(nv, mul3s(ax, f.strength * w * dt));
+                } else if (f.kind == MANIP_RADIAL) {
+                    const float rl = len3(r);
+                    const float3 nn = rl > 1e-5f ? make_float3(r.x / rl, r.y / rl, r.z / rl) : make_float3(0.0f, 0.0f, 0.0f);
+                    nv = addf3(nv, mul3s(nn, f.strength * w * dt));
+                } else if (f.kind == MANIP_SWIRL) {
+                    const float3 perp = sub3(r, scale3(dot3(r, ax), ax));
+                    const float pl = len3(perp);
+                    if (pl > 1e-5f) {
+                        const float3 pn = make_float3(perp.x / pl, perp.y / pl, perp.z / pl);
+                        const float3 tangent = cross3(ax, pn);
+                        nv = addf3(nv, mul3s(sub3(tangent, mul3s(pn, f.param0)), f.strength * w * dt));
+                    }
+                } else if (f.kind == MANIP_DRAG) {
+                    nv = mul3s(nv, expf(-f.strength * w * dt));
+                }
+            }
+            // Colliders.
+            const float radius = p.particle_radius, adh = p.adhesion_accel, adh_range = p.adhesion_range, friction = p.friction;
+            for (uint32_t k = 0; k < p.num_colliders; ++k) {
+                const slosh_collider_t& c = d.colliders[k];
+                const float dist = collider_sdf(c, x);
+                if (adh > 0.0f && dist < radius + adh_range) {
+                    const float3 nn = collider_normal(c, x, 0.25f * h);
+                    const float w = saturatef(1.0f - (dist - radius) / adh_range);
+                    const float3 vs = collider_velocity_at(c, x);
+                    const float vn = dot3(sub3(nv, vs), nn);
+                    nv = sub3(nv, mul3s(nn, fminf(adh * w * dt, fmaxf(vn, 0.0f) + adh * w * dt * 0.25f)));
+                }
+                if (dist < radius) {
+                    const float3 nn = collider_normal(c, x, 0.25f * h);
+                    x = addf3(x, mul3s(nn, radius - dist));
+                    const float3 vs = collider_velocity_at(c, x);
+                    float3 rel = sub3(nv, vs);
+                    const float vn = dot3(rel, nn);
+                    if (vn < 0.0f) {
+                        rel = sub3(rel, scale3(vn, nn));
+                        rel = sub3(rel, scale3(friction, sub3(rel, scale3(dot3(rel, nn), nn))));
+                    }
+                    nv = addf3(vs, rel);
+                }
+            }
+            // Domain walls.
+            uint32_t wall = 0u;
+            float xs[3] = {x.x, x.y, x.z}, vs[3] = {nv.x, nv.y, nv.z};
+            const float his[3] = {hi.x, hi.y, hi.z};
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                if (xs[a] < lo) { xs[a] = lo; vs[a] = fmaxf(vs[a], 0.0f); wall |= 1u << a; }
+                else if (xs[a] > his[a]) { xs[a] = his[a]; vs[a] = fminf(vs[a], 0.0f); wall |= 1u << a; }
+            }
+            if (wall != 0u && friction > 0.0f) {
+#pragma unroll
+                for (int a = 0; a < 3; ++a)
+                    if ((wall & (1u << a)) == 0u) vs[a] = vs[a] * (1.0f - friction);
+            }
+            x = make_float3(xs[0], xs[1], xs[2]);
+            nv = make_float3(vs[0], vs[1], vs[2]);
+            const float speed = len3(nv);
+            if (speed > p.max_speed) {
+                atomicAdd(d.stats + 9, 1u);
+                atomicAdd(d.stats + 10, __float2uint_rz(x.x * 100.0f));
+                atomicAdd(d.stats + 11, __float2uint_rz(x.y * 100.0f));
+                atomicAdd(d.stats + 12, __float2uint_rz(x.z * 100.0f));
+                const int3 sc = make_int3(int(floorf(P.pos.x * inv_h)), int(floorf(P.pos.y * inv_h)), int(floorf(P.pos.z * inv_h)));
+                if (type_of(get_cell_type(d, sc)) == CELL_SOLID) atomicAdd(d.stats + 13, 1u);
+            }
+            bool drained = false;
+            for (uint32_t dr = 0; dr < p.num_manipulators && !drained; ++dr) {
+                const slosh_manipulator_t& f = d.manipulators[dr];
+                if (f.kind != MANIP_DRAIN || manipulator_sdf(f, x) > 0.0f) continue;
+                const float chance = f.param0 > 0.0f ? 1.0f - expf(-f.param0 * dt) : 1.0f;
+                if (chance >= 1.0f || hash_to_unit(pcg_hash(i * 2654435761u + p.frame_seed * 97u + dr)) < chance) {
+                    store_dead(particles, i);
+                    atomicAdd(d.stats + 15, 1u);
+                    drained = true;
+                }
+            }
+            if (!drained) {
+                P.pos = x;
+                P.vel = nv;
+                P.age = P.age + dt;
+                store_particle(particles, i, P);
+                speed_bits = __float_as_uint(speed);
+                const int3 ec = make_int3(clampi(int(floorf(x.x * inv_h)), 0, d.grid.x - 1), clampi(int(floorf(x.y * inv_h)), 0, d.grid.y - 1),
+                                          clampi(int(floorf(x.z * inv_h)), 0, d.grid.z - 1));
+                brick = brick_index_of(d, make_int3(ec.x >> 3, ec.y >> 3, ec.z >> 3));
+            }
+        }
+    }
+    // Touch flags: sorted particles mostly share bricks, so only the first lane of each run writes.
+    const uint32_t prev = __shfl_up_sync(0xFFFFFFFFu, brick, 1);
+    if (brick != NO_BRICK && ((threadIdx.x & 31) == 0 || prev != brick)) d.brick_touch[brick] = 1u;
+    speed_bits = __reduce_max_sync(0xFFFFFFFFu, speed_bits);
+    if ((threadIdx.x & 31) == 0 && speed_bits) atomicMax(d.stats + 0, speed_bits);
+}
+
+}  // namespace
+
+int launch_emit_reserve(uint32_t* particle_count, uint32_t count, cudaStream_t s) {
+    k_emit_reserve<<<1, 1, 0, s>>>(particle_count, count);
+    return 1;
+}
+int launch_emit(const Dev& d, slosh_particle_t* particles, const uint32_t* pc, const slosh_emit_request_t& em, uint32_t count,
+                uint32_t bound, uint32_t capacity, uint32_t seed, cudaStream_t s) {
+    if (count == 0) return 0;
+    k_emit<<<(count + 255u) / 256u, 256, 0, s>>>(d, particles, pc, em, count, bound, capacity, seed);
+    return 1;
+}
+int launch_touch_particles(const Dev& d, const slosh_particle_t* particles, uint32_t n, cudaStream_t s) {
+    if (n == 0) return 0;
+    k_touch<<<(n + 255u) / 256u, 256, 0, s>>>(d, particles, n);
+    return 1;
+}
+int launch_p2g(const Dev& d, const Pass& p, const slosh_particle_t* particles, uint32_t n, cudaStream_t s) {
+    if (n == 0) return 0;
+    static bool configured = false;
+    const int smem = (6 * P2G_TILE_NODES + P2G_TILE_CELLS) * int(sizeof(int));
+    if (!configured) {
+        cudaFuncSetAttribute(k_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        configured = true;
+    }
+    k_p2g<<<(n + P2G_THREADS - 1u) / P2G_THREADS, P2G_THREADS, smem, s>>>(d, p, particles, n);
+    return 1;
+}
+int launch_g2p(const Dev& d, const Pass& p, slosh_particle_t* particles, uint32_t n, const float* vel, const float* disp,
+               bool apply_density, cudaStream_t s) {
+    if (n == 0) return 0;
+    k_g2p<<<(n + G2P_THREADS - 1u) / G2P_THREADS, G2P_THREADS, 0, s>>>(d, p, particles, n, vel, disp, apply_density ? 1u : 0u);
+    return 1;
+}
+
+}  // namespace slosh
