@@ -1,0 +1,327 @@
+#!/usr/bin/env python
+"""Throughput of the B200-native FLIP/APIC substep on the 256^3 sparse dam break + falling sphere.
+
+Workload (default `dam_break_sphere_256`): 256^3 cells (h = 1/256, 8^3 bricks, storage budget 1.0),
+liquid block x < 0.3, y < 0.5 plus a liquid sphere of radius 0.12 at (0.7, 0.75, 0.5) falling at
+2 m/s, 8 jittered particles per fluid cell (seed 1): 20,583,872 particles, 48-byte records (0.99 GB,
+far larger than the 126 MB L2, so no L2 flush is needed between steps). APIC, gravity -9.81 y,
+CFL 1, frame dt 1/120 s, pressure by FP32 MGPCG to a relative residual of 1e-6, spatial sort every 4
+frames, two-sided density projection on the last substep of each frame (the plugin's defaults).
+
+A step is one frame: the CFL substeps of 1/120 s plus the frame's sort and readback. The metric is
+substeps per second (whole job; with --gpus N each rank advances its own replica of the tank, no
+data-path collective, "weak" scaling). `value` is timed with CUDA events on the simulation stream;
+`e2e` is the same loop timed on the host through the C ABI (slosh_step_frame with host frame input,
+host results readback), with the bytes the library copied each way.
+
+`--impl reference` times the reference path's CPU restatement (the C++ oracle, OpenMP over all host
+cores) on the same workload, one substep per step.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "FLIP substeps/s at 256^3 ~16M particles; pressure-solve ms to 1e-6 rel residual"
+HBM_FALLBACK_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["slosh", "reference"], default="slosh")
+    ap.add_argument("--workload", choices=["dam_break_sphere_256", "dam_break_64"], default="dam_break_sphere_256")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def make_scene(workload, default_fn):
+    from slosh_b200 import scenes
+    if workload == "dam_break_64":
+        sc = scenes.dam_break(default_fn, n=64)
+        sc["settings"].sort_interval = 4
+    else:
+        sc = scenes.dam_break_sphere(default_fn, n=256)
+    sc["settings"].max_substeps = 16  # CFL 1 holds; the plugin's default cap of 4 would exceed it
+    return sc
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        rows = [r for r in self.rows if r[0] == str(self.index)] or self.rows
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def cpu_baseline_sample(workload):
+    """One substep of the same workload by the C++ oracle on all host cores (bounded: ~10-30 s)."""
+    from oracle import oracle as O
+    from slosh_b200 import _abi as A
+    O.build()
+    cores = O.set_threads(os.cpu_count() or 1)
+    sc = make_scene(workload, O.settings_default)
+    o = O.Oracle(sc["settings"])
+    o.set_emit_seed(sc["seed"])
+    fi = A.frame_input(sc["settings"], emits=sc["emits"])
+    n, _ = o.begin_frame(fi)
+    t0 = time.perf_counter()
+    o.substep(0)
+    el = time.perf_counter() - t0
+    o.close()
+    return {"value": 1.0 / el, "unit": "substeps/s", "cores": cores, "kind": "port",
+            "sample": f"1 substep (frame 1, substep 0 of {n}) of {sc['name']}, {sc['particles']} particles, "
+                      f"C++ oracle with OpenMP, {el:.2f} s"}
+
+
+def run_reference(args):
+    world, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    from slosh_b200 import _abi as A
+    O.build()
+    cores = O.set_threads(os.cpu_count() or 1)
+    sc = make_scene(args.workload, O.settings_default)
+    o = O.Oracle(sc["settings"])
+    o.set_emit_seed(sc["seed"])
+    fi = A.frame_input(sc["settings"], emits=sc["emits"])
+    fi_next = A.frame_input(sc["settings"])
+    pending = []
+
+    def next_substep():
+        nonlocal fi
+        if not pending:
+            if getattr(next_substep, "open", False):
+                o.end_frame()
+            n, _ = o.begin_frame(fi)
+            fi = fi_next
+            pending.extend(range(n))
+            next_substep.open = True
+        o.substep(pending.pop(0))
+
+    for _ in range(args.warmup):
+        next_substep()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        next_substep()
+    el = time.perf_counter() - t0
+    value = args.steps / el
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "substeps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * el / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": sc["name"], "grid": list(sc["settings"].grid_dim), "particles": sc["particles"],
+                   "solver": "MGPCG", "tolerance": 1e-6, "step": "one substep"},
+        "cpu_baseline": {"value": value, "unit": "substeps/s", "cores": cores, "kind": "port",
+                         "sample": f"{args.steps} substeps of {sc['name']} after {args.warmup} warm-up substeps"},
+        "e2e": {"value": value, "unit": "substeps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_slosh(args):
+    world, rank, local = dist_setup(args.gpus)
+    import torch
+
+    import slosh_b200 as S
+    from slosh_b200 import _abi as A
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    sc = make_scene(args.workload, S.settings_default)
+    sim = S.Simulation(sc["settings"], device=local)
+    stream = torch.cuda.Stream()
+    sim.set_stream(stream.cuda_stream)
+    sim.set_emit_seed(sc["seed"])
+    sim.step_frame(A.frame_input(sc["settings"], emits=sc["emits"]))  # scene creation (frame 1)
+    fi = A.frame_input(sc["settings"])
+    for _ in range(max(args.warmup, 3) - 1):
+        sim.step_frame(fi)
+    sim.enable_phase_timing(True)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    l0 = sim.launch_count()
+    h0, d0 = sim.transfer_bytes()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    phase = {k: 0.0 for k in S.PHASES}
+    substeps = 0
+    iters = []
+    rels = []
+    active = 0
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        sim.step_frame(fi)
+        r = sim.results()
+        substeps += r.substeps
+        iters.append(r.last_solve_iterations)
+        rels.append(r.last_solve_rel_residual)
+        active = max(active, int(r.raw_stats[7]))
+        for k, v in sim.phase_ms().items():
+            phase[k] += v
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    clk = clocks.stop()
+    dev_ms = ev0.elapsed_time(ev1)
+    wall_ms = (t1 - t0) * 1000.0
+    launches = sim.launch_count() - l0
+    h1, d1 = sim.transfer_bytes()
+    if dist:
+        t = torch.tensor([dev_ms, wall_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dev_ms, wall_ms = float(t[0]), float(t[1])
+        s = torch.tensor([float(substeps)], dtype=torch.float64, device="cuda")
+        dist.all_reduce(s, op=dist.ReduceOp.SUM)
+        total_substeps = float(s[0])
+    else:
+        total_substeps = float(substeps)
+    if rank != 0:
+        sim.close()
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+    n_particles = sc["particles"]
+    peak, peak_kind = measured_peak()
+    active_cells = active * 512
+    # Roofline of the dominant single-kernel phase: algorithmic bytes per launch / event-timed duration.
+    algo = {"g2p": 96.0 * n_particles + 16.0 * active_cells, "p2g": 48.0 * n_particles + 28.0 * active_cells}
+    dom = max(("g2p", "p2g"), key=lambda k: phase[k])
+    per_launch_ms = phase[dom] / max(substeps, 1)
+    achieved = algo[dom] / (per_launch_ms * 1e-3) / 1e9 if per_launch_ms > 0 else 0.0
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        try:
+            with open(tp) as f:
+                tj = json.load(f)
+            if dom in tj and tj[dom].get("workload") == sc["name"]:
+                traffic = tj[dom]["bytes_per_launch"]
+        except Exception:
+            traffic = None
+    line = {
+        "metric": METRIC, "value": total_substeps / (dev_ms * 1e-3), "unit": "substeps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": sc["name"], "grid": list(sc["settings"].grid_dim), "particles": n_particles,
+                   "solver": "MGPCG", "tolerance": 1e-6, "transfer": "APIC", "cfl": 1.0, "frame_dt": 1.0 / 120.0,
+                   "sort_interval": 4, "parallelism": f"replicas{world}", "step": "one frame of CFL substeps",
+                   "l2": "inputs larger than L2 (particles 0.99 GB)"},
+        "substeps": total_substeps,
+        "particle_updates_per_s": total_substeps * n_particles / (dev_ms * 1e-3),
+        "pressure_solve_ms": phase["pressure"] / max(substeps, 1),
+        "pressure_iterations_mean": statistics.mean(iters) if iters else None,
+        "pressure_rel_residual_max": max(rels) if rels else None,
+        "phase_ms_per_substep": {k: v / max(substeps, 1) for k, v in phase.items()},
+        "clocks": clk,
+        "e2e": {"value": total_substeps / (wall_ms * 1e-3), "unit": "substeps/s",
+                "h2d_bytes_per_step": (h1 - h0) // args.steps, "d2h_bytes_per_step": (d1 - d0) // args.steps},
+        "gpu_launches": launches,
+        "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
+                     "algorithmic_bytes_per_launch": algo[dom]},
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        sim.close()
+        torch.cuda.synchronize()
+        try:
+            line["cpu_baseline"] = cpu_baseline_sample(args.workload)
+        except Exception as e:  # keep the GPU line even if the host sample fails
+            line["cpu_baseline"] = {"value": None, "unit": "substeps/s", "error": str(e)[:200]}
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_slosh(args)
+
+
+if __name__ == "__main__":
+    main()

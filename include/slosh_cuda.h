@@ -335,6 +335,9 @@ SLOSH_API slosh_status slosh_enable_phase_timing(void* ctx, int32_t enable);
 SLOSH_API slosh_status slosh_get_phase_ms(void* ctx, float* out_ms, int32_t n);
 /* Number of kernel launches this library issued since creation. */
 SLOSH_API uint64_t slosh_launch_count(void* ctx);
+/* Bytes this context copied host->device and device->host since creation (frame inputs,
+ * results, solver residual checks, particle uploads and downloads, buffer reads and writes). */
+SLOSH_API slosh_status slosh_transfer_bytes(void* ctx, uint64_t* out_h2d, uint64_t* out_d2h);
 
 #ifdef __cplusplus
 } /* extern "C" */

@@ -47,6 +47,7 @@ SIGNATURES = {
     "slosh_enable_phase_timing": ([_VP, C.c_int32], C.c_int),
     "slosh_get_phase_ms": ([_VP, C.POINTER(C.c_float), C.c_int32], C.c_int),
     "slosh_launch_count": ([_VP], C.c_uint64),
+    "slosh_transfer_bytes": ([_VP, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)], C.c_int),
 }
 PHASES = ("sort", "pool", "p2g", "grid", "pressure", "project", "density", "extrapolate", "g2p")
 
@@ -191,3 +192,8 @@ class Simulation:
 
     def launch_count(self):
         return int(self._lib.slosh_launch_count(self._ctx))
+
+    def transfer_bytes(self):
+        h2d, d2h = C.c_uint64(), C.c_uint64()
+        _check(self._lib.slosh_transfer_bytes(self._ctx, C.byref(h2d), C.byref(d2h)))
+        return int(h2d.value), int(d2h.value)

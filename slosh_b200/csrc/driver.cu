@@ -181,6 +181,7 @@ struct Ctx {
     std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> phase_events;
     float phase_ms[NUM_PHASES] = {};
     uint64_t launches = 0;
+    uint64_t h2d_bytes = 0, d2h_bytes = 0;
 
     // ---------------------------------------------------------------------------------------------
     template <class T>
@@ -439,11 +440,13 @@ struct Ctx {
         if (num_colliders) {
             std::memcpy(h_colliders, in.colliders, sizeof(slosh_collider_t) * num_colliders);
             CK(cudaMemcpyAsync(colliders_d, h_colliders, sizeof(slosh_collider_t) * num_colliders, cudaMemcpyHostToDevice, stream));
+            h2d_bytes += sizeof(slosh_collider_t) * num_colliders;
         }
         if (num_manipulators) {
             std::memcpy(h_manipulators, in.manipulators, sizeof(slosh_manipulator_t) * num_manipulators);
             CK(cudaMemcpyAsync(manipulators_d, h_manipulators, sizeof(slosh_manipulator_t) * num_manipulators, cudaMemcpyHostToDevice,
                                stream));
+            h2d_bytes += sizeof(slosh_manipulator_t) * num_manipulators;
         }
         const float h = s.cell_size;
         P.num_colliders = num_colliders;
@@ -509,6 +512,7 @@ struct Ctx {
     }
     double read_rel_residual() {
         CK(cudaMemcpyAsync(h_scalars + 4, mg.scalars + 4, 2 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+        d2h_bytes += 2 * sizeof(double);
         CK(cudaStreamSynchronize(stream));
         const double bb = h_scalars[4], rr = h_scalars[5];
         return bb > 0.0 ? std::sqrt(rr / bb) : 0.0;
@@ -552,6 +556,7 @@ struct Ctx {
                 rel_pending = false;
             } else {  // read at the end of the frame, without a sync here
                 CK(cudaMemcpyAsync(h_scalars + 8, mg.scalars + 4, 2 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+                d2h_bytes += 2 * sizeof(double);
                 rel_pending = true;
             }
         }
@@ -699,6 +704,7 @@ void Ctx::end_frame() {
     CK(cudaMemcpyAsync(h_stats + SLOSH_NUM_STATS, particle_count, 16, cudaMemcpyDeviceToHost, stream));
     CK(cudaMemcpyAsync(h_scalars, mg.scalars, 8 * sizeof(double), cudaMemcpyDeviceToHost, stream));
     CK(cudaMemcpyAsync(h_coupling, coupling, SLOSH_MAX_COLLIDERS * SLOSH_COUPLING_STRIDE * 4, cudaMemcpyDeviceToHost, stream));
+    d2h_bytes += SLOSH_NUM_STATS * 4 + 16 + 8 * sizeof(double) + SLOSH_MAX_COLLIDERS * SLOSH_COUPLING_STRIDE * 4;
     CK(cudaStreamSynchronize(stream));
     if (substeps > 0) {
         float ms;
@@ -1002,6 +1008,7 @@ SLOSH_API slosh_status slosh_upload_particles(void* ctx, const slosh_particle_t*
         c->num_particles = count;
         uint32_t pcv[2] = {count, 0u};
         CK(cudaMemcpyAsync(c->particle_count, pcv, 8, cudaMemcpyHostToDevice, c->stream));
+        c->h2d_bytes += sizeof(slosh_particle_t) * count + 8;
         c->count(launch_touch_particles(c->dev(), c->particles[c->pbuf], count, c->stream));
         CK(cudaGetLastError());
         CK(cudaStreamSynchronize(c->stream));
@@ -1015,6 +1022,7 @@ SLOSH_API slosh_status slosh_download_particles(void* ctx, slosh_particle_t* out
         if (!out) return SLOSH_OK;
         const uint32_t n = std::min(capacity, c->num_particles);
         if (n) CK(cudaMemcpyAsync(out, c->particles[c->pbuf], sizeof(slosh_particle_t) * n, cudaMemcpyDeviceToHost, c->stream));
+        c->d2h_bytes += sizeof(slosh_particle_t) * n;
         CK(cudaStreamSynchronize(c->stream));
         return SLOSH_OK;
     });
@@ -1076,6 +1084,7 @@ SLOSH_API slosh_status slosh_read_buffer(void* ctx, int32_t buffer_id, void* hos
         if (bytes < v.bytes || (!host_dst && v.bytes)) throw StatusError{SLOSH_ERR_INVALID_ARG, "destination too small"};
         CK(cudaStreamSynchronize(c->stream));
         if (v.bytes) CK(cudaMemcpy(host_dst, v.ptr, v.bytes, cudaMemcpyDeviceToHost));
+        c->d2h_bytes += v.bytes;
         return SLOSH_OK;
     });
 }
@@ -1113,5 +1122,13 @@ SLOSH_API slosh_status slosh_get_phase_ms(void* ctx, float* out_ms, int32_t n) {
     });
 }
 SLOSH_API uint64_t slosh_launch_count(void* ctx) { return ctx ? static_cast<Ctx*>(ctx)->launches : 0; }
+SLOSH_API slosh_status slosh_transfer_bytes(void* ctx, uint64_t* out_h2d, uint64_t* out_d2h) {
+    return guarded([&]() -> slosh_status {
+        Ctx* c = as_ctx(ctx);
+        if (out_h2d) *out_h2d = c->h2d_bytes;
+        if (out_d2h) *out_d2h = c->d2h_bytes;
+        return SLOSH_OK;
+    });
+}
 
 }  // extern "C"
