@@ -247,15 +247,8 @@ def run_slosh(args):
     wall_ms = (t1 - t0) * 1000.0
     launches = sim.launch_count() - l0
     h1, d1 = sim.transfer_bytes()
-    if dist:
-        t = torch.tensor([dev_ms, wall_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dev_ms, wall_ms = float(t[0]), float(t[1])
-        s = torch.tensor([float(substeps)], dtype=torch.float64, device="cuda")
-        dist.all_reduce(s, op=dist.ReduceOp.SUM)
-        total_substeps = float(s[0])
-    else:
-        total_substeps = float(substeps)
+    from slosh_b200.replicas import reduce_run
+    total_substeps, dev_ms, wall_ms = reduce_run(substeps, dev_ms, wall_ms)
     if rank != 0:
         sim.close()
         if dist:

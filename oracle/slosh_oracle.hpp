@@ -1261,11 +1261,13 @@ public:
         last_solve_converged = !tol_mode || rel() <= double(tolerance);
         return done;
     }
-    void update_d(bool first) {  // PCGUpdateDCS
+    // PCGUpdateDCS: d = z + beta d. The first direction is d = z exactly (the reference computes
+    // z + 0 * d; the two differ only in the sign of a zero or a non-finite stale d).
+    void update_d(bool first) {
         const R beta = first ? R(0) : R(ratio_f(scalars[0], scalars[3]));
         for_active_cells([&](uint32_t i, I3) {
             if (type_of(cell_type[i]) != CELL_FLUID) return;
-            pcg_d[i] = pcg_z[i] + beta * pcg_d[i];
+            pcg_d[i] = first ? pcg_z[i] : pcg_z[i] + beta * pcg_d[i];
         });
     }
     // ||b - A p|| / ||b|| with the level-0 operator (diagnostic of a finished solve).

@@ -20,6 +20,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -173,6 +174,27 @@ struct Ctx {
     bool last_converged = true;
     bool pool_overflow_seen = false;
     bool rel_pending = false;
+    bool solve_tol_mode = false;
+    float solve_tol = 0.0f;
+
+    // MGPCG solves as CUDA graphs: pre-nodes, then a WHILE node whose body is one PCG iteration
+    struct SolveGraph {
+        float* p;
+        const float* div;
+        uint32_t limit;
+        bool tol_mode;
+        float tol;
+        int coarse;
+        cudaGraph_t graph;
+        cudaGraphExec_t exec;
+        int pre_nodes, body_nodes;
+    };
+    std::vector<SolveGraph> graphs;
+    cudaStream_t cap_stream = nullptr, body_stream = nullptr;
+    bool use_graphs = true;
+    uint32_t* h_ctl = nullptr;          // pinned: [0..3] ctl of the pressure solve, [4..7] of the density solve
+    struct SolveRecord { int pre, body, slot; };
+    std::vector<SolveRecord> frame_solves;
 
     // timing
     bool timing = false;
@@ -202,8 +224,16 @@ struct Ctx {
         for (void* p : v) cudaFree(p);
         v.clear();
     }
+    void destroy_graphs() {
+        for (auto& g : graphs) {
+            if (g.exec) cudaGraphExecDestroy(g.exec);
+            if (g.graph) cudaGraphDestroy(g.graph);
+        }
+        graphs.clear();
+    }
     void release() {
         if (stream) cudaStreamSynchronize(stream);
+        destroy_graphs();
         free_list(grid_allocs);
         free_list(particle_allocs);
         grid_bytes = particle_bytes = 0;
@@ -305,10 +335,14 @@ struct Ctx {
         mg.r = dalloc<float>(pc, false);
         mg.z = dalloc<float>(pc, false);
         mg.dvec = dalloc<float>(pc, false);
+        mg.dvec2 = dalloc<float>(pc, false);
+        mg.word = dalloc<uint8_t>(pc, false);
+        mg.nbr_slots = dalloc<uint32_t>(8 * size_t(num_pool_bricks), false);
         mg.q = dalloc<float>(pc, false);
         mg.partials = dalloc<double>(2 * size_t(num_pool_bricks), false);
         mg.scalars = dalloc<double>(8, false);
         mg.counters = dalloc<uint32_t>(8, false);
+        mg.ctl = dalloc<uint32_t>(8, false);
         // zero everything (AddClearUAVPass of every buffer), then the free stack and the slot table
         zero_all();
         std::vector<uint32_t> free_init(num_pool_bricks);
@@ -333,8 +367,10 @@ struct Ctx {
         CK(cudaMemset(face_flags, 0, tf * 4));
         CK(cudaMemset(face_weight, 0, tf * 4));
         for (void* p : {(void*)cell_type, (void*)cell_count, (void*)pressure, (void*)divergence, (void*)cell_diag, (void*)density_q,
-                        (void*)density_rhs, (void*)mg.r, (void*)mg.z, (void*)mg.dvec, (void*)mg.q})
+                        (void*)density_rhs, (void*)mg.r, (void*)mg.z, (void*)mg.dvec, (void*)mg.dvec2, (void*)mg.q})
             CK(cudaMemset(p, 0, pc * 4));
+        CK(cudaMemset(mg.word, 0, pc));
+        CK(cudaMemset(mg.nbr_slots, 0, 8 * size_t(num_pool_bricks) * 4));
         CK(cudaMemset(coupling, 0, SLOSH_MAX_COLLIDERS * SLOSH_COUPLING_STRIDE * 4));
         CK(cudaMemset(stats, 0, SLOSH_NUM_STATS * 4));
         CK(cudaMemset(particle_count, 0, 16));
@@ -352,6 +388,8 @@ struct Ctx {
         }
         CK(cudaMemset(mg.scalars, 0, 8 * sizeof(double)));
         CK(cudaMemset(mg.counters, 0, 8 * 4));
+        CK(cudaMemset(mg.ctl, 0, 8 * 4));
+        CK(cudaMemset(mg.partials, 0, 2 * size_t(num_pool_bricks) * sizeof(double)));
         CK(cudaMemset(particles[0], 0, size_t(capacity) * sizeof(slosh_particle_t)));
     }
 
@@ -491,76 +529,107 @@ struct Ctx {
     }
 
     // ---- MGPCG driver (AddPressureSolveMGPCG, SloshProxy.cpp:807-1020) ----
-    void vcycle(const Dev& d, int coarse_iterations) {
-        const int nl = num_levels;
-        if (nl == 1) {
-            count(launch_mg_coarse_solve(d, mg, 0, coarse_iterations, stream));
-            count(launch_mg_smooth(d, mg, 0, 0u, true, shape, stream));
-            return;
-        }
-        count(launch_mg_smooth(d, mg, 0, 1u, false, shape, stream));
-        for (int l = 0; l < nl - 1; ++l) {
-            count(launch_mg_restrict(d, mg, l, shape, stream));
-            if (l + 1 < nl - 1) count(launch_mg_smooth(d, mg, l + 1, 1u, false, shape, stream));
-        }
-        count(launch_mg_coarse_solve(d, mg, nl - 1, coarse_iterations, stream));
-        for (int l = nl - 2; l >= 0; --l) {
-            count(launch_mg_prolong(d, mg, l, shape, stream));
-            count(launch_mg_smooth(d, mg, l, 1u, false, shape, stream));
-            count(launch_mg_smooth(d, mg, l, 0u, l == 0, shape, stream));
-        }
+    // Sequence of one solve: setup, coarse cell types, PCGInit, then while the device says so:
+    // V-cycle, UpdateD, ApplyA, UpdatePR. This is the reference's order (init, V-cycle, UpdateD(first),
+    // then per iteration ApplyA, UpdatePR and -- unless it was the last -- V-cycle, UpdateD).
+    int enqueue_pre(const Dev& d, float* p, const float* div, uint32_t limit, bool tol_mode, float tol, unsigned long long handle,
+                    cudaStream_t s) {
+        int n = launch_mg_setup(mg, limit, tol_mode, double(tol), s);
+        for (int l = 0; l < num_levels - 1; ++l) n += launch_mg_build_type(d, mg, l, s);
+        n += launch_pcg_init(d, mg, p, div, handle, shape, s);
+        return n;
     }
-    double read_rel_residual() {
-        CK(cudaMemcpyAsync(h_scalars + 4, mg.scalars + 4, 2 * sizeof(double), cudaMemcpyDeviceToHost, stream));
-        d2h_bytes += 2 * sizeof(double);
-        CK(cudaStreamSynchronize(stream));
-        const double bb = h_scalars[4], rr = h_scalars[5];
-        return bb > 0.0 ? std::sqrt(rr / bb) : 0.0;
+    int enqueue_body(const Dev& d, float* p, int coarse, unsigned long long handle, cudaStream_t s) {
+        int n = launch_vcycle(d, mg, coarse, shape, s);
+        n += launch_pcg_update_d(d, mg, shape, s);
+        n += launch_pcg_apply_a(d, mg, shape, s);
+        n += launch_pcg_update_pr(d, mg, p, handle, shape, s);
+        return n;
     }
-    int mgpcg(float* p, const float* div, int fixed_iterations, float tolerance, int max_iterations, int coarse_iterations,
-              bool record) {
+    SolveGraph* solve_graph(float* p, const float* div, uint32_t limit, bool tol_mode, float tol, int coarse) {
+        for (auto& g : graphs)
+            if (g.p == p && g.div == div && g.limit == limit && g.tol_mode == tol_mode && g.tol == tol && g.coarse == coarse) return &g;
         const Dev d = dev();
-        for (int l = 0; l < num_levels - 1; ++l) count(launch_mg_build_type(d, mg, l, stream));
-        count(launch_pcg_init(d, mg, p, div, shape, stream));
+        SolveGraph G{p, div, limit, tol_mode, tol, coarse, nullptr, nullptr, 0, 0};
+        CK(cudaStreamBeginCapture(cap_stream, cudaStreamCaptureModeThreadLocal));
+        cudaGraph_t cg = nullptr;
+        try {
+            cudaStreamCaptureStatus st;
+            const cudaGraphNode_t* deps = nullptr;
+            size_t nd = 0;
+            CK(cudaStreamGetCaptureInfo(cap_stream, &st, nullptr, &cg, &deps, &nd));
+            cudaGraphConditionalHandle h;
+            CK(cudaGraphConditionalHandleCreate(&h, cg, 0, cudaGraphCondAssignDefault));
+            G.pre_nodes = enqueue_pre(d, p, div, limit, tol_mode, tol, h, cap_stream);
+            CK(cudaStreamGetCaptureInfo(cap_stream, &st, nullptr, &cg, &deps, &nd));
+            cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+            cp.conditional.handle = h;
+            cp.conditional.type = cudaGraphCondTypeWhile;
+            cp.conditional.size = 1;
+            cudaGraphNode_t cn;
+            CK(cudaGraphAddNode(&cn, cg, deps, nd, &cp));
+            cudaGraph_t body = cp.conditional.phGraph_out[0];
+            CK(cudaStreamBeginCaptureToGraph(body_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+            G.body_nodes = enqueue_body(d, p, coarse, h, body_stream);
+            CK(cudaStreamEndCapture(body_stream, &body));
+            CK(cudaStreamUpdateCaptureDependencies(cap_stream, &cn, 1, cudaStreamSetCaptureDependencies));
+            CK(cudaStreamEndCapture(cap_stream, &G.graph));
+            CK(cudaGraphInstantiate(&G.exec, G.graph, 0));
+        } catch (...) {
+            cudaGraph_t junk = nullptr;
+            cudaStreamEndCapture(body_stream, &junk);
+            if (junk) cudaGraphDestroy(junk);
+            junk = nullptr;
+            cudaStreamEndCapture(cap_stream, &junk);
+            if (junk) cudaGraphDestroy(junk);
+            if (G.graph) cudaGraphDestroy(G.graph);
+            cudaGetLastError();
+            throw;
+        }
+        graphs.push_back(G);
+        return &graphs.back();
+    }
+    // slot 0: the pressure solve's statistics are read back at the end of the frame; slot 1: density.
+    void mgpcg(float* p, const float* div, int fixed_iterations, float tolerance, int max_iterations, int coarse_iterations,
+               int slot) {
         const bool tol_mode = fixed_iterations <= 0;
-        const int iterations = tol_mode ? std::max(max_iterations, 1) : std::min(std::max(fixed_iterations, 1), 100);
-        double rel = 0.0;
-        if (tol_mode) {
-            rel = read_rel_residual();
-            if (rel <= double(tolerance)) {
-                if (record) { last_iterations = 0; last_rel = float(rel); last_converged = true; }
-                return 0;
+        const uint32_t limit = tol_mode ? uint32_t(std::max(max_iterations, 1)) : uint32_t(std::min(std::max(fixed_iterations, 1), 100));
+        const Dev d = dev();
+        SolveGraph* G = nullptr;
+        if (use_graphs) {
+            try {
+                G = solve_graph(p, div, limit, tol_mode, tolerance, coarse_iterations);
+            } catch (const CudaError& e) {
+                std::fprintf(stderr, "slosh: CUDA graph capture of the solve failed (%s: %s); issuing kernels directly\n", e.what,
+                             cudaGetErrorString(e.code));
+                use_graphs = false;
+                destroy_graphs();
             }
         }
-        vcycle(d, coarse_iterations);
-        count(launch_pcg_update_d(d, mg, true, shape, stream));
-        int done = 0;
-        for (int it = 0; it < iterations; ++it) {
-            count(launch_pcg_apply_a(d, mg, shape, stream));
-            count(launch_pcg_update_pr(d, mg, p, shape, stream));
-            done = it + 1;
-            if (tol_mode) {
-                rel = read_rel_residual();
-                if (rel <= double(tolerance)) break;
+        if (G) {
+            CK(cudaGraphLaunch(G->exec, stream));
+            frame_solves.push_back({G->pre_nodes, G->body_nodes, slot});
+        } else {
+            int pre = enqueue_pre(d, p, div, limit, tol_mode, tolerance, 0ull, stream);
+            int body = 0;
+            for (uint32_t it = 0; it < limit; ++it) {
+                CK(cudaMemcpyAsync(h_ctl + 4 * slot, mg.ctl, 16, cudaMemcpyDeviceToHost, stream));
+                d2h_bytes += 16;
+                CK(cudaStreamSynchronize(stream));
+                if (h_ctl[4 * slot + 3]) break;
+                body = enqueue_body(d, p, coarse_iterations, 0ull, stream);
             }
-            if (it + 1 < iterations) {
-                vcycle(d, coarse_iterations);
-                count(launch_pcg_update_d(d, mg, false, shape, stream));
-            }
+            frame_solves.push_back({pre, body, slot});
         }
-        if (record) {
-            last_iterations = done;
-            last_converged = !tol_mode || rel <= double(tolerance);
-            if (tol_mode) {
-                last_rel = float(rel);
-                rel_pending = false;
-            } else {  // read at the end of the frame, without a sync here
-                CK(cudaMemcpyAsync(h_scalars + 8, mg.scalars + 4, 2 * sizeof(double), cudaMemcpyDeviceToHost, stream));
-                d2h_bytes += 2 * sizeof(double);
-                rel_pending = true;
-            }
+        CK(cudaMemcpyAsync(h_ctl + 4 * slot, mg.ctl, 16, cudaMemcpyDeviceToHost, stream));
+        d2h_bytes += 16;
+        if (slot == 0) {
+            CK(cudaMemcpyAsync(h_scalars + 8, mg.scalars + 4, 2 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+            d2h_bytes += 2 * sizeof(double);
+            rel_pending = true;
+            solve_tol_mode = tol_mode;
+            solve_tol = tolerance;
         }
-        return done;
     }
 
     // ---- frame prologue (Step_RenderThread :339-562) ----
@@ -572,11 +641,13 @@ struct Ctx {
         ++sim_frame;
         event_next = 0;
         phase_events.clear();
+        frame_solves.clear();
         set_pass_params(in);
         bool has_drain = false;
         for (uint32_t m = 0; m < num_manipulators; ++m) has_drain = has_drain || in.manipulators[m].kind == 0u;
         CK(cudaMemsetAsync(coupling, 0, SLOSH_MAX_COLLIDERS * SLOSH_COUPLING_STRIDE * 4, stream));
         CK(cudaMemsetAsync(stats, 0, SLOSH_NUM_STATS * 4, stream));
+        CK(cudaMemsetAsync(mg.ctl + 4, 0, 4, stream));
         if (in.num_emits && !in.emits) throw StatusError{SLOSH_ERR_INVALID_ARG, "emits is NULL"};
         for (uint32_t e = 0; e < in.num_emits; ++e) emit(in.emits[e]);
         if (num_particles > 0 &&
@@ -638,8 +709,8 @@ struct Ctx {
             PhaseScope ps(this, 4);
             if (S.pressure_solver == SLOSH_SOLVER_MGPCG) {
                 const int coarse = clampi_h(S.mg_coarse_iterations, 1, 200);
-                if (S.tolerance > 0.0f) mgpcg(pressure, divergence, 0, S.tolerance, S.max_iterations, coarse, true);
-                else mgpcg(pressure, divergence, S.pcg_iterations, 0.0f, 0, coarse, true);
+                if (S.tolerance > 0.0f) mgpcg(pressure, divergence, 0, S.tolerance, S.max_iterations, coarse, 0);
+                else mgpcg(pressure, divergence, S.pcg_iterations, 0.0f, 0, coarse, 0);
             } else {
                 const float omega = clampf_h(S.sor_weight, 0.5f, 1.95f);
                 for (int it = 0; it < S.pressure_iterations; ++it)
@@ -659,7 +730,7 @@ struct Ctx {
             PhaseScope ps(this, 6);
             count(launch_density_rhs(d, P, shape, stream));
             if (S.pressure_solver == SLOSH_SOLVER_MGPCG) {
-                mgpcg(density_q, density_rhs, 2, 0.0f, 0, clampi_h(S.mg_coarse_iterations, 1, 200), false);
+                mgpcg(density_q, density_rhs, 2, 0.0f, 0, clampi_h(S.mg_coarse_iterations, 1, 200), 1);
             } else {
                 for (int it = 0; it < std::max(S.density_projection_iterations, 1); ++it)
                     for (uint32_t colour = 0; colour < 2u; ++colour)
@@ -703,6 +774,7 @@ void Ctx::end_frame() {
     CK(cudaMemcpyAsync(h_stats, stats, SLOSH_NUM_STATS * 4, cudaMemcpyDeviceToHost, stream));
     CK(cudaMemcpyAsync(h_stats + SLOSH_NUM_STATS, particle_count, 16, cudaMemcpyDeviceToHost, stream));
     CK(cudaMemcpyAsync(h_scalars, mg.scalars, 8 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    CK(cudaMemcpyAsync(h_ctl + 8, mg.ctl + 4, 4, cudaMemcpyDeviceToHost, stream));
     CK(cudaMemcpyAsync(h_coupling, coupling, SLOSH_MAX_COLLIDERS * SLOSH_COUPLING_STRIDE * 4, cudaMemcpyDeviceToHost, stream));
     d2h_bytes += SLOSH_NUM_STATS * 4 + 16 + 8 * sizeof(double) + SLOSH_MAX_COLLIDERS * SLOSH_COUPLING_STRIDE * 4;
     CK(cudaStreamSynchronize(stream));
@@ -716,8 +788,12 @@ void Ctx::end_frame() {
     }
     if (rel_pending) {
         last_rel = float(h_scalars[8] > 0.0 ? std::sqrt(h_scalars[9] / h_scalars[8]) : 0.0);
+        last_iterations = int(h_ctl[0]);
+        last_converged = !solve_tol_mode || double(last_rel) <= double(solve_tol);
         rel_pending = false;
     }
+    for (const auto& r : frame_solves) launches += uint64_t(r.pre) + uint64_t(r.body) * uint64_t(h_ctl[4 * r.slot]);
+    if (h_ctl[8] != 0u) last_converged = false;  // some substep's solve stopped at its iteration limit
     num_particles = std::min(num_particles, h_stats[SLOSH_NUM_STATS + 0]);
     pool_overflow_seen = h_stats[8] != 0u;
     if (timing) {
@@ -874,6 +950,12 @@ SLOSH_API slosh_status slosh_create(const slosh_settings_t* settings, int32_t de
         c->num_sms = prop.multiProcessorCount;
         try {
             CK(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
+            CK(cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking));
+            CK(cudaStreamCreateWithFlags(&c->body_stream, cudaStreamNonBlocking));
+            CK(cudaMallocHost(&c->h_ctl, 16 * sizeof(uint32_t)));
+            std::memset(c->h_ctl, 0, 16 * sizeof(uint32_t));
+            const char* ng = std::getenv("SLOSH_NO_GRAPHS");
+            c->use_graphs = !(ng && ng[0] == '1');
             c->stream = c->own_stream;
             CK(cudaMallocHost(&c->h_colliders, sizeof(slosh_collider_t) * SLOSH_MAX_COLLIDERS));
             CK(cudaMallocHost(&c->h_manipulators, sizeof(slosh_manipulator_t) * SLOSH_MAX_MANIPULATORS));
@@ -905,6 +987,9 @@ SLOSH_API void slosh_destroy(void* ctx) {
     if (c->h_stats) cudaFreeHost(c->h_stats);
     if (c->h_scalars) cudaFreeHost(c->h_scalars);
     if (c->h_coupling) cudaFreeHost(c->h_coupling);
+    if (c->h_ctl) cudaFreeHost(c->h_ctl);
+    if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
+    if (c->body_stream) cudaStreamDestroy(c->body_stream);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
 }
@@ -946,7 +1031,7 @@ SLOSH_API slosh_status slosh_substep(void* ctx, int32_t step_index) {
         Ctx* c = as_ctx(ctx);
         if (step_index < 0 || step_index >= c->substeps) throw StatusError{SLOSH_ERR_INVALID_ARG, "substep index out of range"};
         c->substep(step_index);
-        return c->last_converged ? SLOSH_OK : SLOSH_ERR_NOT_CONVERGED;
+        return SLOSH_OK;
     });
 }
 SLOSH_API slosh_status slosh_end_frame(void* ctx) {
@@ -961,13 +1046,8 @@ SLOSH_API slosh_status slosh_step_frame(void* ctx, const slosh_frame_input_t* in
         Ctx* c = as_ctx(ctx);
         if (!input) throw StatusError{SLOSH_ERR_INVALID_ARG, "input is NULL"};
         const int n = c->begin_frame(*input);
-        bool converged = true;
-        for (int s = 0; s < n; ++s) {
-            c->substep(s);
-            converged = converged && c->last_converged;
-        }
+        for (int s = 0; s < n; ++s) c->substep(s);
         c->end_frame();
-        c->last_converged = converged;
         return frame_status(c);
     });
 }

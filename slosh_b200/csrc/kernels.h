@@ -76,21 +76,26 @@ struct MGState {
     float* z;
     float* dvec;
     float* q;
-    double* partials;     // one per brick entry (capacity num_pool_bricks)
-    double* scalars;      // [0] rho, [1] scratch, [2] d.Ad, [3] previous rho, [4] ||b||^2, [5] ||r||^2, [6] true
+    double* partials;     // one per brick entry, two dots (capacity 2 x num_pool_bricks)
+    double* scalars;      // [0] rho, [2] d.Ad, [3] previous rho, [4] ||b||^2, [5] ||r||^2, [6..7] true residual, [8] tol
     uint32_t* counters;   // last-CTA counters, one per reduction kind
+    uint32_t* ctl;        // [0] completed iterations, [1] limit, [2] tolerance mode, [3] done, [4] frame: a solve hit its limit
+    uint8_t* word;        // level-0 stencil word per pool cell (fluid neighbours, fluid, red)
+    uint32_t* nbr_slots;  // 8 per active-brick entry: slots of the 6 face-neighbour bricks
+    float* dvec2;         // second search-direction buffer (d alternates by iteration parity)
 };
+size_t mg_tail_smem(const MGState& m);
+// First level handled by the single-CTA tail kernel of the V-cycle.
+int mg_tail_level(const MGState& m);
+int launch_mg_setup(const MGState& m, uint32_t limit, bool tol_mode, double tol, cudaStream_t s);
 int launch_mg_build_type(const Dev& d, const MGState& m, int l, cudaStream_t s);
-int launch_pcg_init(const Dev& d, const MGState& m, const float* p, const float* div, const Shape& sh, cudaStream_t s);
-int launch_mg_smooth(const Dev& d, const MGState& m, int l, uint32_t parity, bool dot, const Shape& sh, cudaStream_t s);
-int launch_mg_restrict(const Dev& d, const MGState& m, int l, const Shape& sh, cudaStream_t s);
-int launch_mg_coarse_solve(const Dev& d, const MGState& m, int l, int iterations, cudaStream_t s);
-int launch_mg_prolong(const Dev& d, const MGState& m, int l, const Shape& sh, cudaStream_t s);
+// handle: the WHILE node's condition when the solve runs as a CUDA graph, 0 otherwise.
+int launch_pcg_init(const Dev& d, const MGState& m, const float* p, const float* div, unsigned long long handle, const Shape& sh,
+                    cudaStream_t s);
+int launch_vcycle(const Dev& d, const MGState& m, int coarse_iterations, const Shape& sh, cudaStream_t s);
 int launch_pcg_apply_a(const Dev& d, const MGState& m, const Shape& sh, cudaStream_t s);
-int launch_pcg_update_pr(const Dev& d, const MGState& m, float* p, const Shape& sh, cudaStream_t s);
-int launch_pcg_update_d(const Dev& d, const MGState& m, bool first, const Shape& sh, cudaStream_t s);
+int launch_pcg_update_pr(const Dev& d, const MGState& m, float* p, unsigned long long handle, const Shape& sh, cudaStream_t s);
+int launch_pcg_update_d(const Dev& d, const MGState& m, const Shape& sh, cudaStream_t s);
 int launch_true_residual(const Dev& d, const MGState& m, const float* p, const float* div, const Shape& sh, cudaStream_t s);
-// rho shift after a V-cycle: scalars[3] = scalars[0]; scalars[0] = scalars[1] (the r.z just reduced)
-int launch_shift_rho(const MGState& m, cudaStream_t s);
 
 }  // namespace slosh

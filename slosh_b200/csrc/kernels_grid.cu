@@ -118,8 +118,12 @@ __device__ uint32_t block_scan_1024(uint32_t v, uint32_t* s_warp, uint32_t* tota
 // timing. Here the same stack discipline runs in ascending brick order through block scans: freed
 // slots are pushed in brick order, the j-th brick needing storage pops entry (free count - j), and
 // the active and new-slot lists come out in brick order. This is the serial (canonical) result.
+// Shared-memory budget of the separable dilation: two byte planes of num_bricks.
+constexpr uint32_t POOL_SMEM_BRICKS = 100000u;
+
 __global__ void __launch_bounds__(1024) k_pool_update(Dev d) {
     __shared__ uint32_t s_warp[33];
+    extern __shared__ uint8_t s_flags[];  // [0, nb): touch / z pass, [nb, 2 nb): scratch
     const uint32_t nb = d.num_bricks;
     const uint32_t per = (nb + blockDim.x - 1u) / blockDim.x;
     const uint32_t b0 = min(threadIdx.x * per, nb);
@@ -127,22 +131,50 @@ __global__ void __launch_bounds__(1024) k_pool_update(Dev d) {
     const int f0 = int(d.free_slots[0]);
     const int bx = d.brick_dim.x, by = d.brick_dim.y, bz = d.brick_dim.z;
 
-    // Phase 1: wanted = touched within one brick; unwanted bricks with storage free their slot.
-    uint32_t nfree = 0;
-    for (uint32_t b = b0; b < b1; ++b) {
-        const int3 c = brick_coord_of(d, b);
-        bool wanted = false;
-        for (int z = max(c.z - 1, 0); z <= min(c.z + 1, bz - 1) && !wanted; ++z)
-            for (int y = max(c.y - 1, 0); y <= min(c.y + 1, by - 1) && !wanted; ++y)
-                for (int x = max(c.x - 1, 0); x <= min(c.x + 1, bx - 1); ++x)
-                    if (d.brick_touch[uint32_t(x + bx * (y + by * z))] != 0u) { wanted = true; break; }
-        d.brick_want[b] = wanted ? 1u : 0u;
-        if (!wanted && d.brick_table_w[b] != 0u) ++nfree;
+    // Phase 1: wanted = touched within one brick (3x3x3 dilation); unwanted bricks free their slot.
+    if (nb <= POOL_SMEM_BRICKS) {
+        uint8_t* a = s_flags;
+        uint8_t* t = s_flags + nb;
+        for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) a[b] = d.brick_touch[b] != 0u ? 1 : 0;
+        __syncthreads();
+        for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) {  // x
+            const int x = int(b % uint32_t(bx));
+            t[b] = a[b] | (x > 0 ? a[b - 1] : 0) | (x + 1 < bx ? a[b + 1] : 0);
+        }
+        __syncthreads();
+        for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) {  // y
+            const int y = int((b / uint32_t(bx)) % uint32_t(by));
+            a[b] = t[b] | (y > 0 ? t[b - bx] : 0) | (y + 1 < by ? t[b + bx] : 0);
+        }
+        __syncthreads();
+        const uint32_t plane = uint32_t(bx * by);
+        for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) {  // z
+            const int z = int(b / plane);
+            const uint8_t w = a[b] | (z > 0 ? a[b - plane] : 0) | (z + 1 < bz ? a[b + plane] : 0);
+            t[b] = w;
+            d.brick_want[b] = w;
+        }
+        __syncthreads();
+    } else {
+        for (uint32_t b = b0; b < b1; ++b) {
+            const int3 c = brick_coord_of(d, b);
+            bool wanted = false;
+            for (int z = max(c.z - 1, 0); z <= min(c.z + 1, bz - 1) && !wanted; ++z)
+                for (int y = max(c.y - 1, 0); y <= min(c.y + 1, by - 1) && !wanted; ++y)
+                    for (int x = max(c.x - 1, 0); x <= min(c.x + 1, bx - 1); ++x)
+                        if (d.brick_touch[uint32_t(x + bx * (y + by * z))] != 0u) { wanted = true; break; }
+            d.brick_want[b] = wanted ? 1u : 0u;
+        }
+        __syncthreads();
     }
+    auto want = [&](uint32_t b) -> bool { return nb <= POOL_SMEM_BRICKS ? s_flags[nb + b] != 0 : d.brick_want[b] != 0u; };
+    uint32_t nfree = 0;
+    for (uint32_t b = b0; b < b1; ++b)
+        if (!want(b) && d.brick_table_w[b] != 0u) ++nfree;
     uint32_t total_free;
     uint32_t k = block_scan_1024(nfree, s_warp, &total_free);
     for (uint32_t b = b0; b < b1; ++b) {
-        if (d.brick_want[b] == 0u) {
+        if (!want(b)) {
             const uint32_t slot = d.brick_table_w[b];
             if (slot != 0u) {
                 d.free_slots[1u + uint32_t(f0) + k] = slot;
@@ -158,11 +190,11 @@ __global__ void __launch_bounds__(1024) k_pool_update(Dev d) {
     // Phase 2: wanted bricks without storage pop slots in brick order.
     uint32_t nneed = 0;
     for (uint32_t b = b0; b < b1; ++b)
-        if (d.brick_want[b] != 0u && d.brick_table_w[b] == 0u) ++nneed;
+        if (want(b) && d.brick_table_w[b] == 0u) ++nneed;
     uint32_t total_need;
     uint32_t j = block_scan_1024(nneed, s_warp, &total_need);
     for (uint32_t b = b0; b < b1; ++b) {
-        if (d.brick_want[b] != 0u && d.brick_table_w[b] == 0u) {
+        if (want(b) && d.brick_table_w[b] == 0u) {
             const int count = f - int(j);
             if (count > 0) {
                 const uint32_t slot = d.free_slots[count];
@@ -178,13 +210,12 @@ __global__ void __launch_bounds__(1024) k_pool_update(Dev d) {
     // Phase 3: active list in brick order; touch flags consumed.
     uint32_t nact = 0;
     for (uint32_t b = b0; b < b1; ++b)
-        if (d.brick_want[b] != 0u && d.brick_table_w[b] != 0u) ++nact;
+        if (want(b) && d.brick_table_w[b] != 0u) ++nact;
     uint32_t total_act;
     uint32_t a = block_scan_1024(nact, s_warp, &total_act);
-    for (uint32_t b = b0; b < b1; ++b) {
-        d.brick_touch[b] = 0u;
-        if (d.brick_want[b] != 0u && d.brick_table_w[b] != 0u) d.active_bricks[1u + a++] = b;
-    }
+    for (uint32_t b = b0; b < b1; ++b)
+        if (want(b) && d.brick_table_w[b] != 0u) d.active_bricks[1u + a++] = b;
+    for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) d.brick_touch[b] = 0u;
     if (threadIdx.x == 0) {
         const uint32_t ok = uint32_t(min(int(total_need), max(f, 0)));
         d.new_slots[0] = ok;
@@ -485,7 +516,13 @@ __global__ void __launch_bounds__(GRID_THREADS) k_extrapolate(Dev d, const float
 }  // namespace
 
 int launch_pool_update(const Dev& d, cudaStream_t s) {
-    k_pool_update<<<1, 1024, 0, s>>>(d);
+    const uint32_t smem = d.num_bricks <= POOL_SMEM_BRICKS ? 2u * d.num_bricks : 0u;
+    static uint32_t configured = 0;
+    if (smem > 48u * 1024u && smem > configured) {
+        cudaFuncSetAttribute(k_pool_update, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        configured = smem;
+    }
+    k_pool_update<<<1, 1024, smem, s>>>(d);
     return 1;
 }
 int launch_clear_new_slots(const Dev& d, const Shape& sh, cudaStream_t s) {

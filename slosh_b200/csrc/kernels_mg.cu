@@ -6,11 +6,19 @@
 // (:386-413), MGProlongCS (:418-433), PCGApplyACS (:438-454), PCGFinalizeDotCS (:457-492),
 // PCGUpdatePRCS (:495-524), PCGUpdateDCS (:527-543); driver SloshProxy.cpp:807-1020.
 //
-// Differences in form, not in result: the dot products are accumulated in FP64 through one fixed tree
-// (a partial per active brick, then the last CTA to finish reduces the partials in a fixed order), so
-// they are deterministic and need no separate finalize launch; alpha and beta are formed in FP64 and
-// rounded to FP32. PCGInit and PCGUpdatePR also reduce ||b||^2 and ||r||^2 for the relative-residual
-// stopping test.
+// Same arithmetic in the same order as the reference, different execution:
+//   * dot products accumulate in FP64 through one fixed tree (a partial per active brick, then the
+//     last CTA to finish reduces the partials in a fixed order): deterministic, no finalize launch;
+//     alpha and beta are formed in FP64 and rounded to FP32;
+//   * the iteration loop is controlled on the device: ctl[] holds the iteration count, its limit,
+//     the stopping mode and a done flag; PCGUpdatePR decides whether another iteration runs and, when
+//     the solve is a CUDA graph, sets the WHILE node's condition -- no host round trip per iteration;
+//   * levels 1-3 are visited through the active bricks' footprints (a brick covers (8 >> l)^3 cells
+//     of level l), not by scanning the dense level; every fluid coarse cell lies in such a footprint;
+//   * the small coarse levels (<= 4096 cells) run as one single-CTA kernel (descent, coarse solve,
+//     ascent with block barriers between passes).
+#include <algorithm>
+
 #include "kernels.h"
 
 namespace slosh {
@@ -25,9 +33,10 @@ __device__ __forceinline__ bool inside3(int3 c, int3 dim) {
     return c.x >= 0 && c.y >= 0 && c.z >= 0 && c.x < dim.x && c.y < dim.y && c.z < dim.z;
 }
 __device__ __forceinline__ bool is_red(int3 c) { return (uint32_t(c.x + c.y + c.z) & 1u) == 0u; }
+__device__ __forceinline__ bool solve_done(const MGState& m) { return *(volatile uint32_t*)(m.ctl + 3) != 0u; }
 
 // Level-0 stencil (ghost-fluid diagonal DiagF + epsilon, sum of fluid neighbours of buf).
-__device__ __forceinline__ void stencil0(const Dev& d, const float* __restrict__ buf, uint32_t i, int3 c, float& diag, float& sum) {
+__device__ __forceinline__ void stencil0(const Dev& d, const float* buf, uint32_t i, int3 c, float& diag, float& sum) {
     sum = 0.0f;
 #pragma unroll
     for (int n = 0; n < 6; ++n) {
@@ -38,7 +47,7 @@ __device__ __forceinline__ void stencil0(const Dev& d, const float* __restrict__
     diag = d.cell_diag[i] + DIAG_EPSILON;
 }
 // Dense coarse-level stencil (counted non-solid neighbours + epsilon).
-__device__ __forceinline__ void stencil_dense(const MGLevel& L, const float* __restrict__ buf, int3 c, float& diag, float& sum) {
+__device__ __forceinline__ void stencil_dense(const MGLevel& L, const float* buf, int3 c, float& diag, float& sum) {
     diag = DIAG_EPSILON;
     sum = 0.0f;
 #pragma unroll
@@ -131,7 +140,112 @@ __device__ __forceinline__ void level0_dot_pass(const Dev& d, const MGState& m, 
     }
 }
 
+// Visits the cells of level l (1..3) that lie in the active bricks' footprints: fn(ci, c). Levels
+// whose cells are coarser than a brick are scanned densely.
+template <class Fn>
+__device__ __forceinline__ void for_footprint(const Dev& d, const MGLevel& L, int l, Fn fn) {
+    if (l > 3) {
+        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < L.cells; i += gridDim.x * blockDim.x) fn(i, coord3(i, L.dim));
+        return;
+    }
+    const int side = 8 >> l;
+    const uint32_t per = uint32_t(side * side * side);
+    const uint32_t total = d.active_bricks[0] * per;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        const uint32_t e = t / per, lc = t % per;
+        const int3 bc = brick_coord_of(d, d.active_bricks[1u + e]);
+        const int3 c = make_int3(bc.x * side + int(lc % uint32_t(side)), bc.y * side + int((lc / uint32_t(side)) % uint32_t(side)),
+                                 bc.z * side + int(lc / uint32_t(side * side)));
+        if (inside3(c, L.dim)) fn(lin3(c, L.dim), c);
+    }
+}
+
+// ---- level-0 stencil words ------------------------------------------------------------------------
+// The cell types do not change during a solve, so PCGInit stores per level-0 cell one byte: bits 0-5
+// = neighbour n (-x, +x, -y, +y, -z, +z) is fluid, bit 6 = the cell is fluid, bit 7 = red, and per
+// active brick the slots of its 6 face neighbours. The level-0 passes then load only the word and
+// issue all neighbour loads at once, instead of a type -> brick table -> value chain per neighbour.
+constexpr uint32_t W_FLUID = 1u << 6, W_RED = 1u << 7;
+
+__device__ __forceinline__ uint32_t l0_nbr(uint32_t i, uint32_t l, int n, const uint32_t* ns) {
+    switch (n) {
+        case 0: return (l & 7u) ? i - 1u : ns[0] * BRICK_CELLS + l + 7u;
+        case 1: return ((l & 7u) != 7u) ? i + 1u : ns[1] * BRICK_CELLS + l - 7u;
+        case 2: return (l & 56u) ? i - 8u : ns[2] * BRICK_CELLS + l + 56u;
+        case 3: return ((l & 56u) != 56u) ? i + 8u : ns[3] * BRICK_CELLS + l - 56u;
+        case 4: return (l & 448u) ? i - 64u : ns[4] * BRICK_CELLS + l + 448u;
+        default: return ((l & 448u) != 448u) ? i + 64u : ns[5] * BRICK_CELLS + l - 448u;
+    }
+}
+// Sum of buf over the fluid neighbours, in neighbour order (non-fluid neighbours are skipped, not
+// added as zero, so the rounding is the reference's).
+__device__ __forceinline__ float l0_sum(const float* buf, uint32_t w, uint32_t i, uint32_t l, const uint32_t* ns) {
+    float v[6];
+#pragma unroll
+    for (int n = 0; n < 6; ++n) v[n] = ((w >> n) & 1u) ? buf[l0_nbr(i, l, n, ns)] : 0.0f;
+    float sum = 0.0f;
+#pragma unroll
+    for (int n = 0; n < 6; ++n)
+        if ((w >> n) & 1u) sum = sum + v[n];
+    return sum;
+}
+
+// Level-0 pass over all 512 cells of every active brick; fn(i, l, e, ns, v0, v1) handles one cell
+// (it reads the word to know whether the cell exists and is fluid). With NDOT > 0 it produces dot
+// products through the canonical tree; the last CTA calls store(t0, t1) in thread 0.
+template <int NDOT, class Fn, class Store>
+__device__ __forceinline__ void l0_pass(const Dev& d, const MGState& m, uint32_t counter, Fn fn, Store store) {
+    __shared__ DotSmem sm;
+    const uint32_t active = d.active_bricks[0];
+    const uint32_t cap = d.num_pool_bricks;
+    for (uint32_t e = blockIdx.x; e < active; e += gridDim.x) {
+        const uint32_t slot = __ldg(d.brick_table + d.active_bricks[1u + e]);
+        uint32_t ns[6];
+#pragma unroll
+        for (int n = 0; n < 6; ++n) ns[n] = m.nbr_slots[8u * e + uint32_t(n)];
+        double a0[2] = {0.0, 0.0}, a1[2] = {0.0, 0.0};
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const uint32_t l = threadIdx.x + uint32_t(k) * 256u;
+            fn(slot * BRICK_CELLS + l, l, e, ns, a0[k], a1[k]);
+        }
+        if (NDOT > 0) {
+            const double t0 = brick_reduce(a0[0] + a0[1], sm.w8);
+            if (threadIdx.x == 0) m.partials[e] = t0;
+        }
+        if (NDOT > 1) {
+            const double t1 = brick_reduce(a1[0] + a1[1], sm.w8);
+            if (threadIdx.x == 0) m.partials[cap + e] = t1;
+        }
+    }
+    if (NDOT == 0) return;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) sm.last = (atomicAdd(m.counters + counter, 1u) == gridDim.x - 1u) ? 1u : 0u;
+    __syncthreads();
+    if (sm.last) {
+        __threadfence();
+        const double r0 = final_reduce(m.partials, active, sm);
+        __syncthreads();
+        double r1 = 0.0;
+        if (NDOT > 1) r1 = final_reduce(m.partials + cap, active, sm);
+        if (threadIdx.x == 0) {
+            store(r0, r1);
+            m.counters[counter] = 0u;
+        }
+    }
+}
+
 __device__ __forceinline__ float ratio_f(double num, double den) { return fabs(den) > 1e-30 ? float(num / den) : 0.0f; }
+
+// ---- solve setup: iteration state in ctl[] --------------------------------------------------------------
+__global__ void k_solve_setup(MGState m, uint32_t limit, uint32_t tol_mode, double tol) {
+    m.ctl[0] = 0u;        // completed iterations
+    m.ctl[1] = limit;     // iteration limit
+    m.ctl[2] = tol_mode;  // 1: stop at ||r|| <= tol ||b||
+    m.ctl[3] = 0u;        // done
+    m.scalars[8] = tol;
+}
 
 // ---- MGBuildTypeCS: coarse cell = air if any child is air, else fluid if any child is fluid ---------------
 __global__ void k_build_type(Dev d, MGLevel fine, MGLevel coarse, int fine_is_pool) {
@@ -150,12 +264,43 @@ __global__ void k_build_type(Dev d, MGLevel fine, MGLevel coarse, int fine_is_po
     coarse.type[ci] = any_air ? CELL_AIR : (any_fluid ? CELL_FLUID : CELL_SOLID);
 }
 
-// ---- PCGInitCS (+ ||r0||^2 and ||b||^2) --------------------------------------------------------------
-__global__ void __launch_bounds__(GRID_THREADS) k_pcg_init(Dev d, MGState m, const float* __restrict__ p, const float* __restrict__ div) {
+// ---- PCGInitCS (+ ||r0||^2 and ||b||^2, and the decision whether any iteration runs) ----------------------
+// Also stores the solve's stencil words and the active bricks' neighbour slots.
+__global__ void __launch_bounds__(GRID_THREADS) k_pcg_init(Dev d, MGState m, const float* __restrict__ p, const float* __restrict__ div,
+                                                           unsigned long long handle) {
+    const uint32_t active = d.active_bricks[0];
+    for (uint32_t e = blockIdx.x; e < active; e += gridDim.x) {
+        const uint32_t brick = d.active_bricks[1u + e];
+        const uint32_t slot = __ldg(d.brick_table + brick);
+        const int3 bc = brick_coord_of(d, brick);
+        if (threadIdx.x < 6) {
+            const int3 nb = add3(bc, nbr_off(int(threadIdx.x)));
+            const bool in = nb.x >= 0 && nb.y >= 0 && nb.z >= 0 && nb.x < d.brick_dim.x && nb.y < d.brick_dim.y && nb.z < d.brick_dim.z;
+            m.nbr_slots[8u * e + threadIdx.x] = in ? __ldg(d.brick_table + brick_index_of(d, nb)) : 0u;
+        }
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const uint32_t l = threadIdx.x + uint32_t(k) * 256u;
+            const int3 lc = local_coord_of(l);
+            const int3 c = make_int3(bc.x * 8 + lc.x, bc.y * 8 + lc.y, bc.z * 8 + lc.z);
+            uint32_t w = 0u;
+            if (in_grid(d, c)) {
+                const uint32_t i = slot * BRICK_CELLS + l;
+                if ((d.cell_type[i] & CELL_TYPE_MASK) == CELL_FLUID) w |= W_FLUID;
+                if (is_red(c)) w |= W_RED;
+#pragma unroll
+                for (int n = 0; n < 6; ++n) {
+                    if (!in_grid(d, add3(c, nbr_off(n)))) continue;
+                    if ((d.cell_type[nbr_index(d, i, c, n)] & CELL_TYPE_MASK) == CELL_FLUID) w |= 1u << n;
+                }
+            }
+            m.word[slot * BRICK_CELLS + l] = uint8_t(w);
+        }
+    }
     level0_dot_pass<2>(d, m, 0,
         [&](uint32_t i, int3 c, double& v0, double& v1) {
             if ((d.cell_type[i] & CELL_TYPE_MASK) != CELL_FLUID) {
-                m.r[i] = 0.0f; m.z[i] = 0.0f; m.dvec[i] = 0.0f;
+                m.r[i] = 0.0f; m.z[i] = 0.0f;
                 return;
             }
             float diag, sum;
@@ -167,18 +312,28 @@ __global__ void __launch_bounds__(GRID_THREADS) k_pcg_init(Dev d, MGState m, con
             const float b = -div[i];
             v1 = double(b * b);
         },
-        [&](double rr, double bb) { m.scalars[5] = rr; m.scalars[4] = bb; });
+        [&](double rr, double bb) {
+            m.scalars[5] = rr;
+            m.scalars[4] = bb;
+            const double rel = bb > 0.0 ? sqrt(rr / bb) : 0.0;
+            const bool run = m.ctl[1] > 0u && !(m.ctl[2] != 0u && rel <= m.scalars[8]);
+            if (!run) m.ctl[3] = 1u;
+            if (handle) cudaGraphSetConditional(handle, run ? 1u : 0u);
+        });
 }
 
 // ---- MGSmoothCS on level 0 (z as x, r as b); with dot the r.z reduction shifts rho -----------------------
 __global__ void __launch_bounds__(GRID_THREADS) k_smooth0(Dev d, MGState m, uint32_t parity, int dot) {
+    if (solve_done(m)) return;
+    const uint32_t want_red = parity == 0u ? W_RED : 0u;
     if (dot) {
-        level0_dot_pass<1>(d, m, 1,
-            [&](uint32_t i, int3 c, double& v0, double&) {
-                if ((d.cell_type[i] & CELL_TYPE_MASK) != CELL_FLUID) return;
-                if ((is_red(c) ? 0u : 1u) == parity) {
-                    float diag, sum;
-                    stencil0(d, m.z, i, c, diag, sum);
+        l0_pass<1>(d, m, 1,
+            [&](uint32_t i, uint32_t l, uint32_t, const uint32_t* ns, double& v0, double&) {
+                const uint32_t w = m.word[i];
+                if (!(w & W_FLUID)) return;
+                if ((w & W_RED) == want_red) {
+                    const float sum = l0_sum(m.z, w, i, l, ns);
+                    const float diag = d.cell_diag[i] + DIAG_EPSILON;
                     const float b = m.r[i];
                     const float x = (b + sum) / diag;
                     m.z[i] = x;
@@ -190,40 +345,67 @@ __global__ void __launch_bounds__(GRID_THREADS) k_smooth0(Dev d, MGState m, uint
             [&](double rho, double) { m.scalars[3] = m.scalars[0]; m.scalars[0] = rho; });
         return;
     }
+    l0_pass<0>(d, m, 0,
+        [&](uint32_t i, uint32_t l, uint32_t, const uint32_t* ns, double&, double&) {
+            const uint32_t w = m.word[i];
+            if (!(w & W_FLUID) || (w & W_RED) != want_red) return;
+            const float sum = l0_sum(m.z, w, i, l, ns);
+            m.z[i] = (m.r[i] + sum) / (d.cell_diag[i] + DIAG_EPSILON);
+        },
+        [&](double, double) {});
+}
+
+// ---- MGProlongCS (level 1 -> 0) fused with the following black sweep ------------------------------
+// After the prolongation only the black sweep reads the prolonged values (of its red neighbours) and
+// it overwrites the black cells; the red sweep that follows overwrites the red cells. So the black
+// sweep reads z_n + x_c(parent of n) directly and nothing else needs to be written.
+__global__ void __launch_bounds__(GRID_THREADS) k_prolong_smooth0(Dev d, MGState m) {
+    if (solve_done(m)) return;
+    const MGLevel C = m.lv[1];
     const uint32_t active = d.active_bricks[0];
     for (uint32_t e = blockIdx.x; e < active; e += gridDim.x) {
         const uint32_t brick = d.active_bricks[1u + e];
         const uint32_t slot = __ldg(d.brick_table + brick);
         const int3 bc = brick_coord_of(d, brick);
+        uint32_t ns[6];
+#pragma unroll
+        for (int n = 0; n < 6; ++n) ns[n] = m.nbr_slots[8u * e + uint32_t(n)];
 #pragma unroll
         for (int k = 0; k < 2; ++k) {
             const uint32_t l = threadIdx.x + uint32_t(k) * 256u;
+            const uint32_t i = slot * BRICK_CELLS + l;
+            const uint32_t w = m.word[i];
+            if (!(w & W_FLUID) || (w & W_RED)) continue;
             const int3 lc = local_coord_of(l);
             const int3 c = make_int3(bc.x * 8 + lc.x, bc.y * 8 + lc.y, bc.z * 8 + lc.z);
-            if (!in_grid(d, c) || (is_red(c) ? 0u : 1u) != parity) continue;
-            const uint32_t i = slot * BRICK_CELLS + l;
-            if ((d.cell_type[i] & CELL_TYPE_MASK) != CELL_FLUID) continue;
-            float diag, sum;
-            stencil0(d, m.z, i, c, diag, sum);
-            m.z[i] = (m.r[i] + sum) / diag;
+            float v[6];
+#pragma unroll
+            for (int n = 0; n < 6; ++n) {
+                v[n] = 0.0f;
+                if (!((w >> n) & 1u)) continue;
+                const int3 nb = add3(c, nbr_off(n));
+                const uint32_t pi = lin3(make_int3(nb.x / 2, nb.y / 2, nb.z / 2), C.dim);
+                const float zn = m.z[l0_nbr(i, l, n, ns)];
+                v[n] = (C.type[pi] & CELL_TYPE_MASK) == CELL_FLUID ? zn + C.x[pi] : zn;
+            }
+            float sum = 0.0f;
+#pragma unroll
+            for (int n = 0; n < 6; ++n)
+                if ((w >> n) & 1u) sum = sum + v[n];
+            m.z[i] = (m.r[i] + sum) / (d.cell_diag[i] + DIAG_EPSILON);
         }
     }
 }
 
-// ---- MGSmoothCS on a dense level -------------------------------------------------------------------------
-__global__ void k_smooth_dense(MGLevel L, uint32_t parity) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= L.cells) return;
+// ---- dense-level passes, usable by a grid of CTAs (stride = all threads) or by one CTA -------------------
+__device__ __forceinline__ void smooth_cell(const MGLevel& L, uint32_t i, int3 c, uint32_t parity) {
     if ((L.type[i] & CELL_TYPE_MASK) != CELL_FLUID) return;
-    const int3 c = coord3(i, L.dim);
     if ((is_red(c) ? 0u : 1u) != parity) return;
     float diag, sum;
     stencil_dense(L, L.x, c, diag, sum);
     L.x[i] = (L.b[i] + sum) / diag;
 }
-
-// ---- MGRestrictCS -----------------------------------------------------------------------------------
-__device__ __forceinline__ void restrict_store(MGLevel& C, uint32_t ci, int3 c, float sum) {
+__device__ __forceinline__ void restrict_store(const MGLevel& C, uint32_t ci, int3 c, float sum) {
     const float b = 0.25f * sum;
     C.b[ci] = b;
     float cdiag = DIAG_EPSILON;
@@ -235,37 +417,7 @@ __device__ __forceinline__ void restrict_store(MGLevel& C, uint32_t ci, int3 c, 
     }
     C.x[ci] = is_red(c) ? b / cdiag : 0.0f;
 }
-// Level 0 -> 1 over the 4^3 level-1 cells of every active brick (SparseCoarse).
-__global__ void k_restrict0(Dev d, MGState m) {
-    MGLevel C = m.lv[1];
-    const uint32_t active = d.active_bricks[0];
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < active * 64u; t += gridDim.x * blockDim.x) {
-        const uint32_t e = t >> 6, lc = t & 63u;
-        const uint32_t brick = d.active_bricks[1u + e];
-        const int3 bc = brick_coord_of(d, brick);
-        const int3 c = make_int3(bc.x * 4 + int(lc & 3u), bc.y * 4 + int((lc >> 2) & 3u), bc.z * 4 + int(lc >> 4));
-        if (!inside3(c, C.dim)) continue;
-        const uint32_t ci = lin3(c, C.dim);
-        if ((C.type[ci] & CELL_TYPE_MASK) != CELL_FLUID) { C.b[ci] = 0.0f; C.x[ci] = 0.0f; continue; }
-        const uint32_t slot = __ldg(d.brick_table + brick);
-        float sum = 0.0f;
-#pragma unroll
-        for (int o = 0; o < 8; ++o) {
-            const int3 f = make_int3(c.x * 2 + (o & 1), c.y * 2 + ((o >> 1) & 1), c.z * 2 + ((o >> 2) & 1));
-            if (!in_grid(d, f)) continue;
-            const uint32_t fi = slot * BRICK_CELLS + local_index_of(f);
-            if ((d.cell_type[fi] & CELL_TYPE_MASK) != CELL_FLUID) continue;
-            float diag, nbsum;
-            stencil0(d, m.z, fi, f, diag, nbsum);
-            sum = sum + (m.r[fi] - (diag * m.z[fi] - nbsum));
-        }
-        restrict_store(C, ci, c, sum);
-    }
-}
-__global__ void k_restrict_dense(MGLevel F, MGLevel C) {
-    const uint32_t ci = blockIdx.x * blockDim.x + threadIdx.x;
-    if (ci >= C.cells) return;
-    const int3 c = coord3(ci, C.dim);
+__device__ __forceinline__ void restrict_cell(const MGLevel& F, const MGLevel& C, uint32_t ci, int3 c) {
     if ((C.type[ci] & CELL_TYPE_MASK) != CELL_FLUID) { C.b[ci] = 0.0f; C.x[ci] = 0.0f; return; }
     float sum = 0.0f;
 #pragma unroll
@@ -281,114 +433,287 @@ __global__ void k_restrict_dense(MGLevel F, MGLevel C) {
     restrict_store(C, ci, c, sum);
 }
 
-// ---- MGCoarseSolveCS: red-black sweeps inside one CTA ------------------------------------------------------
-__global__ void __launch_bounds__(1024) k_coarse_solve(Dev d, MGState m, int level, int iterations) {
-    const bool pool = level == 0;
-    const MGLevel L = m.lv[level];
-    float* x = pool ? m.z : L.x;
-    const float* b = pool ? m.r : L.b;
+// Levels 1..3 through the active-brick footprints.
+__global__ void k_smooth_fp(Dev d, MGState m, int l, uint32_t parity) {
+    if (solve_done(m)) return;
+    const MGLevel L = m.lv[l];
+    for_footprint(d, L, l, [&](uint32_t i, int3 c) { smooth_cell(L, i, c, parity); });
+}
+__global__ void k_restrict_fp(Dev d, MGState m, int l) {  // level l -> l + 1, over level l + 1's footprint
+    if (solve_done(m)) return;
+    const MGLevel F = m.lv[l], C = m.lv[l + 1];
+    for_footprint(d, C, l + 1, [&](uint32_t ci, int3 c) { restrict_cell(F, C, ci, c); });
+}
+// Prolongation l + 1 -> l fused with the black sweep of level l (see k_prolong_smooth0).
+__global__ void k_prolong_smooth_fp(Dev d, MGState m, int l) {
+    if (solve_done(m)) return;
+    const MGLevel F = m.lv[l], C = m.lv[l + 1];
+    for_footprint(d, F, l, [&](uint32_t i, int3 c) {
+        if ((F.type[i] & CELL_TYPE_MASK) != CELL_FLUID || is_red(c)) return;
+        float diag = DIAG_EPSILON, sum = 0.0f;
+#pragma unroll
+        for (int n = 0; n < 6; ++n) {
+            const int3 nb = add3(c, nbr_off(n));
+            if (!inside3(nb, F.dim)) continue;
+            const uint32_t ni = lin3(nb, F.dim);
+            const uint32_t t = F.type[ni] & CELL_TYPE_MASK;
+            if (t != CELL_SOLID) diag = diag + 1.0f;
+            if (t == CELL_FLUID) {
+                const uint32_t pi = lin3(make_int3(nb.x / 2, nb.y / 2, nb.z / 2), C.dim);
+                const float xn = F.x[ni];
+                sum = sum + ((C.type[pi] & CELL_TYPE_MASK) == CELL_FLUID ? xn + C.x[pi] : xn);
+            }
+        }
+        F.x[i] = (F.b[i] + sum) / diag;
+    });
+}
+
+// ---- MGRestrictCS level 0 -> 1 over the 4^3 level-1 cells of every active brick (SparseCoarse) -----------
+// A brick pass: each thread forms the fine residual of its 2 cells in shared memory, then 64 threads sum
+// each coarse cell's fluid children in child order (x fastest), as the per-coarse-cell loop does.
+__global__ void __launch_bounds__(GRID_THREADS) k_restrict0(Dev d, MGState m) {
+    if (solve_done(m)) return;
+    __shared__ float s_res[BRICK_CELLS];
+    __shared__ uint8_t s_fluid[BRICK_CELLS];
+    const MGLevel C = m.lv[1];
+    const uint32_t active = d.active_bricks[0];
+    for (uint32_t e = blockIdx.x; e < active; e += gridDim.x) {
+        const uint32_t brick = d.active_bricks[1u + e];
+        const uint32_t slot = __ldg(d.brick_table + brick);
+        uint32_t ns[6];
+#pragma unroll
+        for (int n = 0; n < 6; ++n) ns[n] = m.nbr_slots[8u * e + uint32_t(n)];
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const uint32_t l = threadIdx.x + uint32_t(k) * 256u;
+            const uint32_t i = slot * BRICK_CELLS + l;
+            const uint32_t w = m.word[i];
+            s_fluid[l] = (w & W_FLUID) ? 1 : 0;
+            if (w & W_FLUID) {
+                const float nbsum = l0_sum(m.z, w, i, l, ns);
+                const float diag = d.cell_diag[i] + DIAG_EPSILON;
+                s_res[l] = m.r[i] - (diag * m.z[i] - nbsum);
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x < 64) {
+            const int3 bc = brick_coord_of(d, brick);
+            const uint32_t lc = threadIdx.x;
+            const int3 cl = make_int3(int(lc & 3u), int((lc >> 2) & 3u), int(lc >> 4));
+            const int3 c = make_int3(bc.x * 4 + cl.x, bc.y * 4 + cl.y, bc.z * 4 + cl.z);
+            if (inside3(c, C.dim)) {
+                const uint32_t ci = lin3(c, C.dim);
+                if ((C.type[ci] & CELL_TYPE_MASK) != CELL_FLUID) {
+                    C.b[ci] = 0.0f;
+                    C.x[ci] = 0.0f;
+                } else {
+                    float sum = 0.0f;
+#pragma unroll
+                    for (int o = 0; o < 8; ++o) {
+                        const uint32_t fl = uint32_t((2 * cl.x + (o & 1)) + 8 * ((2 * cl.y + ((o >> 1) & 1)) + 8 * (2 * cl.z + ((o >> 2) & 1))));
+                        if (s_fluid[fl]) sum = sum + s_res[fl];
+                    }
+                    restrict_store(C, ci, c, sum);
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ---- the small coarse levels in one CTA: levels tail..nl-1 of the V-cycle --------------------------------
+// On entry level `tail` holds b and the red-initialised x from the restriction that produced it. The
+// levels are copied into shared memory (type byte, x, b per cell), the descent, the coarse solve and
+// the ascent run there with block barriers between passes, and level tail's x is written back.
+struct SLevel {
+    int3 dim;
+    uint32_t cells;
+    uint8_t* type;
+    float* x;
+    float* b;
+};
+__device__ __forceinline__ void s_stencil(const SLevel& L, int3 c, float& diag, float& sum) {
+    diag = DIAG_EPSILON;
+    sum = 0.0f;
+#pragma unroll
+    for (int n = 0; n < 6; ++n) {
+        const int3 nb = add3(c, nbr_off(n));
+        if (!inside3(nb, L.dim)) continue;
+        const uint32_t ni = lin3(nb, L.dim);
+        const uint32_t t = L.type[ni];
+        if (t != CELL_SOLID) diag = diag + 1.0f;
+        if (t == CELL_FLUID) sum = sum + L.x[ni];
+    }
+}
+__device__ void s_smooth(const SLevel& L, uint32_t parity) {
+    for (uint32_t i = threadIdx.x; i < L.cells; i += blockDim.x) {
+        if (L.type[i] != CELL_FLUID) continue;
+        const int3 c = coord3(i, L.dim);
+        if ((is_red(c) ? 0u : 1u) != parity) continue;
+        float diag, sum;
+        s_stencil(L, c, diag, sum);
+        L.x[i] = (L.b[i] + sum) / diag;
+    }
+    __syncthreads();
+}
+__global__ void __launch_bounds__(1024) k_vcycle_tail(MGState m, int tail, int iterations) {
+    if (solve_done(m)) return;
+    extern __shared__ unsigned char s_tail[];
+    const int nl = m.num_levels;
+    SLevel S[SLOSH_MAX_MG_LEVELS];
+    size_t off = 0;
+    for (int l = tail; l < nl; ++l) {
+        S[l].dim = m.lv[l].dim;
+        S[l].cells = m.lv[l].cells;
+        S[l].x = reinterpret_cast<float*>(s_tail + off);
+        off += size_t(S[l].cells) * 4;
+        S[l].b = reinterpret_cast<float*>(s_tail + off);
+        off += size_t(S[l].cells) * 4;
+        S[l].type = s_tail + off;
+        off += (size_t(S[l].cells) + 15) & ~size_t(15);
+        for (uint32_t i = threadIdx.x; i < S[l].cells; i += blockDim.x) S[l].type[i] = uint8_t(m.lv[l].type[i] & CELL_TYPE_MASK);
+    }
+    for (uint32_t i = threadIdx.x; i < S[tail].cells; i += blockDim.x) {
+        S[tail].x[i] = m.lv[tail].x[i];
+        S[tail].b[i] = m.lv[tail].b[i];
+    }
+    __syncthreads();
+    if (tail < nl - 1) s_smooth(S[tail], 1u);
+    for (int l = tail; l < nl - 1; ++l) {
+        const SLevel F = S[l], C = S[l + 1];
+        for (uint32_t ci = threadIdx.x; ci < C.cells; ci += blockDim.x) {
+            const int3 c = coord3(ci, C.dim);
+            if (C.type[ci] != CELL_FLUID) { C.b[ci] = 0.0f; C.x[ci] = 0.0f; continue; }
+            float sum = 0.0f;
+#pragma unroll
+            for (int o = 0; o < 8; ++o) {
+                const int3 f = make_int3(c.x * 2 + (o & 1), c.y * 2 + ((o >> 1) & 1), c.z * 2 + ((o >> 2) & 1));
+                if (!inside3(f, F.dim)) continue;
+                const uint32_t fi = lin3(f, F.dim);
+                if (F.type[fi] != CELL_FLUID) continue;
+                float diag, nbsum;
+                s_stencil(F, f, diag, nbsum);
+                sum = sum + (F.b[fi] - (diag * F.x[fi] - nbsum));
+            }
+            const float bb = 0.25f * sum;
+            C.b[ci] = bb;
+            float cdiag = DIAG_EPSILON;
+#pragma unroll
+            for (int n = 0; n < 6; ++n) {
+                const int3 nb = add3(c, nbr_off(n));
+                const uint32_t t = inside3(nb, C.dim) ? uint32_t(C.type[lin3(nb, C.dim)]) : CELL_SOLID;
+                cdiag = cdiag + (t != CELL_SOLID ? 1.0f : 0.0f);
+            }
+            C.x[ci] = is_red(c) ? bb / cdiag : 0.0f;
+        }
+        __syncthreads();
+        if (l + 1 < nl - 1) s_smooth(C, 1u);
+    }
+    for (int it = 0; it < iterations; ++it) {
+        s_smooth(S[nl - 1], 0u);
+        s_smooth(S[nl - 1], 1u);
+    }
+    for (int l = nl - 2; l >= tail; --l) {
+        const SLevel F = S[l], C = S[l + 1];
+        for (uint32_t i = threadIdx.x; i < F.cells; i += blockDim.x) {
+            if (F.type[i] != CELL_FLUID) continue;
+            const int3 c = coord3(i, F.dim);
+            const uint32_t pi = lin3(make_int3(c.x / 2, c.y / 2, c.z / 2), C.dim);
+            if (C.type[pi] == CELL_FLUID) F.x[i] = F.x[i] + C.x[pi];
+        }
+        __syncthreads();
+        s_smooth(F, 1u);
+        s_smooth(F, 0u);
+    }
+    for (uint32_t i = threadIdx.x; i < S[tail].cells; i += blockDim.x) m.lv[tail].x[i] = S[tail].x[i];
+}
+
+// ---- the coarse solve directly on level 0 (grids of <= 512 cells have a single level) --------------------
+__global__ void __launch_bounds__(1024) k_coarse_solve0(Dev d, MGState m, int iterations) {
+    if (solve_done(m)) return;
+    const MGLevel L = m.lv[0];
     for (int it = 0; it < iterations; ++it) {
         for (uint32_t colour = 0; colour < 2u; ++colour) {
             for (uint32_t li = threadIdx.x; li < L.cells; li += blockDim.x) {
                 const int3 c = coord3(li, L.dim);
                 if ((is_red(c) ? 0u : 1u) != colour) continue;
-                if (pool) {
-                    const uint32_t i = cell_index(d, c);
-                    if ((d.cell_type[i] & CELL_TYPE_MASK) != CELL_FLUID) continue;
-                    float diag, sum;
-                    stencil0(d, x, i, c, diag, sum);
-                    x[i] = (b[i] + sum) / diag;
-                } else {
-                    if ((L.type[li] & CELL_TYPE_MASK) != CELL_FLUID) continue;
-                    float diag, sum;
-                    stencil_dense(L, x, c, diag, sum);
-                    x[li] = (b[li] + sum) / diag;
-                }
+                const uint32_t i = cell_index(d, c);
+                if ((d.cell_type[i] & CELL_TYPE_MASK) != CELL_FLUID) continue;
+                float diag, sum;
+                stencil0(d, m.z, i, c, diag, sum);
+                m.z[i] = (m.r[i] + sum) / diag;
             }
             __syncthreads();
         }
     }
 }
 
-// ---- MGProlongCS: x_f += x_c(parent) on fluid cells whose parent is fluid ------------------------------------
-__global__ void __launch_bounds__(GRID_THREADS) k_prolong0(Dev d, MGState m) {
-    const MGLevel C = m.lv[1];
-    const uint32_t active = d.active_bricks[0];
-    for (uint32_t e = blockIdx.x; e < active; e += gridDim.x) {
-        const uint32_t brick = d.active_bricks[1u + e];
-        const uint32_t slot = __ldg(d.brick_table + brick);
-        const int3 bc = brick_coord_of(d, brick);
-#pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            const uint32_t l = threadIdx.x + uint32_t(k) * 256u;
-            const int3 lc = local_coord_of(l);
-            const int3 c = make_int3(bc.x * 8 + lc.x, bc.y * 8 + lc.y, bc.z * 8 + lc.z);
-            if (!in_grid(d, c)) continue;
-            const uint32_t i = slot * BRICK_CELLS + l;
-            if ((d.cell_type[i] & CELL_TYPE_MASK) != CELL_FLUID) continue;
-            const uint32_t pi = lin3(make_int3(c.x / 2, c.y / 2, c.z / 2), C.dim);
-            if ((C.type[pi] & CELL_TYPE_MASK) == CELL_FLUID) m.z[i] = m.z[i] + C.x[pi];
-        }
-    }
-}
-__global__ void k_prolong_dense(MGLevel F, MGLevel C) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= F.cells) return;
-    if ((F.type[i] & CELL_TYPE_MASK) != CELL_FLUID) return;
-    const int3 c = coord3(i, F.dim);
-    const uint32_t pi = lin3(make_int3(c.x / 2, c.y / 2, c.z / 2), C.dim);
-    if ((C.type[pi] & CELL_TYPE_MASK) == CELL_FLUID) F.x[i] = F.x[i] + C.x[pi];
-}
+// ---- PCGUpdateDCS fused into PCGApplyACS: d = z + beta d, q = A d, d.q ------------------------------------
+// d is double-buffered by iteration parity (ctl[0] is the number of finished iterations): the pass reads
+// the previous direction from one buffer and writes the new one to the other, and forms each fluid
+// neighbour's new direction z_n + beta d_n itself (bit-identical to what that neighbour writes).
+__device__ __forceinline__ float* dir_buf(const MGState& m, uint32_t parity) { return parity ? m.dvec2 : m.dvec; }
 
-// ---- PCGApplyACS: q = A d, d.q --------------------------------------------------------------------------
 __global__ void __launch_bounds__(GRID_THREADS) k_apply_a(Dev d, MGState m) {
-    level0_dot_pass<1>(d, m, 2,
-        [&](uint32_t i, int3 c, double& v0, double&) {
-            if ((d.cell_type[i] & CELL_TYPE_MASK) != CELL_FLUID) return;
-            float diag, sum;
-            stencil0(d, m.dvec, i, c, diag, sum);
-            const float qi = diag * m.dvec[i] - sum;
+    if (solve_done(m)) return;
+    const uint32_t it = m.ctl[0];
+    const bool first = it == 0u;
+    const float beta = first ? 0.0f : ratio_f(m.scalars[0], m.scalars[3]);
+    const float* dold = dir_buf(m, it & 1u);
+    float* dnew = dir_buf(m, (it + 1u) & 1u);
+    l0_pass<1>(d, m, 2,
+        [&](uint32_t i, uint32_t l, uint32_t, const uint32_t* ns, double& v0, double&) {
+            const uint32_t w = m.word[i];
+            if (!(w & W_FLUID)) return;
+            const float dn = first ? m.z[i] : m.z[i] + beta * dold[i];
+            dnew[i] = dn;
+            float v[6];
+#pragma unroll
+            for (int n = 0; n < 6; ++n) {
+                v[n] = 0.0f;
+                if (!((w >> n) & 1u)) continue;
+                const uint32_t ni = l0_nbr(i, l, n, ns);
+                v[n] = first ? m.z[ni] : m.z[ni] + beta * dold[ni];
+            }
+            float sum = 0.0f;
+#pragma unroll
+            for (int n = 0; n < 6; ++n)
+                if ((w >> n) & 1u) sum = sum + v[n];
+            const float qi = (d.cell_diag[i] + DIAG_EPSILON) * dn - sum;
             m.q[i] = qi;
-            v0 = double(m.dvec[i] * qi);
+            v0 = double(dn * qi);
         },
         [&](double dq, double) { m.scalars[2] = dq; });
 }
 
-// ---- PCGUpdatePRCS: p += alpha d, r -= alpha q, red pre-smooth; ||r||^2 ----------------------------------------
-__global__ void __launch_bounds__(GRID_THREADS) k_update_pr(Dev d, MGState m, float* __restrict__ p) {
+// ---- PCGUpdatePRCS: p += alpha d, r -= alpha q, red pre-smooth; ||r||^2 and the loop decision -------------
+__global__ void __launch_bounds__(GRID_THREADS) k_update_pr(Dev d, MGState m, float* __restrict__ p, unsigned long long handle) {
+    if (solve_done(m)) return;
     const float alpha = ratio_f(m.scalars[0], m.scalars[2]);
-    level0_dot_pass<1>(d, m, 3,
-        [&](uint32_t i, int3 c, double& v0, double&) {
-            if ((d.cell_type[i] & CELL_TYPE_MASK) != CELL_FLUID) return;
-            p[i] = p[i] + alpha * m.dvec[i];
+    const float* dcur = dir_buf(m, (m.ctl[0] + 1u) & 1u);
+    l0_pass<1>(d, m, 3,
+        [&](uint32_t i, uint32_t, uint32_t, const uint32_t*, double& v0, double&) {
+            const uint32_t w = m.word[i];
+            if (!(w & W_FLUID)) return;
+            p[i] = p[i] + alpha * dcur[i];
             const float ri = m.r[i] - alpha * m.q[i];
             m.r[i] = ri;
             const float diag = d.cell_diag[i] + DIAG_EPSILON;
-            m.z[i] = is_red(c) ? ri / diag : 0.0f;
+            m.z[i] = (w & W_RED) ? ri / diag : 0.0f;
             v0 = double(ri * ri);
         },
-        [&](double rr, double) { m.scalars[5] = rr; });
-}
-
-// ---- PCGUpdateDCS: d = z + beta d ----------------------------------------------------------------------
-__global__ void __launch_bounds__(GRID_THREADS) k_update_d(Dev d, MGState m, int first) {
-    const float beta = first ? 0.0f : ratio_f(m.scalars[0], m.scalars[3]);
-    const uint32_t active = d.active_bricks[0];
-    for (uint32_t e = blockIdx.x; e < active; e += gridDim.x) {
-        const uint32_t brick = d.active_bricks[1u + e];
-        const uint32_t slot = __ldg(d.brick_table + brick);
-        const int3 bc = brick_coord_of(d, brick);
-#pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            const uint32_t l = threadIdx.x + uint32_t(k) * 256u;
-            const int3 lc = local_coord_of(l);
-            const int3 c = make_int3(bc.x * 8 + lc.x, bc.y * 8 + lc.y, bc.z * 8 + lc.z);
-            if (!in_grid(d, c)) continue;
-            const uint32_t i = slot * BRICK_CELLS + l;
-            if ((d.cell_type[i] & CELL_TYPE_MASK) != CELL_FLUID) continue;
-            m.dvec[i] = m.z[i] + beta * m.dvec[i];
-        }
-    }
+        [&](double rr, double) {
+            m.scalars[5] = rr;
+            const uint32_t it = m.ctl[0] + 1u;
+            m.ctl[0] = it;
+            const double bb = m.scalars[4];
+            const double rel = bb > 0.0 ? sqrt(rr / bb) : 0.0;
+            const bool converged = m.ctl[2] != 0u && rel <= m.scalars[8];
+            const bool more = it < m.ctl[1] && !converged;
+            if (!more) m.ctl[3] = 1u;
+            if (!more && m.ctl[2] != 0u && !converged) m.ctl[4] = 1u;  // stopped at the limit: sticky for the frame
+            if (handle) cudaGraphSetConditional(handle, more ? 1u : 0u);
+        });
 }
 
 // ---- ||b - A p||^2 and ||b||^2 of a finished solve (diagnostic) ---------------------------------------------
@@ -411,59 +736,93 @@ inline int blocks_for(uint32_t n, int threads) { return int((n + uint32_t(thread
 
 }  // namespace
 
+int mg_tail_level(const MGState& m) {
+    int t = m.num_levels - 1;
+    while (t - 1 >= 1 && m.lv[t - 1].cells <= 4096u) --t;
+    return t;
+}
+
+int launch_mg_setup(const MGState& m, uint32_t limit, bool tol_mode, double tol, cudaStream_t s) {
+    static size_t configured = 0;
+    const size_t smem = mg_tail_smem(m);
+    if (smem > 48u * 1024u && smem > configured) {
+        cudaFuncSetAttribute(k_vcycle_tail, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        configured = smem;
+    }
+    k_solve_setup<<<1, 1, 0, s>>>(m, limit, tol_mode ? 1u : 0u, tol);
+    return 1;
+}
 int launch_mg_build_type(const Dev& d, const MGState& m, int l, cudaStream_t s) {
     const MGLevel& C = m.lv[l + 1];
     k_build_type<<<blocks_for(C.cells, 256), 256, 0, s>>>(d, m.lv[l], C, l == 0 ? 1 : 0);
     return 1;
 }
-int launch_pcg_init(const Dev& d, const MGState& m, const float* p, const float* div, const Shape& sh, cudaStream_t s) {
-    k_pcg_init<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, m, p, div);
+int launch_pcg_init(const Dev& d, const MGState& m, const float* p, const float* div, unsigned long long handle, const Shape& sh,
+                    cudaStream_t s) {
+    k_pcg_init<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, m, p, div, handle);
     return 1;
 }
-int launch_mg_smooth(const Dev& d, const MGState& m, int l, uint32_t parity, bool dot, const Shape& sh, cudaStream_t s) {
-    if (l == 0) {
-        k_smooth0<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, m, parity, dot ? 1 : 0);
-    } else {
-        k_smooth_dense<<<blocks_for(m.lv[l].cells, 256), 256, 0, s>>>(m.lv[l], parity);
+
+size_t mg_tail_smem(const MGState& m) {
+    const int tail = mg_tail_level(m);
+    size_t off = 0;
+    for (int l = tail; l < m.num_levels; ++l) off += size_t(m.lv[l].cells) * 8 + ((size_t(m.lv[l].cells) + 15) & ~size_t(15));
+    return off;
+}
+
+// One V-cycle (SloshProxy.cpp:904-959), leaving rho = r.z in scalars[0] (previous rho in scalars[3]).
+int launch_vcycle(const Dev& d, const MGState& m, int coarse_iterations, const Shape& sh, cudaStream_t s) {
+    const int nl = m.num_levels;
+    if (nl == 1) {
+        k_coarse_solve0<<<1, 1024, 0, s>>>(d, m, coarse_iterations);
+        k_smooth0<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, m, 0u, 1);
+        return 2;
     }
-    return 1;
-}
-int launch_mg_restrict(const Dev& d, const MGState& m, int l, const Shape& sh, cudaStream_t s) {
-    if (l == 0) {
-        k_restrict0<<<sh.brick_ctas, 256, 0, s>>>(d, m);
-    } else {
-        k_restrict_dense<<<blocks_for(m.lv[l + 1].cells, 256), 256, 0, s>>>(m.lv[l], m.lv[l + 1]);
+    const int tail = mg_tail_level(m);
+    // Footprint grids sized to the most cells a level can have in the pool's bricks.
+    auto fp_blocks = [&](int l) {
+        const uint32_t side = l <= 3 ? uint32_t(8 >> l) : 1u;
+        const uint64_t cells = l <= 3 ? uint64_t(d.num_pool_bricks - 1u) * side * side * side : uint64_t(m.lv[l].cells);
+        return int(std::max<uint64_t>(1, std::min<uint64_t>(uint64_t(sh.brick_ctas), (cells + 255u) / 256u)));
+    };
+    int n = 0;
+    k_smooth0<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, m, 1u, 0);
+    ++n;
+    for (int l = 0; l < tail; ++l) {
+        if (l == 0) k_restrict0<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, m);
+        else k_restrict_fp<<<fp_blocks(l + 1), 256, 0, s>>>(d, m, l);
+        ++n;
+        if (l + 1 < tail) {  // the tail kernel does its own first smoothing sweep
+            k_smooth_fp<<<fp_blocks(l + 1), 256, 0, s>>>(d, m, l + 1, 1u);
+            ++n;
+        }
     }
-    return 1;
-}
-int launch_mg_coarse_solve(const Dev& d, const MGState& m, int l, int iterations, cudaStream_t s) {
-    k_coarse_solve<<<1, 1024, 0, s>>>(d, m, l, iterations);
-    return 1;
-}
-int launch_mg_prolong(const Dev& d, const MGState& m, int l, const Shape& sh, cudaStream_t s) {
-    if (l == 0) {
-        k_prolong0<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, m);
-    } else {
-        k_prolong_dense<<<blocks_for(m.lv[l].cells, 256), 256, 0, s>>>(m.lv[l], m.lv[l + 1]);
+    k_vcycle_tail<<<1, 1024, mg_tail_smem(m), s>>>(m, tail, coarse_iterations);
+    ++n;
+    for (int l = tail - 1; l >= 0; --l) {
+        if (l == 0) {
+            k_prolong_smooth0<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, m);
+            k_smooth0<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, m, 0u, 1);
+        } else {
+            k_prolong_smooth_fp<<<fp_blocks(l), 256, 0, s>>>(d, m, l);
+            k_smooth_fp<<<fp_blocks(l), 256, 0, s>>>(d, m, l, 0u);
+        }
+        n += 2;
     }
-    return 1;
+    return n;
 }
 int launch_pcg_apply_a(const Dev& d, const MGState& m, const Shape& sh, cudaStream_t s) {
     k_apply_a<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, m);
     return 1;
 }
-int launch_pcg_update_pr(const Dev& d, const MGState& m, float* p, const Shape& sh, cudaStream_t s) {
-    k_update_pr<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, m, p);
+int launch_pcg_update_pr(const Dev& d, const MGState& m, float* p, unsigned long long handle, const Shape& sh, cudaStream_t s) {
+    k_update_pr<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, m, p, handle);
     return 1;
 }
-int launch_pcg_update_d(const Dev& d, const MGState& m, bool first, const Shape& sh, cudaStream_t s) {
-    k_update_d<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, m, first ? 1 : 0);
-    return 1;
-}
+int launch_pcg_update_d(const Dev&, const MGState&, const Shape&, cudaStream_t) { return 0; }  // fused into ApplyA
 int launch_true_residual(const Dev& d, const MGState& m, const float* p, const float* div, const Shape& sh, cudaStream_t s) {
     k_true_residual<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, m, p, div);
     return 1;
 }
-int launch_shift_rho(const MGState&, cudaStream_t) { return 0; }
 
 }  // namespace slosh

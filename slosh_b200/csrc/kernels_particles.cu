@@ -98,49 +98,50 @@ __global__ void k_touch(Dev d, const slosh_particle_t* __restrict__ particles, u
 }
 
 // ---- P2G --------------------------------------------------------------------------------------------------
-// One CTA takes 256 consecutive (spatially sorted) particles, finds the bounding box of their cells and,
-// when the box plus its one-node halo fits, accumulates the 6 fixed-point quantities (momentum and weight
-// of the three MAC components) and the per-cell counts in shared memory with integer atomics; it then
-// adds each non-zero tile entry to global memory once. A CTA whose box does not fit adds directly to
-// global memory. Integer sums make both paths give identical results.
+// One CTA takes P2G_CHUNK consecutive (spatially sorted) particles; thread t takes the run of
+// P2G_PER_THREAD particles starting at t * P2G_PER_THREAD, so at any instant the 32 lanes of a warp
+// scatter into different cells (consecutive sorted particles share cells; a lane-strided assignment
+// would make whole warps hit the same shared-memory words). The CTA finds the bounding box of its
+// particles' cells and, when the box plus its one-node halo fits, accumulates the 6 fixed-point
+// quantities (momentum and weight of the three MAC components) and the per-cell counts in shared
+// memory with integer atomics, then adds each non-zero tile entry to global memory once. A CTA whose
+// box does not fit adds directly to global memory. Integer sums make both paths identical.
 constexpr int P2G_THREADS = 256;
+constexpr int P2G_PER_THREAD = 4;
+constexpr int P2G_CHUNK = P2G_THREADS * P2G_PER_THREAD;
 constexpr int P2G_TILE_NODES = 2048;  // nodes per quantity (6 quantities) = 48 KB
 constexpr int P2G_TILE_CELLS = 1024;  // counted cells = 4 KB
+
+__device__ __forceinline__ int3 p2g_cell(const Dev& d, float3 pos) {
+    return make_int3(clampi(int(floorf(pos.x * d.inv_h)), 0, d.grid.x - 1), clampi(int(floorf(pos.y * d.inv_h)), 0, d.grid.y - 1),
+                     clampi(int(floorf(pos.z * d.inv_h)), 0, d.grid.z - 1));
+}
 
 __global__ void __launch_bounds__(P2G_THREADS) k_p2g(Dev d, Pass p, const slosh_particle_t* __restrict__ particles, uint32_t n) {
     extern __shared__ int smem[];
     int* tile = smem;                          // [6][P2G_TILE_NODES]
     int* ctile = smem + 6 * P2G_TILE_NODES;    // [P2G_TILE_CELLS]
     __shared__ int s_box[6];
-    const uint32_t i = blockIdx.x * P2G_THREADS + threadIdx.x;
+    const uint32_t first = blockIdx.x * uint32_t(P2G_CHUNK) + threadIdx.x * uint32_t(P2G_PER_THREAD);
     if (threadIdx.x < 3) { s_box[threadIdx.x] = 0x7FFFFFFF; s_box[3 + threadIdx.x] = -0x7FFFFFFF; }
-
-    bool valid = i < n;
-    ParticleF part;
-    if (valid) {
-        float4 a, b;
-        uint4 c;
-        load_particle_raw(particles, i, a, b, c);
-        part = unpack_particle(a, b, c);
-        valid = !is_dead_age(part.age);
-    }
-    int3 cell = make_int3(0, 0, 0);
-    if (valid)
-        cell = make_int3(clampi(int(floorf(part.pos.x * d.inv_h)), 0, d.grid.x - 1),
-                         clampi(int(floorf(part.pos.y * d.inv_h)), 0, d.grid.y - 1),
-                         clampi(int(floorf(part.pos.z * d.inv_h)), 0, d.grid.z - 1));
     __syncthreads();
     {
         const int big = 0x7FFFFFFF;
-        const int mnx = __reduce_min_sync(0xFFFFFFFFu, valid ? cell.x : big);
-        const int mny = __reduce_min_sync(0xFFFFFFFFu, valid ? cell.y : big);
-        const int mnz = __reduce_min_sync(0xFFFFFFFFu, valid ? cell.z : big);
-        const int mxx = __reduce_max_sync(0xFFFFFFFFu, valid ? cell.x : -big);
-        const int mxy = __reduce_max_sync(0xFFFFFFFFu, valid ? cell.y : -big);
-        const int mxz = __reduce_max_sync(0xFFFFFFFFu, valid ? cell.z : -big);
+        int3 mn = make_int3(big, big, big), mx = make_int3(-big, -big, -big);
+        for (int k = 0; k < P2G_PER_THREAD; ++k) {
+            const uint32_t i = first + uint32_t(k);
+            if (i >= n) break;
+            const float4 a = __ldg(reinterpret_cast<const float4*>(particles + i));
+            if (is_dead_age(a.w)) continue;
+            const int3 c = p2g_cell(d, make_float3(a.x, a.y, a.z));
+            mn = make_int3(min(mn.x, c.x), min(mn.y, c.y), min(mn.z, c.z));
+            mx = make_int3(max(mx.x, c.x), max(mx.y, c.y), max(mx.z, c.z));
+        }
+        mn.x = __reduce_min_sync(0xFFFFFFFFu, mn.x); mn.y = __reduce_min_sync(0xFFFFFFFFu, mn.y); mn.z = __reduce_min_sync(0xFFFFFFFFu, mn.z);
+        mx.x = __reduce_max_sync(0xFFFFFFFFu, mx.x); mx.y = __reduce_max_sync(0xFFFFFFFFu, mx.y); mx.z = __reduce_max_sync(0xFFFFFFFFu, mx.z);
         if ((threadIdx.x & 31) == 0) {
-            atomicMin(s_box + 0, mnx); atomicMin(s_box + 1, mny); atomicMin(s_box + 2, mnz);
-            atomicMax(s_box + 3, mxx); atomicMax(s_box + 4, mxy); atomicMax(s_box + 5, mxz);
+            atomicMin(s_box + 0, mn.x); atomicMin(s_box + 1, mn.y); atomicMin(s_box + 2, mn.z);
+            atomicMax(s_box + 3, mx.x); atomicMax(s_box + 4, mx.y); atomicMax(s_box + 5, mx.z);
         }
     }
     __syncthreads();
@@ -160,9 +161,17 @@ __global__ void __launch_bounds__(P2G_THREADS) k_p2g(Dev d, Pass p, const slosh_
     }
     __syncthreads();
 
-    if (valid) {
-        const float inv_h = d.inv_h, h = d.h;
-        const uint32_t tf = d.total_faces;
+    const float inv_h = d.inv_h, h = d.h;
+    const uint32_t tf = d.total_faces;
+    for (int k = 0; k < P2G_PER_THREAD; ++k) {
+        const uint32_t i = first + uint32_t(k);
+        if (i >= n) break;
+        float4 ra, rb;
+        uint4 rc;
+        load_particle_raw(particles, i, ra, rb, rc);
+        if (is_dead_age(ra.w)) continue;
+        const ParticleF part = unpack_particle(ra, rb, rc);
+        const int3 cell = p2g_cell(d, part.pos);
 #pragma unroll
         for (int axis = 0; axis < 3; ++axis) {
             const float3 cp = p.use_apic ? (axis == 0 ? part.cx : (axis == 1 ? part.cy : part.cz)) : make_float3(0.0f, 0.0f, 0.0f);
@@ -242,25 +251,48 @@ __device__ __forceinline__ Stencil stencil_of(const Dev& d, float3 x, int axis) 
     s.fz = gz - float(s.base.z);
     return s;
 }
-__device__ __forceinline__ int3 stencil_node(const Dev& d, const Stencil& s, int o) {
-    return make_int3(clampi(s.base.x + (o & 1), 0, d.grid.x - 1), clampi(s.base.y + ((o >> 1) & 1), 0, d.grid.y - 1),
-                     clampi(s.base.z + ((o >> 2) & 1), 0, d.grid.z - 1));
+// Pool indices of the 8 (clamped) stencil nodes of one MAC component. The nodes span at most two
+// bricks per axis; the brick table is read once for the base node's brick and again only for the
+// neighbouring bricks the stencil actually crosses into.
+__device__ __forceinline__ void stencil_indices(const Dev& d, const Stencil& s, int axis, uint32_t idx[8]) {
+    const int x0 = clampi(s.base.x, 0, d.grid.x - 1), x1 = clampi(s.base.x + 1, 0, d.grid.x - 1);
+    const int y0 = clampi(s.base.y, 0, d.grid.y - 1), y1 = clampi(s.base.y + 1, 0, d.grid.y - 1);
+    const int z0 = clampi(s.base.z, 0, d.grid.z - 1), z1 = clampi(s.base.z + 1, 0, d.grid.z - 1);
+    const bool cx = (x0 >> 3) != (x1 >> 3), cy = (y0 >> 3) != (y1 >> 3), cz = (z0 >> 3) != (z1 >> 3);
+    const uint32_t b000 = brick_index_of(d, make_int3(x0 >> 3, y0 >> 3, z0 >> 3));
+    const uint32_t sx = 1u, sy = uint32_t(d.brick_dim.x), sz = uint32_t(d.brick_dim.x * d.brick_dim.y);
+    uint32_t slot[8];
+    slot[0] = __ldg(d.brick_table + b000);
+    slot[1] = cx ? __ldg(d.brick_table + b000 + sx) : slot[0];
+    slot[2] = cy ? __ldg(d.brick_table + b000 + sy) : slot[0];
+    slot[3] = cy ? (cx ? __ldg(d.brick_table + b000 + sy + sx) : slot[2]) : slot[1];
+    slot[4] = cz ? __ldg(d.brick_table + b000 + sz) : slot[0];
+    slot[5] = cz ? (cx ? __ldg(d.brick_table + b000 + sz + sx) : slot[4]) : slot[1];
+    slot[6] = cz ? (cy ? __ldg(d.brick_table + b000 + sz + sy) : slot[4]) : slot[2];
+    slot[7] = cz ? ((cx || cy) ? (cx && cy ? __ldg(d.brick_table + b000 + sz + sy + sx) : (cx ? slot[5] : slot[6])) : slot[4]) : slot[3];
+    const uint32_t plane = uint32_t(axis) * d.pool_cells;
+#pragma unroll
+    for (int o = 0; o < 8; ++o) {
+        const int x = (o & 1) ? x1 : x0, y = ((o >> 1) & 1) ? y1 : y0, z = ((o >> 2) & 1) ? z1 : z0;
+        idx[o] = plane + slot[o] * BRICK_CELLS + uint32_t((x & 7) + 8 * ((y & 7) + 8 * (z & 7)));
+    }
 }
 
 // GatherComponent (Slosh.usf:1376-1410).
 __device__ __forceinline__ void gather_component(const Dev& d, const Pass& p, int axis, float3 xp, const float* __restrict__ vel,
                                                  float& unew, float& dsum, float& dw, float3& grad) {
     const Stencil s = stencil_of(d, xp, axis);
+    uint32_t idx[8];
+    stencil_indices(d, s, axis, idx);
     unew = 0.0f; dsum = 0.0f; dw = 0.0f;
     grad = make_float3(0.0f, 0.0f, 0.0f);
 #pragma unroll
     for (int o = 0; o < 8; ++o) {
         const int oix = o & 1, oiy = (o >> 1) & 1, oiz = (o >> 2) & 1;
-        const int3 node = stencil_node(d, s, o);
         const float w3x = oix ? s.fx : 1.0f - s.fx, w3y = oiy ? s.fy : 1.0f - s.fy, w3z = oiz ? s.fz : 1.0f - s.fz;
         const float w = w3x * w3y * w3z;
         const float sx = oix ? 1.0f : -1.0f, sy = oiy ? 1.0f : -1.0f, sz = oiz ? 1.0f : -1.0f;
-        const uint32_t f = face_index(d, axis, node);
+        const uint32_t f = idx[o];
         const float u = vel[f];
         unew = unew + w * u;
         if (p.use_apic != 0u) {
@@ -278,13 +310,14 @@ __device__ __forceinline__ float sample_component(const Dev& d, int axis, float3
                                                   const float* __restrict__ vel) {
     const uint32_t known = FACE_VALID | (0xFFFFFFFFu << FACE_EXTRAP_SHIFT);
     const Stencil s = stencil_of(d, xp, axis);
+    uint32_t idx[8];
+    stencil_indices(d, s, axis, idx);
     float u = 0.0f;
 #pragma unroll
     for (int o = 0; o < 8; ++o) {
         const int oix = o & 1, oiy = (o >> 1) & 1, oiz = (o >> 2) & 1;
-        const int3 node = stencil_node(d, s, o);
         const float w3x = oix ? s.fx : 1.0f - s.fx, w3y = oiy ? s.fy : 1.0f - s.fy, w3z = oiz ? s.fz : 1.0f - s.fz;
-        const uint32_t f = face_index(d, axis, node);
+        const uint32_t f = idx[o];
         float uf = vel[f];
         if (check && (d.face_flags[f] & known) == 0u) uf = fallback;
         u = u + w3x * w3y * w3z * uf;
@@ -297,13 +330,14 @@ __device__ __forceinline__ float3 sample_displacement(const Dev& d, float3 xp, c
 #pragma unroll
     for (int axis = 0; axis < 3; ++axis) {
         const Stencil s = stencil_of(d, xp, axis);
+        uint32_t idx[8];
+        stencil_indices(d, s, axis, idx);
         float value = 0.0f;
 #pragma unroll
         for (int o = 0; o < 8; ++o) {
             const int oix = o & 1, oiy = (o >> 1) & 1, oiz = (o >> 2) & 1;
-            const int3 node = stencil_node(d, s, o);
             const float w3x = oix ? s.fx : 1.0f - s.fx, w3y = oiy ? s.fy : 1.0f - s.fy, w3z = oiz ? s.fz : 1.0f - s.fz;
-            value = value + w3x * w3y * w3z * disp[face_index(d, axis, node)];
+            value = value + w3x * w3y * w3z * disp[idx[o]];
         }
         out[axis] = value;
     }
@@ -508,7 +542,7 @@ int launch_p2g(const Dev& d, const Pass& p, const slosh_particle_t* particles, u
         cudaFuncSetAttribute(k_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         configured = true;
     }
-    k_p2g<<<(n + P2G_THREADS - 1u) / P2G_THREADS, P2G_THREADS, smem, s>>>(d, p, particles, n);
+    k_p2g<<<(n + P2G_CHUNK - 1u) / P2G_CHUNK, P2G_THREADS, smem, s>>>(d, p, particles, n);
     return 1;
 }
 int launch_g2p(const Dev& d, const Pass& p, slosh_particle_t* particles, uint32_t n, const float* vel, const float* disp,

@@ -92,3 +92,59 @@ def test_tiny_with_collider(slosh, oracle_mod):
     sc = scenes.tiny(slosh.settings_default, n=24, colliders=True)
     g, o = _pair(slosh, oracle_mod, sc)
     _run_frames(g, o, sc, frames=5)
+
+
+def test_fp64_error(slosh, oracle_mod):
+    """The GPU result's error against the FP64 oracle of the same substep (same starting state)."""
+    from test_oracle_pins import fp64_step_errors
+    sc = scenes.tiny(slosh.settings_default, n=24)
+    g, o = _pair(slosh, oracle_mod, sc)
+    _run_frames(g, o, sc, frames=3, check_every_substep=False)
+    fi = A.frame_input(sc["settings"])
+    g.begin_frame(fi)
+    errs = fp64_step_errors(oracle_mod, o, fi, extra=g)
+    assert errs[("gpu", "PRESSURE")] == errs[("oracle32", "PRESSURE")]  # bit-exact FP32 on both sides
+    assert errs[("gpu", "PRESSURE")] < 1e-4, errs
+    assert errs[("gpu", "VEL")] < 1e-5, errs
+
+
+def test_pool_overflow_parity_and_status(slosh, oracle_mod):
+    """Injected pool exhaustion (storage budget below what the liquid needs): bricks left on the null
+    brick move ballistically, the overflow is counted, and the frame reports SLOSH_WARN_POOL_OVERFLOW."""
+    sc = scenes.tiny(slosh.settings_default, n=32)
+    sc["settings"].sparse_storage_budget = 0.2
+    g, o = _pair(slosh, oracle_mod, sc)
+    fi = A.frame_input(sc["settings"], emits=sc["emits"])
+    rc = g.step_frame(fi)
+    o.step_frame(fi)
+    assert rc == A.WARN_POOL_OVERFLOW
+    assert g.results().pool_overflow_bricks > 0
+    assert g.results().pool_overflow_bricks == o.results().pool_overflow_bricks
+    fi = A.frame_input(sc["settings"])
+    for _ in range(3):
+        g.step_frame(fi)
+        o.step_frame(fi)
+        r = compare_state(g, o)
+        assert not r.failures(FLOAT_TOL), str(r)
+
+
+def test_iteration_cap_reports_not_converged(slosh, oracle_mod):
+    """Injected non-convergence (tolerance far below reach with a 3-iteration cap)."""
+    sc = scenes.tiny(slosh.settings_default, n=16, tolerance=1e-12)
+    sc["settings"].max_iterations = 3
+    g, o = _pair(slosh, oracle_mod, sc)
+    fi = A.frame_input(sc["settings"], emits=sc["emits"])
+    rc = g.step_frame(fi)
+    o.step_frame(fi)
+    assert rc == A.ERR_NOT_CONVERGED
+    assert g.results().last_solve_iterations == 3 == o.results().last_solve_iterations
+    r = compare_state(g, o)
+    assert not r.failures(FLOAT_TOL), str(r)
+
+
+def test_fixed_iteration_mode_matches_reference_semantics(slosh, oracle_mod):
+    """tolerance <= 0: the reference's fixed PCGIterations (8) and no stopping test."""
+    sc = scenes.tiny(slosh.settings_default, n=16, tolerance=0.0)
+    g, o = _pair(slosh, oracle_mod, sc)
+    _run_frames(g, o, sc, frames=3)
+    assert g.results().last_solve_iterations == 8

@@ -1,0 +1,60 @@
+"""The multi-GPU path (independent replicas) with world_size 2 over gloo on the CPU: each rank advances
+its own tank (the CPU oracle stands in for the device) and the run is aggregated as bench.py does."""
+import os
+import socket
+
+import pytest
+import torch.multiprocessing as mp
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _rank_main(rank, world, port, queue):
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, root)
+    import datetime
+
+    import torch.distributed as dist
+
+    from oracle import oracle as O
+    from slosh_b200 import _abi as A, scenes
+    from slosh_b200.replicas import reduce_run
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    sc = scenes.tiny(O.settings_default, n=16)
+    o = O.Oracle(sc["settings"])
+    o.set_emit_seed(sc["seed"])
+    fi = A.frame_input(sc["settings"], emits=sc["emits"])
+    substeps = 0
+    for _ in range(2):
+        o.step_frame(fi)
+        substeps += o.results().substeps
+        fi = A.frame_input(sc["settings"])
+    total, dev_ms, wall_ms = reduce_run(substeps, 10.0 + rank, 20.0 + 3 * rank)
+    queue.put((rank, substeps, total, dev_ms, wall_ms, o.results().fluid_cells))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_rank_replicas():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=180)
+        assert p.exitcode == 0
+    out = sorted(q.get(timeout=5) for _ in range(2))
+    (r0, s0, t0, d0, w0, f0), (r1, s1, t1, d1, w1, f1) = out
+    assert t0 == t1 == s0 + s1
+    assert d0 == d1 == 11.0 and w0 == w1 == 23.0
+    assert f0 == f1  # identical replicas
