@@ -328,8 +328,9 @@ struct Ctx {
                 mg.lv[l].type = dalloc<uint32_t>(level_cells[l], false);
                 mg.lv[l].x = dalloc<float>(level_cells[l], false);
                 mg.lv[l].b = dalloc<float>(level_cells[l], false);
+                mg.lv[l].word = dalloc<uint16_t>(level_cells[l], false);
             } else {
-                mg.lv[l].type = nullptr; mg.lv[l].x = nullptr; mg.lv[l].b = nullptr;
+                mg.lv[l].type = nullptr; mg.lv[l].x = nullptr; mg.lv[l].b = nullptr; mg.lv[l].word = nullptr;
             }
         }
         mg.r = dalloc<float>(pc, false);
@@ -343,6 +344,12 @@ struct Ctx {
         mg.scalars = dalloc<double>(8, false);
         mg.counters = dalloc<uint32_t>(8, false);
         mg.ctl = dalloc<uint32_t>(8, false);
+        {
+            size_t tail_cells = 0;
+            for (int l = 1; l < num_levels; ++l) tail_cells += level_cells[l];
+            mg.tail_list = dalloc<uint32_t>(tail_cells + 1, false);
+            mg.tail_meta = dalloc<uint32_t>(4 * SLOSH_MAX_MG_LEVELS, false);
+        }
         // zero everything (AddClearUAVPass of every buffer), then the free stack and the slot table
         zero_all();
         std::vector<uint32_t> free_init(num_pool_bricks);
@@ -385,6 +392,7 @@ struct Ctx {
             CK(cudaMemset(mg.lv[l].type, 0, level_cells[l] * 4));
             CK(cudaMemset(mg.lv[l].x, 0, level_cells[l] * 4));
             CK(cudaMemset(mg.lv[l].b, 0, level_cells[l] * 4));
+            CK(cudaMemset(mg.lv[l].word, 0, level_cells[l] * 2));
         }
         CK(cudaMemset(mg.scalars, 0, 8 * sizeof(double)));
         CK(cudaMemset(mg.counters, 0, 8 * 4));
@@ -536,6 +544,8 @@ struct Ctx {
                     cudaStream_t s) {
         int n = launch_mg_setup(mg, limit, tol_mode, double(tol), s);
         for (int l = 0; l < num_levels - 1; ++l) n += launch_mg_build_type(d, mg, l, s);
+        for (int l = 1; l < num_levels; ++l) n += launch_mg_words(mg, l, s);
+        n += launch_mg_tail_lists(mg, s);
         n += launch_pcg_init(d, mg, p, div, handle, shape, s);
         return n;
     }

@@ -68,6 +68,7 @@ struct MGLevel {
     uint32_t* type;
     float* x;
     float* b;
+    uint16_t* word;   // per-solve stencil word: bits 0-5 fluid neighbour, 6 fluid, 7 red, 8-13 non-solid neighbour
 };
 struct MGState {
     int num_levels;
@@ -83,7 +84,11 @@ struct MGState {
     uint8_t* word;        // level-0 stencil word per pool cell (fluid neighbours, fluid, red)
     uint32_t* nbr_slots;  // 8 per active-brick entry: slots of the 6 face-neighbour bricks
     float* dvec2;         // second search-direction buffer (d alternates by iteration parity)
+    uint32_t* tail_list;  // per tail level: red fluid cells, then black fluid cells (dense indices)
+    uint32_t* tail_meta;  // per level: [red offset, red count, black offset, black count]
 };
+int launch_mg_words(const MGState& m, int l, cudaStream_t s);
+int launch_mg_tail_lists(const MGState& m, cudaStream_t s);
 size_t mg_tail_smem(const MGState& m);
 // First level handled by the single-CTA tail kernel of the V-cycle.
 int mg_tail_level(const MGState& m);

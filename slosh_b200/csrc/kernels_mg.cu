@@ -46,20 +46,6 @@ __device__ __forceinline__ void stencil0(const Dev& d, const float* buf, uint32_
     }
     diag = d.cell_diag[i] + DIAG_EPSILON;
 }
-// Dense coarse-level stencil (counted non-solid neighbours + epsilon).
-__device__ __forceinline__ void stencil_dense(const MGLevel& L, const float* buf, int3 c, float& diag, float& sum) {
-    diag = DIAG_EPSILON;
-    sum = 0.0f;
-#pragma unroll
-    for (int n = 0; n < 6; ++n) {
-        const int3 nb = add3(c, nbr_off(n));
-        if (!inside3(nb, L.dim)) continue;
-        const uint32_t ni = lin3(nb, L.dim);
-        const uint32_t t = L.type[ni] & CELL_TYPE_MASK;
-        if (t != CELL_SOLID) diag = diag + 1.0f;
-        if (t == CELL_FLUID) sum = sum + buf[ni];
-    }
-}
 
 // ---- canonical FP64 reduction ---------------------------------------------------------------------
 struct DotSmem {
@@ -264,6 +250,46 @@ __global__ void k_build_type(Dev d, MGLevel fine, MGLevel coarse, int fine_is_po
     coarse.type[ci] = any_air ? CELL_AIR : (any_fluid ? CELL_FLUID : CELL_SOLID);
 }
 
+// ---- coarse-level stencil words (once per solve, after the coarse types) -----------------------------------
+constexpr uint32_t CW_FLUID = 1u << 6, CW_RED = 1u << 7, CW_NONSOLID_SHIFT = 8u;
+
+__global__ void k_level_words(MGLevel L) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= L.cells) return;
+    const int3 c = coord3(i, L.dim);
+    uint32_t w = (L.type[i] & CELL_TYPE_MASK) == CELL_FLUID ? CW_FLUID : 0u;
+    if (is_red(c)) w |= CW_RED;
+#pragma unroll
+    for (int n = 0; n < 6; ++n) {
+        const int3 nb = add3(c, nbr_off(n));
+        if (!inside3(nb, L.dim)) continue;
+        const uint32_t t = L.type[lin3(nb, L.dim)] & CELL_TYPE_MASK;
+        if (t == CELL_FLUID) w |= 1u << n;
+        if (t != CELL_SOLID) w |= 1u << (CW_NONSOLID_SHIFT + n);
+    }
+    L.word[i] = uint16_t(w);
+}
+// DiagEpsilon plus one per non-solid neighbour, added in neighbour order like FINE_STENCIL.
+__device__ __forceinline__ float word_diag(uint32_t w) {
+    float d = DIAG_EPSILON;
+#pragma unroll
+    for (int n = 0; n < 6; ++n)
+        if ((w >> (CW_NONSOLID_SHIFT + n)) & 1u) d = d + 1.0f;
+    return d;
+}
+// Sum of x over the fluid neighbours (dense level), in neighbour order.
+__device__ __forceinline__ float word_sum(const float* x, uint32_t w, uint32_t i, uint32_t dx, uint32_t dxy) {
+    const uint32_t off[6] = {i - 1u, i + 1u, i - dx, i + dx, i - dxy, i + dxy};
+    float v[6];
+#pragma unroll
+    for (int n = 0; n < 6; ++n) v[n] = ((w >> n) & 1u) ? x[off[n]] : 0.0f;
+    float sum = 0.0f;
+#pragma unroll
+    for (int n = 0; n < 6; ++n)
+        if ((w >> n) & 1u) sum = sum + v[n];
+    return sum;
+}
+
 // ---- PCGInitCS (+ ||r0||^2 and ||b||^2, and the decision whether any iteration runs) ----------------------
 // Also stores the solve's stencil words and the active bricks' neighbour slots.
 __global__ void __launch_bounds__(GRID_THREADS) k_pcg_init(Dev d, MGState m, const float* __restrict__ p, const float* __restrict__ div,
@@ -386,7 +412,7 @@ __global__ void __launch_bounds__(GRID_THREADS) k_prolong_smooth0(Dev d, MGState
                 const int3 nb = add3(c, nbr_off(n));
                 const uint32_t pi = lin3(make_int3(nb.x / 2, nb.y / 2, nb.z / 2), C.dim);
                 const float zn = m.z[l0_nbr(i, l, n, ns)];
-                v[n] = (C.type[pi] & CELL_TYPE_MASK) == CELL_FLUID ? zn + C.x[pi] : zn;
+                v[n] = (C.word[pi] & CW_FLUID) ? zn + C.x[pi] : zn;
             }
             float sum = 0.0f;
 #pragma unroll
@@ -397,74 +423,73 @@ __global__ void __launch_bounds__(GRID_THREADS) k_prolong_smooth0(Dev d, MGState
     }
 }
 
-// ---- dense-level passes, usable by a grid of CTAs (stride = all threads) or by one CTA -------------------
-__device__ __forceinline__ void smooth_cell(const MGLevel& L, uint32_t i, int3 c, uint32_t parity) {
-    if ((L.type[i] & CELL_TYPE_MASK) != CELL_FLUID) return;
-    if ((is_red(c) ? 0u : 1u) != parity) return;
-    float diag, sum;
-    stencil_dense(L, L.x, c, diag, sum);
-    L.x[i] = (L.b[i] + sum) / diag;
-}
-__device__ __forceinline__ void restrict_store(const MGLevel& C, uint32_t ci, int3 c, float sum) {
-    const float b = 0.25f * sum;
-    C.b[ci] = b;
-    float cdiag = DIAG_EPSILON;
-#pragma unroll
-    for (int n = 0; n < 6; ++n) {
-        const int3 nb = add3(c, nbr_off(n));
-        const uint32_t t = inside3(nb, C.dim) ? (C.type[lin3(nb, C.dim)] & CELL_TYPE_MASK) : CELL_SOLID;
-        cdiag = cdiag + (t != CELL_SOLID ? 1.0f : 0.0f);
-    }
-    C.x[ci] = is_red(c) ? b / cdiag : 0.0f;
-}
-__device__ __forceinline__ void restrict_cell(const MGLevel& F, const MGLevel& C, uint32_t ci, int3 c) {
-    if ((C.type[ci] & CELL_TYPE_MASK) != CELL_FLUID) { C.b[ci] = 0.0f; C.x[ci] = 0.0f; return; }
-    float sum = 0.0f;
-#pragma unroll
-    for (int o = 0; o < 8; ++o) {
-        const int3 f = make_int3(c.x * 2 + (o & 1), c.y * 2 + ((o >> 1) & 1), c.z * 2 + ((o >> 2) & 1));
-        if (!inside3(f, F.dim)) continue;
-        const uint32_t fi = lin3(f, F.dim);
-        if ((F.type[fi] & CELL_TYPE_MASK) != CELL_FLUID) continue;
-        float diag, nbsum;
-        stencil_dense(F, F.x, f, diag, nbsum);
-        sum = sum + (F.b[fi] - (diag * F.x[fi] - nbsum));
-    }
-    restrict_store(C, ci, c, sum);
-}
 
-// Levels 1..3 through the active-brick footprints.
+// Levels 1..3 through the active-brick footprints, with the per-solve stencil words.
 __global__ void k_smooth_fp(Dev d, MGState m, int l, uint32_t parity) {
     if (solve_done(m)) return;
     const MGLevel L = m.lv[l];
-    for_footprint(d, L, l, [&](uint32_t i, int3 c) { smooth_cell(L, i, c, parity); });
+    const uint32_t dx = uint32_t(L.dim.x), dxy = uint32_t(L.dim.x * L.dim.y);
+    const uint32_t want = parity == 0u ? CW_RED : 0u;
+    for_footprint(d, L, l, [&](uint32_t i, int3) {
+        const uint32_t w = L.word[i];
+        if (!(w & CW_FLUID) || (w & CW_RED) != want) return;
+        L.x[i] = (L.b[i] + word_sum(L.x, w, i, dx, dxy)) / word_diag(w);
+    });
 }
-__global__ void k_restrict_fp(Dev d, MGState m, int l) {  // level l -> l + 1, over level l + 1's footprint
+// Restriction l -> l + 1 over level l + 1's footprint: b_c = (sum of the fluid children's residuals) / 4.
+__global__ void k_restrict_fp(Dev d, MGState m, int l) {
     if (solve_done(m)) return;
     const MGLevel F = m.lv[l], C = m.lv[l + 1];
-    for_footprint(d, C, l + 1, [&](uint32_t ci, int3 c) { restrict_cell(F, C, ci, c); });
+    const uint32_t fdx = uint32_t(F.dim.x), fdxy = uint32_t(F.dim.x * F.dim.y);
+    for_footprint(d, C, l + 1, [&](uint32_t ci, int3 c) {
+        const uint32_t cw = C.word[ci];
+        if (!(cw & CW_FLUID)) { C.b[ci] = 0.0f; C.x[ci] = 0.0f; return; }
+        float res[8];
+        uint32_t fl = 0u;
+#pragma unroll
+        for (int o = 0; o < 8; ++o) {
+            res[o] = 0.0f;
+            const int3 f = make_int3(c.x * 2 + (o & 1), c.y * 2 + ((o >> 1) & 1), c.z * 2 + ((o >> 2) & 1));
+            if (!inside3(f, F.dim)) continue;
+            const uint32_t fi = lin3(f, F.dim);
+            const uint32_t w = F.word[fi];
+            if (!(w & CW_FLUID)) continue;
+            fl |= 1u << o;
+            res[o] = F.b[fi] - (word_diag(w) * F.x[fi] - word_sum(F.x, w, fi, fdx, fdxy));
+        }
+        float sum = 0.0f;
+#pragma unroll
+        for (int o = 0; o < 8; ++o)
+            if ((fl >> o) & 1u) sum = sum + res[o];
+        const float bb = 0.25f * sum;
+        C.b[ci] = bb;
+        C.x[ci] = (cw & CW_RED) ? bb / word_diag(cw) : 0.0f;
+    });
 }
 // Prolongation l + 1 -> l fused with the black sweep of level l (see k_prolong_smooth0).
 __global__ void k_prolong_smooth_fp(Dev d, MGState m, int l) {
     if (solve_done(m)) return;
     const MGLevel F = m.lv[l], C = m.lv[l + 1];
+    const uint32_t dx = uint32_t(F.dim.x), dxy = uint32_t(F.dim.x * F.dim.y);
     for_footprint(d, F, l, [&](uint32_t i, int3 c) {
-        if ((F.type[i] & CELL_TYPE_MASK) != CELL_FLUID || is_red(c)) return;
-        float diag = DIAG_EPSILON, sum = 0.0f;
+        const uint32_t w = F.word[i];
+        if (!(w & CW_FLUID) || (w & CW_RED)) return;
+        const uint32_t off[6] = {i - 1u, i + 1u, i - dx, i + dx, i - dxy, i + dxy};
+        float v[6];
 #pragma unroll
         for (int n = 0; n < 6; ++n) {
+            v[n] = 0.0f;
+            if (!((w >> n) & 1u)) continue;
             const int3 nb = add3(c, nbr_off(n));
-            if (!inside3(nb, F.dim)) continue;
-            const uint32_t ni = lin3(nb, F.dim);
-            const uint32_t t = F.type[ni] & CELL_TYPE_MASK;
-            if (t != CELL_SOLID) diag = diag + 1.0f;
-            if (t == CELL_FLUID) {
-                const uint32_t pi = lin3(make_int3(nb.x / 2, nb.y / 2, nb.z / 2), C.dim);
-                const float xn = F.x[ni];
-                sum = sum + ((C.type[pi] & CELL_TYPE_MASK) == CELL_FLUID ? xn + C.x[pi] : xn);
-            }
+            const uint32_t pi = lin3(make_int3(nb.x / 2, nb.y / 2, nb.z / 2), C.dim);
+            const float xn = F.x[off[n]];
+            v[n] = (C.word[pi] & CW_FLUID) ? xn + C.x[pi] : xn;
         }
-        F.x[i] = (F.b[i] + sum) / diag;
+        float sum = 0.0f;
+#pragma unroll
+        for (int n = 0; n < 6; ++n)
+            if ((w >> n) & 1u) sum = sum + v[n];
+        F.x[i] = (F.b[i] + sum) / word_diag(w);
     });
 }
 
@@ -503,7 +528,8 @@ __global__ void __launch_bounds__(GRID_THREADS) k_restrict0(Dev d, MGState m) {
             const int3 c = make_int3(bc.x * 4 + cl.x, bc.y * 4 + cl.y, bc.z * 4 + cl.z);
             if (inside3(c, C.dim)) {
                 const uint32_t ci = lin3(c, C.dim);
-                if ((C.type[ci] & CELL_TYPE_MASK) != CELL_FLUID) {
+                const uint32_t cw = C.word[ci];
+                if (!(cw & CW_FLUID)) {
                     C.b[ci] = 0.0f;
                     C.x[ci] = 0.0f;
                 } else {
@@ -513,7 +539,9 @@ __global__ void __launch_bounds__(GRID_THREADS) k_restrict0(Dev d, MGState m) {
                         const uint32_t fl = uint32_t((2 * cl.x + (o & 1)) + 8 * ((2 * cl.y + ((o >> 1) & 1)) + 8 * (2 * cl.z + ((o >> 2) & 1))));
                         if (s_fluid[fl]) sum = sum + s_res[fl];
                     }
-                    restrict_store(C, ci, c, sum);
+                    const float bb = 0.25f * sum;
+                    C.b[ci] = bb;
+                    C.x[ci] = (cw & CW_RED) ? bb / word_diag(cw) : 0.0f;
                 }
             }
         }
@@ -522,108 +550,155 @@ __global__ void __launch_bounds__(GRID_THREADS) k_restrict0(Dev d, MGState m) {
 }
 
 // ---- the small coarse levels in one CTA: levels tail..nl-1 of the V-cycle --------------------------------
-// On entry level `tail` holds b and the red-initialised x from the restriction that produced it. The
-// levels are copied into shared memory (type byte, x, b per cell), the descent, the coarse solve and
-// the ascent run there with block barriers between passes, and level tail's x is written back.
-struct SLevel {
-    int3 dim;
-    uint32_t cells;
-    uint8_t* type;
-    float* x;
-    float* b;
-};
-__device__ __forceinline__ void s_stencil(const SLevel& L, int3 c, float& diag, float& sum) {
-    diag = DIAG_EPSILON;
-    sum = 0.0f;
+// Once per solve, k_tail_lists stores each tail level's fluid cells by colour. Each V-cycle,
+// k_vcycle_tail copies the tail levels into shared memory (word, diagonal, x, b per cell; the colour
+// lists), runs the descent, the coarse solve and the ascent there -- every sweep visits only the fluid
+// cells of its colour -- and writes level tail's x back. On entry level `tail` holds b and the
+// red-initialised x from the restriction that produced it.
+__global__ void __launch_bounds__(1024) k_tail_lists(MGState m, int tail) {
+    __shared__ uint32_t s_warp[33];
+    uint32_t off = 0;
+    for (int l = tail; l < m.num_levels; ++l) {
+        const MGLevel L = m.lv[l];
+        for (uint32_t colour = 0; colour < 2u; ++colour) {
+            const uint32_t want = colour == 0u ? CW_RED : 0u;
+            uint32_t base = 0;
+            for (uint32_t start = 0; start < L.cells; start += blockDim.x) {
+                const uint32_t i = start + threadIdx.x;
+                const uint32_t w = i < L.cells ? uint32_t(L.word[i]) : 0u;
+                const uint32_t flag = (i < L.cells && (w & CW_FLUID) && (w & CW_RED) == want) ? 1u : 0u;
+                // block-wide exclusive scan of flag
+                const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+                const uint32_t bal = __ballot_sync(0xFFFFFFFFu, flag);
+                if (lane == 0) s_warp[warp] = __popc(bal);
+                __syncthreads();
+                if (warp == 0) {
+                    const uint32_t v = s_warp[lane];
+                    uint32_t x = v;
 #pragma unroll
-    for (int n = 0; n < 6; ++n) {
-        const int3 nb = add3(c, nbr_off(n));
-        if (!inside3(nb, L.dim)) continue;
-        const uint32_t ni = lin3(nb, L.dim);
-        const uint32_t t = L.type[ni];
-        if (t != CELL_SOLID) diag = diag + 1.0f;
-        if (t == CELL_FLUID) sum = sum + L.x[ni];
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+                        if (lane >= o) x += y;
+                    }
+                    s_warp[lane] = x - v;
+                    if (lane == 31) s_warp[32] = x;
+                }
+                __syncthreads();
+                if (flag) m.tail_list[off + base + s_warp[warp] + __popc(bal & ((1u << lane) - 1u))] = i;
+                base += s_warp[32];
+                __syncthreads();
+            }
+            if (threadIdx.x == 0) {
+                m.tail_meta[4 * l + 2 * colour] = off;
+                m.tail_meta[4 * l + 2 * colour + 1] = base;
+            }
+            off += base;
+        }
     }
 }
-__device__ void s_smooth(const SLevel& L, uint32_t parity) {
-    for (uint32_t i = threadIdx.x; i < L.cells; i += blockDim.x) {
-        if (L.type[i] != CELL_FLUID) continue;
-        const int3 c = coord3(i, L.dim);
-        if ((is_red(c) ? 0u : 1u) != parity) continue;
-        float diag, sum;
-        s_stencil(L, c, diag, sum);
-        L.x[i] = (L.b[i] + sum) / diag;
+
+struct SLevel {
+    int3 dim;
+    uint32_t cells, dx, dxy;
+    uint16_t* word;
+    float* diag;
+    float* x;
+    float* b;
+    const uint32_t* list;  // red cells then black cells
+    uint32_t nred, nblack;
+};
+__device__ __forceinline__ void s_sweep(const SLevel& L, uint32_t colour) {
+    const uint32_t n = colour == 0u ? L.nred : L.nblack;
+    const uint32_t* list = L.list + (colour == 0u ? 0u : L.nred);
+    for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) {
+        const uint32_t i = list[j];
+        const uint32_t w = L.word[i];
+        L.x[i] = (L.b[i] + word_sum(L.x, w, i, L.dx, L.dxy)) / L.diag[i];
     }
     __syncthreads();
 }
 __global__ void __launch_bounds__(1024) k_vcycle_tail(MGState m, int tail, int iterations) {
     if (solve_done(m)) return;
-    extern __shared__ unsigned char s_tail[];
+    extern __shared__ __align__(16) unsigned char s_tail[];
     const int nl = m.num_levels;
     SLevel S[SLOSH_MAX_MG_LEVELS];
     size_t off = 0;
     for (int l = tail; l < nl; ++l) {
-        S[l].dim = m.lv[l].dim;
-        S[l].cells = m.lv[l].cells;
-        S[l].x = reinterpret_cast<float*>(s_tail + off);
-        off += size_t(S[l].cells) * 4;
-        S[l].b = reinterpret_cast<float*>(s_tail + off);
-        off += size_t(S[l].cells) * 4;
-        S[l].type = s_tail + off;
-        off += (size_t(S[l].cells) + 15) & ~size_t(15);
-        for (uint32_t i = threadIdx.x; i < S[l].cells; i += blockDim.x) S[l].type[i] = uint8_t(m.lv[l].type[i] & CELL_TYPE_MASK);
+        const MGLevel G = m.lv[l];
+        SLevel& L = S[l];
+        L.dim = G.dim;
+        L.cells = G.cells;
+        L.dx = uint32_t(G.dim.x);
+        L.dxy = uint32_t(G.dim.x * G.dim.y);
+        L.x = reinterpret_cast<float*>(s_tail + off); off += size_t(L.cells) * 4;
+        L.b = reinterpret_cast<float*>(s_tail + off); off += size_t(L.cells) * 4;
+        L.diag = reinterpret_cast<float*>(s_tail + off); off += size_t(L.cells) * 4;
+        L.word = reinterpret_cast<uint16_t*>(s_tail + off); off += (size_t(L.cells) * 2 + 15) & ~size_t(15);
+        const uint32_t ro = m.tail_meta[4 * l], nr = m.tail_meta[4 * l + 1], bo = m.tail_meta[4 * l + 2], nb = m.tail_meta[4 * l + 3];
+        uint32_t* list = reinterpret_cast<uint32_t*>(s_tail + off); off += size_t(nr + nb) * 4;
+        L.list = list;
+        L.nred = nr;
+        L.nblack = nb;
+        for (uint32_t j = threadIdx.x; j < nr; j += blockDim.x) list[j] = m.tail_list[ro + j];
+        for (uint32_t j = threadIdx.x; j < nb; j += blockDim.x) list[nr + j] = m.tail_list[bo + j];
+        for (uint32_t i = threadIdx.x; i < L.cells; i += blockDim.x) {
+            const uint32_t w = G.word[i];
+            L.word[i] = uint16_t(w);
+            L.diag[i] = word_diag(w);
+        }
     }
     for (uint32_t i = threadIdx.x; i < S[tail].cells; i += blockDim.x) {
         S[tail].x[i] = m.lv[tail].x[i];
         S[tail].b[i] = m.lv[tail].b[i];
     }
     __syncthreads();
-    if (tail < nl - 1) s_smooth(S[tail], 1u);
+    if (tail < nl - 1) s_sweep(S[tail], 1u);
     for (int l = tail; l < nl - 1; ++l) {
-        const SLevel F = S[l], C = S[l + 1];
-        for (uint32_t ci = threadIdx.x; ci < C.cells; ci += blockDim.x) {
+        const SLevel& F = S[l];
+        const SLevel& C = S[l + 1];
+        for (uint32_t j = threadIdx.x; j < C.nred + C.nblack; j += blockDim.x) {
+            const uint32_t ci = C.list[j];
             const int3 c = coord3(ci, C.dim);
-            if (C.type[ci] != CELL_FLUID) { C.b[ci] = 0.0f; C.x[ci] = 0.0f; continue; }
-            float sum = 0.0f;
+            float res[8];
+            uint32_t fl = 0u;
 #pragma unroll
             for (int o = 0; o < 8; ++o) {
+                res[o] = 0.0f;
                 const int3 f = make_int3(c.x * 2 + (o & 1), c.y * 2 + ((o >> 1) & 1), c.z * 2 + ((o >> 2) & 1));
                 if (!inside3(f, F.dim)) continue;
                 const uint32_t fi = lin3(f, F.dim);
-                if (F.type[fi] != CELL_FLUID) continue;
-                float diag, nbsum;
-                s_stencil(F, f, diag, nbsum);
-                sum = sum + (F.b[fi] - (diag * F.x[fi] - nbsum));
+                const uint32_t w = F.word[fi];
+                if (!(w & CW_FLUID)) continue;
+                fl |= 1u << o;
+                res[o] = F.b[fi] - (F.diag[fi] * F.x[fi] - word_sum(F.x, w, fi, F.dx, F.dxy));
             }
+            float sum = 0.0f;
+#pragma unroll
+            for (int o = 0; o < 8; ++o)
+                if ((fl >> o) & 1u) sum = sum + res[o];
             const float bb = 0.25f * sum;
             C.b[ci] = bb;
-            float cdiag = DIAG_EPSILON;
-#pragma unroll
-            for (int n = 0; n < 6; ++n) {
-                const int3 nb = add3(c, nbr_off(n));
-                const uint32_t t = inside3(nb, C.dim) ? uint32_t(C.type[lin3(nb, C.dim)]) : CELL_SOLID;
-                cdiag = cdiag + (t != CELL_SOLID ? 1.0f : 0.0f);
-            }
-            C.x[ci] = is_red(c) ? bb / cdiag : 0.0f;
+            C.x[ci] = (C.word[ci] & CW_RED) ? bb / C.diag[ci] : 0.0f;
         }
         __syncthreads();
-        if (l + 1 < nl - 1) s_smooth(C, 1u);
+        if (l + 1 < nl - 1) s_sweep(C, 1u);
     }
     for (int it = 0; it < iterations; ++it) {
-        s_smooth(S[nl - 1], 0u);
-        s_smooth(S[nl - 1], 1u);
+        s_sweep(S[nl - 1], 0u);
+        s_sweep(S[nl - 1], 1u);
     }
     for (int l = nl - 2; l >= tail; --l) {
-        const SLevel F = S[l], C = S[l + 1];
-        for (uint32_t i = threadIdx.x; i < F.cells; i += blockDim.x) {
-            if (F.type[i] != CELL_FLUID) continue;
+        const SLevel& F = S[l];
+        const SLevel& C = S[l + 1];
+        for (uint32_t j = threadIdx.x; j < F.nred + F.nblack; j += blockDim.x) {
+            const uint32_t i = F.list[j];
             const int3 c = coord3(i, F.dim);
             const uint32_t pi = lin3(make_int3(c.x / 2, c.y / 2, c.z / 2), C.dim);
-            if (C.type[pi] == CELL_FLUID) F.x[i] = F.x[i] + C.x[pi];
+            if (C.word[pi] & CW_FLUID) F.x[i] = F.x[i] + C.x[pi];
         }
         __syncthreads();
-        s_smooth(F, 1u);
-        s_smooth(F, 0u);
+        s_sweep(F, 1u);
+        s_sweep(F, 0u);
     }
     for (uint32_t i = threadIdx.x; i < S[tail].cells; i += blockDim.x) m.lv[tail].x[i] = S[tail].x[i];
 }
@@ -766,8 +841,18 @@ int launch_pcg_init(const Dev& d, const MGState& m, const float* p, const float*
 size_t mg_tail_smem(const MGState& m) {
     const int tail = mg_tail_level(m);
     size_t off = 0;
-    for (int l = tail; l < m.num_levels; ++l) off += size_t(m.lv[l].cells) * 8 + ((size_t(m.lv[l].cells) + 15) & ~size_t(15));
+    for (int l = tail; l < m.num_levels; ++l)
+        off += size_t(m.lv[l].cells) * 12 + ((size_t(m.lv[l].cells) * 2 + 15) & ~size_t(15)) + size_t(m.lv[l].cells) * 4;
     return off;
+}
+int launch_mg_words(const MGState& m, int l, cudaStream_t s) {
+    k_level_words<<<blocks_for(m.lv[l].cells, 256), 256, 0, s>>>(m.lv[l]);
+    return 1;
+}
+int launch_mg_tail_lists(const MGState& m, cudaStream_t s) {
+    if (m.num_levels < 2) return 0;
+    k_tail_lists<<<1, 1024, 0, s>>>(m, mg_tail_level(m));
+    return 1;
 }
 
 // One V-cycle (SloshProxy.cpp:904-959), leaving rho = r.z in scalars[0] (previous rho in scalars[3]).
