@@ -361,19 +361,18 @@ inline bool layout_equals(const slosh_settings_t& a, const slosh_settings_t& b) 
 }
 
 // ---- canonical FP64 reduction tree of the PCG dots -------------------------------------------
-// One partial per 8^3 brick: 256 lanes, lane t holds v[t] + v[t + 256]; each warp of 32 lanes folds
-// with offsets 16, 8, 4, 2, 1; the 8 warp results are added in warp order.
+// One partial per 8^3 brick: 32 lanes, lane t adds v[t], v[t + 32], ..., v[t + 480] in order (starting
+// from 0.0); the lanes then fold with offsets 16, 8, 4, 2, 1 (lane j += lane j + off).
 inline double reduce_brick(const double* v) {
-    double s[256];
-    for (int t = 0; t < 256; ++t) s[t] = v[t] + v[t + 256];
-    double total = 0.0;
-    for (int w = 0; w < 8; ++w) {
-        double* l = s + 32 * w;
-        for (int off = 16; off >= 1; off >>= 1)
-            for (int j = 0; j < off; ++j) l[j] = l[j] + l[j + off];
-        total = (w == 0) ? l[0] : total + l[0];
+    double s[32];
+    for (int t = 0; t < 32; ++t) {
+        double acc = 0.0;
+        for (int k = 0; k < 16; ++k) acc = acc + v[t + 32 * k];
+        s[t] = acc;
     }
-    return total;
+    for (int off = 16; off >= 1; off >>= 1)
+        for (int j = 0; j < off; ++j) s[j] = s[j] + s[j + off];
+    return s[0];
 }
 // Over bricks: 1024 lanes, lane t sums entries t, t + 1024, ... in order; each warp folds as above;
 // the 32 warp results are added in warp order.

@@ -82,50 +82,6 @@ __device__ double final_reduce(const double* partials, uint32_t n, DotSmem& sm) 
     return total;
 }
 
-// Level-0 pass over the active bricks producing up to two dot products. fn(i, c, v0, v1) handles one
-// in-grid cell and sets its contributions; every thread runs the same number of brick iterations.
-// The last CTA to finish reduces the partials and calls store(t0, t1) in thread 0.
-template <int NDOT, class Fn, class Store>
-__device__ __forceinline__ void level0_dot_pass(const Dev& d, const MGState& m, uint32_t counter, Fn fn, Store store) {
-    __shared__ DotSmem sm;
-    const uint32_t active = d.active_bricks[0];
-    const uint32_t cap = d.num_pool_bricks;
-    for (uint32_t e = blockIdx.x; e < active; e += gridDim.x) {
-        const uint32_t brick = d.active_bricks[1u + e];
-        const uint32_t slot = __ldg(d.brick_table + brick);
-        const int3 bc = brick_coord_of(d, brick);
-        double a0[2] = {0.0, 0.0}, a1[2] = {0.0, 0.0};
-#pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            const uint32_t l = threadIdx.x + uint32_t(k) * 256u;
-            const int3 lc = local_coord_of(l);
-            const int3 c = make_int3(bc.x * 8 + lc.x, bc.y * 8 + lc.y, bc.z * 8 + lc.z);
-            if (in_grid(d, c)) fn(slot * BRICK_CELLS + l, c, a0[k], a1[k]);
-        }
-        const double t0 = brick_reduce(a0[0] + a0[1], sm.w8);
-        if (threadIdx.x == 0) m.partials[e] = t0;
-        if (NDOT > 1) {
-            const double t1 = brick_reduce(a1[0] + a1[1], sm.w8);
-            if (threadIdx.x == 0) m.partials[cap + e] = t1;
-        }
-    }
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) sm.last = (atomicAdd(m.counters + counter, 1u) == gridDim.x - 1u) ? 1u : 0u;
-    __syncthreads();
-    if (sm.last) {
-        __threadfence();
-        const double r0 = final_reduce(m.partials, active, sm);
-        __syncthreads();
-        double r1 = 0.0;
-        if (NDOT > 1) r1 = final_reduce(m.partials + cap, active, sm);
-        if (threadIdx.x == 0) {
-            store(r0, r1);
-            m.counters[counter] = 0u;
-        }
-    }
-}
-
 // Visits the cells of level l (1..3) that lie in the active bricks' footprints: fn(ci, c). Levels
 // whose cells are coarser than a brick are scanned densely.
 template <class Fn>
@@ -164,16 +120,69 @@ __device__ __forceinline__ uint32_t l0_nbr(uint32_t i, uint32_t l, int n, const 
     }
 }
 // Sum of buf over the fluid neighbours, in neighbour order (non-fluid neighbours are skipped, not
-// added as zero, so the rounding is the reference's).
+// added as zero, so the rounding is the reference's). Every neighbour index is in bounds (a missing
+// neighbour brick resolves to the null slot), so all six loads are issued unconditionally.
 __device__ __forceinline__ float l0_sum(const float* buf, uint32_t w, uint32_t i, uint32_t l, const uint32_t* ns) {
     float v[6];
 #pragma unroll
-    for (int n = 0; n < 6; ++n) v[n] = ((w >> n) & 1u) ? buf[l0_nbr(i, l, n, ns)] : 0.0f;
+    for (int n = 0; n < 6; ++n) v[n] = buf[l0_nbr(i, l, n, ns)];
     float sum = 0.0f;
 #pragma unroll
     for (int n = 0; n < 6; ++n)
         if ((w >> n) & 1u) sum = sum + v[n];
     return sum;
+}
+
+// Level-0 pass, one warp per active brick: lane t visits cells t, t + 32, ..., t + 480 of the brick, so
+// every load instruction of the warp covers 32 consecutive cells, and the brick's dot-product partial
+// is the lane sums folded by warp shuffles (the canonical tree). nbr_slots[8 e + 0..5] are the face
+// neighbours' slots, [8 e + 6] the brick's own slot (stored by PCGInit). fn(i, l, ns, v0, v1) handles
+// one cell; the last CTA to finish reduces the partials and calls store(t0, t1) in thread 0.
+template <int NDOT, class Fn, class Store>
+__device__ __forceinline__ void w0_pass(const Dev& d, const MGState& m, uint32_t counter, Fn fn, Store store) {
+    __shared__ DotSmem sm;
+    const uint32_t active = d.active_bricks[0];
+    const uint32_t cap = d.num_pool_bricks;
+    const uint32_t lane = threadIdx.x & 31u, wpb = blockDim.x >> 5;
+    for (uint32_t e = blockIdx.x * wpb + (threadIdx.x >> 5); e < active; e += gridDim.x * wpb) {
+        const uint4 s0 = *reinterpret_cast<const uint4*>(m.nbr_slots + 8u * e);
+        const uint4 s1 = *reinterpret_cast<const uint4*>(m.nbr_slots + 8u * e + 4u);
+        const uint32_t ns[6] = {s0.x, s0.y, s0.z, s0.w, s1.x, s1.y};
+        const uint32_t base = s1.z * BRICK_CELLS;
+        double acc0 = 0.0, acc1 = 0.0;
+#pragma unroll 4
+        for (uint32_t k = 0; k < 16u; ++k) {
+            const uint32_t l = lane + 32u * k;
+            double v0 = 0.0, v1 = 0.0;
+            fn(base + l, l, ns, v0, v1);
+            acc0 = acc0 + v0;
+            acc1 = acc1 + v1;
+        }
+        if (NDOT > 0) {
+            const double t0 = warp_fold(acc0);
+            if (lane == 0) m.partials[e] = t0;
+        }
+        if (NDOT > 1) {
+            const double t1 = warp_fold(acc1);
+            if (lane == 0) m.partials[cap + e] = t1;
+        }
+    }
+    if (NDOT == 0) return;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) sm.last = (atomicAdd(m.counters + counter, 1u) == gridDim.x - 1u) ? 1u : 0u;
+    __syncthreads();
+    if (sm.last) {
+        __threadfence();
+        const double r0 = final_reduce(m.partials, active, sm);
+        __syncthreads();
+        double r1 = 0.0;
+        if (NDOT > 1) r1 = final_reduce(m.partials + cap, active, sm);
+        if (threadIdx.x == 0) {
+            store(r0, r1);
+            m.counters[counter] = 0u;
+        }
+    }
 }
 
 // Level-0 pass over all 512 cells of every active brick; fn(i, l, e, ns, v0, v1) handles one cell
@@ -220,6 +229,94 @@ __device__ __forceinline__ void l0_pass(const Dev& d, const MGState& m, uint32_t
             m.counters[counter] = 0u;
         }
     }
+}
+
+// Batched form of w0_pass: for each group of B cells of a lane, load(i, l, ns) gathers everything a cell
+// needs into a value struct first, then apply(i, l, vals, v0, v1) computes and stores. All loads of the
+// group are issued before any of its stores, so they overlap (plain pointers may alias, which otherwise
+// keeps the compiler from hoisting the next cell's loads above this cell's stores).
+template <int NDOT, int B, class Load, class Apply, class Store>
+__device__ __forceinline__ void w0_batched(const Dev& d, const MGState& m, uint32_t counter, Load load, Apply apply, Store store) {
+    __shared__ DotSmem sm;
+    const uint32_t active = d.active_bricks[0];
+    const uint32_t cap = d.num_pool_bricks;
+    const uint32_t lane = threadIdx.x & 31u, wpb = blockDim.x >> 5;
+    for (uint32_t e = blockIdx.x * wpb + (threadIdx.x >> 5); e < active; e += gridDim.x * wpb) {
+        const uint4 s0 = *reinterpret_cast<const uint4*>(m.nbr_slots + 8u * e);
+        const uint4 s1 = *reinterpret_cast<const uint4*>(m.nbr_slots + 8u * e + 4u);
+        const uint32_t ns[6] = {s0.x, s0.y, s0.z, s0.w, s1.x, s1.y};
+        const uint32_t base = s1.z * BRICK_CELLS;
+        double acc0 = 0.0, acc1 = 0.0;
+        for (uint32_t k0 = 0; k0 < 16u; k0 += B) {
+            decltype(load(0u, 0u, ns)) vals[B];
+#pragma unroll
+            for (int b = 0; b < B; ++b) {
+                const uint32_t l = lane + 32u * (k0 + uint32_t(b));
+                vals[b] = load(base + l, l, ns);
+            }
+#pragma unroll
+            for (int b = 0; b < B; ++b) {
+                const uint32_t l = lane + 32u * (k0 + uint32_t(b));
+                double v0 = 0.0, v1 = 0.0;
+                apply(base + l, l, vals[b], v0, v1);
+                acc0 = acc0 + v0;
+                acc1 = acc1 + v1;
+            }
+        }
+        if (NDOT > 0) {
+            const double t0 = warp_fold(acc0);
+            if (lane == 0) m.partials[e] = t0;
+        }
+        if (NDOT > 1) {
+            const double t1 = warp_fold(acc1);
+            if (lane == 0) m.partials[cap + e] = t1;
+        }
+    }
+    if (NDOT == 0) return;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) sm.last = (atomicAdd(m.counters + counter, 1u) == gridDim.x - 1u) ? 1u : 0u;
+    __syncthreads();
+    if (sm.last) {
+        __threadfence();
+        const double r0 = final_reduce(m.partials, active, sm);
+        __syncthreads();
+        double r1 = 0.0;
+        if (NDOT > 1) r1 = final_reduce(m.partials + cap, active, sm);
+        if (threadIdx.x == 0) {
+            store(r0, r1);
+            m.counters[counter] = 0u;
+        }
+    }
+}
+
+struct Nb6 {
+    uint32_t w;
+    float c0, c1, c2;
+    float n[6];
+};
+struct Nb12 {
+    uint32_t w;
+    float c0, c1, c2;
+    float n[6], m[6];
+};
+__device__ __forceinline__ Nb6 load_nb6(const float* buf, const float* a, const float* b, const float* c, const uint8_t* word,
+                                        uint32_t i, uint32_t l, const uint32_t* ns) {
+    Nb6 v;
+    v.w = word[i];
+    v.c0 = a[i];
+    v.c1 = b[i];
+    v.c2 = c[i];
+#pragma unroll
+    for (int n = 0; n < 6; ++n) v.n[n] = buf[l0_nbr(i, l, n, ns)];
+    return v;
+}
+__device__ __forceinline__ float nb_sum(const float* v, uint32_t w) {
+    float sum = 0.0f;
+#pragma unroll
+    for (int n = 0; n < 6; ++n)
+        if ((w >> n) & 1u) sum = sum + v[n];
+    return sum;
 }
 
 __device__ __forceinline__ float ratio_f(double num, double den) { return fabs(den) > 1e-30 ? float(num / den) : 0.0f; }
@@ -291,22 +388,26 @@ __device__ __forceinline__ float word_sum(const float* x, uint32_t w, uint32_t i
 }
 
 // ---- PCGInitCS (+ ||r0||^2 and ||b||^2, and the decision whether any iteration runs) ----------------------
-// Also stores the solve's stencil words and the active bricks' neighbour slots.
-__global__ void __launch_bounds__(GRID_THREADS) k_pcg_init(Dev d, MGState m, const float* __restrict__ p, const float* __restrict__ div,
-                                                           unsigned long long handle) {
+// First stores the solve's stencil words and each active brick's neighbour and own slots; the residual
+// pass itself reads the cell types directly (its neighbours' words may not be written yet).
+__global__ void __launch_bounds__(GRID_THREADS) k_pcg_words(Dev d, MGState m) {
     const uint32_t active = d.active_bricks[0];
-    for (uint32_t e = blockIdx.x; e < active; e += gridDim.x) {
+    const uint32_t lane = threadIdx.x & 31u, wpb = blockDim.x >> 5;
+    for (uint32_t e = blockIdx.x * wpb + (threadIdx.x >> 5); e < active; e += gridDim.x * wpb) {
         const uint32_t brick = d.active_bricks[1u + e];
         const uint32_t slot = __ldg(d.brick_table + brick);
         const int3 bc = brick_coord_of(d, brick);
-        if (threadIdx.x < 6) {
-            const int3 nb = add3(bc, nbr_off(int(threadIdx.x)));
+        if (lane < 6) {
+            const int3 nb = add3(bc, nbr_off(int(lane)));
             const bool in = nb.x >= 0 && nb.y >= 0 && nb.z >= 0 && nb.x < d.brick_dim.x && nb.y < d.brick_dim.y && nb.z < d.brick_dim.z;
-            m.nbr_slots[8u * e + threadIdx.x] = in ? __ldg(d.brick_table + brick_index_of(d, nb)) : 0u;
+            m.nbr_slots[8u * e + lane] = in ? __ldg(d.brick_table + brick_index_of(d, nb)) : 0u;
+        } else if (lane == 6) {
+            m.nbr_slots[8u * e + 6u] = slot;
+        } else if (lane == 7) {
+            m.nbr_slots[8u * e + 7u] = brick;
         }
-#pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            const uint32_t l = threadIdx.x + uint32_t(k) * 256u;
+        for (uint32_t k = 0; k < 16u; ++k) {
+            const uint32_t l = lane + 32u * k;
             const int3 lc = local_coord_of(l);
             const int3 c = make_int3(bc.x * 8 + lc.x, bc.y * 8 + lc.y, bc.z * 8 + lc.z);
             uint32_t w = 0u;
@@ -323,17 +424,22 @@ __global__ void __launch_bounds__(GRID_THREADS) k_pcg_init(Dev d, MGState m, con
             m.word[slot * BRICK_CELLS + l] = uint8_t(w);
         }
     }
-    level0_dot_pass<2>(d, m, 0,
-        [&](uint32_t i, int3 c, double& v0, double& v1) {
-            if ((d.cell_type[i] & CELL_TYPE_MASK) != CELL_FLUID) {
-                m.r[i] = 0.0f; m.z[i] = 0.0f;
+}
+__global__ void __launch_bounds__(GRID_THREADS) k_pcg_init(Dev d, MGState m, const float* __restrict__ p, const float* __restrict__ div,
+                                                           unsigned long long handle) {
+    w0_pass<2>(d, m, 0,
+        [&](uint32_t i, uint32_t l, const uint32_t* ns, double& v0, double& v1) {
+            const uint32_t w = m.word[i];
+            if (!(w & W_FLUID)) {
+                m.r[i] = 0.0f;
+                m.z[i] = 0.0f;
                 return;
             }
-            float diag, sum;
-            stencil0(d, p, i, c, diag, sum);
+            const float diag = d.cell_diag[i] + DIAG_EPSILON;
+            const float sum = l0_sum(p, w, i, l, ns);
             const float ri = -div[i] - (diag * p[i] - sum);
             m.r[i] = ri;
-            m.z[i] = is_red(c) ? ri / diag : 0.0f;
+            m.z[i] = (w & W_RED) ? ri / diag : 0.0f;
             v0 = double(ri * ri);
             const float b = -div[i];
             v1 = double(b * b);
@@ -352,31 +458,27 @@ __global__ void __launch_bounds__(GRID_THREADS) k_pcg_init(Dev d, MGState m, con
 __global__ void __launch_bounds__(GRID_THREADS) k_smooth0(Dev d, MGState m, uint32_t parity, int dot) {
     if (solve_done(m)) return;
     const uint32_t want_red = parity == 0u ? W_RED : 0u;
+    // c0 = r (b of the level), c1 = z, c2 = diagonal
+    auto load = [&](uint32_t i, uint32_t l, const uint32_t* ns) { return load_nb6(m.z, m.r, m.z, d.cell_diag, m.word, i, l, ns); };
     if (dot) {
-        l0_pass<1>(d, m, 1,
-            [&](uint32_t i, uint32_t l, uint32_t, const uint32_t* ns, double& v0, double&) {
-                const uint32_t w = m.word[i];
-                if (!(w & W_FLUID)) return;
-                if ((w & W_RED) == want_red) {
-                    const float sum = l0_sum(m.z, w, i, l, ns);
-                    const float diag = d.cell_diag[i] + DIAG_EPSILON;
-                    const float b = m.r[i];
-                    const float x = (b + sum) / diag;
+        w0_batched<1, 4>(d, m, 1, load,
+            [&](uint32_t i, uint32_t, const Nb6& v, double& v0, double&) {
+                if (!(v.w & W_FLUID)) return;
+                if ((v.w & W_RED) == want_red) {
+                    const float x = (v.c0 + nb_sum(v.n, v.w)) / (v.c2 + DIAG_EPSILON);
                     m.z[i] = x;
-                    v0 = double(b * x);
+                    v0 = double(v.c0 * x);
                 } else {
-                    v0 = double(m.r[i] * m.z[i]);
+                    v0 = double(v.c0 * v.c1);
                 }
             },
             [&](double rho, double) { m.scalars[3] = m.scalars[0]; m.scalars[0] = rho; });
         return;
     }
-    l0_pass<0>(d, m, 0,
-        [&](uint32_t i, uint32_t l, uint32_t, const uint32_t* ns, double&, double&) {
-            const uint32_t w = m.word[i];
-            if (!(w & W_FLUID) || (w & W_RED) != want_red) return;
-            const float sum = l0_sum(m.z, w, i, l, ns);
-            m.z[i] = (m.r[i] + sum) / (d.cell_diag[i] + DIAG_EPSILON);
+    w0_batched<0, 4>(d, m, 0, load,
+        [&](uint32_t i, uint32_t, const Nb6& v, double&, double&) {
+            if (!(v.w & W_FLUID) || (v.w & W_RED) != want_red) return;
+            m.z[i] = (v.c0 + nb_sum(v.n, v.w)) / (v.c2 + DIAG_EPSILON);
         },
         [&](double, double) {});
 }
@@ -389,17 +491,17 @@ __global__ void __launch_bounds__(GRID_THREADS) k_prolong_smooth0(Dev d, MGState
     if (solve_done(m)) return;
     const MGLevel C = m.lv[1];
     const uint32_t active = d.active_bricks[0];
-    for (uint32_t e = blockIdx.x; e < active; e += gridDim.x) {
-        const uint32_t brick = d.active_bricks[1u + e];
-        const uint32_t slot = __ldg(d.brick_table + brick);
-        const int3 bc = brick_coord_of(d, brick);
-        uint32_t ns[6];
-#pragma unroll
-        for (int n = 0; n < 6; ++n) ns[n] = m.nbr_slots[8u * e + uint32_t(n)];
-#pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            const uint32_t l = threadIdx.x + uint32_t(k) * 256u;
-            const uint32_t i = slot * BRICK_CELLS + l;
+    const uint32_t lane = threadIdx.x & 31u, wpb = blockDim.x >> 5;
+    for (uint32_t e = blockIdx.x * wpb + (threadIdx.x >> 5); e < active; e += gridDim.x * wpb) {
+        const uint4 s0 = *reinterpret_cast<const uint4*>(m.nbr_slots + 8u * e);
+        const uint4 s1 = *reinterpret_cast<const uint4*>(m.nbr_slots + 8u * e + 4u);
+        const uint32_t ns[6] = {s0.x, s0.y, s0.z, s0.w, s1.x, s1.y};
+        const uint32_t base = s1.z * BRICK_CELLS;
+        const int3 bc = brick_coord_of(d, s1.w);
+#pragma unroll 2
+        for (uint32_t k = 0; k < 16u; ++k) {
+            const uint32_t l = lane + 32u * k;
+            const uint32_t i = base + l;
             const uint32_t w = m.word[i];
             if (!(w & W_FLUID) || (w & W_RED)) continue;
             const int3 lc = local_coord_of(l);
@@ -410,7 +512,7 @@ __global__ void __launch_bounds__(GRID_THREADS) k_prolong_smooth0(Dev d, MGState
                 v[n] = 0.0f;
                 if (!((w >> n) & 1u)) continue;
                 const int3 nb = add3(c, nbr_off(n));
-                const uint32_t pi = lin3(make_int3(nb.x / 2, nb.y / 2, nb.z / 2), C.dim);
+                const uint32_t pi = lin3(make_int3(nb.x >> 1, nb.y >> 1, nb.z >> 1), C.dim);
                 const float zn = m.z[l0_nbr(i, l, n, ns)];
                 v[n] = (C.word[pi] & CW_FLUID) ? zn + C.x[pi] : zn;
             }
@@ -422,7 +524,6 @@ __global__ void __launch_bounds__(GRID_THREADS) k_prolong_smooth0(Dev d, MGState
         }
     }
 }
-
 
 // Levels 1..3 through the active-brick footprints, with the per-solve stencil words.
 __global__ void k_smooth_fp(Dev d, MGState m, int l, uint32_t parity) {
@@ -494,58 +595,58 @@ __global__ void k_prolong_smooth_fp(Dev d, MGState m, int l) {
 }
 
 // ---- MGRestrictCS level 0 -> 1 over the 4^3 level-1 cells of every active brick (SparseCoarse) -----------
-// A brick pass: each thread forms the fine residual of its 2 cells in shared memory, then 64 threads sum
-// each coarse cell's fluid children in child order (x fastest), as the per-coarse-cell loop does.
+// One warp per brick: the lanes form the fine residuals of the brick's 512 cells in warp-private shared
+// memory, then sum each of the 64 coarse cells' fluid children in child order (x fastest), as the
+// per-coarse-cell loop does.
 __global__ void __launch_bounds__(GRID_THREADS) k_restrict0(Dev d, MGState m) {
     if (solve_done(m)) return;
-    __shared__ float s_res[BRICK_CELLS];
-    __shared__ uint8_t s_fluid[BRICK_CELLS];
+    constexpr int WARPS = GRID_THREADS / 32;
+    __shared__ float s_res[WARPS][BRICK_CELLS];
+    __shared__ uint8_t s_fluid[WARPS][BRICK_CELLS];
     const MGLevel C = m.lv[1];
     const uint32_t active = d.active_bricks[0];
-    for (uint32_t e = blockIdx.x; e < active; e += gridDim.x) {
-        const uint32_t brick = d.active_bricks[1u + e];
-        const uint32_t slot = __ldg(d.brick_table + brick);
-        uint32_t ns[6];
-#pragma unroll
-        for (int n = 0; n < 6; ++n) ns[n] = m.nbr_slots[8u * e + uint32_t(n)];
-#pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            const uint32_t l = threadIdx.x + uint32_t(k) * 256u;
-            const uint32_t i = slot * BRICK_CELLS + l;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+    for (uint32_t e = blockIdx.x * wpb + warp; e < active; e += gridDim.x * wpb) {
+        const uint4 s0 = *reinterpret_cast<const uint4*>(m.nbr_slots + 8u * e);
+        const uint4 s1 = *reinterpret_cast<const uint4*>(m.nbr_slots + 8u * e + 4u);
+        const uint32_t ns[6] = {s0.x, s0.y, s0.z, s0.w, s1.x, s1.y};
+        const uint32_t base = s1.z * BRICK_CELLS;
+#pragma unroll 4
+        for (uint32_t k = 0; k < 16u; ++k) {
+            const uint32_t l = lane + 32u * k;
+            const uint32_t i = base + l;
             const uint32_t w = m.word[i];
-            s_fluid[l] = (w & W_FLUID) ? 1 : 0;
-            if (w & W_FLUID) {
-                const float nbsum = l0_sum(m.z, w, i, l, ns);
-                const float diag = d.cell_diag[i] + DIAG_EPSILON;
-                s_res[l] = m.r[i] - (diag * m.z[i] - nbsum);
-            }
+            const float ri = m.r[i], zi = m.z[i], diag = d.cell_diag[i] + DIAG_EPSILON;
+            const float nbsum = l0_sum(m.z, w, i, l, ns);
+            s_fluid[warp][l] = (w & W_FLUID) ? 1 : 0;
+            if (w & W_FLUID) s_res[warp][l] = ri - (diag * zi - nbsum);
         }
-        __syncthreads();
-        if (threadIdx.x < 64) {
-            const int3 bc = brick_coord_of(d, brick);
-            const uint32_t lc = threadIdx.x;
+        __syncwarp();
+        const int3 bc = brick_coord_of(d, s1.w);
+#pragma unroll
+        for (uint32_t h = 0; h < 2u; ++h) {
+            const uint32_t lc = lane + 32u * h;
             const int3 cl = make_int3(int(lc & 3u), int((lc >> 2) & 3u), int(lc >> 4));
             const int3 c = make_int3(bc.x * 4 + cl.x, bc.y * 4 + cl.y, bc.z * 4 + cl.z);
-            if (inside3(c, C.dim)) {
-                const uint32_t ci = lin3(c, C.dim);
-                const uint32_t cw = C.word[ci];
-                if (!(cw & CW_FLUID)) {
-                    C.b[ci] = 0.0f;
-                    C.x[ci] = 0.0f;
-                } else {
-                    float sum = 0.0f;
-#pragma unroll
-                    for (int o = 0; o < 8; ++o) {
-                        const uint32_t fl = uint32_t((2 * cl.x + (o & 1)) + 8 * ((2 * cl.y + ((o >> 1) & 1)) + 8 * (2 * cl.z + ((o >> 2) & 1))));
-                        if (s_fluid[fl]) sum = sum + s_res[fl];
-                    }
-                    const float bb = 0.25f * sum;
-                    C.b[ci] = bb;
-                    C.x[ci] = (cw & CW_RED) ? bb / word_diag(cw) : 0.0f;
-                }
+            if (!inside3(c, C.dim)) continue;
+            const uint32_t ci = lin3(c, C.dim);
+            const uint32_t cw = C.word[ci];
+            if (!(cw & CW_FLUID)) {
+                C.b[ci] = 0.0f;
+                C.x[ci] = 0.0f;
+                continue;
             }
+            float sum = 0.0f;
+#pragma unroll
+            for (int o = 0; o < 8; ++o) {
+                const uint32_t fl = uint32_t((2 * cl.x + (o & 1)) + 8 * ((2 * cl.y + ((o >> 1) & 1)) + 8 * (2 * cl.z + ((o >> 2) & 1))));
+                if (s_fluid[warp][fl]) sum = sum + s_res[warp][fl];
+            }
+            const float bb = 0.25f * sum;
+            C.b[ci] = bb;
+            C.x[ci] = (cw & CW_RED) ? bb / word_diag(cw) : 0.0f;
         }
-        __syncthreads();
+        __syncwarp();
     }
 }
 
@@ -736,25 +837,30 @@ __global__ void __launch_bounds__(GRID_THREADS) k_apply_a(Dev d, MGState m) {
     const float beta = first ? 0.0f : ratio_f(m.scalars[0], m.scalars[3]);
     const float* dold = dir_buf(m, it & 1u);
     float* dnew = dir_buf(m, (it + 1u) & 1u);
-    l0_pass<1>(d, m, 2,
-        [&](uint32_t i, uint32_t l, uint32_t, const uint32_t* ns, double& v0, double&) {
-            const uint32_t w = m.word[i];
-            if (!(w & W_FLUID)) return;
-            const float dn = first ? m.z[i] : m.z[i] + beta * dold[i];
-            dnew[i] = dn;
-            float v[6];
+    w0_batched<1, 4>(d, m, 2,
+        [&](uint32_t i, uint32_t l, const uint32_t* ns) {
+            Nb12 v;
+            v.w = m.word[i];
+            v.c0 = m.z[i];
+            v.c1 = dold[i];
+            v.c2 = d.cell_diag[i];
 #pragma unroll
             for (int n = 0; n < 6; ++n) {
-                v[n] = 0.0f;
-                if (!((w >> n) & 1u)) continue;
                 const uint32_t ni = l0_nbr(i, l, n, ns);
-                v[n] = first ? m.z[ni] : m.z[ni] + beta * dold[ni];
+                v.n[n] = m.z[ni];
+                v.m[n] = dold[ni];
             }
+            return v;
+        },
+        [&](uint32_t i, uint32_t, const Nb12& v, double& v0, double&) {
+            if (!(v.w & W_FLUID)) return;
+            const float dn = first ? v.c0 : v.c0 + beta * v.c1;
             float sum = 0.0f;
 #pragma unroll
             for (int n = 0; n < 6; ++n)
-                if ((w >> n) & 1u) sum = sum + v[n];
-            const float qi = (d.cell_diag[i] + DIAG_EPSILON) * dn - sum;
+                if ((v.w >> n) & 1u) sum = sum + (first ? v.n[n] : v.n[n] + beta * v.m[n]);
+            dnew[i] = dn;
+            const float qi = (v.c2 + DIAG_EPSILON) * dn - sum;
             m.q[i] = qi;
             v0 = double(dn * qi);
         },
@@ -762,19 +868,31 @@ __global__ void __launch_bounds__(GRID_THREADS) k_apply_a(Dev d, MGState m) {
 }
 
 // ---- PCGUpdatePRCS: p += alpha d, r -= alpha q, red pre-smooth; ||r||^2 and the loop decision -------------
+struct PR {
+    uint32_t w;
+    float p, d, r, q, diag;
+};
 __global__ void __launch_bounds__(GRID_THREADS) k_update_pr(Dev d, MGState m, float* __restrict__ p, unsigned long long handle) {
     if (solve_done(m)) return;
     const float alpha = ratio_f(m.scalars[0], m.scalars[2]);
     const float* dcur = dir_buf(m, (m.ctl[0] + 1u) & 1u);
-    l0_pass<1>(d, m, 3,
-        [&](uint32_t i, uint32_t, uint32_t, const uint32_t*, double& v0, double&) {
-            const uint32_t w = m.word[i];
-            if (!(w & W_FLUID)) return;
-            p[i] = p[i] + alpha * dcur[i];
-            const float ri = m.r[i] - alpha * m.q[i];
+    w0_batched<1, 8>(d, m, 3,
+        [&](uint32_t i, uint32_t, const uint32_t*) {
+            PR v;
+            v.w = m.word[i];
+            v.p = p[i];
+            v.d = dcur[i];
+            v.r = m.r[i];
+            v.q = m.q[i];
+            v.diag = d.cell_diag[i];
+            return v;
+        },
+        [&](uint32_t i, uint32_t, const PR& v, double& v0, double&) {
+            if (!(v.w & W_FLUID)) return;
+            p[i] = v.p + alpha * v.d;
+            const float ri = v.r - alpha * v.q;
             m.r[i] = ri;
-            const float diag = d.cell_diag[i] + DIAG_EPSILON;
-            m.z[i] = (w & W_RED) ? ri / diag : 0.0f;
+            m.z[i] = (v.w & W_RED) ? ri / (v.diag + DIAG_EPSILON) : 0.0f;
             v0 = double(ri * ri);
         },
         [&](double rr, double) {
@@ -794,12 +912,12 @@ __global__ void __launch_bounds__(GRID_THREADS) k_update_pr(Dev d, MGState m, fl
 // ---- ||b - A p||^2 and ||b||^2 of a finished solve (diagnostic) ---------------------------------------------
 __global__ void __launch_bounds__(GRID_THREADS) k_true_residual(Dev d, MGState m, const float* __restrict__ p,
                                                                 const float* __restrict__ div) {
-    level0_dot_pass<2>(d, m, 4,
-        [&](uint32_t i, int3 c, double& v0, double& v1) {
-            if ((d.cell_type[i] & CELL_TYPE_MASK) != CELL_FLUID) return;
-            float diag, sum;
-            stencil0(d, p, i, c, diag, sum);
-            const float r = -div[i] - (diag * p[i] - sum);
+    w0_pass<2>(d, m, 4,
+        [&](uint32_t i, uint32_t l, const uint32_t* ns, double& v0, double& v1) {
+            const uint32_t w = m.word[i];
+            if (!(w & W_FLUID)) return;
+            const float diag = d.cell_diag[i] + DIAG_EPSILON;
+            const float r = -div[i] - (diag * p[i] - l0_sum(p, w, i, l, ns));
             v0 = double(r * r);
             const float b = -div[i];
             v1 = double(b * b);
@@ -834,8 +952,9 @@ int launch_mg_build_type(const Dev& d, const MGState& m, int l, cudaStream_t s) 
 }
 int launch_pcg_init(const Dev& d, const MGState& m, const float* p, const float* div, unsigned long long handle, const Shape& sh,
                     cudaStream_t s) {
+    k_pcg_words<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, m);
     k_pcg_init<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, m, p, div, handle);
-    return 1;
+    return 2;
 }
 
 size_t mg_tail_smem(const MGState& m) {

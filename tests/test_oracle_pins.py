@@ -272,13 +272,15 @@ def test_canonical_reductions(oracle_mod):
     lib = oracle_mod.lib()
     rng = np.random.default_rng(9)
     v = rng.normal(size=512) * 10.0 ** rng.integers(-8, 8, size=512)
-    s = v[:256] + v[256:]
-    total = None
-    for w in range(8):
-        lane = s[32 * w:32 * w + 32].copy()
-        for off in (16, 8, 4, 2, 1):
-            lane[:off] = lane[:off] + lane[off:2 * off]
-        total = lane[0] if w == 0 else total + lane[0]
+    lanes = np.zeros(32)
+    for t in range(32):
+        acc = 0.0
+        for k in range(16):
+            acc = acc + v[t + 32 * k]
+        lanes[t] = acc
+    for off in (16, 8, 4, 2, 1):
+        lanes[:off] = lanes[:off] + lanes[off:2 * off]
+    total = lanes[0]
     vv = np.ascontiguousarray(v)
     assert lib.oracle_reduce_brick(vv.ctypes.data) == total
     for n in (1, 7, 1024, 3000, 7001):
