@@ -58,13 +58,27 @@ struct DotSmem {
 // Final reduction over n brick partials: lanes t = 0..1023 sum entries t, t + 1024, ... in order, each
 // group of 32 lanes folds with shfl_down 16..1, and the 32 group results are added in order.
 __device__ double final_reduce(const double* partials, uint32_t n, DotSmem& sm) {
+    // Thread x owns lanes x + 256 k (k = 0..3); lane t adds partials t, t + 1024, ... in that order.
+    // The loads of four 1024-partial rounds are issued before any of them is added, so the pass costs
+    // about one L2 round trip per 4096 partials instead of one per partial of a lane.
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    for (uint32_t base = 0; base < n; base += 4096u) {
+        double v[4][4];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const uint32_t t = threadIdx.x + 256u * uint32_t(k);
-        double acc = 0.0;
-        for (uint32_t e = t; e < n; e += 1024u) acc = acc + __ldcg(partials + e);
-        sm.lanes[t] = acc;
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const uint32_t e = base + 1024u * uint32_t(r) + threadIdx.x + 256u * uint32_t(k);
+                v[r][k] = e < n ? __ldcg(partials + e) : 0.0;
+            }
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (base + 1024u * uint32_t(r) + threadIdx.x + 256u * uint32_t(k) < n) acc[k] = acc[k] + v[r][k];
     }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) sm.lanes[threadIdx.x + 256u * uint32_t(k)] = acc[k];
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -290,6 +304,40 @@ __device__ __forceinline__ void w0_batched(const Dev& d, const MGState& m, uint3
     }
 }
 
+// The 256 black cells ((x + y + z) odd) of every active brick, one warp per brick, 8 cells per lane:
+// round k takes plane z = k, row y = lane >> 2 and x = 2 (lane & 3) + ((y + z + 1) & 1), so no lane
+// idles on a red cell. prep(brick, lane) runs once per brick before its cells (all lanes of the warp);
+// the loads of a group of B cells are issued before any of them is applied.
+__device__ __forceinline__ uint32_t black_local(uint32_t lane, uint32_t k) {
+    const uint32_t y = lane >> 2;
+    return 2u * (lane & 3u) + ((y + k + 1u) & 1u) + 8u * y + 64u * k;
+}
+template <int B, class Prep, class Load, class Apply>
+__device__ __forceinline__ void w0_black(const Dev& d, const MGState& m, Prep prep, Load load, Apply apply) {
+    const uint32_t active = d.active_bricks[0];
+    const uint32_t lane = threadIdx.x & 31u, wpb = blockDim.x >> 5;
+    for (uint32_t e = blockIdx.x * wpb + (threadIdx.x >> 5); e < active; e += gridDim.x * wpb) {
+        const uint4 s0 = *reinterpret_cast<const uint4*>(m.nbr_slots + 8u * e);
+        const uint4 s1 = *reinterpret_cast<const uint4*>(m.nbr_slots + 8u * e + 4u);
+        const uint32_t ns[6] = {s0.x, s0.y, s0.z, s0.w, s1.x, s1.y};
+        const uint32_t base = s1.z * BRICK_CELLS;
+        prep(s1.w, lane);
+        for (uint32_t k0 = 0; k0 < 8u; k0 += B) {
+            decltype(load(0u, 0u, ns)) vals[B];
+#pragma unroll
+            for (int b = 0; b < B; ++b) {
+                const uint32_t l = black_local(lane, k0 + uint32_t(b));
+                vals[b] = load(base + l, l, ns);
+            }
+#pragma unroll
+            for (int b = 0; b < B; ++b) {
+                const uint32_t l = black_local(lane, k0 + uint32_t(b));
+                apply(base + l, l, vals[b]);
+            }
+        }
+    }
+}
+
 struct Nb6 {
     uint32_t w;
     float c0, c1, c2;
@@ -455,74 +503,97 @@ __global__ void __launch_bounds__(GRID_THREADS) k_pcg_init(Dev d, MGState m, con
 }
 
 // ---- MGSmoothCS on level 0 (z as x, r as b); with dot the r.z reduction shifts rho -----------------------
-__global__ void __launch_bounds__(GRID_THREADS) k_smooth0(Dev d, MGState m, uint32_t parity, int dot) {
+// What a black sweep reads of a cell: word, r, diagonal and the six neighbours' z (c1 unused).
+__device__ __forceinline__ Nb6 load_black(const Dev& d, const MGState& m, uint32_t i, uint32_t l, const uint32_t* ns) {
+    Nb6 v;
+    v.w = m.word[i];
+    v.c0 = m.r[i];
+    v.c1 = 0.0f;
+    v.c2 = d.cell_diag[i];
+#pragma unroll
+    for (int n = 0; n < 6; ++n) v.n[n] = m.z[l0_nbr(i, l, n, ns)];
+    return v;
+}
+
+// Red sweep with rho = r . z over all cells (red: the new value, black: the current z).
+__global__ void __launch_bounds__(GRID_THREADS) k_smooth0(Dev d, MGState m) {
     if (solve_done(m)) return;
-    const uint32_t want_red = parity == 0u ? W_RED : 0u;
     // c0 = r (b of the level), c1 = z, c2 = diagonal
-    auto load = [&](uint32_t i, uint32_t l, const uint32_t* ns) { return load_nb6(m.z, m.r, m.z, d.cell_diag, m.word, i, l, ns); };
-    if (dot) {
-        w0_batched<1, 4>(d, m, 1, load,
-            [&](uint32_t i, uint32_t, const Nb6& v, double& v0, double&) {
-                if (!(v.w & W_FLUID)) return;
-                if ((v.w & W_RED) == want_red) {
-                    const float x = (v.c0 + nb_sum(v.n, v.w)) / (v.c2 + DIAG_EPSILON);
-                    m.z[i] = x;
-                    v0 = double(v.c0 * x);
-                } else {
-                    v0 = double(v.c0 * v.c1);
-                }
-            },
-            [&](double rho, double) { m.scalars[3] = m.scalars[0]; m.scalars[0] = rho; });
-        return;
-    }
-    w0_batched<0, 4>(d, m, 0, load,
-        [&](uint32_t i, uint32_t, const Nb6& v, double&, double&) {
-            if (!(v.w & W_FLUID) || (v.w & W_RED) != want_red) return;
-            m.z[i] = (v.c0 + nb_sum(v.n, v.w)) / (v.c2 + DIAG_EPSILON);
+    w0_batched<1, 4>(d, m, 1,
+        [&](uint32_t i, uint32_t l, const uint32_t* ns) { return load_nb6(m.z, m.r, m.z, d.cell_diag, m.word, i, l, ns); },
+        [&](uint32_t i, uint32_t, const Nb6& v, double& v0, double&) {
+            if (!(v.w & W_FLUID)) return;
+            if (v.w & W_RED) {
+                const float x = (v.c0 + nb_sum(v.n, v.w)) / (v.c2 + DIAG_EPSILON);
+                m.z[i] = x;
+                v0 = double(v.c0 * x);
+            } else {
+                v0 = double(v.c0 * v.c1);
+            }
         },
-        [&](double, double) {});
+        [&](double rho, double) { m.scalars[3] = m.scalars[0]; m.scalars[0] = rho; });
+}
+
+// Black sweep (no dot product).
+__global__ void __launch_bounds__(GRID_THREADS) k_smooth0_black(Dev d, MGState m) {
+    if (solve_done(m)) return;
+    w0_black<4>(d, m, [](uint32_t, uint32_t) {},
+        [&](uint32_t i, uint32_t l, const uint32_t* ns) { return load_black(d, m, i, l, ns); },
+        [&](uint32_t i, uint32_t, const Nb6& v) {
+            if (!(v.w & W_FLUID)) return;
+            m.z[i] = (v.c0 + nb_sum(v.n, v.w)) / (v.c2 + DIAG_EPSILON);
+        });
 }
 
 // ---- MGProlongCS (level 1 -> 0) fused with the following black sweep ------------------------------
 // After the prolongation only the black sweep reads the prolonged values (of its red neighbours) and
 // it overwrites the black cells; the red sweep that follows overwrites the red cells. So the black
-// sweep reads z_n + x_c(parent of n) directly and nothing else needs to be written.
+// sweep reads z_n + x_c(parent of n) directly and nothing else needs to be written. Each warp first
+// stages the level-1 correction of its brick's 4^3 parents and their face neighbours (a 6^3 block,
+// x_c where the parent is fluid and 0 elsewhere) in shared memory. Adding +0 instead of skipping the
+// addition changes at most the sign of a zero z_n, which the neighbour sum (started at +0) absorbs.
 __global__ void __launch_bounds__(GRID_THREADS) k_prolong_smooth0(Dev d, MGState m) {
     if (solve_done(m)) return;
+    constexpr int WARPS = GRID_THREADS / 32;
+    __shared__ float s_cx[WARPS][216];
     const MGLevel C = m.lv[1];
-    const uint32_t active = d.active_bricks[0];
-    const uint32_t lane = threadIdx.x & 31u, wpb = blockDim.x >> 5;
-    for (uint32_t e = blockIdx.x * wpb + (threadIdx.x >> 5); e < active; e += gridDim.x * wpb) {
-        const uint4 s0 = *reinterpret_cast<const uint4*>(m.nbr_slots + 8u * e);
-        const uint4 s1 = *reinterpret_cast<const uint4*>(m.nbr_slots + 8u * e + 4u);
-        const uint32_t ns[6] = {s0.x, s0.y, s0.z, s0.w, s1.x, s1.y};
-        const uint32_t base = s1.z * BRICK_CELLS;
-        const int3 bc = brick_coord_of(d, s1.w);
-#pragma unroll 2
-        for (uint32_t k = 0; k < 16u; ++k) {
-            const uint32_t l = lane + 32u * k;
-            const uint32_t i = base + l;
-            const uint32_t w = m.word[i];
-            if (!(w & W_FLUID) || (w & W_RED)) continue;
-            const int3 lc = local_coord_of(l);
-            const int3 c = make_int3(bc.x * 8 + lc.x, bc.y * 8 + lc.y, bc.z * 8 + lc.z);
-            float v[6];
+    float* cx = s_cx[threadIdx.x >> 5];
+    w0_black<4>(d, m,
+        [&](uint32_t brick, uint32_t lane) {
+            const int3 bc = brick_coord_of(d, brick);
+            __syncwarp();
+            float v[7];
 #pragma unroll
-            for (int n = 0; n < 6; ++n) {
-                v[n] = 0.0f;
-                if (!((w >> n) & 1u)) continue;
-                const int3 nb = add3(c, nbr_off(n));
-                const uint32_t pi = lin3(make_int3(nb.x >> 1, nb.y >> 1, nb.z >> 1), C.dim);
-                const float zn = m.z[l0_nbr(i, l, n, ns)];
-                v[n] = (C.word[pi] & CW_FLUID) ? zn + C.x[pi] : zn;
+            for (int r = 0; r < 7; ++r) {
+                const uint32_t j = lane + 32u * uint32_t(r);
+                const int3 c = make_int3(bc.x * 4 - 1 + int(j % 6u), bc.y * 4 - 1 + int((j / 6u) % 6u), bc.z * 4 - 1 + int(j / 36u));
+                v[r] = 0.0f;
+                if (j < 216u && inside3(c, C.dim)) {
+                    const uint32_t ci = lin3(c, C.dim);
+                    const float x = C.x[ci];
+                    v[r] = (C.word[ci] & CW_FLUID) ? x : 0.0f;
+                }
             }
+#pragma unroll
+            for (int r = 0; r < 7; ++r) {
+                const uint32_t j = lane + 32u * uint32_t(r);
+                if (j < 216u) cx[j] = v[r];
+            }
+            __syncwarp();
+        },
+        [&](uint32_t i, uint32_t l, const uint32_t* ns) { return load_black(d, m, i, l, ns); },
+        [&](uint32_t i, uint32_t l, const Nb6& v) {
+            if (!(v.w & W_FLUID)) return;
+            const int x = int(l & 7u), y = int((l >> 3) & 7u), z = int(l >> 6);
+            const int p = ((x >> 1) + 1) + 6 * ((y >> 1) + 1) + 36 * ((z >> 1) + 1);
+            const int px = (x & 1) ? 1 : 0, py = (y & 1) ? 6 : 0, pz = (z & 1) ? 36 : 0;
+            const int po[6] = {p - 1 + px, p + px, p - 6 + py, p + py, p - 36 + pz, p + pz};
             float sum = 0.0f;
 #pragma unroll
             for (int n = 0; n < 6; ++n)
-                if ((w >> n) & 1u) sum = sum + v[n];
-            m.z[i] = (m.r[i] + sum) / (d.cell_diag[i] + DIAG_EPSILON);
-        }
-    }
+                if ((v.w >> n) & 1u) sum = sum + (v.n[n] + cx[po[n]]);
+            m.z[i] = (v.c0 + sum) / (v.c2 + DIAG_EPSILON);
+        });
 }
 
 // Levels 1..3 through the active-brick footprints, with the per-solve stencil words.
@@ -979,7 +1050,7 @@ int launch_vcycle(const Dev& d, const MGState& m, int coarse_iterations, const S
     const int nl = m.num_levels;
     if (nl == 1) {
         k_coarse_solve0<<<1, 1024, 0, s>>>(d, m, coarse_iterations);
-        k_smooth0<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, m, 0u, 1);
+        k_smooth0<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, m);
         return 2;
     }
     const int tail = mg_tail_level(m);
@@ -990,7 +1061,7 @@ int launch_vcycle(const Dev& d, const MGState& m, int coarse_iterations, const S
         return int(std::max<uint64_t>(1, std::min<uint64_t>(uint64_t(sh.brick_ctas), (cells + 255u) / 256u)));
     };
     int n = 0;
-    k_smooth0<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, m, 1u, 0);
+    k_smooth0_black<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, m);
     ++n;
     for (int l = 0; l < tail; ++l) {
         if (l == 0) k_restrict0<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, m);
@@ -1006,7 +1077,7 @@ int launch_vcycle(const Dev& d, const MGState& m, int coarse_iterations, const S
     for (int l = tail - 1; l >= 0; --l) {
         if (l == 0) {
             k_prolong_smooth0<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, m);
-            k_smooth0<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, m, 0u, 1);
+            k_smooth0<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, m);
         } else {
             k_prolong_smooth_fp<<<fp_blocks(l), 256, 0, s>>>(d, m, l);
             k_smooth_fp<<<fp_blocks(l), 256, 0, s>>>(d, m, l, 0u);
