@@ -306,6 +306,22 @@ SLOSH_API slosh_status slosh_end_frame(void* ctx);
 /* ---- individual phases (harness control; SloshProxy.cpp:1022-1087, 582-592) ---- */
 /* Spatial sort + compaction of the particle buffer (AddSpatialSort). */
 SLOSH_API slosh_status slosh_sort_particles(void* ctx);
+/* Allocation-free spatial sort of caller-owned device particles. No counterpart in the reference
+ * (whose sort, AddSpatialSort, only runs on the proxy's own buffers): it is for hosts that must not
+ * allocate device memory while they run. Same keys, order and outputs as slosh_sort_particles, on
+ * the current device, enqueued on cuda_stream (NULL = default stream) without waiting for it.
+ * Scratch is one static device array per device, sized for SLOSH_STATIC_SORT_MAX_PARTICLES particles
+ * and SLOSH_STATIC_SORT_MAX_KEYS sort keys (grids up to 256^3); larger inputs return
+ * SLOSH_ERR_CAPACITY. The first call on a device resolves that array's address (make it before any
+ * stream capture starts on the device). Overlapping calls on one device race on the shared scratch:
+ * order them. particles_out must not alias particles_in; perm_out (count words), key_offsets_out
+ * (sort-key count words) and live_count_out (1 word) are optional device outputs. */
+#define SLOSH_STATIC_SORT_MAX_PARTICLES 262144u
+#define SLOSH_STATIC_SORT_MAX_KEYS (262144u + 1u)
+SLOSH_API slosh_status slosh_sort_particles_static(const slosh_particle_t* particles_in, slosh_particle_t* particles_out,
+                                                   uint32_t count, const int32_t grid_dim[3], float cell_size,
+                                                   uint32_t* perm_out, uint32_t* key_offsets_out, uint32_t* live_count_out,
+                                                   void* cuda_stream);
 /* One emission request (EmitReserveCS + EmitParticlesCS, Slosh.usf:272-358). */
 SLOSH_API slosh_status slosh_emit(void* ctx, const slosh_emit_request_t* request);
 /* Sets the proxy's emission seed counter (FSloshProxy::EmitSeed, SloshProxy.h:80; starts at 1

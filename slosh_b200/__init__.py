@@ -34,6 +34,7 @@ SIGNATURES = {
     "slosh_substep": ([_VP, C.c_int32], C.c_int),
     "slosh_end_frame": ([_VP], C.c_int),
     "slosh_sort_particles": ([_VP], C.c_int),
+    "slosh_sort_particles_static": ([_VP, _VP, C.c_uint32, C.POINTER(C.c_int32), C.c_float, _VP, _VP, _VP, _VP], C.c_int),
     "slosh_emit": ([_VP, C.POINTER(EmitRequest)], C.c_int),
     "slosh_set_emit_seed": ([_VP, C.c_uint32], C.c_int),
     "slosh_upload_particles": ([_VP, _VP, C.c_uint32], C.c_int),
@@ -89,6 +90,20 @@ def _check(rc, allow_warnings=True):
         return rc
     msg = load_library().slosh_last_error_string()
     raise SloshError(rc, msg.decode() if msg else "")
+
+
+def sort_particles_static(particles_in, particles_out, count, grid_dim, cell_size, perm_out=0, key_offsets_out=0,
+                          live_count_out=0, stream=0):
+    """Allocation-free sort of caller-owned device particle records (slosh_sort_particles_static).
+
+    Pointers are device addresses (ints) on the current device; the call is enqueued on `stream` (a
+    cudaStream_t as int, 0 = default stream) and returns without waiting for it."""
+    lib = load_library()
+    dims = (C.c_int32 * 3)(*[int(v) for v in grid_dim])
+    _check(lib.slosh_sort_particles_static(C.c_void_p(particles_in), C.c_void_p(particles_out), int(count), dims,
+                                           float(cell_size), C.c_void_p(perm_out or None),
+                                           C.c_void_p(key_offsets_out or None), C.c_void_p(live_count_out or None),
+                                           C.c_void_p(stream or None)), allow_warnings=False)
 
 
 class Simulation:

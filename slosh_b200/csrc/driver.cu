@@ -927,6 +927,9 @@ Ctx* as_ctx(void* p) {
 }
 
 }  // namespace
+// Error text for entry points defined in other files of the library.
+void set_last_error(const char* message) { g_error = message ? message : ""; }
+
 }  // namespace slosh
 
 using namespace slosh;
