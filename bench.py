@@ -39,7 +39,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["slosh", "reference"], default="slosh")
-    ap.add_argument("--workload", choices=["dam_break_sphere_256", "dam_break_64"], default="dam_break_sphere_256")
+    # dam_break_sphere_<n>: the same scene on an n^3 grid (256 is the benchmark; 192 is the small
+    # profiling case, 8.7M particles, about 2 GB on the device)
+    ap.add_argument("--workload", default="dam_break_sphere_256",
+                    help="dam_break_sphere_<n> (n multiple of 8, 32..256) or dam_break_64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -49,8 +52,11 @@ def make_scene(workload, default_fn):
     if workload == "dam_break_64":
         sc = scenes.dam_break(default_fn, n=64)
         sc["settings"].sort_interval = 4
+    elif workload.startswith("dam_break_sphere_") and workload[17:].isdigit() and int(workload[17:]) % 8 == 0 \
+            and 32 <= int(workload[17:]) <= 256:
+        sc = scenes.dam_break_sphere(default_fn, n=int(workload[17:]))
     else:
-        sc = scenes.dam_break_sphere(default_fn, n=256)
+        raise SystemExit(f"unknown workload {workload!r}")
     sc["settings"].max_substeps = 16  # CFL 1 holds; the plugin's default cap of 4 would exceed it
     return sc
 

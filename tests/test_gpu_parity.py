@@ -88,6 +88,18 @@ def test_tiny_dam_break_substeps(slosh, oracle_mod, solver):
     _run_frames(g, o, sc, frames=6)
 
 
+@pytest.mark.parametrize("n", [64, 96])
+def test_sparse_sphere_coarse_levels(slosh, oracle_mod, n):
+    """Sparse dam break + falling sphere large enough that MGPCG visits coarse levels through the
+    active bricks' footprints (64^3: levels 1 and the single-CTA tail from level 2; 96^3: levels 1-2,
+    tail from level 3), bit-exact substep by substep."""
+    sc = scenes.dam_break_sphere(slosh.settings_default, n=n)
+    sc["settings"].max_substeps = 16
+    g, o = _pair(slosh, oracle_mod, sc)
+    assert g.layout().num_mg_levels >= 4
+    _run_frames(g, o, sc, frames=2)
+
+
 def test_tiny_with_collider(slosh, oracle_mod):
     sc = scenes.tiny(slosh.settings_default, n=24, colliders=True)
     g, o = _pair(slosh, oracle_mod, sc)
