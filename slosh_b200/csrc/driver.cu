@@ -326,8 +326,8 @@ struct Ctx {
             mg.lv[l].cells = level_cells[l];
             if (l > 0) {
                 mg.lv[l].type = dalloc<uint32_t>(level_cells[l], false);
-                mg.lv[l].x = dalloc<float>(level_cells[l], false);
-                mg.lv[l].b = dalloc<float>(level_cells[l], false);
+                mg.lv[l].x = dalloc<float>((level_cells[l] + 3u) & ~3u, false);  // padded: read as 16-byte chunks
+                mg.lv[l].b = dalloc<float>((level_cells[l] + 3u) & ~3u, false);
                 mg.lv[l].word = dalloc<uint16_t>(level_cells[l], false);
             } else {
                 mg.lv[l].type = nullptr; mg.lv[l].x = nullptr; mg.lv[l].b = nullptr; mg.lv[l].word = nullptr;
@@ -349,6 +349,7 @@ struct Ctx {
             for (int l = 1; l < num_levels; ++l) tail_cells += level_cells[l];
             mg.tail_list = dalloc<uint32_t>(tail_cells + 1, false);
             mg.tail_meta = dalloc<uint32_t>(4 * SLOSH_MAX_MG_LEVELS, false);
+            mg.tail_image = dalloc<unsigned char>(mg_tail_smem(mg) + 16, false);
         }
         // zero everything (AddClearUAVPass of every buffer), then the free stack and the slot table
         zero_all();

@@ -86,6 +86,7 @@ struct MGState {
     float* dvec2;         // second search-direction buffer (d alternates by iteration parity)
     uint32_t* tail_list;  // per tail level: red fluid cells, then black fluid cells (dense indices)
     uint32_t* tail_meta;  // per level: [red offset, red count, black offset, black count]
+    unsigned char* tail_image;  // per solve: the tail kernel's shared memory minus x and b (mg_tail_smem bytes)
 };
 int launch_mg_words(const MGState& m, int l, cudaStream_t s);
 int launch_mg_tail_lists(const MGState& m, cudaStream_t s);

@@ -47,6 +47,30 @@ __device__ __forceinline__ void stencil0(const Dev& d, const float* buf, uint32_
     diag = d.cell_diag[i] + DIAG_EPSILON;
 }
 
+// Shared-memory layout of the tail levels (byte offsets; every array padded to 4 cells, so each starts
+// on 16 bytes): per level x, b, diag (f32), word (u16), colour list (u32; red then black). Level `tail`'s
+// x and b come first. The same layout is used for the per-solve image in global memory.
+struct TailOffsets {
+    uint32_t x, b, diag, word, list;
+};
+__host__ __device__ __forceinline__ uint32_t tail_pad4(uint32_t cells) { return (cells + 3u) & ~3u; }
+__host__ __device__ __forceinline__ TailOffsets tail_offsets(const MGState& m, int tail, int level, uint32_t* total) {
+    uint32_t off = 0;
+    TailOffsets o{};
+    for (int l = tail; l < m.num_levels; ++l) {
+        const uint32_t c4 = tail_pad4(m.lv[l].cells);
+        TailOffsets t;
+        t.x = off; off += c4 * 4u;
+        t.b = off; off += c4 * 4u;
+        t.diag = off; off += c4 * 4u;
+        t.word = off; off += (c4 * 2u + 15u) & ~15u;
+        t.list = off; off += c4 * 4u;
+        if (l == level) o = t;
+    }
+    if (total) *total = off;
+    return o;
+}
+
 // ---- canonical FP64 reduction ---------------------------------------------------------------------
 struct DotSmem {
     double w8[GRID_THREADS / 32];
@@ -767,6 +791,22 @@ __global__ void __launch_bounds__(1024) k_tail_lists(MGState m, int tail) {
             off += base;
         }
     }
+    // The static part of the tail's shared-memory image for this solve: diagonals, words, colour lists.
+    __syncthreads();
+    for (int l = tail; l < m.num_levels; ++l) {
+        const MGLevel L = m.lv[l];
+        const TailOffsets o = tail_offsets(m, tail, l, nullptr);
+        float* diag = reinterpret_cast<float*>(m.tail_image + o.diag);
+        uint16_t* word = reinterpret_cast<uint16_t*>(m.tail_image + o.word);
+        uint32_t* list = reinterpret_cast<uint32_t*>(m.tail_image + o.list);
+        for (uint32_t i = threadIdx.x; i < L.cells; i += blockDim.x) {
+            const uint32_t w = L.word[i];
+            word[i] = uint16_t(w);
+            diag[i] = word_diag(w);
+        }
+        const uint32_t first = m.tail_meta[4 * l], n = m.tail_meta[4 * l + 1] + m.tail_meta[4 * l + 3];
+        for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) list[j] = m.tail_list[first + j];
+    }
 }
 
 struct SLevel {
@@ -779,7 +819,7 @@ struct SLevel {
     const uint32_t* list;  // red cells then black cells
     uint32_t nred, nblack;
 };
-__device__ __forceinline__ void s_sweep(const SLevel& L, uint32_t colour) {
+__device__ __forceinline__ void s_sweep(const SLevel L, uint32_t colour) {
     const uint32_t n = colour == 0u ? L.nred : L.nblack;
     const uint32_t* list = L.list + (colour == 0u ? 0u : L.nred);
     for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) {
@@ -789,45 +829,76 @@ __device__ __forceinline__ void s_sweep(const SLevel& L, uint32_t colour) {
     }
     __syncthreads();
 }
+// The coarsest level's red-black iterations on the first 4 warps, synchronised by a 128-thread named
+// barrier (the level has at most 512 cells, so 128 threads visit each colour in a few rounds).
+__device__ __forceinline__ void s_coarse_solve(const SLevel L, int iterations) {
+    if (threadIdx.x < 128u) {
+        for (int it = 0; it < iterations; ++it) {
+#pragma unroll
+            for (uint32_t colour = 0; colour < 2u; ++colour) {
+                const uint32_t n = colour == 0u ? L.nred : L.nblack;
+                const uint32_t* list = L.list + (colour == 0u ? 0u : L.nred);
+                for (uint32_t j = threadIdx.x; j < n; j += 128u) {
+                    const uint32_t i = list[j];
+                    const uint32_t w = L.word[i];
+                    L.x[i] = (L.b[i] + word_sum(L.x, w, i, L.dx, L.dxy)) / L.diag[i];
+                }
+                asm volatile("bar.sync 1, 128;" ::: "memory");
+            }
+        }
+    }
+    __syncthreads();
+}
 __global__ void __launch_bounds__(1024) k_vcycle_tail(MGState m, int tail, int iterations) {
     if (solve_done(m)) return;
     extern __shared__ __align__(16) unsigned char s_tail[];
     const int nl = m.num_levels;
     SLevel S[SLOSH_MAX_MG_LEVELS];
-    size_t off = 0;
+    uint32_t total = 0;
     for (int l = tail; l < nl; ++l) {
         const MGLevel G = m.lv[l];
+        const TailOffsets o = tail_offsets(m, tail, l, &total);
         SLevel& L = S[l];
         L.dim = G.dim;
         L.cells = G.cells;
         L.dx = uint32_t(G.dim.x);
         L.dxy = uint32_t(G.dim.x * G.dim.y);
-        L.x = reinterpret_cast<float*>(s_tail + off); off += size_t(L.cells) * 4;
-        L.b = reinterpret_cast<float*>(s_tail + off); off += size_t(L.cells) * 4;
-        L.diag = reinterpret_cast<float*>(s_tail + off); off += size_t(L.cells) * 4;
-        L.word = reinterpret_cast<uint16_t*>(s_tail + off); off += (size_t(L.cells) * 2 + 15) & ~size_t(15);
-        const uint32_t ro = m.tail_meta[4 * l], nr = m.tail_meta[4 * l + 1], bo = m.tail_meta[4 * l + 2], nb = m.tail_meta[4 * l + 3];
-        uint32_t* list = reinterpret_cast<uint32_t*>(s_tail + off); off += size_t(nr + nb) * 4;
-        L.list = list;
-        L.nred = nr;
-        L.nblack = nb;
-        for (uint32_t j = threadIdx.x; j < nr; j += blockDim.x) list[j] = m.tail_list[ro + j];
-        for (uint32_t j = threadIdx.x; j < nb; j += blockDim.x) list[nr + j] = m.tail_list[bo + j];
-        for (uint32_t i = threadIdx.x; i < L.cells; i += blockDim.x) {
-            const uint32_t w = G.word[i];
-            L.word[i] = uint16_t(w);
-            L.diag[i] = word_diag(w);
-        }
+        L.x = reinterpret_cast<float*>(s_tail + o.x);
+        L.b = reinterpret_cast<float*>(s_tail + o.b);
+        L.diag = reinterpret_cast<float*>(s_tail + o.diag);
+        L.word = reinterpret_cast<uint16_t*>(s_tail + o.word);
+        L.list = reinterpret_cast<const uint32_t*>(s_tail + o.list);
+        L.nred = m.tail_meta[4 * l + 1];
+        L.nblack = m.tail_meta[4 * l + 3];
     }
-    for (uint32_t i = threadIdx.x; i < S[tail].cells; i += blockDim.x) {
-        S[tail].x[i] = m.lv[tail].x[i];
-        S[tail].b[i] = m.lv[tail].b[i];
+    // One round trip: level tail's x and b from the level arrays, everything static (diagonals, words,
+    // colour lists of all tail levels) from the image k_tail_lists built for this solve.
+    {
+        const uint32_t c16 = tail_pad4(m.lv[tail].cells) / 4u;  // 16-byte chunks of one level-tail array
+        const uint32_t n16 = total / 16u;
+        const uint4* gx = reinterpret_cast<const uint4*>(m.lv[tail].x);
+        const uint4* gb = reinterpret_cast<const uint4*>(m.lv[tail].b);
+        const uint4* img = reinterpret_cast<const uint4*>(m.tail_image);
+        uint4* dst = reinterpret_cast<uint4*>(s_tail);
+        for (uint32_t k0 = 0; k0 < n16; k0 += 8u * 1024u) {
+            uint4 v[8];
+#pragma unroll
+            for (int r = 0; r < 8; ++r) {
+                const uint32_t k = k0 + uint32_t(r) * 1024u + threadIdx.x;
+                if (k < n16) v[r] = k < c16 ? gx[k] : (k < 2u * c16 ? gb[k - c16] : img[k]);
+            }
+#pragma unroll
+            for (int r = 0; r < 8; ++r) {
+                const uint32_t k = k0 + uint32_t(r) * 1024u + threadIdx.x;
+                if (k < n16) dst[k] = v[r];
+            }
+        }
     }
     __syncthreads();
     if (tail < nl - 1) s_sweep(S[tail], 1u);
     for (int l = tail; l < nl - 1; ++l) {
-        const SLevel& F = S[l];
-        const SLevel& C = S[l + 1];
+        const SLevel F = S[l];
+        const SLevel C = S[l + 1];
         for (uint32_t j = threadIdx.x; j < C.nred + C.nblack; j += blockDim.x) {
             const uint32_t ci = C.list[j];
             const int3 c = coord3(ci, C.dim);
@@ -855,13 +926,10 @@ __global__ void __launch_bounds__(1024) k_vcycle_tail(MGState m, int tail, int i
         __syncthreads();
         if (l + 1 < nl - 1) s_sweep(C, 1u);
     }
-    for (int it = 0; it < iterations; ++it) {
-        s_sweep(S[nl - 1], 0u);
-        s_sweep(S[nl - 1], 1u);
-    }
+    s_coarse_solve(S[nl - 1], iterations);
     for (int l = nl - 2; l >= tail; --l) {
-        const SLevel& F = S[l];
-        const SLevel& C = S[l + 1];
+        const SLevel F = S[l];
+        const SLevel C = S[l + 1];
         for (uint32_t j = threadIdx.x; j < F.nred + F.nblack; j += blockDim.x) {
             const uint32_t i = F.list[j];
             const int3 c = coord3(i, F.dim);
@@ -872,7 +940,12 @@ __global__ void __launch_bounds__(1024) k_vcycle_tail(MGState m, int tail, int i
         s_sweep(F, 1u);
         s_sweep(F, 0u);
     }
-    for (uint32_t i = threadIdx.x; i < S[tail].cells; i += blockDim.x) m.lv[tail].x[i] = S[tail].x[i];
+    {
+        const uint32_t c16 = tail_pad4(m.lv[tail].cells) / 4u;
+        const uint4* src = reinterpret_cast<const uint4*>(s_tail);
+        uint4* gx = reinterpret_cast<uint4*>(m.lv[tail].x);
+        for (uint32_t k = threadIdx.x; k < c16; k += blockDim.x) gx[k] = src[k];
+    }
 }
 
 // ---- the coarse solve directly on level 0 (grids of <= 512 cells have a single level) --------------------
@@ -1029,11 +1102,9 @@ int launch_pcg_init(const Dev& d, const MGState& m, const float* p, const float*
 }
 
 size_t mg_tail_smem(const MGState& m) {
-    const int tail = mg_tail_level(m);
-    size_t off = 0;
-    for (int l = tail; l < m.num_levels; ++l)
-        off += size_t(m.lv[l].cells) * 12 + ((size_t(m.lv[l].cells) * 2 + 15) & ~size_t(15)) + size_t(m.lv[l].cells) * 4;
-    return off;
+    uint32_t total = 0;
+    tail_offsets(m, mg_tail_level(m), -1, &total);
+    return total;
 }
 int launch_mg_words(const MGState& m, int l, cudaStream_t s) {
     k_level_words<<<blocks_for(m.lv[l].cells, 256), 256, 0, s>>>(m.lv[l]);
