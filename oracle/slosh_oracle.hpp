@@ -361,13 +361,19 @@ inline bool layout_equals(const slosh_settings_t& a, const slosh_settings_t& b) 
 }
 
 // ---- canonical FP64 reduction tree of the PCG dots -------------------------------------------
-// One partial per 8^3 brick: 32 lanes, lane t adds v[t], v[t + 32], ..., v[t + 480] in order (starting
-// from 0.0); the lanes then fold with offsets 16, 8, 4, 2, 1 (lane j += lane j + off).
+// One partial per 8^3 brick (v in local order x + 8 y + 64 z): 32 lanes; in round k = 0..3 lane t owns
+// the 4 cells x = 4h .. 4h + 3 of row y in plane z (h = t & 1, y = (t >> 1) & 7, z = 2k + (t >> 4)) and
+// adds them round by round, x ascending, starting from 0.0; the lanes then fold with offsets 16, 8, 4,
+// 2, 1 (lane j += lane j + off).
 inline double reduce_brick(const double* v) {
     double s[32];
     for (int t = 0; t < 32; ++t) {
         double acc = 0.0;
-        for (int k = 0; k < 16; ++k) acc = acc + v[t + 32 * k];
+        const int h = t & 1, y = (t >> 1) & 7;
+        for (int k = 0; k < 4; ++k) {
+            const int z = 2 * k + (t >> 4);
+            for (int j = 0; j < 4; ++j) acc = acc + v[4 * h + j + 8 * y + 64 * z];
+        }
         s[t] = acc;
     }
     for (int off = 16; off >= 1; off >>= 1)

@@ -157,124 +157,73 @@ __device__ __forceinline__ uint32_t l0_nbr(uint32_t i, uint32_t l, int n, const 
         default: return ((l & 448u) != 448u) ? i + 64u : ns[5] * BRICK_CELLS + l - 448u;
     }
 }
-// Sum of buf over the fluid neighbours, in neighbour order (non-fluid neighbours are skipped, not
-// added as zero, so the rounding is the reference's). Every neighbour index is in bounds (a missing
-// neighbour brick resolves to the null slot), so all six loads are issued unconditionally.
-__device__ __forceinline__ float l0_sum(const float* buf, uint32_t w, uint32_t i, uint32_t l, const uint32_t* ns) {
-    float v[6];
-#pragma unroll
-    for (int n = 0; n < 6; ++n) v[n] = buf[l0_nbr(i, l, n, ns)];
-    float sum = 0.0f;
-#pragma unroll
-    for (int n = 0; n < 6; ++n)
-        if ((w >> n) & 1u) sum = sum + v[n];
-    return sum;
+
+// ---- level-0 passes in half rows --------------------------------------------------------------------
+// One warp per active brick (nbr_slots[8 e + 0..5] = face-neighbour slots, [8 e + 6] = own slot, [8 e + 7]
+// = brick index, stored by PCGInit). In round k = 0..3 lane t takes the 4 consecutive cells x = 4h .. 4h+3
+// of row y in plane z (h = t & 1, y = (t >> 1) & 7, z = 2k + (t >> 4)): one 16-byte load or store per
+// array, the +-y and +-z neighbours as 16-byte loads of the adjacent rows (of the face-neighbour brick at
+// the brick's faces; a missing neighbour is the all-zero null slot), the +-x neighbours inside the row from
+// the lane's own quad or its partner lane t ^ 1, and one scalar load from the -x (h = 0) or +x (h = 1)
+// neighbour brick. A brick's dot-product partial is the canonical per-brick tree: lane t adds its cells
+// round by round, x ascending, starting from 0.0, and the lanes fold with shfl_down 16..1.
+struct Geo {
+    uint32_t i, l, h, y, z;  // pool and local index of the quad's first cell; half, row, plane
+};
+__device__ __forceinline__ Geo geo_of(uint32_t base, uint32_t lane, uint32_t k) {
+    Geo g;
+    g.h = lane & 1u;
+    g.y = (lane >> 1) & 7u;
+    g.z = 2u * k + (lane >> 4);
+    g.l = 4u * g.h + 8u * g.y + 64u * g.z;
+    g.i = base + g.l;
+    return g;
+}
+__device__ __forceinline__ float4 ld4(const float* q) { return *reinterpret_cast<const float4*>(q); }
+__device__ __forceinline__ void st4(float* q, const float (&v)[4]) { *reinterpret_cast<float4*>(q) = make_float4(v[0], v[1], v[2], v[3]); }
+__device__ __forceinline__ float comp(const float4& v, int j) { return j == 0 ? v.x : (j == 1 ? v.y : (j == 2 ? v.z : v.w)); }
+__device__ __forceinline__ uint32_t quad_words(const MGState& m, const Geo& g) { return *reinterpret_cast<const uint32_t*>(m.word + g.i); }
+__device__ __forceinline__ uint32_t word_of(uint32_t w4, int j) { return (w4 >> (8 * j)) & 0xFFu; }
+
+struct Q6 {  // a quad of one array and its face neighbours
+    float4 c, ym, yp, zm, zp;
+    float xb;  // h = 0: cell (7, y, z) of the -x brick; h = 1: cell (0, y, z) of the +x brick
+};
+__device__ __forceinline__ Q6 load_q6(const float* buf, const Geo& g, const uint32_t* ns) {
+    Q6 q;
+    q.c = ld4(buf + g.i);
+    q.ym = ld4(buf + (g.y > 0u ? g.i - 8u : ns[2] * BRICK_CELLS + g.l + 56u));
+    q.yp = ld4(buf + (g.y < 7u ? g.i + 8u : ns[3] * BRICK_CELLS + g.l - 56u));
+    q.zm = ld4(buf + (g.z > 0u ? g.i - 64u : ns[4] * BRICK_CELLS + g.l + 448u));
+    q.zp = ld4(buf + (g.z < 7u ? g.i + 64u : ns[5] * BRICK_CELLS + g.l - 448u));
+    q.xb = buf[g.h == 0u ? ns[0] * BRICK_CELLS + g.l + 7u : ns[1] * BRICK_CELLS + g.l - 4u];
+    return q;
+}
+// The partner lane's last (pw) and first (px) cell; every lane shuffles before any per-cell branch.
+struct X2 {
+    float pw, px;
+};
+__device__ __forceinline__ X2 partner(const Q6& q) {
+    X2 x;
+    x.pw = __shfl_xor_sync(0xFFFFFFFFu, q.c.w, 1);
+    x.px = __shfl_xor_sync(0xFFFFFFFFu, q.c.x, 1);
+    return x;
+}
+// Neighbour values of cell j of the quad, in the order -x, +x, -y, +y, -z, +z.
+__device__ __forceinline__ void nbrs6(const Q6& q, const X2& x, uint32_t h, int j, float n[6]) {
+    n[0] = j == 0 ? (h ? x.pw : q.xb) : comp(q.c, j - 1);
+    n[1] = j == 3 ? (h ? q.xb : x.px) : comp(q.c, j + 1);
+    n[2] = comp(q.ym, j);
+    n[3] = comp(q.yp, j);
+    n[4] = comp(q.zm, j);
+    n[5] = comp(q.zp, j);
 }
 
-// Level-0 pass, one warp per active brick: lane t visits cells t, t + 32, ..., t + 480 of the brick, so
-// every load instruction of the warp covers 32 consecutive cells, and the brick's dot-product partial
-// is the lane sums folded by warp shuffles (the canonical tree). nbr_slots[8 e + 0..5] are the face
-// neighbours' slots, [8 e + 6] the brick's own slot (stored by PCGInit). fn(i, l, ns, v0, v1) handles
-// one cell; the last CTA to finish reduces the partials and calls store(t0, t1) in thread 0.
-template <int NDOT, class Fn, class Store>
-__device__ __forceinline__ void w0_pass(const Dev& d, const MGState& m, uint32_t counter, Fn fn, Store store) {
-    __shared__ DotSmem sm;
-    const uint32_t active = d.active_bricks[0];
-    const uint32_t cap = d.num_pool_bricks;
-    const uint32_t lane = threadIdx.x & 31u, wpb = blockDim.x >> 5;
-    for (uint32_t e = blockIdx.x * wpb + (threadIdx.x >> 5); e < active; e += gridDim.x * wpb) {
-        const uint4 s0 = *reinterpret_cast<const uint4*>(m.nbr_slots + 8u * e);
-        const uint4 s1 = *reinterpret_cast<const uint4*>(m.nbr_slots + 8u * e + 4u);
-        const uint32_t ns[6] = {s0.x, s0.y, s0.z, s0.w, s1.x, s1.y};
-        const uint32_t base = s1.z * BRICK_CELLS;
-        double acc0 = 0.0, acc1 = 0.0;
-#pragma unroll 4
-        for (uint32_t k = 0; k < 16u; ++k) {
-            const uint32_t l = lane + 32u * k;
-            double v0 = 0.0, v1 = 0.0;
-            fn(base + l, l, ns, v0, v1);
-            acc0 = acc0 + v0;
-            acc1 = acc1 + v1;
-        }
-        if (NDOT > 0) {
-            const double t0 = warp_fold(acc0);
-            if (lane == 0) m.partials[e] = t0;
-        }
-        if (NDOT > 1) {
-            const double t1 = warp_fold(acc1);
-            if (lane == 0) m.partials[cap + e] = t1;
-        }
-    }
-    if (NDOT == 0) return;
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) sm.last = (atomicAdd(m.counters + counter, 1u) == gridDim.x - 1u) ? 1u : 0u;
-    __syncthreads();
-    if (sm.last) {
-        __threadfence();
-        const double r0 = final_reduce(m.partials, active, sm);
-        __syncthreads();
-        double r1 = 0.0;
-        if (NDOT > 1) r1 = final_reduce(m.partials + cap, active, sm);
-        if (threadIdx.x == 0) {
-            store(r0, r1);
-            m.counters[counter] = 0u;
-        }
-    }
-}
-
-// Level-0 pass over all 512 cells of every active brick; fn(i, l, e, ns, v0, v1) handles one cell
-// (it reads the word to know whether the cell exists and is fluid). With NDOT > 0 it produces dot
-// products through the canonical tree; the last CTA calls store(t0, t1) in thread 0.
-template <int NDOT, class Fn, class Store>
-__device__ __forceinline__ void l0_pass(const Dev& d, const MGState& m, uint32_t counter, Fn fn, Store store) {
-    __shared__ DotSmem sm;
-    const uint32_t active = d.active_bricks[0];
-    const uint32_t cap = d.num_pool_bricks;
-    for (uint32_t e = blockIdx.x; e < active; e += gridDim.x) {
-        const uint32_t slot = __ldg(d.brick_table + d.active_bricks[1u + e]);
-        uint32_t ns[6];
-#pragma unroll
-        for (int n = 0; n < 6; ++n) ns[n] = m.nbr_slots[8u * e + uint32_t(n)];
-        double a0[2] = {0.0, 0.0}, a1[2] = {0.0, 0.0};
-#pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            const uint32_t l = threadIdx.x + uint32_t(k) * 256u;
-            fn(slot * BRICK_CELLS + l, l, e, ns, a0[k], a1[k]);
-        }
-        if (NDOT > 0) {
-            const double t0 = brick_reduce(a0[0] + a0[1], sm.w8);
-            if (threadIdx.x == 0) m.partials[e] = t0;
-        }
-        if (NDOT > 1) {
-            const double t1 = brick_reduce(a1[0] + a1[1], sm.w8);
-            if (threadIdx.x == 0) m.partials[cap + e] = t1;
-        }
-    }
-    if (NDOT == 0) return;
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) sm.last = (atomicAdd(m.counters + counter, 1u) == gridDim.x - 1u) ? 1u : 0u;
-    __syncthreads();
-    if (sm.last) {
-        __threadfence();
-        const double r0 = final_reduce(m.partials, active, sm);
-        __syncthreads();
-        double r1 = 0.0;
-        if (NDOT > 1) r1 = final_reduce(m.partials + cap, active, sm);
-        if (threadIdx.x == 0) {
-            store(r0, r1);
-            m.counters[counter] = 0u;
-        }
-    }
-}
-
-// Batched form of w0_pass: for each group of B cells of a lane, load(i, l, ns) gathers everything a cell
-// needs into a value struct first, then apply(i, l, vals, v0, v1) computes and stores. All loads of the
-// group are issued before any of its stores, so they overlap (plain pointers may alias, which otherwise
-// keeps the compiler from hoisting the next cell's loads above this cell's stores).
+// load(g, ns) gathers a round's values; apply(g, vals, v0[4], v1[4]) computes and stores one round and
+// yields the cells' dot terms. The loads of B rounds are issued before any of them is applied. With
+// NDOT > 0 the last CTA reduces the brick partials (canonical tree) and calls store(t0, t1) in thread 0.
 template <int NDOT, int B, class Load, class Apply, class Store>
-__device__ __forceinline__ void w0_batched(const Dev& d, const MGState& m, uint32_t counter, Load load, Apply apply, Store store) {
+__device__ __forceinline__ void w4_pass(const Dev& d, const MGState& m, uint32_t counter, Load load, Apply apply, Store store) {
     __shared__ DotSmem sm;
     const uint32_t active = d.active_bricks[0];
     const uint32_t cap = d.num_pool_bricks;
@@ -285,20 +234,20 @@ __device__ __forceinline__ void w0_batched(const Dev& d, const MGState& m, uint3
         const uint32_t ns[6] = {s0.x, s0.y, s0.z, s0.w, s1.x, s1.y};
         const uint32_t base = s1.z * BRICK_CELLS;
         double acc0 = 0.0, acc1 = 0.0;
-        for (uint32_t k0 = 0; k0 < 16u; k0 += B) {
-            decltype(load(0u, 0u, ns)) vals[B];
+#pragma unroll
+        for (uint32_t k0 = 0; k0 < 4u; k0 += uint32_t(B)) {
+            decltype(load(Geo{}, ns)) vals[B];
+#pragma unroll
+            for (int b = 0; b < B; ++b) vals[b] = load(geo_of(base, lane, k0 + uint32_t(b)), ns);
 #pragma unroll
             for (int b = 0; b < B; ++b) {
-                const uint32_t l = lane + 32u * (k0 + uint32_t(b));
-                vals[b] = load(base + l, l, ns);
-            }
+                double v0[4] = {0.0, 0.0, 0.0, 0.0}, v1[4] = {0.0, 0.0, 0.0, 0.0};
+                apply(geo_of(base, lane, k0 + uint32_t(b)), vals[b], v0, v1);
 #pragma unroll
-            for (int b = 0; b < B; ++b) {
-                const uint32_t l = lane + 32u * (k0 + uint32_t(b));
-                double v0 = 0.0, v1 = 0.0;
-                apply(base + l, l, vals[b], v0, v1);
-                acc0 = acc0 + v0;
-                acc1 = acc1 + v1;
+                for (int j = 0; j < 4; ++j) {
+                    acc0 = acc0 + v0[j];
+                    acc1 = acc1 + v1[j];
+                }
             }
         }
         if (NDOT > 0) {
@@ -367,28 +316,27 @@ struct Nb6 {
     float c0, c1, c2;
     float n[6];
 };
-struct Nb12 {
-    uint32_t w;
-    float c0, c1, c2;
-    float n[6], m[6];
-};
-__device__ __forceinline__ Nb6 load_nb6(const float* buf, const float* a, const float* b, const float* c, const uint8_t* word,
-                                        uint32_t i, uint32_t l, const uint32_t* ns) {
-    Nb6 v;
-    v.w = word[i];
-    v.c0 = a[i];
-    v.c1 = b[i];
-    v.c2 = c[i];
-#pragma unroll
-    for (int n = 0; n < 6; ++n) v.n[n] = buf[l0_nbr(i, l, n, ns)];
-    return v;
-}
 __device__ __forceinline__ float nb_sum(const float* v, uint32_t w) {
     float sum = 0.0f;
 #pragma unroll
     for (int n = 0; n < 6; ++n)
         if ((w >> n) & 1u) sum = sum + v[n];
     return sum;
+}
+
+// What a sweep or the restriction reads of a quad: z with its neighbours, r, the diagonal and the words.
+struct SweepQ {
+    Q6 z;
+    float4 r, dg;
+    uint32_t w;
+};
+__device__ __forceinline__ SweepQ load_sweep(const Dev& d, const MGState& m, const Geo& g, const uint32_t* ns) {
+    SweepQ v;
+    v.z = load_q6(m.z, g, ns);
+    v.r = ld4(m.r + g.i);
+    v.dg = ld4(d.cell_diag + g.i);
+    v.w = quad_words(m, g);
+    return v;
 }
 
 __device__ __forceinline__ float ratio_f(double num, double den) { return fabs(den) > 1e-30 ? float(num / den) : 0.0f; }
@@ -499,22 +447,41 @@ __global__ void __launch_bounds__(GRID_THREADS) k_pcg_words(Dev d, MGState m) {
 }
 __global__ void __launch_bounds__(GRID_THREADS) k_pcg_init(Dev d, MGState m, const float* __restrict__ p, const float* __restrict__ div,
                                                            unsigned long long handle) {
-    w0_pass<2>(d, m, 0,
-        [&](uint32_t i, uint32_t l, const uint32_t* ns, double& v0, double& v1) {
-            const uint32_t w = m.word[i];
-            if (!(w & W_FLUID)) {
-                m.r[i] = 0.0f;
-                m.z[i] = 0.0f;
-                return;
+    struct V {
+        Q6 p;
+        float4 dv, dg;
+        uint32_t w;
+    };
+    w4_pass<2, 1>(d, m, 0,
+        [&](const Geo& g, const uint32_t* ns) {
+            V v;
+            v.p = load_q6(p, g, ns);
+            v.dv = ld4(div + g.i);
+            v.dg = ld4(d.cell_diag + g.i);
+            v.w = quad_words(m, g);
+            return v;
+        },
+        [&](const Geo& g, const V& v, double* v0, double* v1) {
+            const X2 x = partner(v.p);
+            float r[4], z[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const uint32_t w = word_of(v.w, j);
+                r[j] = 0.0f;
+                z[j] = 0.0f;
+                if (!(w & W_FLUID)) continue;
+                const float diag = comp(v.dg, j) + DIAG_EPSILON;
+                float n[6];
+                nbrs6(v.p, x, g.h, j, n);
+                const float b = -comp(v.dv, j);
+                const float ri = b - (diag * comp(v.p.c, j) - nb_sum(n, w));
+                r[j] = ri;
+                z[j] = (w & W_RED) ? ri / diag : 0.0f;
+                v0[j] = double(ri * ri);
+                v1[j] = double(b * b);
             }
-            const float diag = d.cell_diag[i] + DIAG_EPSILON;
-            const float sum = l0_sum(p, w, i, l, ns);
-            const float ri = -div[i] - (diag * p[i] - sum);
-            m.r[i] = ri;
-            m.z[i] = (w & W_RED) ? ri / diag : 0.0f;
-            v0 = double(ri * ri);
-            const float b = -div[i];
-            v1 = double(b * b);
+            st4(m.r + g.i, r);
+            st4(m.z + g.i, z);
         },
         [&](double rr, double bb) {
             m.scalars[5] = rr;
@@ -539,21 +506,32 @@ __device__ __forceinline__ Nb6 load_black(const Dev& d, const MGState& m, uint32
     return v;
 }
 
-// Red sweep with rho = r . z over all cells (red: the new value, black: the current z).
-__global__ void __launch_bounds__(GRID_THREADS) k_smooth0(Dev d, MGState m) {
+// Red sweep with rho = r . z over all cells (red: the new value, black: the current z). Cells the sweep
+// does not update are stored back unchanged (each cell belongs to one warp's brick).
+__global__ void __launch_bounds__(GRID_THREADS, 3) k_smooth0(Dev d, MGState m) {
     if (solve_done(m)) return;
-    // c0 = r (b of the level), c1 = z, c2 = diagonal
-    w0_batched<1, 4>(d, m, 1,
-        [&](uint32_t i, uint32_t l, const uint32_t* ns) { return load_nb6(m.z, m.r, m.z, d.cell_diag, m.word, i, l, ns); },
-        [&](uint32_t i, uint32_t, const Nb6& v, double& v0, double&) {
-            if (!(v.w & W_FLUID)) return;
-            if (v.w & W_RED) {
-                const float x = (v.c0 + nb_sum(v.n, v.w)) / (v.c2 + DIAG_EPSILON);
-                m.z[i] = x;
-                v0 = double(v.c0 * x);
-            } else {
-                v0 = double(v.c0 * v.c1);
+    w4_pass<1, 1>(d, m, 1,
+        [&](const Geo& g, const uint32_t* ns) { return load_sweep(d, m, g, ns); },
+        [&](const Geo& g, const SweepQ& v, double* v0, double*) {
+            const X2 x = partner(v.z);
+            float out[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const uint32_t w = word_of(v.w, j);
+                const float zj = comp(v.z.c, j), rj = comp(v.r, j);
+                out[j] = zj;
+                if (!(w & W_FLUID)) continue;
+                if (w & W_RED) {
+                    float n[6];
+                    nbrs6(v.z, x, g.h, j, n);
+                    const float val = (rj + nb_sum(n, w)) / (comp(v.dg, j) + DIAG_EPSILON);
+                    out[j] = val;
+                    v0[j] = double(rj * val);
+                } else {
+                    v0[j] = double(rj * zj);
+                }
             }
+            st4(m.z + g.i, out);
         },
         [&](double rho, double) { m.scalars[3] = m.scalars[0]; m.scalars[0] = rho; });
 }
@@ -706,15 +684,20 @@ __global__ void __launch_bounds__(GRID_THREADS) k_restrict0(Dev d, MGState m) {
         const uint4 s1 = *reinterpret_cast<const uint4*>(m.nbr_slots + 8u * e + 4u);
         const uint32_t ns[6] = {s0.x, s0.y, s0.z, s0.w, s1.x, s1.y};
         const uint32_t base = s1.z * BRICK_CELLS;
-#pragma unroll 4
-        for (uint32_t k = 0; k < 16u; ++k) {
-            const uint32_t l = lane + 32u * k;
-            const uint32_t i = base + l;
-            const uint32_t w = m.word[i];
-            const float ri = m.r[i], zi = m.z[i], diag = d.cell_diag[i] + DIAG_EPSILON;
-            const float nbsum = l0_sum(m.z, w, i, l, ns);
-            s_fluid[warp][l] = (w & W_FLUID) ? 1 : 0;
-            if (w & W_FLUID) s_res[warp][l] = ri - (diag * zi - nbsum);
+#pragma unroll
+        for (uint32_t k = 0; k < 4u; ++k) {
+            const Geo g = geo_of(base, lane, k);
+            const SweepQ v = load_sweep(d, m, g, ns);
+            const X2 x = partner(v.z);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const uint32_t w = word_of(v.w, j);
+                float n[6];
+                nbrs6(v.z, x, g.h, j, n);
+                const float diag = comp(v.dg, j) + DIAG_EPSILON;
+                s_fluid[warp][g.l + uint32_t(j)] = (w & W_FLUID) ? 1 : 0;
+                if (w & W_FLUID) s_res[warp][g.l + uint32_t(j)] = comp(v.r, j) - (diag * comp(v.z.c, j) - nb_sum(n, w));
+            }
         }
         __syncwarp();
         const int3 bc = brick_coord_of(d, s1.w);
@@ -974,70 +957,93 @@ __global__ void __launch_bounds__(1024) k_coarse_solve0(Dev d, MGState m, int it
 // neighbour's new direction z_n + beta d_n itself (bit-identical to what that neighbour writes).
 __device__ __forceinline__ float* dir_buf(const MGState& m, uint32_t parity) { return parity ? m.dvec2 : m.dvec; }
 
-__global__ void __launch_bounds__(GRID_THREADS) k_apply_a(Dev d, MGState m) {
+__global__ void __launch_bounds__(GRID_THREADS, 3) k_apply_a(Dev d, MGState m) {
     if (solve_done(m)) return;
     const uint32_t it = m.ctl[0];
     const bool first = it == 0u;
     const float beta = first ? 0.0f : ratio_f(m.scalars[0], m.scalars[3]);
     const float* dold = dir_buf(m, it & 1u);
     float* dnew = dir_buf(m, (it + 1u) & 1u);
-    w0_batched<1, 4>(d, m, 2,
-        [&](uint32_t i, uint32_t l, const uint32_t* ns) {
-            Nb12 v;
-            v.w = m.word[i];
-            v.c0 = m.z[i];
-            v.c1 = dold[i];
-            v.c2 = d.cell_diag[i];
-#pragma unroll
-            for (int n = 0; n < 6; ++n) {
-                const uint32_t ni = l0_nbr(i, l, n, ns);
-                v.n[n] = m.z[ni];
-                v.m[n] = dold[ni];
-            }
+    struct V {
+        Q6 z, dd;
+        float4 dg;
+        uint32_t w;
+    };
+    w4_pass<1, 1>(d, m, 2,
+        [&](const Geo& g, const uint32_t* ns) {
+            V v;
+            v.z = load_q6(m.z, g, ns);
+            v.dd = load_q6(dold, g, ns);
+            v.dg = ld4(d.cell_diag + g.i);
+            v.w = quad_words(m, g);
             return v;
         },
-        [&](uint32_t i, uint32_t, const Nb12& v, double& v0, double&) {
-            if (!(v.w & W_FLUID)) return;
-            const float dn = first ? v.c0 : v.c0 + beta * v.c1;
-            float sum = 0.0f;
+        [&](const Geo& g, const V& v, double* v0, double*) {
+            const X2 xz = partner(v.z), xd = partner(v.dd);
+            float dn[4], q[4];
 #pragma unroll
-            for (int n = 0; n < 6; ++n)
-                if ((v.w >> n) & 1u) sum = sum + (first ? v.n[n] : v.n[n] + beta * v.m[n]);
-            dnew[i] = dn;
-            const float qi = (v.c2 + DIAG_EPSILON) * dn - sum;
-            m.q[i] = qi;
-            v0 = double(dn * qi);
+            for (int j = 0; j < 4; ++j) {
+                const uint32_t w = word_of(v.w, j);
+                dn[j] = 0.0f;
+                q[j] = 0.0f;
+                if (!(w & W_FLUID)) continue;
+                const float dj = first ? comp(v.z.c, j) : comp(v.z.c, j) + beta * comp(v.dd.c, j);
+                float nz[6], nd[6];
+                nbrs6(v.z, xz, g.h, j, nz);
+                nbrs6(v.dd, xd, g.h, j, nd);
+                float sum = 0.0f;
+#pragma unroll
+                for (int n = 0; n < 6; ++n)
+                    if ((w >> n) & 1u) sum = sum + (first ? nz[n] : nz[n] + beta * nd[n]);
+                const float qi = (comp(v.dg, j) + DIAG_EPSILON) * dj - sum;
+                dn[j] = dj;
+                q[j] = qi;
+                v0[j] = double(dj * qi);
+            }
+            st4(dnew + g.i, dn);
+            st4(m.q + g.i, q);
         },
         [&](double dq, double) { m.scalars[2] = dq; });
 }
 
 // ---- PCGUpdatePRCS: p += alpha d, r -= alpha q, red pre-smooth; ||r||^2 and the loop decision -------------
-struct PR {
-    uint32_t w;
-    float p, d, r, q, diag;
-};
-__global__ void __launch_bounds__(GRID_THREADS) k_update_pr(Dev d, MGState m, float* __restrict__ p, unsigned long long handle) {
+__global__ void __launch_bounds__(GRID_THREADS, 3) k_update_pr(Dev d, MGState m, float* __restrict__ p, unsigned long long handle) {
     if (solve_done(m)) return;
     const float alpha = ratio_f(m.scalars[0], m.scalars[2]);
     const float* dcur = dir_buf(m, (m.ctl[0] + 1u) & 1u);
-    w0_batched<1, 8>(d, m, 3,
-        [&](uint32_t i, uint32_t, const uint32_t*) {
-            PR v;
-            v.w = m.word[i];
-            v.p = p[i];
-            v.d = dcur[i];
-            v.r = m.r[i];
-            v.q = m.q[i];
-            v.diag = d.cell_diag[i];
+    struct V {
+        float4 p, d, r, q, dg;
+        uint32_t w;
+    };
+    w4_pass<1, 2>(d, m, 3,
+        [&](const Geo& g, const uint32_t*) {
+            V v;
+            v.p = ld4(p + g.i);
+            v.d = ld4(dcur + g.i);
+            v.r = ld4(m.r + g.i);
+            v.q = ld4(m.q + g.i);
+            v.dg = ld4(d.cell_diag + g.i);
+            v.w = quad_words(m, g);
             return v;
         },
-        [&](uint32_t i, uint32_t, const PR& v, double& v0, double&) {
-            if (!(v.w & W_FLUID)) return;
-            p[i] = v.p + alpha * v.d;
-            const float ri = v.r - alpha * v.q;
-            m.r[i] = ri;
-            m.z[i] = (v.w & W_RED) ? ri / (v.diag + DIAG_EPSILON) : 0.0f;
-            v0 = double(ri * ri);
+        [&](const Geo& g, const V& v, double* v0, double*) {
+            float po[4], ro[4], zo[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const uint32_t w = word_of(v.w, j);
+                po[j] = comp(v.p, j);
+                ro[j] = comp(v.r, j);
+                zo[j] = 0.0f;
+                if (!(w & W_FLUID)) continue;
+                po[j] = comp(v.p, j) + alpha * comp(v.d, j);
+                const float ri = comp(v.r, j) - alpha * comp(v.q, j);
+                ro[j] = ri;
+                zo[j] = (w & W_RED) ? ri / (comp(v.dg, j) + DIAG_EPSILON) : 0.0f;
+                v0[j] = double(ri * ri);
+            }
+            st4(p + g.i, po);
+            st4(m.r + g.i, ro);
+            st4(m.z + g.i, zo);
         },
         [&](double rr, double) {
             m.scalars[5] = rr;
@@ -1056,15 +1062,34 @@ __global__ void __launch_bounds__(GRID_THREADS) k_update_pr(Dev d, MGState m, fl
 // ---- ||b - A p||^2 and ||b||^2 of a finished solve (diagnostic) ---------------------------------------------
 __global__ void __launch_bounds__(GRID_THREADS) k_true_residual(Dev d, MGState m, const float* __restrict__ p,
                                                                 const float* __restrict__ div) {
-    w0_pass<2>(d, m, 4,
-        [&](uint32_t i, uint32_t l, const uint32_t* ns, double& v0, double& v1) {
-            const uint32_t w = m.word[i];
-            if (!(w & W_FLUID)) return;
-            const float diag = d.cell_diag[i] + DIAG_EPSILON;
-            const float r = -div[i] - (diag * p[i] - l0_sum(p, w, i, l, ns));
-            v0 = double(r * r);
-            const float b = -div[i];
-            v1 = double(b * b);
+    struct V {
+        Q6 p;
+        float4 dv, dg;
+        uint32_t w;
+    };
+    w4_pass<2, 1>(d, m, 4,
+        [&](const Geo& g, const uint32_t* ns) {
+            V v;
+            v.p = load_q6(p, g, ns);
+            v.dv = ld4(div + g.i);
+            v.dg = ld4(d.cell_diag + g.i);
+            v.w = quad_words(m, g);
+            return v;
+        },
+        [&](const Geo& g, const V& v, double* v0, double* v1) {
+            const X2 x = partner(v.p);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const uint32_t w = word_of(v.w, j);
+                if (!(w & W_FLUID)) continue;
+                const float diag = comp(v.dg, j) + DIAG_EPSILON;
+                float n[6];
+                nbrs6(v.p, x, g.h, j, n);
+                const float b = -comp(v.dv, j);
+                const float r = b - (diag * comp(v.p.c, j) - nb_sum(n, w));
+                v0[j] = double(r * r);
+                v1[j] = double(b * b);
+            }
         },
         [&](double num, double den) { m.scalars[6] = num; m.scalars[7] = den; });
 }

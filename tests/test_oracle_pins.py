@@ -275,8 +275,11 @@ def test_canonical_reductions(oracle_mod):
     lanes = np.zeros(32)
     for t in range(32):
         acc = 0.0
-        for k in range(16):
-            acc = acc + v[t + 32 * k]
+        h, y = t & 1, (t >> 1) & 7
+        for k in range(4):
+            z = 2 * k + (t >> 4)
+            for j in range(4):
+                acc = acc + v[4 * h + j + 8 * y + 64 * z]
         lanes[t] = acc
     for off in (16, 8, 4, 2, 1):
         lanes[:off] = lanes[:off] + lanes[off:2 * off]
