@@ -130,10 +130,14 @@ __device__ __forceinline__ void for_footprint(const Dev& d, const MGLevel& L, in
     }
     const int side = 8 >> l;
     const uint32_t per = uint32_t(side * side * side);
-    const uint32_t total = d.active_bricks[0] * per;
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    const uint32_t count = d.active_bricks[0];
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;; t += gridDim.x * blockDim.x) {
         const uint32_t e = t / per, lc = t % per;
-        const int3 bc = brick_coord_of(d, d.active_bricks[1u + e]);
+        // The brick index is loaded before the bound is known (clamped into the list), so it overlaps
+        // the load of the active count.
+        const uint32_t brick = d.active_bricks[1u + min(e, d.num_bricks - 1u)];
+        if (e >= count) break;
+        const int3 bc = brick_coord_of(d, brick);
         const int3 c = make_int3(bc.x * side + int(lc % uint32_t(side)), bc.y * side + int((lc / uint32_t(side)) % uint32_t(side)),
                                  bc.z * side + int(lc / uint32_t(side * side)));
         if (inside3(c, L.dim)) fn(lin3(c, L.dim), c);
@@ -394,6 +398,20 @@ __device__ __forceinline__ float word_diag(uint32_t w) {
         if ((w >> (CW_NONSOLID_SHIFT + n)) & 1u) d = d + 1.0f;
     return d;
 }
+// Sum of x over the fluid neighbours of a dense global level, in neighbour order. All six values are
+// loaded unconditionally (indices clamped into the level, so a missing neighbour reads some cell of
+// the level) and then selected by the word, so the loads overlap the word's.
+__device__ __forceinline__ float word_sum_g(const float* x, uint32_t w, uint32_t i, uint32_t dx, uint32_t dxy, uint32_t last) {
+    const uint32_t off[6] = {i - 1u, i + 1u, i - dx, i + dx, i - dxy, i + dxy};
+    float v[6];
+#pragma unroll
+    for (int n = 0; n < 6; ++n) v[n] = x[min(off[n], last)];
+    float sum = 0.0f;
+#pragma unroll
+    for (int n = 0; n < 6; ++n)
+        if ((w >> n) & 1u) sum = sum + v[n];
+    return sum;
+}
 // Sum of x over the fluid neighbours (dense level), in neighbour order.
 __device__ __forceinline__ float word_sum(const float* x, uint32_t w, uint32_t i, uint32_t dx, uint32_t dxy) {
     const uint32_t off[6] = {i - 1u, i + 1u, i - dx, i + dx, i - dxy, i + dxy};
@@ -604,10 +622,13 @@ __global__ void k_smooth_fp(Dev d, MGState m, int l, uint32_t parity) {
     const MGLevel L = m.lv[l];
     const uint32_t dx = uint32_t(L.dim.x), dxy = uint32_t(L.dim.x * L.dim.y);
     const uint32_t want = parity == 0u ? CW_RED : 0u;
+    const uint32_t last = L.cells - 1u;
     for_footprint(d, L, l, [&](uint32_t i, int3) {
         const uint32_t w = L.word[i];
+        const float b = L.b[i];
+        const float sum = word_sum_g(L.x, w, i, dx, dxy, last);
         if (!(w & CW_FLUID) || (w & CW_RED) != want) return;
-        L.x[i] = (L.b[i] + word_sum(L.x, w, i, dx, dxy)) / word_diag(w);
+        L.x[i] = (b + sum) / word_diag(w);
     });
 }
 // Restriction l -> l + 1 over level l + 1's footprint: b_c = (sum of the fluid children's residuals) / 4.
@@ -615,22 +636,26 @@ __global__ void k_restrict_fp(Dev d, MGState m, int l) {
     if (solve_done(m)) return;
     const MGLevel F = m.lv[l], C = m.lv[l + 1];
     const uint32_t fdx = uint32_t(F.dim.x), fdxy = uint32_t(F.dim.x * F.dim.y);
+    const uint32_t flast = F.cells - 1u;
     for_footprint(d, C, l + 1, [&](uint32_t ci, int3 c) {
+        // Every child's word, b, x and neighbours are loaded before any of them is tested.
         const uint32_t cw = C.word[ci];
-        if (!(cw & CW_FLUID)) { C.b[ci] = 0.0f; C.x[ci] = 0.0f; return; }
         float res[8];
         uint32_t fl = 0u;
 #pragma unroll
         for (int o = 0; o < 8; ++o) {
-            res[o] = 0.0f;
             const int3 f = make_int3(c.x * 2 + (o & 1), c.y * 2 + ((o >> 1) & 1), c.z * 2 + ((o >> 2) & 1));
-            if (!inside3(f, F.dim)) continue;
-            const uint32_t fi = lin3(f, F.dim);
+            const bool in = inside3(f, F.dim);
+            const uint32_t fi = in ? lin3(f, F.dim) : 0u;
             const uint32_t w = F.word[fi];
-            if (!(w & CW_FLUID)) continue;
-            fl |= 1u << o;
-            res[o] = F.b[fi] - (word_diag(w) * F.x[fi] - word_sum(F.x, w, fi, fdx, fdxy));
+            const float r = F.b[fi] - (word_diag(w) * F.x[fi] - word_sum_g(F.x, w, fi, fdx, fdxy, flast));
+            res[o] = 0.0f;
+            if (in && (w & CW_FLUID)) {
+                fl |= 1u << o;
+                res[o] = r;
+            }
         }
+        if (!(cw & CW_FLUID)) { C.b[ci] = 0.0f; C.x[ci] = 0.0f; return; }
         float sum = 0.0f;
 #pragma unroll
         for (int o = 0; o < 8; ++o)
@@ -645,25 +670,29 @@ __global__ void k_prolong_smooth_fp(Dev d, MGState m, int l) {
     if (solve_done(m)) return;
     const MGLevel F = m.lv[l], C = m.lv[l + 1];
     const uint32_t dx = uint32_t(F.dim.x), dxy = uint32_t(F.dim.x * F.dim.y);
+    const uint32_t last = F.cells - 1u, clast = C.cells - 1u;
     for_footprint(d, F, l, [&](uint32_t i, int3 c) {
+        // The neighbours' x and their parents' words and x are loaded before the word is tested
+        // (indices clamped into the levels; values of non-fluid neighbours are not used).
         const uint32_t w = F.word[i];
-        if (!(w & CW_FLUID) || (w & CW_RED)) return;
+        const float b = F.b[i];
         const uint32_t off[6] = {i - 1u, i + 1u, i - dx, i + dx, i - dxy, i + dxy};
         float v[6];
 #pragma unroll
         for (int n = 0; n < 6; ++n) {
-            v[n] = 0.0f;
-            if (!((w >> n) & 1u)) continue;
             const int3 nb = add3(c, nbr_off(n));
-            const uint32_t pi = lin3(make_int3(nb.x / 2, nb.y / 2, nb.z / 2), C.dim);
-            const float xn = F.x[off[n]];
-            v[n] = (C.word[pi] & CW_FLUID) ? xn + C.x[pi] : xn;
+            const uint32_t pi = min(lin3(make_int3(nb.x / 2, nb.y / 2, nb.z / 2), C.dim), clast);
+            const float xn = F.x[min(off[n], last)];
+            const uint32_t pw = C.word[pi];
+            const float px = C.x[pi];
+            v[n] = (pw & CW_FLUID) ? xn + px : xn;
         }
+        if (!(w & CW_FLUID) || (w & CW_RED)) return;
         float sum = 0.0f;
 #pragma unroll
         for (int n = 0; n < 6; ++n)
             if ((w >> n) & 1u) sum = sum + v[n];
-        F.x[i] = (F.b[i] + sum) / word_diag(w);
+        F.x[i] = (b + sum) / word_diag(w);
     });
 }
 
