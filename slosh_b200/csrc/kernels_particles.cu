@@ -350,7 +350,7 @@ __device__ __forceinline__ float3 sample_displacement(const Dev& d, float3 xp, c
 constexpr int G2P_THREADS = 256;
 
 // AdvectParticle + G2PAdvectCS (Slosh.usf:1452-1678).
-__global__ void __launch_bounds__(G2P_THREADS) k_g2p(Dev d, Pass p, slosh_particle_t* __restrict__ particles, uint32_t n,
+__global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p(Dev d, Pass p, slosh_particle_t* __restrict__ particles, uint32_t n,
                                                      const float* __restrict__ vel, const float* __restrict__ disp,
                                                      uint32_t apply_density) {
     const uint32_t i = blockIdx.x * G2P_THREADS + threadIdx.x;
