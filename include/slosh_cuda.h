@@ -142,6 +142,11 @@ typedef struct slosh_collider_t {
     float pad1;
 } slosh_collider_t;
 
+/* ESloshManipulatorKind / ESloshManipulatorShape (SloshTypes.h:47-63). Shapes 0-2 are the collider
+ * shapes (sphere, box, capsule); EVERYWHERE applies in the whole domain. */
+enum { SLOSH_MANIP_DRAIN = 0, SLOSH_MANIP_DIRECTIONAL = 1, SLOSH_MANIP_RADIAL = 2, SLOSH_MANIP_SWIRL = 3, SLOSH_MANIP_DRAG = 4 };
+enum { SLOSH_SHAPE_SPHERE = 0, SLOSH_SHAPE_BOX = 1, SLOSH_SHAPE_CAPSULE = 2, SLOSH_SHAPE_EVERYWHERE = 3 };
+
 /* FSloshManipulatorGPU (SloshTypes.h:66-80). */
 typedef struct slosh_manipulator_t {
     float center[3];

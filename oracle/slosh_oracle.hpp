@@ -360,6 +360,13 @@ inline bool layout_equals(const slosh_settings_t& a, const slosh_settings_t& b) 
            a.sparse_storage_budget == b.sparse_storage_budget;
 }
 
+// Transcendentals of emission, drag and drain: evaluated in double and rounded to float, as the CUDA
+// path does (float sinf/cosf/expf/powf of the C library and of CUDA differ in the last bit).
+inline float sin_r(float x) { return float(std::sin(double(x))); }
+inline float cos_r(float x) { return float(std::cos(double(x))); }
+inline float exp_r(float x) { return float(std::exp(double(x))); }
+inline float pow_r(float x, float y) { return float(std::pow(double(x), double(y))); }
+
 // ---- canonical FP64 reduction tree of the PCG dots -------------------------------------------
 // One partial per 8^3 brick (v in local order x + 8 y + 64 z): 32 lanes; in round k = 0..3 lane t owns
 // the 4 cells x = 4h .. 4h + 3 of row y in plane z (h = t & 1, y = (t >> 1) & 7, z = 2k + (t >> 4)) and
@@ -647,8 +654,8 @@ public:
                 float cos_t = 2.0f * rnd.x - 1.0f;
                 float sin_t = std::sqrt(saturate(1.0f - cos_t * cos_t));
                 float phi = 6.28318530718f * rnd.y;
-                float r = em.extent[0] * std::pow(std::fmax(hash_to_unit(h3), 1e-6f), 1.0f / 3.0f);
-                V3<float> dir{sin_t * std::cos(phi), sin_t * std::sin(phi), cos_t};
+                float r = em.extent[0] * pow_r(std::fmax(hash_to_unit(h3), 1e-6f), 1.0f / 3.0f);
+                V3<float> dir{sin_t * cos_r(phi), sin_t * sin_r(phi), cos_t};
                 p = V3<float>{em.center[0], em.center[1], em.center[2]} + r * dir;
             } else {
                 V3<float> q{(2.0f * rnd.x - 1.0f) * em.extent[0], (2.0f * rnd.y - 1.0f) * em.extent[1],
@@ -667,10 +674,10 @@ public:
                 float t0l = length(t0);
                 t0 = V3<float>{t0.x / t0l, t0.y / t0l, t0.z / t0l};
                 V3<float> t1 = cross(dir, t0);
-                float cos_a = 1.0f + hash_to_unit(h4) * (std::cos(em.velocity_spread) - 1.0f);
+                float cos_a = 1.0f + hash_to_unit(h4) * (cos_r(em.velocity_spread) - 1.0f);
                 float sin_a = std::sqrt(saturate(1.0f - cos_a * cos_a));
                 float phi = 6.28318530718f * hash_to_unit(h5);
-                dir = cos_a * dir + sin_a * (std::cos(phi) * t0 + std::sin(phi) * t1);
+                dir = cos_a * dir + sin_a * (cos_r(phi) * t0 + sin_r(phi) * t1);
                 velocity = dir * speed * std::fmax(1.0f + em.speed_jitter * (2.0f * hash_to_unit(h6) - 1.0f), 0.0f);
             }
             ParticleU<float> part;
@@ -1554,7 +1561,7 @@ public:
                     new_vel = new_vel + (tangent - pn * R(f.param0)) * (R(f.strength) * w * dt);
                 }
             } else if (f.kind == MANIP_DRAG) {
-                new_vel = new_vel * R(std::exp(float(-R(f.strength) * w * dt)));
+                new_vel = new_vel * R(exp_r(float(-R(f.strength) * w * dt)));
             }
         }
         // Colliders (Slosh.usf:1561-1592).
@@ -1605,7 +1612,7 @@ public:
         for (uint32_t dr = 0; dr < P.num_manipulators; ++dr) {
             const slosh_manipulator_t& f = manipulators[dr];
             if (f.kind != MANIP_DRAIN || manipulator_sdf<R>(f, x) > R(0)) continue;
-            float chance = f.param0 > 0.0f ? 1.0f - std::exp(-f.param0 * P.dt) : 1.0f;
+            float chance = f.param0 > 0.0f ? 1.0f - exp_r(-f.param0 * P.dt) : 1.0f;
             if (chance >= 1.0f || hash_to_unit(pcg_hash(i * 2654435761u + P.frame_seed * 97u + dr)) < chance) {
                 particles[i] = dead_particle();
                 local_stats[15] += 1u;

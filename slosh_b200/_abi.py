@@ -28,6 +28,8 @@ ERR_CAPACITY = 8
 WARNINGS = (WARN_POOL_OVERFLOW, ERR_NOT_CONVERGED)
 
 TRANSFER_FLIP, TRANSFER_APIC = 0, 1
+MANIP_DRAIN, MANIP_DIRECTIONAL, MANIP_RADIAL, MANIP_SWIRL, MANIP_DRAG = 0, 1, 2, 3, 4
+SHAPE_SPHERE, SHAPE_BOX, SHAPE_CAPSULE, SHAPE_EVERYWHERE = 0, 1, 2, 3
 SOLVER_RBGS, SOLVER_MGPCG = 0, 1
 COLLIDER_SPHERE, COLLIDER_BOX, COLLIDER_CAPSULE = 0, 1, 2
 EMIT_FILL_CELLS, EMIT_SPHERE, EMIT_BOX = 0, 1, 2

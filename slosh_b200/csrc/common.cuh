@@ -227,6 +227,14 @@ __device__ __forceinline__ float3 collider_normal(const slosh_collider_t& c, flo
 __device__ __forceinline__ float3 collider_velocity_at(const slosh_collider_t& c, float3 p) {
     return addf3(ld3(c.linear_velocity), cross3(ld3(c.angular_velocity), sub3(p, ld3(c.center))));
 }
+// The few transcendental functions of the path (emission shapes and velocity spread, drag, drain
+// chance) are evaluated in double and rounded to float. The CPU restatement does the same with the C
+// library's double functions, so both sides agree unless the exact value lies within a few double ulps
+// of a float rounding boundary (float sinf/cosf/expf/powf of the two libraries differ in the last bit).
+__device__ __forceinline__ float sin_r(float x) { return float(sin(double(x))); }
+__device__ __forceinline__ float cos_r(float x) { return float(cos(double(x))); }
+__device__ __forceinline__ float exp_r(float x) { return float(exp(double(x))); }
+__device__ __forceinline__ float pow_r(float x, float y) { return float(pow(double(x), double(y))); }
 __device__ __forceinline__ float manipulator_sdf(const slosh_manipulator_t& f, float3 p) {
     if (f.shape == MANIP_SHAPE_EVERYWHERE) return -1.0f;
     slosh_collider_t c;

@@ -49,8 +49,8 @@ __global__ void k_emit(Dev d, slosh_particle_t* __restrict__ particles, const ui
         const float cos_t = 2.0f * rnd.x - 1.0f;
         const float sin_t = sqrtf(saturatef(1.0f - cos_t * cos_t));
         const float phi = 6.28318530718f * rnd.y;
-        const float r = em.extent[0] * powf(fmaxf(hash_to_unit(h3), 1e-6f), 1.0f / 3.0f);
-        pos = addf3(ld3(em.center), scale3(r, make_float3(sin_t * cosf(phi), sin_t * sinf(phi), cos_t)));
+        const float r = em.extent[0] * pow_r(fmaxf(hash_to_unit(h3), 1e-6f), 1.0f / 3.0f);
+        pos = addf3(ld3(em.center), scale3(r, make_float3(sin_t * cos_r(phi), sin_t * sin_r(phi), cos_t)));
     } else {
         const float3 q = make_float3((2.0f * rnd.x - 1.0f) * em.extent[0], (2.0f * rnd.y - 1.0f) * em.extent[1],
                                      (2.0f * rnd.z - 1.0f) * em.extent[2]);
@@ -68,10 +68,10 @@ __global__ void k_emit(Dev d, slosh_particle_t* __restrict__ particles, const ui
         const float t0l = len3(t0);
         t0 = make_float3(t0.x / t0l, t0.y / t0l, t0.z / t0l);
         const float3 t1 = cross3(dir, t0);
-        const float cos_a = 1.0f + hash_to_unit(h4) * (cosf(em.velocity_spread) - 1.0f);
+        const float cos_a = 1.0f + hash_to_unit(h4) * (cos_r(em.velocity_spread) - 1.0f);
         const float sin_a = sqrtf(saturatef(1.0f - cos_a * cos_a));
         const float phi = 6.28318530718f * hash_to_unit(h5);
-        dir = addf3(scale3(cos_a, dir), scale3(sin_a, addf3(scale3(cosf(phi), t0), scale3(sinf(phi), t1))));
+        dir = addf3(scale3(cos_a, dir), scale3(sin_a, addf3(scale3(cos_r(phi), t0), scale3(sin_r(phi), t1))));
         velocity = mul3s(mul3s(dir, speed), fmaxf(1.0f + em.speed_jitter * (2.0f * hash_to_unit(h6) - 1.0f), 0.0f));
     }
     ParticleF p;
@@ -434,7 +434,7 @@ __global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p(Dev d, Pass p, slosh_par
                         nv = addf3(nv, mul3s(sub3(tangent, mul3s(pn, f.param0)), f.strength * w * dt));
                     }
                 } else if (f.kind == MANIP_DRAG) {
-                    nv = mul3s(nv, expf(-f.strength * w * dt));
+                    nv = mul3s(nv, exp_r(-f.strength * w * dt));
                 }
             }
             // Colliders.
@@ -491,7 +491,7 @@ __global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p(Dev d, Pass p, slosh_par
             for (uint32_t dr = 0; dr < p.num_manipulators && !drained; ++dr) {
                 const slosh_manipulator_t& f = d.manipulators[dr];
                 if (f.kind != MANIP_DRAIN || manipulator_sdf(f, x) > 0.0f) continue;
-                const float chance = f.param0 > 0.0f ? 1.0f - expf(-f.param0 * dt) : 1.0f;
+                const float chance = f.param0 > 0.0f ? 1.0f - exp_r(-f.param0 * dt) : 1.0f;
                 if (chance >= 1.0f || hash_to_unit(pcg_hash(i * 2654435761u + p.frame_seed * 97u + dr)) < chance) {
                     store_dead(particles, i);
                     atomicAdd(d.stats + 15, 1u);

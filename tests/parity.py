@@ -4,6 +4,8 @@ Pool buffers are compared over the slots of the active bricks (stale data in fre
 plus the null slot 0, which must stay all zeros in both."""
 import numpy as np
 
+from slosh_b200 import _abi as A
+
 POOL_CELL = ("CELL_TYPE", "CELL_COUNT", "PRESSURE", "DIVERGENCE", "CELL_DIAG", "DENSITY_Q", "DENSITY_RHS")
 POOL_FACE = ("VEL", "FACE_FLAGS", "FACE_WEIGHT")
 TABLES = ("BRICK_TABLE", "SLOT_BRICK", "FREE_SLOTS", "ACTIVE_BRICKS", "NEW_SLOTS", "BRICK_TOUCH")
@@ -87,3 +89,40 @@ def compare_state(gpu, orc, report=None, particles=True):
     r.add("STATS", gpu.read("STATS"), orc.read("STATS"))
     r.add("PARTICLE_COUNT", gpu.read("PARTICLE_COUNT"), orc.read("PARTICLE_COUNT"))
     return r
+
+
+def pair(slosh, oracle_mod, sc):
+    """A GPU context and an oracle on the same scene settings and emission seed."""
+    g = slosh.Simulation(sc["settings"])
+    o = oracle_mod.Oracle(sc["settings"])
+    g.set_emit_seed(sc["seed"])
+    o.set_emit_seed(sc["seed"])
+    return g, o
+
+
+def run_frames(g, o, sc, frames, check_every_substep=True, tol=1e-5):
+    """Steps GPU and oracle frame by frame (emits on the first frame; colliders and manipulators every
+    frame) and compares the whole state after every substep and the results after every frame."""
+    extra = dict(colliders=sc.get("colliders", []), manipulators=sc.get("manipulators", []))
+    fi = A.frame_input(sc["settings"], emits=sc["emits"], **extra)
+    reports = []
+    for f in range(frames):
+        ng, dtg = g.begin_frame(fi)
+        no, dto = o.begin_frame(fi)
+        assert (ng, dtg) == (no, dto), f"frame {f}: substeps/dt differ {ng, dtg} vs {no, dto}"
+        for s in range(ng):
+            g.substep(s)
+            o.substep(s)
+            if check_every_substep:
+                r = compare_state(g, o)
+                bad = r.failures(tol)
+                assert not bad, f"frame {f} substep {s}:\n{r}"
+                reports.append(r)
+        g.end_frame()
+        o.end_frame()
+        rg, ro = g.results(), o.results()
+        assert rg.fluid_cells == ro.fluid_cells
+        assert rg.max_particle_speed == ro.max_particle_speed
+        assert rg.last_solve_iterations == ro.last_solve_iterations
+        fi = A.frame_input(sc["settings"], **extra)
+    return reports

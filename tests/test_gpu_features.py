@@ -1,0 +1,106 @@
+"""GPU parity of the paths the default scene does not exercise, each against the oracle, state compared
+after every substep (bit-exact; 1e-5 relative L2 is the stated float tolerance): FLIP transfer, viscosity,
+manipulators and drains, sphere/box emission with velocity spread and speed jitter, one-sided density
+correction, warm start from zero, the dense (non-sparse) pool, and red-black SOR on a sparse scene large
+enough to use every pool path."""
+import pytest
+
+from slosh_b200 import _abi as A
+from slosh_b200 import scenes
+
+from parity import pair, run_frames
+
+pytestmark = pytest.mark.gpu
+
+
+def _manip(kind, shape, center, extent=(0.2, 0.2, 0.2), axis=(0.0, 1.0, 0.0), strength=5.0, falloff=0.1,
+           param0=0.0, param1=0.0):
+    m = A.Manipulator()
+    m.center[:] = list(center)
+    m.kind = kind
+    m.rotation[:] = [0.0, 0.0, 0.0, 1.0]
+    m.extent[:] = list(extent)
+    m.shape = shape
+    m.axis[:] = list(axis)
+    m.strength = strength
+    m.falloff = falloff
+    m.param0 = param0
+    m.param1 = param1
+    return m
+
+
+def _emit(shape, center, extent, velocity, count, spread=0.3, jitter=0.2):
+    e = A.EmitRequest()
+    e.shape = shape
+    e.center[:] = list(center)
+    e.extent[:] = list(extent)
+    e.velocity[:] = list(velocity)
+    e.rotation[:] = [0.0, 0.38268343, 0.0, 0.92387953]
+    e.velocity_spread = spread
+    e.speed_jitter = jitter
+    e.count = count
+    e.fill_jitter = 0.8
+    return e
+
+
+def test_flip_transfer(slosh, oracle_mod):
+    sc = scenes.tiny(slosh.settings_default, n=16)
+    sc["settings"].transfer_mode = A.TRANSFER_FLIP
+    sc["settings"].flip_ratio = 0.95
+    run_frames(*pair(slosh, oracle_mod, sc), sc, frames=4)
+
+
+def test_viscosity(slosh, oracle_mod):
+    sc = scenes.tiny(slosh.settings_default, n=16)
+    sc["settings"].kinematic_viscosity = 0.05
+    sc["settings"].viscosity_iterations = 4
+    run_frames(*pair(slosh, oracle_mod, sc), sc, frames=4)
+
+
+def test_manipulators_and_drain(slosh, oracle_mod):
+    sc = scenes.tiny(slosh.settings_default, n=24)
+    sc["manipulators"] = [
+        _manip(A.MANIP_DIRECTIONAL, A.SHAPE_SPHERE, (0.25, 0.3, 0.5), extent=(0.15, 0, 0), axis=(1.0, 0.0, 0.0)),
+        _manip(A.MANIP_RADIAL, A.SHAPE_BOX, (0.6, 0.2, 0.5), extent=(0.1, 0.1, 0.3), strength=-3.0),
+        _manip(A.MANIP_SWIRL, A.SHAPE_EVERYWHERE, (0.5, 0.5, 0.5), axis=(0.0, 1.0, 0.0), strength=2.0, param0=0.5),
+        _manip(A.MANIP_DRAG, A.SHAPE_CAPSULE, (0.3, 0.2, 0.5), extent=(0.08, 0.2, 0), strength=4.0),
+        _manip(A.MANIP_DRAIN, A.SHAPE_BOX, (0.1, 0.08, 0.5), extent=(0.08, 0.06, 0.2), param0=20.0),
+    ]
+    g, o = pair(slosh, oracle_mod, sc)
+    run_frames(g, o, sc, frames=5)
+    assert g.results().drained_particles == o.results().drained_particles
+
+
+def test_sphere_and_box_emission(slosh, oracle_mod):
+    sc = scenes.tiny(slosh.settings_default, n=24)
+    sc["settings"].particle_capacity = sc["particles"] + 20000
+    sc["emits"] = list(sc["emits"]) + [
+        _emit(A.EMIT_SPHERE, (0.7, 0.7, 0.5), (0.12, 0, 0), (0.0, -1.5, 0.3), 6000),
+        _emit(A.EMIT_BOX, (0.75, 0.35, 0.4), (0.08, 0.05, 0.1), (-0.5, 0.0, 0.0), 5000, spread=0.0, jitter=0.5),
+    ]
+    run_frames(*pair(slosh, oracle_mod, sc), sc, frames=4)
+
+
+def test_one_sided_density_correction(slosh, oracle_mod):
+    sc = scenes.tiny(slosh.settings_default, n=16)
+    sc["settings"].two_sided_density_projection = 0
+    sc["settings"].density_correction = 0.15
+    run_frames(*pair(slosh, oracle_mod, sc), sc, frames=4)
+
+
+def test_warm_start_zero(slosh, oracle_mod):
+    sc = scenes.tiny(slosh.settings_default, n=16)
+    sc["settings"].warm_start = A.WARM_START_ZERO
+    run_frames(*pair(slosh, oracle_mod, sc), sc, frames=3)
+
+
+def test_dense_pool(slosh, oracle_mod):
+    sc = scenes.tiny(slosh.settings_default, n=24)
+    sc["settings"].sparse_bricks = 0
+    run_frames(*pair(slosh, oracle_mod, sc), sc, frames=3)
+
+
+def test_rbgs_sparse_scene(slosh, oracle_mod):
+    sc = scenes.dam_break_sphere(slosh.settings_default, n=64, solver=A.SOLVER_RBGS, sor_iterations=60)
+    sc["settings"].max_substeps = 16
+    run_frames(*pair(slosh, oracle_mod, sc), sc, frames=2)

@@ -9,44 +9,19 @@ import pytest
 from slosh_b200 import _abi as A
 from slosh_b200 import scenes
 
-from parity import compare_state
+from parity import compare_state, pair, run_frames
 
 pytestmark = pytest.mark.gpu
 
-FLOAT_TOL = 1e-5
+FLOAT_TOL = 1e-5  # stated float tolerance (relative L2); the states match bit for bit
 
 
 def _pair(slosh, oracle_mod, sc):
-    g = slosh.Simulation(sc["settings"])
-    o = oracle_mod.Oracle(sc["settings"])
-    g.set_emit_seed(sc["seed"])
-    o.set_emit_seed(sc["seed"])
-    return g, o
+    return pair(slosh, oracle_mod, sc)
 
 
 def _run_frames(g, o, sc, frames, check_every_substep=True):
-    fi = A.frame_input(sc["settings"], emits=sc["emits"], colliders=sc.get("colliders", []))
-    reports = []
-    for f in range(frames):
-        ng, dtg = g.begin_frame(fi)
-        no, dto = o.begin_frame(fi)
-        assert (ng, dtg) == (no, dto), f"frame {f}: substeps/dt differ {ng, dtg} vs {no, dto}"
-        for s in range(ng):
-            g.substep(s)
-            o.substep(s)
-            if check_every_substep:
-                r = compare_state(g, o)
-                bad = r.failures(FLOAT_TOL)
-                assert not bad, f"frame {f} substep {s}:\n{r}"
-                reports.append(r)
-        g.end_frame()
-        o.end_frame()
-        rg, ro = g.results(), o.results()
-        assert rg.fluid_cells == ro.fluid_cells
-        assert rg.max_particle_speed == ro.max_particle_speed
-        assert rg.last_solve_iterations == ro.last_solve_iterations
-        fi = A.frame_input(sc["settings"], colliders=sc.get("colliders", []))
-    return reports
+    return run_frames(g, o, sc, frames, check_every_substep, FLOAT_TOL)
 
 
 def test_emission_bit_exact(slosh, oracle_mod):
