@@ -280,6 +280,7 @@ typedef enum slosh_buffer_id {
     SLOSH_BUF_PARTICLE_COUNT = 22, /* u32[4] */
     SLOSH_BUF_ACCUM = 23,       /* i32[2 * total_faces] */
     SLOSH_BUF_VEL_EXTRAP = 24,  /* f32[total_faces]: displacement / scratch velocity buffer of the last G2P */
+    SLOSH_BUF_COUPLING = 25,    /* i32[SLOSH_MAX_COLLIDERS * SLOSH_COUPLING_STRIDE]: this frame's collider accumulators */
     SLOSH_BUF_COUNT_
 } slosh_buffer_id;
 

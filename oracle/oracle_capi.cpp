@@ -134,6 +134,7 @@ View<R> view(Sim<R>& s, int id) {
         case SLOSH_BUF_PARTICLE_COUNT: v.ptr = s.particle_count; v.count = 4; v.elem = 4; break;
         case SLOSH_BUF_ACCUM: i32(s.accum, s.accum.size()); break;
         case SLOSH_BUF_VEL_EXTRAP: real(s.vel[s.last_disp_index]); break;
+        case SLOSH_BUF_COUPLING: v.ptr = s.coupling; v.count = SLOSH_MAX_COLLIDERS * SLOSH_COUPLING_STRIDE; v.elem = 4; break;
         default: break;
     }
     return v;

@@ -1299,7 +1299,215 @@ public:
         return den > 0.0 ? std::sqrt(num / den) : 0.0;
     }
 
-    // ---- ProjectFace, Slosh.usf:995-1052 (coupling accumulation is the next tier) ---------------------------
+    // ---- two-way collider coupling (Slosh.usf:897-993, 1062-1216, 1316-1370) ------------------------------
+    // Per-collider integer accumulators in 1/1024 fixed point (CouplingScale): the sums do not depend on
+    // the order of the additions. Slots: 0-2 force, 3-5 torque, 6 wetted faces, 7 submerged cells,
+    // 8-10 fluid velocity sum, 11 solid cells, 12-14 submerged centroid offset sum.
+    bool two_way(uint32_t k) const { return (colliders[k].flags & COLLIDER_FLAG_TWO_WAY) != 0u; }
+    // The cell loops run under OpenMP, so the additions are atomic (wrapping, as the GPU's integer atomics).
+    void coupling_add_i(uint32_t k, int slot, int32_t v) {
+        uint32_t* a = reinterpret_cast<uint32_t*>(&coupling[k * SLOSH_COUPLING_STRIDE + uint32_t(slot)]);
+        #pragma omp atomic
+        *a += uint32_t(v);
+    }
+    void coupling_add(uint32_t k, int slot, R v) { coupling_add_i(k, slot, to_i32_rn<R>(v * R(P.coupling_scale))); }
+    void coupling_count(uint32_t k, int slot) { coupling_add_i(k, slot, 1); }
+    V3<R> collider_center(uint32_t k) const { return {R(colliders[k].center[0]), R(colliders[k].center[1]), R(colliders[k].center[2])}; }
+    // CellCenterVelocity, Slosh.usf:897-906.
+    V3<R> cell_center_velocity(const std::vector<R>& v, I3 c) const {
+        R out[3];
+        for (int a = 0; a < 3; ++a) out[a] = R(0.5f) * (v[face_index(a, c)] + v[face_index(a, c + axis_offset(a))]);
+        return {out[0], out[1], out[2]};
+    }
+    // AccumulatePressureForce, Slosh.usf:913-925.
+    void accumulate_pressure_force(uint32_t k, V3<R> face_pos, V3<R> into, R p_hat) {
+        const R pa = p_hat * R(P.pressure_to_pascal);
+        const R h = R(P.cell_size);
+        const V3<R> force = ((pa * h) * h) * into;
+        const V3<R> torque = cross(face_pos - collider_center(k), force);
+        coupling_add(k, 0, force.x); coupling_add(k, 1, force.y); coupling_add(k, 2, force.z);
+        coupling_add(k, 3, torque.x); coupling_add(k, 4, torque.y); coupling_add(k, 5, torque.z);
+    }
+    // AccumulateCoupling, Slosh.usf:929-946: wetted face of a two-way collider (+ binary force when the
+    // smoothed estimator is off).
+    void accumulate_coupling(uint32_t k, const std::vector<R>& v, I3 fluid_cell, V3<R> face_pos, V3<R> into, R p_hat) {
+        if (!two_way(k)) return;
+        if (P.smooth_coupling == 0u) accumulate_pressure_force(k, face_pos, into, p_hat);
+        const V3<R> fv = cell_center_velocity(v, fluid_cell);
+        coupling_count(k, 6);
+        coupling_add(k, 8, fv.x); coupling_add(k, 9, fv.y); coupling_add(k, 10, fv.z);
+    }
+    // EstimateSeepagePressure, Slosh.usf:952-977: mean pressure of the liquid first met by horizontal walks
+    // (x+, x-, y+, y-; up to 16 cells) out of body `id`.
+    bool seepage_pressure(I3 body, uint32_t id, R& p_hat) const {
+        const I3 dirs[4] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}};
+        R sum = R(0), count = R(0);
+        for (int k = 0; k < 4; ++k) {
+            I3 q = body;
+            for (int step = 0; step < 16; ++step) {
+                q = q + dirs[k];
+                const uint32_t t = get_cell_type(q);
+                if (type_of(t) != CELL_SOLID || collider_of(t) != id) {
+                    if (type_of(t) == CELL_FLUID) {
+                        sum = sum + pressure[cell_index(q)];
+                        count = count + R(1);
+                    }
+                    break;
+                }
+            }
+        }
+        p_hat = count > R(0) ? sum / count : R(0);
+        return count > R(0);
+    }
+    // AccumulateContact, Slosh.usf:979-992.
+    void accumulate_contact(uint32_t solid_packed, I3 body, V3<R> face_pos, V3<R> into) {
+        const uint32_t id = collider_of(solid_packed);
+        if (id == 0u || !two_way(id - 1u)) return;
+        R ph;
+        if (seepage_pressure(body, id, ph)) accumulate_pressure_force(id - 1u, face_pos, into, ph);
+    }
+    // The coupling terms of ProjectFace (Slosh.usf:1004-1029), evaluated after the projection pass on the
+    // projected field (the reference samples the wetted-face velocity while the same pass writes it).
+    void coupling_faces(const std::vector<R>& v) {
+        if (P.num_colliders == 0u) return;
+        for_active_cells([&](uint32_t, I3 c) {
+            for (int axis = 0; axis < 3; ++axis) {
+                const I3 ca = c - axis_offset(axis), cb = c;
+                const uint32_t a = get_cell_type(ca), b = get_cell_type(cb);
+                const V3<R> e{axis == 0 ? R(1) : R(0), axis == 1 ? R(1) : R(0), axis == 2 ? R(1) : R(0)};
+                const V3<R> ne{axis == 0 ? R(-1) : R(0), axis == 1 ? R(-1) : R(0), axis == 2 ? R(-1) : R(0)};
+                if (type_of(a) == CELL_SOLID && type_of(b) == CELL_SOLID) {
+                    if (collider_of(a) != collider_of(b)) {
+                        const V3<R> fp = face_position(axis, c);
+                        accumulate_contact(b, cb, fp, e);
+                        accumulate_contact(a, ca, fp, ne);
+                    }
+                } else if (type_of(a) == CELL_SOLID || type_of(b) == CELL_SOLID) {
+                    if (type_of(a) == CELL_FLUID && collider_of(b) != 0u)
+                        accumulate_coupling(collider_of(b) - 1u, v, ca, face_position(axis, c), e, pressure[cell_index(ca)]);
+                    else if (type_of(b) == CELL_FLUID && collider_of(a) != 0u)
+                        accumulate_coupling(collider_of(a) - 1u, v, cb, face_position(axis, c), ne, pressure[cell_index(cb)]);
+                }
+            }
+        });
+    }
+    // FluidPressureGradient, Slosh.usf:1086-1101.
+    V3<R> fluid_pressure_gradient(I3 c, R pc) const {
+        R g[3];
+        for (int a = 0; a < 3; ++a) {
+            const I3 e = axis_offset(a);
+            const bool bp = type_of(get_cell_type(c + e)) == CELL_FLUID, bm = type_of(get_cell_type(c - e)) == CELL_FLUID;
+            const R pp = bp ? pressure[cell_index(c + e)] : R(0);
+            const R pm = bm ? pressure[cell_index(c - e)] : R(0);
+            g[a] = bp && bm ? (pp - pm) * R(0.5f) : (bp ? pp - pc : (bm ? pc - pm : R(0)));
+        }
+        const R ih = R(P.inv_cell_size);
+        return {g[0] * ih, g[1] * ih, g[2] * ih};
+    }
+    // BodySurfacePressure, Slosh.usf:1105-1125.
+    bool body_surface_pressure(I3 c, R& p_hat) const {
+        R sum = R(0), count = R(0);
+        for (int n = 0; n < 6; ++n) {
+            I3 d{0, 0, 0};
+            d[n >> 1] = (n & 1) ? 1 : -1;
+            const I3 nb = c + d;
+            if (type_of(get_cell_type(nb)) == CELL_FLUID) {
+                const R pn = pressure[cell_index(nb)];
+                const R slope = type_of(get_cell_type(nb + d)) == CELL_FLUID ? pressure[cell_index(nb + d)] - pn : R(0);
+                sum = sum + (pn - R(0.5f) * slope);
+                count = count + R(1);
+            }
+        }
+        p_hat = count > R(0) ? sum / count : R(0);
+        return count > R(0);
+    }
+    // CouplingForceCS, Slosh.usf:1127-1216: smoothed pressure force and torque on two-way colliders.
+    void coupling_force() {
+        const R h = R(P.cell_size), ih = R(P.inv_cell_size);
+        for_active_cells([&](uint32_t index, I3 c) {
+            const uint32_t packed = cell_type[index];
+            const uint32_t type = type_of(packed);
+            if (type == CELL_AIR) return;
+            const V3<R> x{(R(c.x) + R(0.5f)) * h, (R(c.y) + R(0.5f)) * h, (R(c.z) + R(0.5f)) * h};
+            R p_hat = R(0);
+            V3<R> g{R(0), R(0), R(0)};
+            bool have = false;
+            if (type == CELL_FLUID) {
+                p_hat = pressure[index];
+                g = fluid_pressure_gradient(c, p_hat);
+                have = true;
+            } else if (collider_of(packed) != 0u) {
+                have = body_surface_pressure(c, p_hat);
+            }
+            if (!have) return;
+            for (uint32_t k = 0; k < P.num_colliders; ++k) {
+                const slosh_collider_t& col = colliders[k];
+                if ((col.flags & COLLIDER_FLAG_TWO_WAY) == 0u || std::fabs(collider_sdf<R>(col, x)) > h) continue;
+                if (type == CELL_SOLID && collider_of(packed) != k + 1u) continue;
+                R sp = p_hat;
+                if (type == CELL_FLUID) {
+                    const R phi = collider_sdf<R>(col, x);
+                    sp = sp + dot(g, (-phi) * collider_normal<R>(col, x, R(0.25f) * h));
+                }
+                const R scale = (((-sp) * R(P.pressure_to_pascal)) * h) * h;
+                V3<R> force{R(0), R(0), R(0)}, torque{R(0), R(0), R(0)};
+                const V3<R> center = collider_center(k);
+                for (int n = 0; n < 6; ++n) {
+                    V3<R> normal{R(0), R(0), R(0)};
+                    I3 d{0, 0, 0};
+                    const R sgn = (n & 1) ? R(1) : R(-1);
+                    if (n >> 1 == 0) { normal.x = sgn; d.x = (n & 1) ? 1 : -1; }
+                    else if (n >> 1 == 1) { normal.y = sgn; d.y = (n & 1) ? 1 : -1; }
+                    else { normal.z = sgn; d.z = (n & 1) ? 1 : -1; }
+                    const V3<R> fp = x + (R(0.5f) * h) * normal;
+                    if (type == CELL_SOLID) {
+                        const uint32_t nbp = get_cell_type(c + d);
+                        if (type_of(nbp) == CELL_SOLID && collider_of(nbp) != k + 1u) continue;
+                    }
+                    const R w = saturate(R(0.5f) + collider_sdf<R>(col, fp) * ih);
+                    const V3<R> df = (scale * w) * normal;
+                    force = force + df;
+                    torque = torque + cross(fp - center, df);
+                }
+                coupling_add(k, 0, force.x); coupling_add(k, 1, force.y); coupling_add(k, 2, force.z);
+                coupling_add(k, 3, torque.x); coupling_add(k, 4, torque.y); coupling_add(k, 5, torque.z);
+            }
+        });
+    }
+    // SubmergedCS, Slosh.usf:1316-1370: solid cells per collider and the submerged ones (a horizontal walk out
+    // of the body meets dense fluid with no air in the three cells below), with their centroid offset.
+    void submerged() {
+        const R h = R(P.cell_size);
+        const I3 dirs[4] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}};
+        for_active_cells([&](uint32_t index, I3 c) {
+            const uint32_t packed = cell_type[index];
+            const uint32_t id = collider_of(packed);
+            if (type_of(packed) != CELL_SOLID || id == 0u) return;
+            coupling_count(id - 1u, 11);
+            bool sub = false;
+            for (int k = 0; k < 4; ++k) {
+                I3 q = c;
+                for (int step = 0; step < 12; ++step) {
+                    q = q + dirs[k];
+                    const uint32_t t = get_cell_type(q);
+                    if (type_of(t) != CELL_SOLID || collider_of(t) != id) {
+                        bool liquid = type_of(t) == CELL_FLUID && (t & CELL_DENSE_FLAG) != 0u;
+                        for (int below = 1; below <= 3; ++below)
+                            liquid = liquid && type_of(get_cell_type(q - I3{0, 0, below})) != CELL_AIR;
+                        sub = sub || liquid;
+                        break;
+                    }
+                }
+            }
+            if (sub) {
+                const V3<R> off = V3<R>{(R(c.x) + R(0.5f)) * h, (R(c.y) + R(0.5f)) * h, (R(c.z) + R(0.5f)) * h} - collider_center(id - 1u);
+                coupling_count(id - 1u, 7);
+                coupling_add(id - 1u, 12, off.x); coupling_add(id - 1u, 13, off.y); coupling_add(id - 1u, 14, off.z);
+            }
+        });
+    }
+
+    // ---- ProjectFace, Slosh.usf:995-1052 (the coupling terms are accumulated by coupling_faces) -------------
     void project(std::vector<R>& v) {
         for_active_cells([&](uint32_t index, I3 c) {
             for (int axis = 0; axis < 3; ++axis) {
@@ -1761,6 +1969,8 @@ public:
             if (S.pressure_solver != SLOSH_SOLVER_MGPCG) last_solve_rel_residual = last_solve_true_rel_residual;
         }
         project(vel[c]);
+        coupling_faces(vel[c]);
+        if (P.num_colliders > 0u && P.smooth_coupling != 0u) coupling_force();
         if (last) residual(vel[c]);
         const bool density = density_projection_this_frame && last;
         if (density) {
@@ -1789,6 +1999,7 @@ public:
     }
 
     void end_frame() {
+        if (P.num_colliders > 0u && substeps > 0) submerged();  // once per frame, after the last substep
         // AccumulateStatsCS (Slosh.usf:264-270)
         particle_count[2] += stats[15];
         stats[14] = particle_count[0];

@@ -41,7 +41,7 @@ BUF = dict(
     PARTICLES=0, VEL=1, VEL_OLD=2, FACE_FLAGS=3, FACE_WEIGHT=4, CELL_TYPE=5, CELL_COUNT=6, PRESSURE=7,
     DIVERGENCE=8, CELL_DIAG=9, DENSITY_Q=10, DENSITY_RHS=11, BRICK_TABLE=12, SLOT_BRICK=13, FREE_SLOTS=14,
     ACTIVE_BRICKS=15, NEW_SLOTS=16, BRICK_TOUCH=17, STATS=18, SORT_COUNTS=19, SORT_OFFSETS=20, SORT_PERM=21,
-    PARTICLE_COUNT=22, ACCUM=23, VEL_EXTRAP=24,
+    PARTICLE_COUNT=22, ACCUM=23, VEL_EXTRAP=24, COUPLING=25,
 )
 BUF_DTYPE = dict(
     PARTICLES=None, VEL=np.float32, VEL_OLD=np.float32, FACE_FLAGS=np.uint32, FACE_WEIGHT=np.float32,
@@ -49,7 +49,7 @@ BUF_DTYPE = dict(
     DENSITY_Q=np.float32, DENSITY_RHS=np.float32, BRICK_TABLE=np.uint32, SLOT_BRICK=np.uint32,
     FREE_SLOTS=np.uint32, ACTIVE_BRICKS=np.uint32, NEW_SLOTS=np.uint32, BRICK_TOUCH=np.uint32, STATS=np.uint32,
     SORT_COUNTS=np.uint32, SORT_OFFSETS=np.uint32, SORT_PERM=np.uint32, PARTICLE_COUNT=np.uint32,
-    ACCUM=np.int32, VEL_EXTRAP=np.float32,
+    ACCUM=np.int32, VEL_EXTRAP=np.float32, COUPLING=np.int32,
 )
 
 

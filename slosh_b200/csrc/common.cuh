@@ -20,6 +20,8 @@ namespace slosh {
 
 constexpr uint32_t CELL_AIR = 0u, CELL_FLUID = 1u, CELL_SOLID = 2u, CELL_TYPE_MASK = 3u;
 constexpr uint32_t CELL_DENSE_FLAG = 4u, CELL_COLLIDER_SHIFT = 8u;
+constexpr uint32_t COLLIDER_FLAG_TWO_WAY = 1u;  // SloshCommon.ush:42
+constexpr float COUPLING_SCALE = 1024.0f;      // fixed point of the coupling accumulators (CouplingFixedScale)
 constexpr uint32_t FACE_VALID = 1u, FACE_SOLID = 2u, FACE_HAS_WEIGHT = 4u, FACE_EXTRAP_SHIFT = 4u;
 constexpr uint32_t BRICK_CELLS = 512u, NO_BRICK = 0xFFFFFFFFu;
 constexpr float P2G_FIXED_SCALE = 1048576.0f;
@@ -71,7 +73,7 @@ struct Pass {
     float flip_ratio, max_speed, friction, adhesion_accel, adhesion_range, particle_radius;
     float viscosity_alpha, warm_start_scale, pressure_to_pascal, density_correction, target_ppc;
     float density_deadband, density_relaxation;
-    uint32_t use_apic, ghost_fluid, num_colliders, num_manipulators, frame_seed;
+    uint32_t use_apic, ghost_fluid, num_colliders, num_manipulators, frame_seed, smooth_coupling;
 };
 
 // ---- small helpers ------------------------------------------------------------------------------

@@ -512,6 +512,7 @@ struct Ctx {
         P.density_deadband = std::max(s.density_deadband, 0.0f);
         P.warm_start_scale = 1.0f;
         P.ghost_fluid = s.ghost_fluid ? 1u : 0u;
+        P.smooth_coupling = s.smooth_coupling_force ? 1u : 0u;
         const int interval = clampi_h(s.density_projection_interval, 1, 8);
         P.density_relaxation = 1.0f - std::pow(1.0f - clampf_h(s.density_relaxation, 0.0f, 1.0f), float(interval));
     }
@@ -734,6 +735,7 @@ struct Ctx {
         {
             PhaseScope ps(this, 5);
             count(launch_project(d, P, V[c], shape, stream));
+            count(launch_coupling(d, P, V[c], shape, stream));
             if (last) count(launch_residual(d, P, V[c], shape, stream));
         }
         const bool density = density_frame && last;
@@ -779,6 +781,7 @@ __global__ void k_accumulate_stats(uint32_t* stats, uint32_t* pc) {  // Accumula
 }
 
 void Ctx::end_frame() {
+    if (num_colliders > 0 && substeps > 0) count(launch_submerged(dev(), shape, stream));  // SloshProxy.cpp:715-718
     k_accumulate_stats<<<1, 1, 0, stream>>>(stats, particle_count);
     count(1);
     CK(cudaGetLastError());
@@ -896,6 +899,7 @@ BufView buffer_view(Ctx& c, int id) {
         case SLOSH_BUF_PARTICLE_COUNT: v = {c.particle_count, 16}; break;
         case SLOSH_BUF_ACCUM: v = {c.accum, 2 * tf * 4}; break;
         case SLOSH_BUF_VEL_EXTRAP: v = {c.vel[c.disp_phys], tf * 4}; break;
+        case SLOSH_BUF_COUPLING: v = {c.coupling, size_t(SLOSH_MAX_COLLIDERS) * SLOSH_COUPLING_STRIDE * 4}; break;
         default: break;
     }
     return v;

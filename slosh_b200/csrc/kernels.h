@@ -29,6 +29,10 @@ int launch_divergence(const Dev& d, const Pass& p, const float* vel, const Shape
 int launch_rbgs(const Dev& d, float* pres, const float* rhs, uint32_t parity, float omega, const Shape& sh, cudaStream_t s);
 int launch_project(const Dev& d, const Pass& p, float* vel, const Shape& sh, cudaStream_t s);
 int launch_residual(const Dev& d, const Pass& p, const float* vel, const Shape& sh, cudaStream_t s);
+// Two-way collider coupling after the projection (wetted faces, binary force, seepage contacts and, with
+// smooth coupling, the SDF-weighted force), and the per-frame submerged-cell estimate.
+int launch_coupling(const Dev& d, const Pass& p, const float* vel, const Shape& sh, cudaStream_t s);
+int launch_submerged(const Dev& d, const Shape& sh, cudaStream_t s);
 int launch_density_rhs(const Dev& d, const Pass& p, const Shape& sh, cudaStream_t s);
 int launch_density_displacement(const Dev& d, float* dst, const Shape& sh, cudaStream_t s);
 int launch_extrapolate(const Dev& d, const float* src, float* dst, uint32_t iteration, const Shape& sh, cudaStream_t s);

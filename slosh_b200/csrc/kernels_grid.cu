@@ -395,7 +395,7 @@ __global__ void __launch_bounds__(GRID_THREADS) k_rbgs(Dev d, float* __restrict_
     });
 }
 
-// ---- ProjectFace (the two-way coupling accumulation is not part of this pass) -----------------------------
+// ---- ProjectFace (its two-way coupling terms are accumulated by k_coupling_faces after the pass) ---------
 __global__ void __launch_bounds__(GRID_THREADS) k_project(Dev d, Pass p, float* __restrict__ vel) {
     for_active_cells(d, [&](uint32_t index, int3 c) {
         const uint32_t b = d.cell_type[index];
@@ -424,6 +424,216 @@ __global__ void __launch_bounds__(GRID_THREADS) k_project(Dev d, Pass p, float* 
                 flags |= FACE_VALID;
             }
             d.face_flags[f] = flags;
+        }
+    });
+}
+
+// ---- two-way collider coupling (Slosh.usf:897-993, 1062-1216, 1316-1370) ---------------------------------
+// Per-collider integer accumulators in 1/1024 fixed point, so the totals do not depend on the order of the
+// atomic additions. Slots: 0-2 force, 3-5 torque, 6 wetted faces, 7 submerged cells, 8-10 fluid velocity
+// sum, 11 solid cells, 12-14 submerged centroid offset sum.
+__device__ __forceinline__ bool two_way(const Dev& d, uint32_t k) { return (d.colliders[k].flags & COLLIDER_FLAG_TWO_WAY) != 0u; }
+__device__ __forceinline__ void coupling_add(const Dev& d, uint32_t k, int slot, float v) {
+    atomicAdd(d.coupling + k * SLOSH_COUPLING_STRIDE + uint32_t(slot), __float2int_rn(v * COUPLING_SCALE));
+}
+__device__ __forceinline__ void coupling_count(const Dev& d, uint32_t k, int slot) {
+    atomicAdd(d.coupling + k * SLOSH_COUPLING_STRIDE + uint32_t(slot), 1);
+}
+__device__ __forceinline__ float3 face_position(const Dev& d, int axis, int3 f) {  // Slosh.usf:204-208
+    return make_float3((float(f.x) + (axis == 0 ? 0.0f : 0.5f)) * d.h, (float(f.y) + (axis == 1 ? 0.0f : 0.5f)) * d.h,
+                       (float(f.z) + (axis == 2 ? 0.0f : 0.5f)) * d.h);
+}
+// CellCenterVelocity, Slosh.usf:897-906.
+__device__ __forceinline__ float3 cell_center_velocity(const Dev& d, const float* vel, int3 c) {
+    float out[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) out[a] = 0.5f * (vel[face_index(d, a, c)] + vel[face_index(d, a, add3(c, nbr_off(2 * a + 1)))]);
+    return make_float3(out[0], out[1], out[2]);
+}
+// AccumulatePressureForce, Slosh.usf:913-925.
+__device__ void accumulate_pressure_force(const Dev& d, const Pass& p, uint32_t k, float3 face_pos, float3 into, float p_hat) {
+    const float pa = p_hat * p.pressure_to_pascal;
+    const float3 force = scale3((pa * d.h) * d.h, into);
+    const float3 torque = cross3(sub3(face_pos, ld3(d.colliders[k].center)), force);
+    coupling_add(d, k, 0, force.x); coupling_add(d, k, 1, force.y); coupling_add(d, k, 2, force.z);
+    coupling_add(d, k, 3, torque.x); coupling_add(d, k, 4, torque.y); coupling_add(d, k, 5, torque.z);
+}
+// AccumulateCoupling, Slosh.usf:929-946.
+__device__ void accumulate_coupling(const Dev& d, const Pass& p, const float* vel, uint32_t k, int3 fluid_cell, float3 face_pos,
+                                    float3 into, float p_hat) {
+    if (!two_way(d, k)) return;
+    if (p.smooth_coupling == 0u) accumulate_pressure_force(d, p, k, face_pos, into, p_hat);
+    const float3 fv = cell_center_velocity(d, vel, fluid_cell);
+    coupling_count(d, k, 6);
+    coupling_add(d, k, 8, fv.x); coupling_add(d, k, 9, fv.y); coupling_add(d, k, 10, fv.z);
+}
+// EstimateSeepagePressure, Slosh.usf:952-977.
+__device__ bool seepage_pressure(const Dev& d, int3 body, uint32_t id, float& p_hat) {
+    const int3 dirs[4] = {make_int3(1, 0, 0), make_int3(-1, 0, 0), make_int3(0, 1, 0), make_int3(0, -1, 0)};
+    float sum = 0.0f, count = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        int3 q = body;
+        for (int step = 0; step < 16; ++step) {
+            q = add3(q, dirs[k]);
+            const uint32_t t = get_cell_type(d, q);
+            if (type_of(t) != CELL_SOLID || collider_of(t) != id) {
+                if (type_of(t) == CELL_FLUID) {
+                    sum = sum + d.pressure[cell_index(d, q)];
+                    count = count + 1.0f;
+                }
+                break;
+            }
+        }
+    }
+    p_hat = count > 0.0f ? sum / count : 0.0f;
+    return count > 0.0f;
+}
+// AccumulateContact, Slosh.usf:979-992.
+__device__ void accumulate_contact(const Dev& d, const Pass& p, uint32_t solid_packed, int3 body, float3 face_pos, float3 into) {
+    const uint32_t id = collider_of(solid_packed);
+    if (id == 0u || !two_way(d, id - 1u)) return;
+    float ph;
+    if (seepage_pressure(d, body, id, ph)) accumulate_pressure_force(d, p, id - 1u, face_pos, into, ph);
+}
+// The coupling terms of ProjectFace (Slosh.usf:1004-1029), on the projected field after the projection
+// pass (the reference samples the wetted-face velocity while the same pass writes it).
+__global__ void __launch_bounds__(GRID_THREADS) k_coupling_faces(Dev d, Pass p, const float* __restrict__ vel) {
+    for_active_cells(d, [&](uint32_t index, int3 c) {
+        const uint32_t b = d.cell_type[index];
+#pragma unroll
+        for (int axis = 0; axis < 3; ++axis) {
+            const int3 ca = add3(c, nbr_off(2 * axis));
+            const uint32_t a = get_cell_type(d, ca);
+            const float3 e = make_float3(axis == 0 ? 1.0f : 0.0f, axis == 1 ? 1.0f : 0.0f, axis == 2 ? 1.0f : 0.0f);
+            const float3 ne = make_float3(axis == 0 ? -1.0f : 0.0f, axis == 1 ? -1.0f : 0.0f, axis == 2 ? -1.0f : 0.0f);
+            if (type_of(a) == CELL_SOLID && type_of(b) == CELL_SOLID) {
+                if (collider_of(a) != collider_of(b)) {
+                    const float3 fp = face_position(d, axis, c);
+                    accumulate_contact(d, p, b, c, fp, e);
+                    accumulate_contact(d, p, a, ca, fp, ne);
+                }
+            } else if (type_of(a) == CELL_SOLID || type_of(b) == CELL_SOLID) {
+                if (type_of(a) == CELL_FLUID && collider_of(b) != 0u)
+                    accumulate_coupling(d, p, vel, collider_of(b) - 1u, ca, face_position(d, axis, c), e, d.pressure[cell_index(d, ca)]);
+                else if (type_of(b) == CELL_FLUID && collider_of(a) != 0u)
+                    accumulate_coupling(d, p, vel, collider_of(a) - 1u, c, face_position(d, axis, c), ne, d.pressure[index]);
+            }
+        }
+    });
+}
+// FluidPressureGradient, Slosh.usf:1086-1101.
+__device__ float3 fluid_pressure_gradient(const Dev& d, int3 c, float pc) {
+    float g[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const int3 cp = add3(c, nbr_off(2 * a + 1)), cm = add3(c, nbr_off(2 * a));
+        const bool bp = type_of(get_cell_type(d, cp)) == CELL_FLUID, bm = type_of(get_cell_type(d, cm)) == CELL_FLUID;
+        const float pp = bp ? d.pressure[cell_index(d, cp)] : 0.0f;
+        const float pm = bm ? d.pressure[cell_index(d, cm)] : 0.0f;
+        g[a] = bp && bm ? (pp - pm) * 0.5f : (bp ? pp - pc : (bm ? pc - pm : 0.0f));
+    }
+    return make_float3(g[0] * d.inv_h, g[1] * d.inv_h, g[2] * d.inv_h);
+}
+// BodySurfacePressure, Slosh.usf:1105-1125.
+__device__ bool body_surface_pressure(const Dev& d, int3 c, float& p_hat) {
+    float sum = 0.0f, count = 0.0f;
+#pragma unroll
+    for (int n = 0; n < 6; ++n) {
+        const int3 dd = nbr_off(n);
+        const int3 nb = add3(c, dd);
+        if (type_of(get_cell_type(d, nb)) == CELL_FLUID) {
+            const float pn = d.pressure[cell_index(d, nb)];
+            const int3 nb2 = add3(nb, dd);
+            const float slope = type_of(get_cell_type(d, nb2)) == CELL_FLUID ? d.pressure[cell_index(d, nb2)] - pn : 0.0f;
+            sum = sum + (pn - 0.5f * slope);
+            count = count + 1.0f;
+        }
+    }
+    p_hat = count > 0.0f ? sum / count : 0.0f;
+    return count > 0.0f;
+}
+// CouplingForceCS, Slosh.usf:1127-1216.
+__global__ void __launch_bounds__(GRID_THREADS) k_coupling_force(Dev d, Pass p) {
+    for_active_cells(d, [&](uint32_t index, int3 c) {
+        const uint32_t packed = d.cell_type[index];
+        const uint32_t type = type_of(packed);
+        if (type == CELL_AIR) return;
+        const float h = d.h;
+        const float3 x = make_float3((float(c.x) + 0.5f) * h, (float(c.y) + 0.5f) * h, (float(c.z) + 0.5f) * h);
+        float p_hat = 0.0f;
+        float3 g = make_float3(0.0f, 0.0f, 0.0f);
+        bool have = false;
+        if (type == CELL_FLUID) {
+            p_hat = d.pressure[index];
+            g = fluid_pressure_gradient(d, c, p_hat);
+            have = true;
+        } else if (collider_of(packed) != 0u) {
+            have = body_surface_pressure(d, c, p_hat);
+        }
+        if (!have) return;
+        for (uint32_t k = 0; k < p.num_colliders; ++k) {
+            const slosh_collider_t& col = d.colliders[k];
+            if ((col.flags & COLLIDER_FLAG_TWO_WAY) == 0u || fabsf(collider_sdf(col, x)) > h) continue;
+            if (type == CELL_SOLID && collider_of(packed) != k + 1u) continue;
+            float sp = p_hat;
+            if (type == CELL_FLUID) {
+                const float phi = collider_sdf(col, x);
+                sp = sp + dot3(g, scale3(-phi, collider_normal(col, x, 0.25f * h)));
+            }
+            const float scale = (((-sp) * p.pressure_to_pascal) * h) * h;
+            float3 force = make_float3(0.0f, 0.0f, 0.0f), torque = make_float3(0.0f, 0.0f, 0.0f);
+            const float3 center = ld3(col.center);
+#pragma unroll
+            for (int n = 0; n < 6; ++n) {
+                const int3 dd = nbr_off(n);
+                const float3 normal = make_float3(float(dd.x), float(dd.y), float(dd.z));
+                const float3 fp = addf3(x, scale3(0.5f * h, normal));
+                if (type == CELL_SOLID) {
+                    const uint32_t nbp = get_cell_type(d, add3(c, dd));
+                    if (type_of(nbp) == CELL_SOLID && collider_of(nbp) != k + 1u) continue;
+                }
+                const float w = saturatef(0.5f + collider_sdf(col, fp) * d.inv_h);
+                const float3 df = scale3(scale * w, normal);
+                force = addf3(force, df);
+                torque = addf3(torque, cross3(sub3(fp, center), df));
+            }
+            coupling_add(d, k, 0, force.x); coupling_add(d, k, 1, force.y); coupling_add(d, k, 2, force.z);
+            coupling_add(d, k, 3, torque.x); coupling_add(d, k, 4, torque.y); coupling_add(d, k, 5, torque.z);
+        }
+    });
+}
+// SubmergedCS, Slosh.usf:1316-1370.
+__global__ void __launch_bounds__(GRID_THREADS) k_submerged(Dev d) {
+    for_active_cells(d, [&](uint32_t index, int3 c) {
+        const uint32_t packed = d.cell_type[index];
+        const uint32_t id = collider_of(packed);
+        if (type_of(packed) != CELL_SOLID || id == 0u) return;
+        coupling_count(d, id - 1u, 11);
+        const int3 dirs[4] = {make_int3(1, 0, 0), make_int3(-1, 0, 0), make_int3(0, 1, 0), make_int3(0, -1, 0)};
+        bool sub = false;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            int3 q = c;
+            for (int step = 0; step < 12; ++step) {
+                q = add3(q, dirs[k]);
+                const uint32_t t = get_cell_type(d, q);
+                if (type_of(t) != CELL_SOLID || collider_of(t) != id) {
+                    bool liquid = type_of(t) == CELL_FLUID && (t & CELL_DENSE_FLAG) != 0u;
+#pragma unroll
+                    for (int below = 1; below <= 3; ++below)
+                        liquid = liquid && type_of(get_cell_type(d, make_int3(q.x, q.y, q.z - below))) != CELL_AIR;
+                    sub = sub || liquid;
+                    break;
+                }
+            }
+        }
+        if (sub) {
+            const float h = d.h;
+            const float3 off = sub3(make_float3((float(c.x) + 0.5f) * h, (float(c.y) + 0.5f) * h, (float(c.z) + 0.5f) * h),
+                                    ld3(d.colliders[id - 1u].center));
+            coupling_count(d, id - 1u, 7);
+            coupling_add(d, id - 1u, 12, off.x); coupling_add(d, id - 1u, 13, off.y); coupling_add(d, id - 1u, 14, off.z);
         }
     });
 }
@@ -551,6 +761,17 @@ int launch_rbgs(const Dev& d, float* pres, const float* rhs, uint32_t parity, fl
 }
 int launch_project(const Dev& d, const Pass& p, float* vel, const Shape& sh, cudaStream_t s) {
     k_project<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, p, vel);
+    return 1;
+}
+int launch_coupling(const Dev& d, const Pass& p, const float* vel, const Shape& sh, cudaStream_t s) {
+    if (p.num_colliders == 0u) return 0;
+    k_coupling_faces<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, p, vel);
+    if (p.smooth_coupling == 0u) return 1;
+    k_coupling_force<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, p);
+    return 2;
+}
+int launch_submerged(const Dev& d, const Shape& sh, cudaStream_t s) {
+    k_submerged<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d);
     return 1;
 }
 int launch_residual(const Dev& d, const Pass& p, const float* vel, const Shape& sh, cudaStream_t s) {

@@ -87,6 +87,7 @@ def compare_state(gpu, orc, report=None, particles=True):
         r.add(name, a, b, fm)
         r.add(name + "[null]", a.reshape(3, pc)[:, :512], np.zeros((3, 512), dtype=a.dtype))
     r.add("STATS", gpu.read("STATS"), orc.read("STATS"))
+    r.add("COUPLING", gpu.read("COUPLING"), orc.read("COUPLING"))
     r.add("PARTICLE_COUNT", gpu.read("PARTICLE_COUNT"), orc.read("PARTICLE_COUNT"))
     return r
 
@@ -124,5 +125,11 @@ def run_frames(g, o, sc, frames, check_every_substep=True, tol=1e-5):
         assert rg.fluid_cells == ro.fluid_cells
         assert rg.max_particle_speed == ro.max_particle_speed
         assert rg.last_solve_iterations == ro.last_solve_iterations
+        assert rg.num_colliders == ro.num_colliders
+        for k in range(rg.num_colliders):
+            fg, fo = rg.colliders[k], ro.colliders[k]
+            for name, _ in A.ColliderFeedback._fields_:
+                assert list(getattr(fg, name)) == list(getattr(fo, name)) if hasattr(getattr(fg, name), "__len__") \
+                    else getattr(fg, name) == getattr(fo, name), f"frame {f} collider {k} {name}"
         fi = A.frame_input(sc["settings"], **extra)
     return reports

@@ -1,8 +1,10 @@
 """GPU parity of the paths the default scene does not exercise, each against the oracle, state compared
 after every substep (bit-exact; 1e-5 relative L2 is the stated float tolerance): FLIP transfer, viscosity,
 manipulators and drains, sphere/box emission with velocity spread and speed jitter, one-sided density
-correction, warm start from zero, the dense (non-sparse) pool, and red-black SOR on a sparse scene large
-enough to use every pool path."""
+correction, warm start from zero, the dense (non-sparse) pool, red-black SOR on a sparse scene large
+enough to use every pool path, and two-way collider coupling (the per-collider integer accumulators and
+their decoded feedback)."""
+import numpy as np
 import pytest
 
 from slosh_b200 import _abi as A
@@ -104,3 +106,32 @@ def test_rbgs_sparse_scene(slosh, oracle_mod):
     sc = scenes.dam_break_sphere(slosh.settings_default, n=64, solver=A.SOLVER_RBGS, sor_iterations=60)
     sc["settings"].max_substeps = 16
     run_frames(*pair(slosh, oracle_mod, sc), sc, frames=2)
+
+
+def _collider(ctype, center, extent, two_way=True, velocity=(0.0, 0.0, 0.0), spin=(0.0, 0.0, 0.0)):
+    c = A.Collider()
+    c.center[:] = list(center)
+    c.type = ctype
+    c.rotation[:] = [0.0, 0.0, 0.0, 1.0]
+    c.extent[:] = list(extent)
+    c.flags = 1 if two_way else 0
+    c.linear_velocity[:] = list(velocity)
+    c.angular_velocity[:] = list(spin)
+    return c
+
+
+@pytest.mark.parametrize("smooth", [1, 0])
+def test_two_way_coupling(slosh, oracle_mod, smooth):
+    sc = scenes.tiny(slosh.settings_default, n=24)
+    sc["settings"].smooth_coupling_force = smooth
+    sc["colliders"] = [
+        _collider(A.COLLIDER_SPHERE, (0.25, 0.22, 0.5), (0.09, 0.0, 0.0), spin=(0.0, 0.0, 1.0)),
+        _collider(A.COLLIDER_BOX, (0.55, 0.12, 0.5), (0.07, 0.09, 0.12), velocity=(0.1, 0.0, 0.0)),
+        _collider(A.COLLIDER_CAPSULE, (0.3, 0.4, 0.3), (0.05, 0.1, 0.0), two_way=False),
+    ]
+    g, o = pair(slosh, oracle_mod, sc)
+    run_frames(g, o, sc, frames=4)
+    acc = g.read("COUPLING").reshape(A.MAX_COLLIDERS, -1)
+    assert np.any(acc[0, :6] != 0) and acc[0, 6] > 0, "the submerged sphere collected no force or wetted faces"
+    assert acc[0, 11] > 0 and acc[1, 11] > 0, "solid cells of the two-way bodies were not counted"
+    assert not np.any(acc[2, :7]) and not np.any(acc[2, 8:11]), "a one-way collider received coupling terms"
