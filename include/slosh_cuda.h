@@ -281,6 +281,13 @@ typedef enum slosh_buffer_id {
     SLOSH_BUF_ACCUM = 23,       /* i32[2 * total_faces] */
     SLOSH_BUF_VEL_EXTRAP = 24,  /* f32[total_faces]: displacement / scratch velocity buffer of the last G2P */
     SLOSH_BUF_COUPLING = 25,    /* i32[SLOSH_MAX_COLLIDERS * SLOSH_COUPLING_STRIDE]: this frame's collider accumulators */
+    /* outputs of the last slosh_build_surface */
+    SLOSH_BUF_SURFACE_FIELD = 26,     /* u16 (f16 bits)[field voxels], x fastest */
+    SLOSH_BUF_SURFACE_BRICKS = 27,    /* u32[field bricks]: occupancy of 8^3-voxel bricks */
+    SLOSH_BUF_SURFACE_POSITIONS = 28, /* f32[3 * num_vertices], sim metres */
+    SLOSH_BUF_SURFACE_NORMALS = 29,   /* f32[3 * num_vertices] */
+    SLOSH_BUF_SURFACE_TANGENTS = 30,  /* f32[3 * num_vertices] */
+    SLOSH_BUF_SURFACE_INDICES = 31,   /* u32[num_indices], triangles */
     SLOSH_BUF_COUNT_
 } slosh_buffer_id;
 
@@ -360,6 +367,35 @@ SLOSH_API uint64_t slosh_launch_count(void* ctx);
 /* Bytes this context copied host->device and device->host since creation (frame inputs,
  * results, solver residual checks, particle uploads and downloads, buffer reads and writes). */
 SLOSH_API slosh_status slosh_transfer_bytes(void* ctx, uint64_t* out_h2d, uint64_t* out_d2h);
+
+/* ---- headless liquid surface: the renderer's density field and surface nets (SloshSurface.usf:54-470,
+ * SloshRenderer.cpp:118-170), written into device buffers of the context instead of UE textures and
+ * vertex buffers. Particles are splatted as spheres (the renderer's Anisotropy = 0). */
+typedef struct slosh_surface_params_t {
+    float field_resolution;      /* FSloshRenderSettings::FieldResolution: field voxels per solver cell (0.5-3) */
+    float surface_smoothing;     /* SurfaceSmoothing: kernel radius in splat radii (0.5-6) */
+    float particle_radius_scale; /* ParticleRadiusScale: splat radius in cells */
+    float iso_level;             /* IsoLevel (0.02-0.98): 0.5 = surface at the particle radius */
+    uint32_t build_mesh;         /* 0: field and brick occupancy only; 1: also the surface-nets mesh */
+    uint32_t max_vertices;       /* capacity of the vertex buffers */
+    uint32_t max_indices;        /* capacity of the index buffer */
+} slosh_surface_params_t;
+typedef struct slosh_surface_info_t {
+    int32_t field_dim[3];
+    int32_t brick_dim[3];
+    float voxel_size;            /* sim metres */
+    uint32_t vertices_requested; /* surface cells found (can exceed max_vertices) */
+    uint32_t num_vertices;       /* vertices written: min(requested, max_vertices) */
+    uint32_t indices_requested;
+    uint32_t num_indices;        /* min(requested, max_indices) in whole quads (6 indices): only those are written */
+} slosh_surface_info_t;
+SLOSH_API void slosh_surface_params_default(slosh_surface_params_t* out);
+/* Builds the field (and mesh) from the current particles on the context's stream and waits for it.
+ * Vertices and triangles are numbered in cell order (deterministic). */
+SLOSH_API slosh_status slosh_build_surface(void* ctx, const slosh_surface_params_t* params, slosh_surface_info_t* out);
+/* Device pointers of the last build (valid until the next build or slosh_destroy); any may be NULL. */
+SLOSH_API slosh_status slosh_surface_device_ptrs(void* ctx, void** field_f16, void** positions, void** normals, void** tangents,
+                                                 void** indices);
 
 #ifdef __cplusplus
 } /* extern "C" */

@@ -53,6 +53,7 @@ def lib():
         L.oracle_buffer_bytes.argtypes = [vp, C.c_int, C.POINTER(C.c_size_t)]
         L.oracle_read_buffer.argtypes = [vp, C.c_int, C.c_void_p, C.c_size_t]
         L.oracle_read_buffer_f64.argtypes = [vp, C.c_int, C.c_void_p, C.c_size_t]
+        L.oracle_build_surface.argtypes = [vp, C.POINTER(A.SurfaceParams), C.POINTER(A.SurfaceInfo)]
         L.oracle_write_buffer.argtypes = [vp, C.c_int, C.c_void_p, C.c_size_t]
         L.oracle_copy_state.argtypes = [vp, vp]
         L.oracle_settings_default.argtypes = [C.POINTER(A.Settings)]
@@ -147,6 +148,11 @@ class Oracle:
         r = A.Results()
         _check(lib().oracle_get_results(self._h, C.byref(r)), "results")
         return r
+
+    def build_surface(self, params):
+        info = A.SurfaceInfo()
+        _check(lib().oracle_build_surface(self._h, C.byref(params), C.byref(info)), "build_surface")
+        return info
 
     def read(self, name):
         bid = A.BUF[name]

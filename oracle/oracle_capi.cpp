@@ -135,6 +135,12 @@ View<R> view(Sim<R>& s, int id) {
         case SLOSH_BUF_ACCUM: i32(s.accum, s.accum.size()); break;
         case SLOSH_BUF_VEL_EXTRAP: real(s.vel[s.last_disp_index]); break;
         case SLOSH_BUF_COUPLING: v.ptr = s.coupling; v.count = SLOSH_MAX_COLLIDERS * SLOSH_COUPLING_STRIDE; v.elem = 4; break;
+        case SLOSH_BUF_SURFACE_FIELD: v.ptr = s.surface.field.data(); v.count = s.surface.field.size(); v.elem = 2; break;
+        case SLOSH_BUF_SURFACE_BRICKS: u32(s.surface.bricks, s.surface.bricks.size()); break;
+        case SLOSH_BUF_SURFACE_POSITIONS: v.ptr = s.surface.positions.data(); v.count = 3u * s.surface.num_vertices; v.elem = 4; break;
+        case SLOSH_BUF_SURFACE_NORMALS: v.ptr = s.surface.normals.data(); v.count = 3u * s.surface.num_vertices; v.elem = 4; break;
+        case SLOSH_BUF_SURFACE_TANGENTS: v.ptr = s.surface.tangents.data(); v.count = 3u * s.surface.num_vertices; v.elem = 4; break;
+        case SLOSH_BUF_SURFACE_INDICES: u32(s.surface.indices, s.surface.num_indices); break;
         default: break;
     }
     return v;
@@ -326,4 +332,22 @@ ORACLE_API int oracle_copy_state(void* dst, void* src) {
     else if (S->fp64) copy(*D->f, *S->d);
     else copy(*D->f, *S->f);
     return SLOSH_OK;
+}
+
+// Headless surface of the current particles (slosh_build_surface).
+ORACLE_API int oracle_build_surface(void* h, const slosh_surface_params_t* q, slosh_surface_info_t* out) {
+    if (!h || !q) return int(SLOSH_ERR_INVALID_ARG);
+    return dispatch(h, [&](auto& s) {
+        build_surface(s.particles.data(), s.num_particles, s.L.grid, s.S.cell_size, *q, s.surface);
+        if (out) {
+            std::memset(out, 0, sizeof(*out));
+            for (int a = 0; a < 3; ++a) { out->field_dim[a] = s.surface.dim[a]; out->brick_dim[a] = s.surface.bdim[a]; }
+            out->voxel_size = s.surface.voxel;
+            out->vertices_requested = s.surface.vertices_requested;
+            out->num_vertices = s.surface.num_vertices;
+            out->indices_requested = s.surface.indices_requested;
+            out->num_indices = s.surface.num_indices;
+        }
+        return int(SLOSH_OK);
+    });
 }

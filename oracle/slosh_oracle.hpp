@@ -421,6 +421,216 @@ struct PassParams {
 // =============================================================================================
 // The simulation state and its kernels.
 // =============================================================================================
+// ---- headless surface (SloshSurface.usf:54-470; parameters SloshRenderer.cpp:118-170) -------------------------
+// Density splat of sphere-mode ellipsoids, resolve to the f16 Zhu & Bridson field with dilated brick
+// occupancy, and surface nets with vertices and quads numbered in cell order (the CUDA path numbers them
+// the same way through scans). Computed in FP32 from the particle records, whatever the simulation's R.
+struct SurfaceOut {
+    int dim[3] = {0, 0, 0}, bdim[3] = {0, 0, 0};
+    float voxel = 0.0f;
+    std::vector<uint16_t> field;
+    std::vector<uint32_t> bricks;
+    std::vector<float> positions, normals, tangents;
+    std::vector<uint32_t> indices;
+    uint32_t vertices_requested = 0, indices_requested = 0, num_vertices = 0, num_indices = 0;
+};
+inline void build_surface(const slosh_particle_t* particles, uint32_t n, I3 grid, float cell, const slosh_surface_params_t& q, SurfaceOut& o) {
+    const float res = clampr(q.field_resolution, 0.5f, 3.0f);
+    o.voxel = cell / res;
+    const float inv_voxel = 1.0f / o.voxel;
+    const int dim[3] = {int(std::ceil(float(grid.x) * res)), int(std::ceil(float(grid.y) * res)), int(std::ceil(float(grid.z) * res))};
+    for (int a = 0; a < 3; ++a) { o.dim[a] = dim[a]; o.bdim[a] = (dim[a] + 7) / 8; }
+    const float support = clampr(q.surface_smoothing, 0.5f, 6.0f), max_fp = 4.0f;
+    const float radius_voxels = q.particle_radius_scale * res, splat_radius = cell * q.particle_radius_scale;
+    const float iso = clampr(q.iso_level, 0.02f, 0.98f);
+    const size_t nv = size_t(dim[0]) * dim[1] * dim[2], nb = size_t(o.bdim[0]) * o.bdim[1] * o.bdim[2];
+    auto vox = [&](int x, int y, int z) { return size_t(x) + size_t(dim[0]) * (size_t(y) + size_t(dim[1]) * size_t(z)); };
+    auto fbrick = [&](int x, int y, int z) {
+        const int bx = clampi(x >> 3, 0, o.bdim[0] - 1), by = clampi(y >> 3, 0, o.bdim[1] - 1), bz = clampi(z >> 3, 0, o.bdim[2] - 1);
+        return size_t(bx) + size_t(o.bdim[0]) * (size_t(by) + size_t(o.bdim[1]) * size_t(bz));
+    };
+    auto add = [](int32_t& a, int32_t v) { a = int32_t(uint32_t(a) + uint32_t(v)); };
+    // DensitySplatCS
+    std::vector<int32_t> acc(nv * 5, 0);
+    for (uint32_t i = 0; i < n; ++i) {
+        const slosh_particle_t& p = particles[i];
+        if (is_dead_age(p.age)) continue;
+        const V3<float> axis[3] = {{splat_radius, 0.0f, 0.0f}, {0.0f, splat_radius, 0.0f}, {0.0f, 0.0f, splat_radius}};
+        const float k = support * inv_voxel;
+        const V3<float> c{p.pos[0] * inv_voxel, p.pos[1] * inv_voxel, p.pos[2] * inv_voxel};
+        V3<float> w[3];
+        float amax = 0.0f;
+        for (int a = 0; a < 3; ++a) {
+            const V3<float> u{axis[a].x * k, axis[a].y * k, axis[a].z * k};
+            const float aa = std::fmax(dot(u, u), 1e-8f);
+            w[a] = V3<float>{u.x / aa, u.y / aa, u.z / aa};
+            amax = a == 0 ? aa : std::fmax(amax, aa);
+        }
+        const float rr = std::fmin(std::sqrt(amax), max_fp);
+        const int lo[3] = {std::max(int(std::floor(c.x - rr - 0.5f)), 0), std::max(int(std::floor(c.y - rr - 0.5f)), 0),
+                           std::max(int(std::floor(c.z - rr - 0.5f)), 0)};
+        const int hi[3] = {std::min(int(std::ceil(c.x + rr - 0.5f)), dim[0] - 1), std::min(int(std::ceil(c.y + rr - 0.5f)), dim[1] - 1),
+                           std::min(int(std::ceil(c.z + rr - 0.5f)), dim[2] - 1)};
+        for (int z = lo[2]; z <= hi[2]; ++z)
+            for (int y = lo[1]; y <= hi[1]; ++y)
+                for (int x = lo[0]; x <= hi[0]; ++x) {
+                    const V3<float> d{(float(x) + 0.5f) - c.x, (float(y) + 0.5f) - c.y, (float(z) + 0.5f) - c.z};
+                    const V3<float> qv{dot(d, w[0]), dot(d, w[1]), dot(d, w[2])};
+                    const float q2 = dot(qv, qv);
+                    if (q2 < 1.0f) {
+                        float wk = 1.0f - q2;
+                        wk = wk * wk * wk;
+                        int32_t* a = acc.data() + vox(x, y, z) * 5;
+                        add(a[0], int32_t(wk * 1024.0f + 0.5f));
+                        add(a[1], to_i32_rn<float>(-d.x * wk * 256.0f));
+                        add(a[2], to_i32_rn<float>(-d.y * wk * 256.0f));
+                        add(a[3], to_i32_rn<float>(-d.z * wk * 256.0f));
+                        add(a[4], to_i32_rn<float>(radius_voxels * wk * 256.0f));
+                    }
+                }
+    }
+    // FieldResolveCS
+    o.field.assign(nv, 0);
+    o.bricks.assign(nb, 0u);
+    for (int z = 0; z < dim[2]; ++z)
+        for (int y = 0; y < dim[1]; ++y)
+            for (int x = 0; x < dim[0]; ++x) {
+                const size_t i = vox(x, y, z);
+                const int32_t* a = acc.data() + i * 5;
+                const float w = float(a[0]) / 1024.0f;
+                float f = 0.0f;
+                if (w > 1e-3f) {
+                    const float den = 256.0f * w;
+                    const V3<float> mo{float(a[1]) / den, float(a[2]) / den, float(a[3]) / den};
+                    const float rbar = std::fmax(float(a[4]) / den, 1e-3f);
+                    const float phi = std::sqrt(dot(mo, mo)) - rbar;
+                    f = saturate(0.5f - 0.5f * phi / rbar);
+                }
+                o.field[i] = f32_to_f16(f);
+                if (f <= 0.0f) continue;
+                const int ib[3] = {x & 7, y & 7, z & 7};
+                for (int k = 0; k < 8; ++k) {
+                    const int ox = (k & 1) * 2 - 1, oy = ((k >> 1) & 1) * 2 - 1, oz = (k >> 2) * 2 - 1;
+                    const int nx = x + ox * int(ib[0] == (ox < 0 ? 0 : 7)), ny = y + oy * int(ib[1] == (oy < 0 ? 0 : 7));
+                    const int nz = z + oz * int(ib[2] == (oz < 0 ? 0 : 7));
+                    if (nx >= 0 && ny >= 0 && nz >= 0 && nx < dim[0] && ny < dim[1] && nz < dim[2]) o.bricks[fbrick(nx, ny, nz)] |= 1u;
+                }
+            }
+    o.positions.clear(); o.normals.clear(); o.tangents.clear(); o.indices.clear();
+    o.vertices_requested = o.indices_requested = o.num_vertices = o.num_indices = 0;
+    if (!q.build_mesh) return;
+    auto fat = [&](int x, int y, int z) { return f16_to_f32(o.field[vox(x, y, z)]); };
+    const int cd[3] = {std::max(dim[0] - 1, 0), std::max(dim[1] - 1, 0), std::max(dim[2] - 1, 0)};
+    const size_t nc = size_t(cd[0]) * cd[1] * cd[2];
+    auto cell_of = [&](int x, int y, int z) { return size_t(x) + size_t(cd[0]) * (size_t(y) + size_t(cd[1]) * size_t(z)); };
+    auto corners = [&](int x, int y, int z, float fc[8]) {
+        uint32_t mask = 0u;
+        for (int k = 0; k < 8; ++k) {
+            fc[k] = fat(x + (k & 1), y + ((k >> 1) & 1), z + (k >> 2));
+            mask |= (fc[k] >= iso ? 1u : 0u) << k;
+        }
+        return mask;
+    };
+    auto sample = [&](float px, float py, float pz) {
+        const float x = px - 0.5f, y = py - 0.5f, z = pz - 0.5f;
+        const float fx0 = std::floor(x), fy0 = std::floor(y), fz0 = std::floor(z);
+        const float tx = x - fx0, ty = y - fy0, tz = z - fz0;
+        const int x0 = int(fx0), y0 = int(fy0), z0 = int(fz0);
+        const int xs[2] = {clampi(x0, 0, dim[0] - 1), clampi(x0 + 1, 0, dim[0] - 1)};
+        const int ys[2] = {clampi(y0, 0, dim[1] - 1), clampi(y0 + 1, 0, dim[1] - 1)};
+        const int zs[2] = {clampi(z0, 0, dim[2] - 1), clampi(z0 + 1, 0, dim[2] - 1)};
+        float cz[2];
+        for (int k = 0; k < 2; ++k) {
+            float cy[2];
+            for (int j = 0; j < 2; ++j) {
+                const float a = fat(xs[0], ys[j], zs[k]), b = fat(xs[1], ys[j], zs[k]);
+                cy[j] = a + tx * (b - a);
+            }
+            cz[k] = cy[0] + ty * (cy[1] - cy[0]);
+        }
+        return cz[0] + tz * (cz[1] - cz[0]);
+    };
+    auto normalize_div = [](V3<float> v) {
+        const float l = std::sqrt(dot(v, v));
+        return V3<float>{v.x / l, v.y / l, v.z / l};
+    };
+    // SurfaceNetsVerticesCS in cell order
+    const uint32_t NO_VERTEX = 0xFFFFFFFFu;
+    std::vector<uint32_t> cell_vertex(nc, NO_VERTEX);
+    uint32_t next = 0;
+    for (int z = 0; z < cd[2]; ++z)
+        for (int y = 0; y < cd[1]; ++y)
+            for (int x = 0; x < cd[0]; ++x) {
+                if (o.bricks[fbrick(x, y, z)] == 0u) continue;
+                float fc[8];
+                const uint32_t mask = corners(x, y, z, fc);
+                if (mask == 0u || mask == 0xFFu) continue;
+                const uint32_t vi = next++;
+                if (vi >= q.max_vertices) continue;
+                cell_vertex[cell_of(x, y, z)] = vi;
+                float sx = 0.0f, sy = 0.0f, sz = 0.0f, count = 0.0f;
+                for (int a = 0; a < 8; ++a)
+                    for (int bit = 1; bit <= 4; bit <<= 1) {
+                        if (a & bit) continue;
+                        const int b = a | bit;
+                        if (((mask >> a) & 1u) == ((mask >> b) & 1u)) continue;
+                        const float t = saturate((iso - fc[a]) / (fc[b] - fc[a]));
+                        const float px = (a & 1) == (b & 1) ? float(a & 1) : ((b & 1) ? t : 1.0f - t);
+                        const float py = ((a >> 1) & 1) == ((b >> 1) & 1) ? float((a >> 1) & 1) : (((b >> 1) & 1) ? t : 1.0f - t);
+                        const float pz = (a >> 2) == (b >> 2) ? float(a >> 2) : ((b >> 2) ? t : 1.0f - t);
+                        sx = sx + px;
+                        sy = sy + py;
+                        sz = sz + pz;
+                        count = count + 1.0f;
+                    }
+                const V3<float> pv{(float(x) + 0.5f) + sx / count, (float(y) + 0.5f) + sy / count, (float(z) + 0.5f) + sz / count};
+                o.positions.push_back(pv.x * o.voxel);
+                o.positions.push_back(pv.y * o.voxel);
+                o.positions.push_back(pv.z * o.voxel);
+                const V3<float> g{sample(pv.x + 1.0f, pv.y, pv.z) - sample(pv.x - 1.0f, pv.y, pv.z),
+                                  sample(pv.x, pv.y + 1.0f, pv.z) - sample(pv.x, pv.y - 1.0f, pv.z),
+                                  sample(pv.x, pv.y, pv.z + 1.0f) - sample(pv.x, pv.y, pv.z - 1.0f)};
+                V3<float> nrm{0.0f, 0.0f, 1.0f};
+                if (std::sqrt(dot(g, g)) > 1e-8f) {
+                    const V3<float> ng = normalize_div(g);
+                    nrm = V3<float>{-ng.x, -ng.y, -ng.z};
+                }
+                const V3<float> ref = std::fabs(nrm.z) < 0.9f ? V3<float>{0.0f, 0.0f, 1.0f} : V3<float>{1.0f, 0.0f, 0.0f};
+                const V3<float> tx = normalize_div(cross(nrm, ref));
+                o.normals.push_back(nrm.x); o.normals.push_back(nrm.y); o.normals.push_back(nrm.z);
+                o.tangents.push_back(tx.x); o.tangents.push_back(tx.y); o.tangents.push_back(tx.z);
+            }
+    o.vertices_requested = next;
+    o.num_vertices = std::min(next, q.max_vertices);
+    // SurfaceNetsFacesCS in cell order
+    uint32_t quads = 0;
+    for (int z = 0; z < cd[2]; ++z)
+        for (int y = 0; y < cd[1]; ++y)
+            for (int x = 0; x < cd[0]; ++x) {
+                if (o.bricks[fbrick(x, y, z)] == 0u) continue;
+                const bool in0 = fat(x, y, z) >= iso;
+                for (int axis = 0; axis < 3; ++axis) {
+                    const int e[3] = {axis == 0, axis == 1, axis == 2};
+                    const bool in1 = fat(x + e[0], y + e[1], z + e[2]) >= iso;
+                    if (in0 == in1) continue;
+                    const int eu[3] = {axis == 2, axis == 0, axis == 1}, ev[3] = {axis == 1, axis == 2, axis == 0};
+                    const int c11[3] = {x - eu[0] - ev[0], y - eu[1] - ev[1], z - eu[2] - ev[2]};
+                    if (c11[0] < 0 || c11[1] < 0 || c11[2] < 0) continue;
+                    const uint32_t v00 = cell_vertex[cell_of(x, y, z)], v10 = cell_vertex[cell_of(x - eu[0], y - eu[1], z - eu[2])];
+                    const uint32_t v11 = cell_vertex[cell_of(c11[0], c11[1], c11[2])], v01 = cell_vertex[cell_of(x - ev[0], y - ev[1], z - ev[2])];
+                    if (v00 == NO_VERTEX || v10 == NO_VERTEX || v11 == NO_VERTEX || v01 == NO_VERTEX) continue;
+                    const uint32_t base = 6u * quads++;
+                    if (base + 6u > q.max_indices) continue;
+                    const uint32_t tri[6] = {v00, in0 ? v11 : v10, in0 ? v10 : v11, v00, in0 ? v01 : v11, in0 ? v11 : v01};
+                    for (int k = 0; k < 6; ++k) o.indices.push_back(tri[k]);
+                }
+            }
+    o.indices_requested = 6u * quads;
+    const uint32_t ni = std::min(o.indices_requested, q.max_indices);
+    o.num_indices = ni - ni % 6u;  // whole quads (only whole quads are written)
+    o.indices.resize(o.num_indices);
+}
+
 template <class R>
 class Sim {
 public:
@@ -431,6 +641,7 @@ public:
     PassParams P;
 
     std::vector<slosh_particle_t> particles, particles_sorted;
+    SurfaceOut surface;  // last build_surface
     uint32_t num_particles = 0;
     uint32_t particle_count[4] = {0, 0, 0, 0};
     uint64_t total_emitted = 0, sim_frame = 0;

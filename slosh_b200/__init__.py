@@ -13,7 +13,8 @@ import os
 import numpy as np
 
 from . import _abi
-from ._abi import (BUF, EmitRequest, FrameInput, Layout, Particle, PARTICLE_DTYPE, Results, Settings,  # noqa: F401
+from ._abi import (BUF, EmitRequest, FrameInput, Layout, Particle, PARTICLE_DTYPE, Results, Settings, SurfaceInfo,  # noqa: F401
+                   SurfaceParams,
                    frame_input)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -49,6 +50,9 @@ SIGNATURES = {
     "slosh_get_phase_ms": ([_VP, C.POINTER(C.c_float), C.c_int32], C.c_int),
     "slosh_launch_count": ([_VP], C.c_uint64),
     "slosh_transfer_bytes": ([_VP, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)], C.c_int),
+    "slosh_surface_params_default": ([C.POINTER(SurfaceParams)], None),
+    "slosh_build_surface": ([_VP, C.POINTER(SurfaceParams), C.POINTER(SurfaceInfo)], C.c_int),
+    "slosh_surface_device_ptrs": ([_VP, C.POINTER(_VP), C.POINTER(_VP), C.POINTER(_VP), C.POINTER(_VP), C.POINTER(_VP)], C.c_int),
 }
 PHASES = ("sort", "pool", "p2g", "grid", "pressure", "project", "density", "extrapolate", "g2p")
 
@@ -77,6 +81,12 @@ def load_library(path=None):
     if path is None:
         _lib = lib
     return lib
+
+
+def surface_params_default():
+    q = SurfaceParams()
+    load_library().slosh_surface_params_default(C.byref(q))
+    return q
 
 
 def settings_default():
@@ -204,6 +214,14 @@ class Simulation:
         out = (C.c_float * len(PHASES))()
         _check(self._lib.slosh_get_phase_ms(self._ctx, out, len(PHASES)))
         return dict(zip(PHASES, list(out)))
+
+    # ---- headless surface ----
+    def build_surface(self, params=None):
+        """Density field and surface-nets mesh of the current particles (slosh_build_surface)."""
+        q = params or surface_params_default()
+        info = SurfaceInfo()
+        _check(self._lib.slosh_build_surface(self._ctx, C.byref(q), C.byref(info)), allow_warnings=False)
+        return info
 
     def launch_count(self):
         return int(self._lib.slosh_launch_count(self._ctx))

@@ -42,6 +42,8 @@ BUF = dict(
     DIVERGENCE=8, CELL_DIAG=9, DENSITY_Q=10, DENSITY_RHS=11, BRICK_TABLE=12, SLOT_BRICK=13, FREE_SLOTS=14,
     ACTIVE_BRICKS=15, NEW_SLOTS=16, BRICK_TOUCH=17, STATS=18, SORT_COUNTS=19, SORT_OFFSETS=20, SORT_PERM=21,
     PARTICLE_COUNT=22, ACCUM=23, VEL_EXTRAP=24, COUPLING=25,
+    SURFACE_FIELD=26, SURFACE_BRICKS=27, SURFACE_POSITIONS=28, SURFACE_NORMALS=29, SURFACE_TANGENTS=30,
+    SURFACE_INDICES=31,
 )
 BUF_DTYPE = dict(
     PARTICLES=None, VEL=np.float32, VEL_OLD=np.float32, FACE_FLAGS=np.uint32, FACE_WEIGHT=np.float32,
@@ -50,6 +52,8 @@ BUF_DTYPE = dict(
     FREE_SLOTS=np.uint32, ACTIVE_BRICKS=np.uint32, NEW_SLOTS=np.uint32, BRICK_TOUCH=np.uint32, STATS=np.uint32,
     SORT_COUNTS=np.uint32, SORT_OFFSETS=np.uint32, SORT_PERM=np.uint32, PARTICLE_COUNT=np.uint32,
     ACCUM=np.int32, VEL_EXTRAP=np.float32, COUPLING=np.int32,
+    SURFACE_FIELD=np.uint16, SURFACE_BRICKS=np.uint32, SURFACE_POSITIONS=np.float32, SURFACE_NORMALS=np.float32,
+    SURFACE_TANGENTS=np.float32, SURFACE_INDICES=np.uint32,
 )
 
 
@@ -99,6 +103,21 @@ class EmitRequest(C.Structure):
         ("rotation", C.c_float * 4), ("velocity_spread", C.c_float), ("speed_jitter", C.c_float),
         ("cell_min", C.c_int32 * 3), ("cell_dims", C.c_int32 * 3), ("count", C.c_uint32),
         ("fill_jitter", C.c_float),
+    ]
+
+
+class SurfaceParams(C.Structure):
+    _fields_ = [
+        ("field_resolution", C.c_float), ("surface_smoothing", C.c_float), ("particle_radius_scale", C.c_float),
+        ("iso_level", C.c_float), ("build_mesh", C.c_uint32), ("max_vertices", C.c_uint32), ("max_indices", C.c_uint32),
+    ]
+
+
+class SurfaceInfo(C.Structure):
+    _fields_ = [
+        ("field_dim", C.c_int32 * 3), ("brick_dim", C.c_int32 * 3), ("voxel_size", C.c_float),
+        ("vertices_requested", C.c_uint32), ("num_vertices", C.c_uint32), ("indices_requested", C.c_uint32),
+        ("num_indices", C.c_uint32),
     ]
 
 

@@ -231,11 +231,34 @@ struct Ctx {
         }
         graphs.clear();
     }
+    // ---- headless surface (SloshSurface.usf) ----
+    SurfaceDev surf{};
+    std::vector<void*> surface_allocs;
+    uint64_t surf_voxels_cap = 0, surf_cells_cap = 0, surf_bricks_cap = 0, surf_vert_cap = 0, surf_idx_cap = 0;
+    slosh_surface_info_t surf_info{};
+    uint32_t* h_surf = nullptr;  // pinned: the two counters
+    template <class T>
+    T* salloc(uint64_t count) {
+        void* p = nullptr;
+        const size_t bytes = size_t(std::max<uint64_t>(count, 1)) * sizeof(T);
+        if (cudaMalloc(&p, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            throw StatusError{SLOSH_ERR_OUT_OF_MEMORY, "cudaMalloc of " + std::to_string(bytes) + " bytes for the surface failed"};
+        }
+        surface_allocs.push_back(p);
+        return static_cast<T*>(p);
+    }
+    void build_surface(const slosh_surface_params_t& q);
+
     void release() {
         if (stream) cudaStreamSynchronize(stream);
         destroy_graphs();
         free_list(grid_allocs);
         free_list(particle_allocs);
+        free_list(surface_allocs);
+        surf_voxels_cap = surf_cells_cap = surf_bricks_cap = surf_vert_cap = surf_idx_cap = 0;
+        surf = SurfaceDev{};
+        surf_info = slosh_surface_info_t{};
         grid_bytes = particle_bytes = 0;
         allocated = false;
     }
@@ -819,6 +842,66 @@ void Ctx::end_frame() {
     }
 }
 
+// Field and mesh sizes as BuildDensityField / FillFieldParameters derive them (SloshRenderer.cpp:118-170).
+void Ctx::build_surface(const slosh_surface_params_t& q) {
+    const float res = clampf_h(q.field_resolution, 0.5f, 3.0f);
+    const float cell = S.cell_size;
+    SurfaceDev& d = surf;
+    d.voxel = cell / res;
+    d.inv_voxel = 1.0f / d.voxel;
+    d.dim = make_int3(int(std::ceil(float(grid.x) * res)), int(std::ceil(float(grid.y) * res)), int(std::ceil(float(grid.z) * res)));
+    d.bdim = make_int3((d.dim.x + 7) / 8, (d.dim.y + 7) / 8, (d.dim.z + 7) / 8);
+    d.support = clampf_h(q.surface_smoothing, 0.5f, 6.0f);
+    d.max_footprint = 4.0f;
+    d.radius_voxels = q.particle_radius_scale * res;
+    d.splat_radius = cell * q.particle_radius_scale;
+    d.iso = clampf_h(q.iso_level, 0.02f, 0.98f);
+    d.max_vertices = q.max_vertices;
+    d.max_indices = q.max_indices;
+    const uint64_t nv = uint64_t(d.dim.x) * uint64_t(d.dim.y) * uint64_t(d.dim.z);
+    const uint64_t nb = uint64_t(d.bdim.x) * uint64_t(d.bdim.y) * uint64_t(d.bdim.z);
+    const uint64_t nc = uint64_t(std::max(d.dim.x - 1, 0)) * uint64_t(std::max(d.dim.y - 1, 0)) * uint64_t(std::max(d.dim.z - 1, 0));
+    if (nv * 5u > 0xFFFFFFFFull) throw StatusError{SLOSH_ERR_INVALID_ARG, "surface field too large"};
+    if (nv > surf_voxels_cap || nb > surf_bricks_cap || nc > surf_cells_cap || q.max_vertices > surf_vert_cap || q.max_indices > surf_idx_cap) {
+        CK(cudaStreamSynchronize(stream));
+        free_list(surface_allocs);
+        surf_voxels_cap = nv; surf_bricks_cap = nb; surf_cells_cap = nc; surf_vert_cap = q.max_vertices; surf_idx_cap = q.max_indices;
+        d.accum = salloc<int32_t>(nv * 5u);
+        d.field = salloc<uint16_t>(nv);
+        d.bricks = salloc<uint32_t>(nb);
+        d.vflag = salloc<uint32_t>(nc);
+        d.vbase = salloc<uint32_t>(nc);
+        d.cell_vertex = salloc<uint32_t>(nc);
+        d.qflag = salloc<uint32_t>(nc);
+        d.qbase = salloc<uint32_t>(nc);
+        d.scan_tmp = salloc<uint32_t>(exclusive_scan_tmp_size(uint32_t(nc)));
+        d.positions = salloc<float>(3ull * q.max_vertices);
+        d.normals = salloc<float>(3ull * q.max_vertices);
+        d.tangents = salloc<float>(3ull * q.max_vertices);
+        d.indices = salloc<uint32_t>(q.max_indices);
+        d.counters = salloc<uint32_t>(2);
+    }
+    count(launch_surface(d, particles[pbuf], num_particles, q.build_mesh != 0u, stream));
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(h_surf, d.counters, 8, cudaMemcpyDeviceToHost, stream));
+    d2h_bytes += 8;
+    CK(cudaStreamSynchronize(stream));
+    slosh_surface_info_t& o = surf_info;
+    o = slosh_surface_info_t{};
+    o.field_dim[0] = d.dim.x; o.field_dim[1] = d.dim.y; o.field_dim[2] = d.dim.z;
+    o.brick_dim[0] = d.bdim.x; o.brick_dim[1] = d.bdim.y; o.brick_dim[2] = d.bdim.z;
+    o.voxel_size = d.voxel;
+    if (q.build_mesh) {
+        o.vertices_requested = h_surf[0];
+        o.num_vertices = std::min(h_surf[0], q.max_vertices);
+        o.indices_requested = h_surf[1];
+        // Whole quads only: a quad is written only when all six of its indices fit (SurfaceNetsFacesCS); the
+        // reference's argument pass rounds to triangles and so can draw up to three indices never written.
+        const uint32_t ni = std::min(h_surf[1], q.max_indices);
+        o.num_indices = ni - ni % 6u;
+    }
+}
+
 void decode_results(const Ctx& c, slosh_results_t* out) {
     std::memset(out, 0, sizeof(*out));
     const uint32_t* st = c.h_stats;
@@ -900,6 +983,16 @@ BufView buffer_view(Ctx& c, int id) {
         case SLOSH_BUF_ACCUM: v = {c.accum, 2 * tf * 4}; break;
         case SLOSH_BUF_VEL_EXTRAP: v = {c.vel[c.disp_phys], tf * 4}; break;
         case SLOSH_BUF_COUPLING: v = {c.coupling, size_t(SLOSH_MAX_COLLIDERS) * SLOSH_COUPLING_STRIDE * 4}; break;
+        case SLOSH_BUF_SURFACE_FIELD:
+            v = {c.surf.field, c.surf.field ? size_t(c.surf_info.field_dim[0]) * c.surf_info.field_dim[1] * c.surf_info.field_dim[2] * 2 : 0};
+            break;
+        case SLOSH_BUF_SURFACE_BRICKS:
+            v = {c.surf.bricks, c.surf.bricks ? size_t(c.surf_info.brick_dim[0]) * c.surf_info.brick_dim[1] * c.surf_info.brick_dim[2] * 4 : 0};
+            break;
+        case SLOSH_BUF_SURFACE_POSITIONS: v = {c.surf.positions, size_t(c.surf_info.num_vertices) * 12}; break;
+        case SLOSH_BUF_SURFACE_NORMALS: v = {c.surf.normals, size_t(c.surf_info.num_vertices) * 12}; break;
+        case SLOSH_BUF_SURFACE_TANGENTS: v = {c.surf.tangents, size_t(c.surf_info.num_vertices) * 12}; break;
+        case SLOSH_BUF_SURFACE_INDICES: v = {c.surf.indices, size_t(c.surf_info.num_indices) * 4}; break;
         default: break;
     }
     return v;
@@ -971,6 +1064,7 @@ SLOSH_API slosh_status slosh_create(const slosh_settings_t* settings, int32_t de
             CK(cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking));
             CK(cudaStreamCreateWithFlags(&c->body_stream, cudaStreamNonBlocking));
             CK(cudaMallocHost(&c->h_ctl, 16 * sizeof(uint32_t)));
+            CK(cudaMallocHost(&c->h_surf, 2 * sizeof(uint32_t)));
             std::memset(c->h_ctl, 0, 16 * sizeof(uint32_t));
             const char* ng = std::getenv("SLOSH_NO_GRAPHS");
             c->use_graphs = !(ng && ng[0] == '1');
@@ -1005,6 +1099,7 @@ SLOSH_API void slosh_destroy(void* ctx) {
     if (c->h_stats) cudaFreeHost(c->h_stats);
     if (c->h_scalars) cudaFreeHost(c->h_scalars);
     if (c->h_coupling) cudaFreeHost(c->h_coupling);
+    if (c->h_surf) cudaFreeHost(c->h_surf);
     if (c->h_ctl) cudaFreeHost(c->h_ctl);
     if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
     if (c->body_stream) cudaStreamDestroy(c->body_stream);
@@ -1162,6 +1257,41 @@ SLOSH_API slosh_status slosh_get_layout(void* ctx, slosh_layout_t* out) {
         out->num_particles = c->num_particles;
         out->particle_capacity = c->capacity;
         out->current_vel = uint32_t(c->vmap[0]);
+        return SLOSH_OK;
+    });
+}
+
+SLOSH_API void slosh_surface_params_default(slosh_surface_params_t* out) {
+    if (!out) return;
+    // FSloshRenderSettings defaults (SloshRenderer.h:34-46); capacities for a 256^3 domain's surface.
+    out->field_resolution = 1.0f;
+    out->surface_smoothing = 2.0f;
+    out->particle_radius_scale = 0.6f;
+    out->iso_level = 0.5f;
+    out->build_mesh = 1u;
+    out->max_vertices = 1u << 22;
+    out->max_indices = 1u << 24;
+}
+
+SLOSH_API slosh_status slosh_build_surface(void* ctx, const slosh_surface_params_t* params, slosh_surface_info_t* out) {
+    return guarded([&]() -> slosh_status {
+        Ctx* c = as_ctx(ctx);
+        if (!params) throw StatusError{SLOSH_ERR_INVALID_ARG, "params is NULL"};
+        c->build_surface(*params);
+        if (out) *out = c->surf_info;
+        return SLOSH_OK;
+    });
+}
+
+SLOSH_API slosh_status slosh_surface_device_ptrs(void* ctx, void** field_f16, void** positions, void** normals, void** tangents,
+                                                 void** indices) {
+    return guarded([&]() -> slosh_status {
+        Ctx* c = as_ctx(ctx);
+        if (field_f16) *field_f16 = c->surf.field;
+        if (positions) *positions = c->surf.positions;
+        if (normals) *normals = c->surf.normals;
+        if (tangents) *tangents = c->surf.tangents;
+        if (indices) *indices = c->surf.indices;
         return SLOSH_OK;
     });
 }

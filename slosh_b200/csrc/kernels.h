@@ -63,6 +63,9 @@ int3 sort_brick_dim(int3 grid);
 int launch_sort(const Dev& d, const SortBuffers& b, const slosh_particle_t* in, slosh_particle_t* out, uint32_t n,
                 uint32_t num_sort_keys, int3 sort_dim, cudaStream_t s);
 size_t sort_tile_hist_size(uint32_t capacity);
+// Exclusive prefix sum of n u32 (in place allowed); tmp holds exclusive_scan_tmp_size(n) words.
+int launch_exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* tmp, cudaStream_t s);
+size_t exclusive_scan_tmp_size(uint32_t n);
 size_t sort_scan_tmp_size(uint32_t capacity, uint32_t num_sort_keys);
 
 // ---- MGPCG (SloshPressureMG.usf) ----
@@ -107,5 +110,34 @@ int launch_pcg_apply_a(const Dev& d, const MGState& m, const Shape& sh, cudaStre
 int launch_pcg_update_pr(const Dev& d, const MGState& m, float* p, unsigned long long handle, const Shape& sh, cudaStream_t s);
 int launch_pcg_update_d(const Dev& d, const MGState& m, const Shape& sh, cudaStream_t s);
 int launch_true_residual(const Dev& d, const MGState& m, const float* p, const float* div, const Shape& sh, cudaStream_t s);
+
+// ---- headless surface (SloshSurface.usf): density field and surface nets ----
+struct SurfaceDev {
+    int3 dim;               // field voxels
+    int3 bdim;              // 8^3-voxel bricks of the field
+    float inv_voxel, voxel; // voxels per sim metre, sim metres per voxel
+    float support;          // SupportScale: kernel radius in splat radii
+    float max_footprint;    // MaxFootprint (voxels)
+    float radius_voxels;    // ParticleRadiusVoxels
+    float splat_radius;     // SplatRadiusSim (sim metres)
+    float iso;              // IsoLevel
+    uint32_t max_vertices, max_indices;
+    int32_t* accum;         // 5 fixed-point moments per voxel
+    uint16_t* field;        // f16 field per voxel
+    uint32_t* bricks;       // occupancy per field brick
+    uint32_t* vflag;        // per cell (dim - 1)^3: has a vertex
+    uint32_t* vbase;        // exclusive scan of vflag
+    uint32_t* cell_vertex;  // vertex index or 0xFFFFFFFF
+    uint32_t* qflag;        // quads per cell
+    uint32_t* qbase;        // exclusive scan of qflag
+    uint32_t* scan_tmp;
+    float* positions;       // 3 per vertex (sim metres)
+    float* normals;         // 3 per vertex
+    float* tangents;        // 3 per vertex
+    uint32_t* indices;      // 6 per quad
+    uint32_t* counters;     // [0] vertices requested, [1] indices requested
+};
+// Splat, resolve and (with mesh) surface nets of the first n particle records.
+int launch_surface(const SurfaceDev& s, const slosh_particle_t* particles, uint32_t n, bool mesh, cudaStream_t st);
 
 }  // namespace slosh

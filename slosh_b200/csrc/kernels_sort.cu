@@ -236,6 +236,11 @@ __global__ void k_live_count(const uint32_t* offsets, uint32_t num_keys, uint32_
 
 }  // namespace
 
+int launch_exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* tmp, cudaStream_t s) {
+    return exclusive_scan(in, out, n, tmp, s);
+}
+size_t exclusive_scan_tmp_size(uint32_t n) { return (size_t(n) + SCAN_TILE - 1) / SCAN_TILE + 1; }
+
 int3 sort_brick_dim(int3 g) { return make_int3((g.x + 3) / 4, (g.y + 3) / 4, (g.z + 3) / 4); }
 
 size_t sort_tile_hist_size(uint32_t capacity) {
