@@ -44,17 +44,23 @@ def parse():
     ap.add_argument("--workload", default="dam_break_sphere_256",
                     help="dam_break_sphere_<n> (n multiple of 8, 32..256) or dam_break_64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    # mgpcg: MGPCG to a relative residual of 1e-6 (the benchmark); rbgs: red-black SOR, omega 1.9, 200 iterations
+    ap.add_argument("--solver", choices=["mgpcg", "rbgs"], default="mgpcg")
     return ap.parse_args()
 
 
-def make_scene(workload, default_fn):
+def make_scene(workload, default_fn, solver="mgpcg"):
+    from slosh_b200 import _abi as A
     from slosh_b200 import scenes
+    sv = A.SOLVER_RBGS if solver == "rbgs" else A.SOLVER_MGPCG
     if workload == "dam_break_64":
-        sc = scenes.dam_break(default_fn, n=64)
+        sc = scenes.dam_break(default_fn, n=64, solver=sv)
         sc["settings"].sort_interval = 4
+        sc["settings"].sor_weight = 1.9
+        sc["settings"].pressure_iterations = 200
     elif workload.startswith("dam_break_sphere_") and workload[17:].isdigit() and int(workload[17:]) % 8 == 0 \
             and 32 <= int(workload[17:]) <= 256:
-        sc = scenes.dam_break_sphere(default_fn, n=int(workload[17:]))
+        sc = scenes.dam_break_sphere(default_fn, n=int(workload[17:]), solver=sv, sor_iterations=200)
     else:
         raise SystemExit(f"unknown workload {workload!r}")
     sc["settings"].max_substeps = 16  # CFL 1 holds; the plugin's default cap of 4 would exceed it
@@ -134,13 +140,13 @@ def dist_setup(n_gpus):
     return world, rank, local
 
 
-def cpu_baseline_sample(workload):
+def cpu_baseline_sample(workload, solver="mgpcg"):
     """One substep of the same workload by the C++ oracle on all host cores (bounded: ~10-30 s)."""
     from oracle import oracle as O
     from slosh_b200 import _abi as A
     O.build()
     cores = O.set_threads(os.cpu_count() or 1)
-    sc = make_scene(workload, O.settings_default)
+    sc = make_scene(workload, O.settings_default, solver)
     o = O.Oracle(sc["settings"])
     o.set_emit_seed(sc["seed"])
     fi = A.frame_input(sc["settings"], emits=sc["emits"])
@@ -162,7 +168,7 @@ def run_reference(args):
     from slosh_b200 import _abi as A
     O.build()
     cores = O.set_threads(os.cpu_count() or 1)
-    sc = make_scene(args.workload, O.settings_default)
+    sc = make_scene(args.workload, O.settings_default, args.solver)
     o = O.Oracle(sc["settings"])
     o.set_emit_seed(sc["seed"])
     fi = A.frame_input(sc["settings"], emits=sc["emits"])
@@ -192,7 +198,7 @@ def run_reference(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * el / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": sc["name"], "grid": list(sc["settings"].grid_dim), "particles": sc["particles"],
-                   "solver": "MGPCG", "tolerance": 1e-6, "step": "one substep"},
+                   "solver": "MGPCG" if args.solver == "mgpcg" else "RBGS omega 1.9 x200", "tolerance": 1e-6 if args.solver == "mgpcg" else None, "step": "one substep"},
         "cpu_baseline": {"value": value, "unit": "substeps/s", "cores": cores, "kind": "port",
                          "sample": f"{args.steps} substeps of {sc['name']} after {args.warmup} warm-up substeps"},
         "e2e": {"value": value, "unit": "substeps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -210,7 +216,7 @@ def run_slosh(args):
     dist = None
     if world > 1:
         import torch.distributed as dist
-    sc = make_scene(args.workload, S.settings_default)
+    sc = make_scene(args.workload, S.settings_default, args.solver)
     sim = S.Simulation(sc["settings"], device=local)
     stream = torch.cuda.Stream()
     sim.set_stream(stream.cuda_stream)
@@ -284,14 +290,14 @@ def run_slosh(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": sc["name"], "grid": list(sc["settings"].grid_dim), "particles": n_particles,
-                   "solver": "MGPCG", "tolerance": 1e-6, "transfer": "APIC", "cfl": 1.0, "frame_dt": 1.0 / 120.0,
+                   "solver": "MGPCG" if args.solver == "mgpcg" else "RBGS omega 1.9 x200", "tolerance": 1e-6 if args.solver == "mgpcg" else None, "transfer": "APIC", "cfl": 1.0, "frame_dt": 1.0 / 120.0,
                    "sort_interval": 4, "parallelism": f"replicas{world}", "step": "one frame of CFL substeps",
                    "l2": "inputs larger than L2 (particles 0.99 GB)"},
         "substeps": total_substeps,
         "particle_updates_per_s": total_substeps * n_particles / (dev_ms * 1e-3),
         "pressure_solve_ms": phase["pressure"] / max(substeps, 1),
         "pressure_iterations_mean": statistics.mean(iters) if iters else None,
-        "pressure_rel_residual_max": max(rels) if rels else None,
+        "pressure_rel_residual_max": (max(rels) if rels else None) if args.solver == "mgpcg" else None,
         "phase_ms_per_substep": {k: v / max(substeps, 1) for k, v in phase.items()},
         "clocks": clk,
         "e2e": {"value": total_substeps / (wall_ms * 1e-3), "unit": "substeps/s",
@@ -305,7 +311,7 @@ def run_slosh(args):
         sim.close()
         torch.cuda.synchronize()
         try:
-            line["cpu_baseline"] = cpu_baseline_sample(args.workload)
+            line["cpu_baseline"] = cpu_baseline_sample(args.workload, args.solver)
         except Exception as e:  # keep the GPU line even if the host sample fails
             line["cpu_baseline"] = {"value": None, "unit": "substeps/s", "error": str(e)[:200]}
     print(json.dumps(line), flush=True)

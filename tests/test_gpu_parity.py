@@ -75,6 +75,15 @@ def test_sparse_sphere_coarse_levels(slosh, oracle_mod, n):
     _run_frames(g, o, sc, frames=2)
 
 
+def test_dam_break_64_per_substep(slosh, oracle_mod):
+    """The 64^3 dam break (cells [1,26) x [1,39) x [1,63), 8 per cell: 471,200 particles), APIC, MGPCG to
+    1e-6, g = -9.81 y, CFL 1, frame dt 1/120: bit-exact after every substep for 4 frames."""
+    sc = scenes.dam_break(slosh.settings_default, n=64)
+    assert sc["particles"] == 471200
+    g, o = _pair(slosh, oracle_mod, sc)
+    _run_frames(g, o, sc, frames=4)
+
+
 def test_tiny_with_collider(slosh, oracle_mod):
     sc = scenes.tiny(slosh.settings_default, n=24, colliders=True)
     g, o = _pair(slosh, oracle_mod, sc)
