@@ -309,6 +309,12 @@ SLOSH_API slosh_status slosh_synchronize(void* ctx);
 /* ---- frame: replaces SubmitFrame_GameThread + Step_RenderThread (SloshProxy.cpp:146-161, 339-737).
  * Emission, the periodic spatial sort, CFL substep count and all substeps of one frame. */
 SLOSH_API slosh_status slosh_step_frame(void* ctx, const slosh_frame_input_t* input);
+/* Batched tanks (no reference counterpart; the plugin steps one proxy per volume): one frame of each of
+ * `count` independent contexts. All frames are enqueued on the contexts' own streams before any is
+ * waited for, so small tanks overlap on the device. statuses (optional, count entries) receives each
+ * context's frame status; the return value is the first non-OK one. */
+SLOSH_API slosh_status slosh_step_frames(void* const* ctxs, const slosh_frame_input_t* inputs, uint32_t count,
+                                         slosh_status* statuses);
 /* Split form of slosh_step_frame for per-substep harnesses: begin_frame does the frame prologue
  * (settings, emission, sort) and returns the substep count and dt; substep(i) runs one substep. */
 SLOSH_API slosh_status slosh_begin_frame(void* ctx, const slosh_frame_input_t* input,

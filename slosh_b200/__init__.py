@@ -50,6 +50,7 @@ SIGNATURES = {
     "slosh_get_phase_ms": ([_VP, C.POINTER(C.c_float), C.c_int32], C.c_int),
     "slosh_launch_count": ([_VP], C.c_uint64),
     "slosh_transfer_bytes": ([_VP, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)], C.c_int),
+    "slosh_step_frames": ([C.POINTER(_VP), C.POINTER(FrameInput), C.c_uint32, C.POINTER(C.c_int)], C.c_int),
     "slosh_surface_params_default": ([C.POINTER(SurfaceParams)], None),
     "slosh_build_surface": ([_VP, C.POINTER(SurfaceParams), C.POINTER(SurfaceInfo)], C.c_int),
     "slosh_surface_device_ptrs": ([_VP, C.POINTER(_VP), C.POINTER(_VP), C.POINTER(_VP), C.POINTER(_VP), C.POINTER(_VP)], C.c_int),
@@ -81,6 +82,19 @@ def load_library(path=None):
     if path is None:
         _lib = lib
     return lib
+
+
+def step_frames(sims, inputs):
+    """One frame of each Simulation in `sims` with the matching FrameInput, overlapped on the device
+    (slosh_step_frames). Returns the per-simulation status codes."""
+    n = len(sims)
+    if n != len(inputs):
+        raise ValueError("one frame input per simulation")
+    ctxs = (_VP * max(n, 1))(*[s._ctx for s in sims])
+    fis = (FrameInput * max(n, 1))(*inputs)
+    st = (C.c_int * max(n, 1))()
+    _check(load_library().slosh_step_frames(ctxs, fis, n, st))
+    return list(st)[:n]
 
 
 def surface_params_default():

@@ -794,7 +794,12 @@ struct Ctx {
     }
 
     // ---- frame epilogue: AccumulateStatsCS + the readback decode ----
-    void end_frame();
+    void end_frame() {
+        end_frame_enqueue();
+        end_frame_finish();
+    }
+    void end_frame_enqueue();  // frame epilogue and result copies on the stream
+    void end_frame_finish();   // waits for them and decodes
 };
 
 __global__ void k_accumulate_stats(uint32_t* stats, uint32_t* pc) {  // AccumulateStatsCS (Slosh.usf:264-270)
@@ -803,7 +808,7 @@ __global__ void k_accumulate_stats(uint32_t* stats, uint32_t* pc) {  // Accumula
     stats[15] = pc[2];
 }
 
-void Ctx::end_frame() {
+void Ctx::end_frame_enqueue() {
     if (num_colliders > 0 && substeps > 0) count(launch_submerged(dev(), shape, stream));  // SloshProxy.cpp:715-718
     k_accumulate_stats<<<1, 1, 0, stream>>>(stats, particle_count);
     count(1);
@@ -814,6 +819,9 @@ void Ctx::end_frame() {
     CK(cudaMemcpyAsync(h_ctl + 8, mg.ctl + 4, 4, cudaMemcpyDeviceToHost, stream));
     CK(cudaMemcpyAsync(h_coupling, coupling, SLOSH_MAX_COLLIDERS * SLOSH_COUPLING_STRIDE * 4, cudaMemcpyDeviceToHost, stream));
     d2h_bytes += SLOSH_NUM_STATS * 4 + 16 + 8 * sizeof(double) + SLOSH_MAX_COLLIDERS * SLOSH_COUPLING_STRIDE * 4;
+}
+
+void Ctx::end_frame_finish() {
     CK(cudaStreamSynchronize(stream));
     if (substeps > 0) {
         float ms;
@@ -1162,6 +1170,32 @@ SLOSH_API slosh_status slosh_step_frame(void* ctx, const slosh_frame_input_t* in
         for (int s = 0; s < n; ++s) c->substep(s);
         c->end_frame();
         return frame_status(c);
+    });
+}
+
+// Several independent tanks one frame each (batched tanks). Every context's frame is enqueued on its own
+// stream before any is waited for, so small tanks overlap on the device; then each frame is finished and
+// decoded in order. statuses (optional) receives each context's status; the return value is the first
+// status that is not SLOSH_OK (a warning or an error), else SLOSH_OK.
+SLOSH_API slosh_status slosh_step_frames(void* const* ctxs, const slosh_frame_input_t* inputs, uint32_t count,
+                                         slosh_status* statuses) {
+    return guarded([&]() -> slosh_status {
+        if (count && (!ctxs || !inputs)) throw StatusError{SLOSH_ERR_INVALID_ARG, "ctxs or inputs is NULL"};
+        for (uint32_t i = 0; i < count; ++i) {
+            Ctx* c = as_ctx(ctxs[i]);
+            const int n = c->begin_frame(inputs[i]);
+            for (int k = 0; k < n; ++k) c->substep(k);
+            c->end_frame_enqueue();
+        }
+        slosh_status first = SLOSH_OK;
+        for (uint32_t i = 0; i < count; ++i) {
+            Ctx* c = as_ctx(ctxs[i]);
+            c->end_frame_finish();
+            const slosh_status st = frame_status(c);
+            if (statuses) statuses[i] = st;
+            if (first == SLOSH_OK) first = st;
+        }
+        return first;
     });
 }
 

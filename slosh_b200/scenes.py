@@ -119,3 +119,25 @@ def tiny(lib_default, n=16, seed=0, solver=A.SOLVER_MGPCG, tolerance=1e-6, colli
         c.extent[:] = [0.15, 0, 0]
         sc["colliders"] = [c]
     return sc
+
+
+def tank_batch(lib_default, count=64, seed=3, lo=32, hi=128, tolerance=1e-6):
+    """Independent tanks for batched stepping: per-axis size log-uniform in [lo, hi] cells, h = 1/64 m
+    (the same cell for every tank), dam block x < U[0.2, 0.5], y < U[0.3, 0.7], full z, 8 particles per
+    cell, MGPCG to `tolerance`, sort every 4 frames. Returns a list of scene dicts (seeds seed * 1000 + k)."""
+    rng = np.random.default_rng(seed)
+    tanks = []
+    for k in range(count):
+        grid = tuple(int(round(math.exp(rng.uniform(math.log(lo), math.log(hi))))) for _ in range(3))
+        xf, yf = float(rng.uniform(0.2, 0.5)), float(rng.uniform(0.3, 0.7))
+        mn, dims = box_cells(grid, (0.0, 0.0, 0.0), (xf, yf, 1.0))
+        n = dims[0] * dims[1] * dims[2] * 8
+        s = base_settings(lib_default, grid, n)
+        s.cell_size = 1.0 / 64.0
+        s.tolerance = tolerance
+        s.max_iterations = 200
+        s.sort_interval = 4
+        s.max_substeps = 16
+        tanks.append(dict(settings=s, emits=[fill_cells(mn, dims)], seed=seed * 1000 + k, particles=n,
+                          name=f"tank{k}_{grid[0]}x{grid[1]}x{grid[2]}", cost=float(grid[0] * grid[1] * grid[2] + n)))
+    return tanks
