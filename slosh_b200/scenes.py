@@ -141,3 +141,40 @@ def tank_batch(lib_default, count=64, seed=3, lo=32, hi=128, tolerance=1e-6):
         tanks.append(dict(settings=s, emits=[fill_cells(mn, dims)], seed=seed * 1000 + k, particles=n,
                           name=f"tank{k}_{grid[0]}x{grid[1]}x{grid[2]}", cost=float(grid[0] * grid[1] * grid[2] + n)))
     return tanks
+
+
+def boxes_512(lib_default, seed=2, tolerance=1e-6, box_count=(6, 10), size=(0.1, 0.4), spheres=3):
+    """512 x 256 x 256 cells (h = 1/256 m): `box_count` non-overlapping liquid boxes (drawn in order, a box
+    that overlaps an earlier one is redrawn), each side a fraction U[size] of the domain side, 8 particles
+    per cell, plus `spheres` static collider spheres (radius U[0.04, 0.08] m) above the liquid's floor."""
+    rng = np.random.default_rng(seed)
+    grid = (512, 256, 256)
+    n_boxes = int(rng.integers(box_count[0], box_count[1] + 1))
+    boxes = []
+    attempts = 0
+    while len(boxes) < n_boxes and attempts < 1000:
+        attempts += 1
+        fr = rng.uniform(size[0], size[1], size=3)
+        lo = rng.uniform(0.0, 1.0 - fr)
+        mn, dims = box_cells(grid, tuple(lo), tuple(lo + fr))
+        if any(all(mn[a] < b[0][a] + b[1][a] and b[0][a] < mn[a] + dims[a] for a in range(3)) for b in boxes):
+            continue
+        boxes.append((mn, dims))
+    emits = [fill_cells(mn, dims) for mn, dims in boxes]
+    count = sum(d[0] * d[1] * d[2] * 8 for _, d in boxes)
+    s = base_settings(lib_default, grid, count)
+    s.cell_size = 1.0 / 256.0
+    s.tolerance = tolerance
+    s.max_iterations = 200
+    s.sort_interval = 4
+    s.max_substeps = 16
+    colliders = []
+    for _ in range(spheres):
+        c = A.Collider()
+        r = float(rng.uniform(0.04, 0.08))
+        c.center[:] = [float(rng.uniform(0.2, 1.8)), float(rng.uniform(0.1, 0.6)), float(rng.uniform(0.2, 0.8))]
+        c.type = A.COLLIDER_SPHERE
+        c.rotation[:] = [0.0, 0.0, 0.0, 1.0]
+        c.extent[:] = [r, 0.0, 0.0]
+        colliders.append(c)
+    return dict(settings=s, emits=emits, seed=seed, particles=count, colliders=colliders, name="boxes_512x256x256")
