@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     # mgpcg: MGPCG to a relative residual of 1e-6 (the benchmark); rbgs: red-black SOR, omega 1.9, 200 iterations
     ap.add_argument("--solver", choices=["mgpcg", "rbgs"], default="mgpcg")
+    # storage of the V-cycle's coarse levels (precision_mode); the CG vectors and level 0 stay FP32
+    ap.add_argument("--precision", choices=["fp32", "fp16", "bf16"], default="fp32")
     # tanks_64: 64 independent tanks (32^3-128^3), LPT-partitioned over the ranks; each step is one frame of
     # every tank, overlapped on the device by slosh_step_frames, and the same frames are then timed sequentially
     ap.add_argument("--tanks", type=int, default=64)
@@ -223,6 +225,8 @@ def run_slosh(args):
     if world > 1:
         import torch.distributed as dist
     sc = make_scene(args.workload, S.settings_default, args.solver)
+    sc["settings"].precision_mode = {"fp32": A.PRECISION_FP32, "fp16": A.PRECISION_FP16_STORAGE,
+                                     "bf16": A.PRECISION_BF16_STORAGE}[args.precision]
     sim = S.Simulation(sc["settings"], device=local)
     stream = torch.cuda.Stream()
     sim.set_stream(stream.cuda_stream)
@@ -300,6 +304,7 @@ def run_slosh(args):
         "config": {"workload": sc["name"], "grid": list(sc["settings"].grid_dim), "particles": n_particles,
                    "solver": "MGPCG" if args.solver == "mgpcg" else "RBGS omega 1.9 x200", "tolerance": 1e-6 if args.solver == "mgpcg" else None, "transfer": "APIC", "cfl": 1.0, "frame_dt": 1.0 / 120.0,
                    "sort_interval": 4, "parallelism": f"replicas{world}", "step": "one frame of CFL substeps",
+                   "mg_coarse_storage": args.precision,
                    "l2": f"inputs larger than L2 (particles {48.0 * n_particles / 1e9:.2f} GB)"},
         "substeps": total_substeps,
         "particle_updates_per_s": total_substeps * n_particles / (dev_ms * 1e-3),

@@ -60,6 +60,8 @@ def lib():
         L.oracle_settings_default.restype = None
         L.oracle_f32_to_f16.argtypes = [C.c_float]
         L.oracle_f32_to_f16.restype = C.c_uint16
+        L.oracle_f32_to_bf16.argtypes = [C.c_float]
+        L.oracle_f32_to_bf16.restype = C.c_uint16
         L.oracle_f16_to_f32.argtypes = [C.c_uint16]
         L.oracle_f16_to_f32.restype = C.c_float
         L.oracle_pcg_hash.argtypes = [C.c_uint32]

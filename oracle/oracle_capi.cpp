@@ -150,6 +150,7 @@ View<R> view(Sim<R>& s, int id) {
 
 ORACLE_API void oracle_settings_default(slosh_settings_t* out) { settings_default(out); }
 ORACLE_API uint16_t oracle_f32_to_f16(float f) { return f32_to_f16(f); }
+ORACLE_API uint16_t oracle_f32_to_bf16(float f) { return f32_to_bf16(f); }
 ORACLE_API float oracle_f16_to_f32(uint16_t h) { return f16_to_f32(h); }
 ORACLE_API uint32_t oracle_pcg_hash(uint32_t v) { return pcg_hash(v); }
 ORACLE_API float oracle_hash_to_unit(uint32_t v) { return hash_to_unit(v); }

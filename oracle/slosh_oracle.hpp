@@ -92,6 +92,20 @@ inline uint16_t f32_to_f16(float f) {
 }
 
 // f16tof32 (exact).
+// FP32 -> BF16, round to nearest even (NaN stays NaN, quiet); BF16 -> FP32 is exact.
+inline uint16_t f32_to_bf16(float f) {
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    if ((u & 0x7FFFFFFFu) > 0x7F800000u) return uint16_t((u >> 16) | 0x40u);
+    u += 0x7FFFu + ((u >> 16) & 1u);
+    return uint16_t(u >> 16);
+}
+inline float bf16_to_f32(uint16_t h) {
+    const uint32_t u = uint32_t(h) << 16;
+    float f;
+    std::memcpy(&f, &u, 4);
+    return f;
+}
 inline float f16_to_f32(uint16_t h) {
     const uint32_t sign = uint32_t(h & 0x8000u) << 16;
     const uint32_t exp = (h >> 10) & 0x1Fu;
@@ -415,6 +429,7 @@ struct PassParams {
     float pressure_to_pascal = 0, density_correction = 0, target_ppc = 8.0f, density_deadband = 0;
     float coupling_scale = 1024.0f, density_relaxation = 0;
     uint32_t use_apic = 1, smooth_coupling = 1, ghost_fluid = 1, num_colliders = 0, num_manipulators = 0;
+    uint32_t precision_mode = SLOSH_PRECISION_FP32;  // storage of the coarse MG levels
     uint32_t frame_seed = 0;
 };
 
@@ -1233,6 +1248,13 @@ public:
         }
         if (l == 0) out_diag = (*diag_f)[i] + R(DIAG_EPSILON);
     }
+    // Storage precision of the coarse levels (precision_mode): every store to a level >= 1 rounds to it.
+    R store_q(int l, R v) const {
+        if (l == 0) return v;
+        if (P.precision_mode == SLOSH_PRECISION_FP16_STORAGE) return R(f16_to_f32(f32_to_f16(float(v))));
+        if (P.precision_mode == SLOSH_PRECISION_BF16_STORAGE) return R(bf16_to_f32(f32_to_bf16(float(v))));
+        return v;
+    }
     std::vector<R>& level_x(int l) { return l == 0 ? pcg_z : mg[l].x; }
     std::vector<R>& level_b(int l) { return l == 0 ? pcg_r : mg[l].b; }
 
@@ -1285,7 +1307,7 @@ public:
                     R diag, sum;
                     stencil(l, xf, c, i, &cell_diag, diag, sum);
                     R b = bf[i];
-                    R x = (b + sum) / diag;
+                    R x = store_q(l, (b + sum) / diag);
                     xf[i] = x;
                     dv = double(b * x);
                 } else if (dot) {
@@ -1322,14 +1344,14 @@ public:
                 }
             }
             R b = R(0.25f) * sum;
-            cl.b[ci] = b;
+            cl.b[ci] = store_q(l + 1, b);
             R cdiag = R(DIAG_EPSILON);
             for (int n = 0; n < 6; ++n) {
                 I3 nb = c + neighbour_offset(n);
                 uint32_t t = inside(nb, cl.dim) ? (cl.type[lin(nb, cl.dim)] & CELL_TYPE_MASK) : CELL_SOLID;
                 cdiag = cdiag + (t != CELL_SOLID ? R(1) : R(0));
             }
-            cl.x[ci] = is_red(c) ? b / cdiag : R(0);
+            cl.x[ci] = store_q(l + 1, is_red(c) ? b / cdiag : R(0));
         };
         if (l == 0) {
             // SparseCoarse: the 4^3 level-1 cells of every active brick.
@@ -1361,7 +1383,7 @@ public:
                     if ((level_type_raw(l, i) & CELL_TYPE_MASK) == CELL_FLUID && (is_red(c) ? 0u : 1u) == colour) {
                         R diag, sum;
                         stencil(l, xf, c, i, &cell_diag, diag, sum);
-                        xf[i] = (bf[i] + sum) / diag;
+                        xf[i] = store_q(l, (bf[i] + sum) / diag);
                     }
                 }
     }
@@ -1373,7 +1395,7 @@ public:
             if ((level_type_raw(l, i) & CELL_TYPE_MASK) != CELL_FLUID) return;
             I3 parent{c.x / 2, c.y / 2, c.z / 2};
             uint32_t pi = lin(parent, cl.dim);
-            if ((cl.type[pi] & CELL_TYPE_MASK) == CELL_FLUID) xf[i] = xf[i] + cl.x[pi];
+            if ((cl.type[pi] & CELL_TYPE_MASK) == CELL_FLUID) xf[i] = store_q(l, xf[i] + cl.x[pi]);
         };
         if (l == 0) {
             for_active_cells(fine);
@@ -2096,6 +2118,7 @@ public:
         P.coupling_scale = 1024.0f;
         P.warm_start_scale = 1.0f;
         P.smooth_coupling = s.smooth_coupling_force ? 1u : 0u;
+        P.precision_mode = s.precision_mode <= uint32_t(SLOSH_PRECISION_BF16_STORAGE) ? s.precision_mode : uint32_t(SLOSH_PRECISION_FP32);
         P.ghost_fluid = s.ghost_fluid ? 1u : 0u;
         const int interval = clampi(s.density_projection_interval, 1, 8);
         P.density_relaxation = 1.0f - std::pow(1.0f - clampr(s.density_relaxation, 0.0f, 1.0f), float(interval));

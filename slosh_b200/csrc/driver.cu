@@ -172,6 +172,7 @@ struct Ctx {
     int last_iterations = 0;
     float last_rel = 0.0f, last_true_rel = 0.0f;
     bool last_converged = true;
+    uint32_t mg_prec = SLOSH_PRECISION_FP32;  // storage precision of the coarse MG levels (precision_mode)
     bool pool_overflow_seen = false;
     bool rel_pending = false;
     bool solve_tol_mode = false;
@@ -352,8 +353,10 @@ struct Ctx {
                 mg.lv[l].x = dalloc<float>((level_cells[l] + 3u) & ~3u, false);  // padded: read as 16-byte chunks
                 mg.lv[l].b = dalloc<float>((level_cells[l] + 3u) & ~3u, false);
                 mg.lv[l].word = dalloc<uint16_t>(level_cells[l], false);
+                mg.lv[l].prec = mg_prec;
             } else {
                 mg.lv[l].type = nullptr; mg.lv[l].x = nullptr; mg.lv[l].b = nullptr; mg.lv[l].word = nullptr;
+                mg.lv[l].prec = SLOSH_PRECISION_FP32;  // level 0 (the pool) is always FP32
             }
         }
         mg.r = dalloc<float>(pc, false);
@@ -673,6 +676,15 @@ struct Ctx {
         if (in.reset || !allocated || !layout_equals(s, S)) allocate(s);
         ensure_capacity(s.particle_capacity);
         S = s;
+        {  // storage precision of the coarse MG levels; the solve graphs hold the level descriptors
+            const uint32_t prec = s.precision_mode <= uint32_t(SLOSH_PRECISION_BF16_STORAGE) ? s.precision_mode : uint32_t(SLOSH_PRECISION_FP32);
+            if (prec != mg_prec) {
+                CK(cudaStreamSynchronize(stream));
+                destroy_graphs();
+                mg_prec = prec;
+                for (int l = 1; l < mg.num_levels; ++l) mg.lv[l].prec = prec;
+            }
+        }
         ++sim_frame;
         event_next = 0;
         phase_events.clear();

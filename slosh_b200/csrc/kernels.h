@@ -76,6 +76,7 @@ struct MGLevel {
     float* x;
     float* b;
     uint16_t* word;   // per-solve stencil word: bits 0-5 fluid neighbour, 6 fluid, 7 red, 8-13 non-solid neighbour
+    uint32_t prec;    // storage of x and b: SLOSH_PRECISION_FP32, _FP16_STORAGE (2-byte halves) or _BF16_STORAGE
 };
 struct MGState {
     int num_levels;

@@ -19,11 +19,35 @@
 //     ascent with block barriers between passes).
 #include <algorithm>
 
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
 #include "kernels.h"
 
 namespace slosh {
 
 namespace {
+
+// ---- storage precision of the coarse levels (precision_mode) --------------------------------------------
+// Coarse-level x and b are computed in FP32; with FP16 or BF16 storage every store rounds to the format
+// (round to nearest even) and the arrays hold 2-byte elements. Level 0 and the CG vectors stay FP32.
+__device__ __forceinline__ float q_prec(float v, uint32_t prec) {
+    if (prec == SLOSH_PRECISION_FP16_STORAGE) return __half2float(__float2half_rn(v));
+    if (prec == SLOSH_PRECISION_BF16_STORAGE) return __bfloat162float(__float2bfloat16_rn(v));
+    return v;
+}
+__device__ __forceinline__ float lv_ld(const float* a, uint32_t i, uint32_t prec) {
+    if (prec == SLOSH_PRECISION_FP32) return a[i];
+    const uint16_t h = reinterpret_cast<const uint16_t*>(a)[i];
+    return prec == SLOSH_PRECISION_FP16_STORAGE ? __half2float(__ushort_as_half(h)) : __uint_as_float(uint32_t(h) << 16);
+}
+__device__ __forceinline__ uint16_t to_storage16(float v, uint32_t prec) {
+    return prec == SLOSH_PRECISION_FP16_STORAGE ? __half_as_ushort(__float2half_rn(v)) : __bfloat16_as_ushort(__float2bfloat16_rn(v));
+}
+__device__ __forceinline__ void lv_st(float* a, uint32_t i, uint32_t prec, float v) {
+    if (prec == SLOSH_PRECISION_FP32) a[i] = v;
+    else reinterpret_cast<uint16_t*>(a)[i] = to_storage16(v, prec);
+}
 
 __device__ __forceinline__ uint32_t lin3(int3 c, int3 dim) { return uint32_t(c.x + dim.x * (c.y + dim.y * c.z)); }
 __device__ __forceinline__ int3 coord3(uint32_t i, int3 dim) {
@@ -401,11 +425,12 @@ __device__ __forceinline__ float word_diag(uint32_t w) {
 // Sum of x over the fluid neighbours of a dense global level, in neighbour order. All six values are
 // loaded unconditionally (indices clamped into the level, so a missing neighbour reads some cell of
 // the level) and then selected by the word, so the loads overlap the word's.
-__device__ __forceinline__ float word_sum_g(const float* x, uint32_t w, uint32_t i, uint32_t dx, uint32_t dxy, uint32_t last) {
+__device__ __forceinline__ float word_sum_g(const float* x, uint32_t prec, uint32_t w, uint32_t i, uint32_t dx, uint32_t dxy,
+                                            uint32_t last) {
     const uint32_t off[6] = {i - 1u, i + 1u, i - dx, i + dx, i - dxy, i + dxy};
     float v[6];
 #pragma unroll
-    for (int n = 0; n < 6; ++n) v[n] = x[min(off[n], last)];
+    for (int n = 0; n < 6; ++n) v[n] = lv_ld(x, min(off[n], last), prec);
     float sum = 0.0f;
 #pragma unroll
     for (int n = 0; n < 6; ++n)
@@ -590,7 +615,7 @@ __global__ void __launch_bounds__(GRID_THREADS) k_prolong_smooth0(Dev d, MGState
                 v[r] = 0.0f;
                 if (j < 216u && inside3(c, C.dim)) {
                     const uint32_t ci = lin3(c, C.dim);
-                    const float x = C.x[ci];
+                    const float x = lv_ld(C.x, ci, C.prec);
                     v[r] = (C.word[ci] & CW_FLUID) ? x : 0.0f;
                 }
             }
@@ -625,10 +650,10 @@ __global__ void k_smooth_fp(Dev d, MGState m, int l, uint32_t parity) {
     const uint32_t last = L.cells - 1u;
     for_footprint(d, L, l, [&](uint32_t i, int3) {
         const uint32_t w = L.word[i];
-        const float b = L.b[i];
-        const float sum = word_sum_g(L.x, w, i, dx, dxy, last);
+        const float b = lv_ld(L.b, i, L.prec);
+        const float sum = word_sum_g(L.x, L.prec, w, i, dx, dxy, last);
         if (!(w & CW_FLUID) || (w & CW_RED) != want) return;
-        L.x[i] = (b + sum) / word_diag(w);
+        lv_st(L.x, i, L.prec, (b + sum) / word_diag(w));
     });
 }
 // Restriction l -> l + 1 over level l + 1's footprint: b_c = (sum of the fluid children's residuals) / 4.
@@ -648,21 +673,21 @@ __global__ void k_restrict_fp(Dev d, MGState m, int l) {
             const bool in = inside3(f, F.dim);
             const uint32_t fi = in ? lin3(f, F.dim) : 0u;
             const uint32_t w = F.word[fi];
-            const float r = F.b[fi] - (word_diag(w) * F.x[fi] - word_sum_g(F.x, w, fi, fdx, fdxy, flast));
+            const float r = lv_ld(F.b, fi, F.prec) - (word_diag(w) * lv_ld(F.x, fi, F.prec) - word_sum_g(F.x, F.prec, w, fi, fdx, fdxy, flast));
             res[o] = 0.0f;
             if (in && (w & CW_FLUID)) {
                 fl |= 1u << o;
                 res[o] = r;
             }
         }
-        if (!(cw & CW_FLUID)) { C.b[ci] = 0.0f; C.x[ci] = 0.0f; return; }
+        if (!(cw & CW_FLUID)) { lv_st(C.b, ci, C.prec, 0.0f); lv_st(C.x, ci, C.prec, 0.0f); return; }
         float sum = 0.0f;
 #pragma unroll
         for (int o = 0; o < 8; ++o)
             if ((fl >> o) & 1u) sum = sum + res[o];
         const float bb = 0.25f * sum;
-        C.b[ci] = bb;
-        C.x[ci] = (cw & CW_RED) ? bb / word_diag(cw) : 0.0f;
+        lv_st(C.b, ci, C.prec, bb);
+        lv_st(C.x, ci, C.prec, (cw & CW_RED) ? bb / word_diag(cw) : 0.0f);
     });
 }
 // Prolongation l + 1 -> l fused with the black sweep of level l (see k_prolong_smooth0).
@@ -675,24 +700,24 @@ __global__ void k_prolong_smooth_fp(Dev d, MGState m, int l) {
         // The neighbours' x and their parents' words and x are loaded before the word is tested
         // (indices clamped into the levels; values of non-fluid neighbours are not used).
         const uint32_t w = F.word[i];
-        const float b = F.b[i];
+        const float b = lv_ld(F.b, i, F.prec);
         const uint32_t off[6] = {i - 1u, i + 1u, i - dx, i + dx, i - dxy, i + dxy};
         float v[6];
 #pragma unroll
         for (int n = 0; n < 6; ++n) {
             const int3 nb = add3(c, nbr_off(n));
             const uint32_t pi = min(lin3(make_int3(nb.x / 2, nb.y / 2, nb.z / 2), C.dim), clast);
-            const float xn = F.x[min(off[n], last)];
+            const float xn = lv_ld(F.x, min(off[n], last), F.prec);
             const uint32_t pw = C.word[pi];
-            const float px = C.x[pi];
-            v[n] = (pw & CW_FLUID) ? xn + px : xn;
+            const float px = lv_ld(C.x, pi, C.prec);
+            v[n] = (pw & CW_FLUID) ? q_prec(xn + px, F.prec) : xn;  // the prolonged value as it would be stored
         }
         if (!(w & CW_FLUID) || (w & CW_RED)) return;
         float sum = 0.0f;
 #pragma unroll
         for (int n = 0; n < 6; ++n)
             if ((w >> n) & 1u) sum = sum + v[n];
-        F.x[i] = (b + sum) / word_diag(w);
+        lv_st(F.x, i, F.prec, (b + sum) / word_diag(w));
     });
 }
 
@@ -739,8 +764,8 @@ __global__ void __launch_bounds__(GRID_THREADS) k_restrict0(Dev d, MGState m) {
             const uint32_t ci = lin3(c, C.dim);
             const uint32_t cw = C.word[ci];
             if (!(cw & CW_FLUID)) {
-                C.b[ci] = 0.0f;
-                C.x[ci] = 0.0f;
+                lv_st(C.b, ci, C.prec, 0.0f);
+                lv_st(C.x, ci, C.prec, 0.0f);
                 continue;
             }
             float sum = 0.0f;
@@ -750,8 +775,8 @@ __global__ void __launch_bounds__(GRID_THREADS) k_restrict0(Dev d, MGState m) {
                 if (s_fluid[warp][fl]) sum = sum + s_res[warp][fl];
             }
             const float bb = 0.25f * sum;
-            C.b[ci] = bb;
-            C.x[ci] = (cw & CW_RED) ? bb / word_diag(cw) : 0.0f;
+            lv_st(C.b, ci, C.prec, bb);
+            lv_st(C.x, ci, C.prec, (cw & CW_RED) ? bb / word_diag(cw) : 0.0f);
         }
         __syncwarp();
     }
@@ -830,6 +855,7 @@ struct SLevel {
     float* b;
     const uint32_t* list;  // red cells then black cells
     uint32_t nred, nblack;
+    uint32_t prec;         // storage precision: stores round to it (the values stay FP32 in shared memory)
 };
 __device__ __forceinline__ void s_sweep(const SLevel L, uint32_t colour) {
     const uint32_t n = colour == 0u ? L.nred : L.nblack;
@@ -837,7 +863,7 @@ __device__ __forceinline__ void s_sweep(const SLevel L, uint32_t colour) {
     for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) {
         const uint32_t i = list[j];
         const uint32_t w = L.word[i];
-        L.x[i] = (L.b[i] + word_sum(L.x, w, i, L.dx, L.dxy)) / L.diag[i];
+        L.x[i] = q_prec((L.b[i] + word_sum(L.x, w, i, L.dx, L.dxy)) / L.diag[i], L.prec);
     }
     __syncthreads();
 }
@@ -853,7 +879,7 @@ __device__ __forceinline__ void s_coarse_solve(const SLevel L, int iterations) {
                 for (uint32_t j = threadIdx.x; j < n; j += 128u) {
                     const uint32_t i = list[j];
                     const uint32_t w = L.word[i];
-                    L.x[i] = (L.b[i] + word_sum(L.x, w, i, L.dx, L.dxy)) / L.diag[i];
+                    L.x[i] = q_prec((L.b[i] + word_sum(L.x, w, i, L.dx, L.dxy)) / L.diag[i], L.prec);
                 }
                 asm volatile("bar.sync 1, 128;" ::: "memory");
             }
@@ -882,6 +908,7 @@ __global__ void __launch_bounds__(1024) k_vcycle_tail(MGState m, int tail, int i
         L.list = reinterpret_cast<const uint32_t*>(s_tail + o.list);
         L.nred = m.tail_meta[4 * l + 1];
         L.nblack = m.tail_meta[4 * l + 3];
+        L.prec = G.prec;
     }
     // One round trip: level tail's x and b from the level arrays, everything static (diagonals, words,
     // colour lists of all tail levels) from the image k_tail_lists built for this solve.
@@ -897,7 +924,18 @@ __global__ void __launch_bounds__(1024) k_vcycle_tail(MGState m, int tail, int i
 #pragma unroll
             for (int r = 0; r < 8; ++r) {
                 const uint32_t k = k0 + uint32_t(r) * 1024u + threadIdx.x;
-                if (k < n16) v[r] = k < c16 ? gx[k] : (k < 2u * c16 ? gb[k - c16] : img[k]);
+                if (k < n16) {
+                    if (k < 2u * c16 && m.lv[tail].prec != SLOSH_PRECISION_FP32) {
+                        // 2-byte storage: four elements per 16-byte chunk of shared memory
+                        const float* src = k < c16 ? m.lv[tail].x : m.lv[tail].b;
+                        const uint32_t e = 4u * (k < c16 ? k : k - c16);
+                        const uint32_t pr = m.lv[tail].prec;
+                        v[r] = make_uint4(__float_as_uint(lv_ld(src, e, pr)), __float_as_uint(lv_ld(src, e + 1u, pr)),
+                                          __float_as_uint(lv_ld(src, e + 2u, pr)), __float_as_uint(lv_ld(src, e + 3u, pr)));
+                    } else {
+                        v[r] = k < c16 ? gx[k] : (k < 2u * c16 ? gb[k - c16] : img[k]);
+                    }
+                }
             }
 #pragma unroll
             for (int r = 0; r < 8; ++r) {
@@ -932,8 +970,8 @@ __global__ void __launch_bounds__(1024) k_vcycle_tail(MGState m, int tail, int i
             for (int o = 0; o < 8; ++o)
                 if ((fl >> o) & 1u) sum = sum + res[o];
             const float bb = 0.25f * sum;
-            C.b[ci] = bb;
-            C.x[ci] = (C.word[ci] & CW_RED) ? bb / C.diag[ci] : 0.0f;
+            C.b[ci] = q_prec(bb, C.prec);
+            C.x[ci] = q_prec((C.word[ci] & CW_RED) ? bb / C.diag[ci] : 0.0f, C.prec);
         }
         __syncthreads();
         if (l + 1 < nl - 1) s_sweep(C, 1u);
@@ -946,7 +984,7 @@ __global__ void __launch_bounds__(1024) k_vcycle_tail(MGState m, int tail, int i
             const uint32_t i = F.list[j];
             const int3 c = coord3(i, F.dim);
             const uint32_t pi = lin3(make_int3(c.x / 2, c.y / 2, c.z / 2), C.dim);
-            if (C.word[pi] & CW_FLUID) F.x[i] = F.x[i] + C.x[pi];
+            if (C.word[pi] & CW_FLUID) F.x[i] = q_prec(F.x[i] + C.x[pi], F.prec);
         }
         __syncthreads();
         s_sweep(F, 1u);
@@ -955,8 +993,14 @@ __global__ void __launch_bounds__(1024) k_vcycle_tail(MGState m, int tail, int i
     {
         const uint32_t c16 = tail_pad4(m.lv[tail].cells) / 4u;
         const uint4* src = reinterpret_cast<const uint4*>(s_tail);
-        uint4* gx = reinterpret_cast<uint4*>(m.lv[tail].x);
-        for (uint32_t k = threadIdx.x; k < c16; k += blockDim.x) gx[k] = src[k];
+        const uint32_t pr = m.lv[tail].prec;
+        if (pr == SLOSH_PRECISION_FP32) {
+            uint4* gx = reinterpret_cast<uint4*>(m.lv[tail].x);
+            for (uint32_t k = threadIdx.x; k < c16; k += blockDim.x) gx[k] = src[k];
+        } else {
+            const float* sx = reinterpret_cast<const float*>(s_tail);
+            for (uint32_t e = threadIdx.x; e < 4u * c16; e += blockDim.x) lv_st(m.lv[tail].x, e, pr, sx[e]);
+        }
     }
 }
 

@@ -156,3 +156,17 @@ def test_step_frames_matches_individual_frames(slosh):
         assert np.array_equal(a.particles().view(np.uint32), b.particles().view(np.uint32))
         assert np.array_equal(a.read("PRESSURE").view(np.uint32), b.read("PRESSURE").view(np.uint32))
         assert a.results().substeps == b.results().substeps
+
+
+@pytest.mark.parametrize("mode", [A.PRECISION_FP16_STORAGE, A.PRECISION_BF16_STORAGE])
+@pytest.mark.parametrize("n", [64, 96])
+def test_coarse_storage_precision(slosh, oracle_mod, mode, n):
+    """FP16 / BF16 storage of the V-cycle's coarse levels: bit-exact against the oracle run at the same
+    storage precision, and the solve still reaches its tolerance."""
+    sc = scenes.dam_break_sphere(slosh.settings_default, n=n)
+    sc["settings"].max_substeps = 16
+    sc["settings"].precision_mode = mode
+    g, o = pair(slosh, oracle_mod, sc)
+    run_frames(g, o, sc, frames=2)
+    r = g.results()
+    assert r.last_solve_rel_residual <= 1e-6

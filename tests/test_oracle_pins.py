@@ -344,3 +344,15 @@ def test_fp32_error_against_fp64_oracle(oracle_mod):
     # MGPCG stops at a 1e-6 relative residual; FP32 storage adds ~1e-7 relative rounding per pass.
     assert errs[("oracle32", "PRESSURE")] < 1e-4, errs
     assert errs[("oracle32", "VEL")] < 1e-5, errs
+
+
+def test_bf16_conversion_matches_torch(oracle_mod):
+    """The oracle's FP32 -> BF16 rounding (coarse-level storage) against torch's round-to-nearest-even."""
+    import torch
+    rng = np.random.default_rng(5)
+    x = np.concatenate([rng.normal(size=20000).astype(np.float32) * np.float32(10.0) ** rng.integers(-6, 6, 20000),
+                        np.array([0.0, -0.0, 1.0, 65504.0, 3.4e38, -3.4e38, 1e-40], dtype=np.float32)]).astype(np.float32)
+    want = torch.from_numpy(x).to(torch.bfloat16).view(torch.int16).numpy().view(np.uint16)
+    lib = oracle_mod.lib()
+    got = np.array([lib.oracle_f32_to_bf16(float(v)) for v in x], dtype=np.uint16)
+    assert np.array_equal(got, want)
