@@ -17,16 +17,35 @@ namespace slosh {
 
 namespace {
 
+// Slots of the six face-neighbour bricks (-x, +x, -y, +y, -z, +z; 0 = the null slot when the neighbour
+// brick lies outside the grid) of the brick this CTA visits in for_active_cells, loaded once per brick, so
+// that a neighbour across the brick's faces costs no brick-table read.
+__device__ __forceinline__ uint32_t* cta_nbr_slots() {
+    __shared__ uint32_t s_slots[6];
+    return s_slots;
+}
+// Neighbour n of cell (c, index) of the current brick: a fixed offset inside the brick, otherwise the
+// same local cell with the axis coordinate wrapped in the neighbour brick's slot. Valid inside
+// for_active_cells only; equal to nbr_index (common.cuh) there.
+__device__ __forceinline__ uint32_t nbr_index_cta(uint32_t index, int3 c, int n) {
+    const int a = n >> 1;
+    const int l = comp(c, a) & 7;
+    const bool plus = (n & 1) != 0;
+    const uint32_t stride = a == 0 ? 1u : (a == 1 ? 8u : 64u);
+    if (plus ? l < 7 : l > 0) return plus ? index + stride : index - stride;
+    const uint32_t local = index & (BRICK_CELLS - 1u);
+    return cta_nbr_slots()[n] * BRICK_CELLS + (plus ? local - 7u * stride : local + 7u * stride);
+}
 // In-grid neighbour n of cell (c, index); out-of-grid neighbours resolve into the null brick.
 __device__ __forceinline__ uint32_t nidx(const Dev& d, uint32_t index, int3 c, int n) {
     const int3 nb = add3(c, nbr_off(n));
     if (!in_grid(d, nb)) return local_index_of(nb);
-    return nbr_index(d, index, c, n);
+    return nbr_index_cta(index, c, n);
 }
 __device__ __forceinline__ uint32_t ntype(const Dev& d, uint32_t index, int3 c, int n) {
     const int3 nb = add3(c, nbr_off(n));
     if (!in_grid(d, nb)) return CELL_SOLID;
-    return d.cell_type[nbr_index(d, index, c, n)];
+    return d.cell_type[nbr_index_cta(index, c, n)];
 }
 
 // CellDensity (Slosh.usf:211-224).
@@ -65,14 +84,23 @@ __device__ __forceinline__ bool touches_air(const Dev& d, uint32_t index, int3 c
     return t;
 }
 
-// Visits the in-grid cells of the active bricks: fn(index, c). fn must not contain CTA barriers.
+// Visits the in-grid cells of the active bricks: fn(index, c). fn must not contain CTA barriers; every
+// thread of the CTA must call it (it loads the brick's neighbour slots between two barriers).
 template <class Fn>
 __device__ __forceinline__ void for_active_cells(const Dev& d, Fn fn) {
     const uint32_t active = d.active_bricks[0];
+    uint32_t* ns = cta_nbr_slots();
     for (uint32_t e = blockIdx.x; e < active; e += gridDim.x) {
         const uint32_t brick = d.active_bricks[1u + e];
-        const uint32_t slot = __ldg(d.brick_table + brick);
         const int3 bc = brick_coord_of(d, brick);
+        __syncthreads();  // the previous brick's cells are done with the neighbour slots
+        if (threadIdx.x < 6u) {
+            const int3 nb = add3(bc, nbr_off(int(threadIdx.x)));
+            const bool in = nb.x >= 0 && nb.y >= 0 && nb.z >= 0 && nb.x < d.brick_dim.x && nb.y < d.brick_dim.y && nb.z < d.brick_dim.z;
+            ns[threadIdx.x] = in ? __ldg(d.brick_table + brick_index_of(d, nb)) : 0u;
+        }
+        const uint32_t slot = __ldg(d.brick_table + brick);
+        __syncthreads();
 #pragma unroll
         for (int k = 0; k < 2; ++k) {
             const uint32_t l = threadIdx.x + uint32_t(k) * 256u;
@@ -328,7 +356,7 @@ __global__ void __launch_bounds__(GRID_THREADS) k_viscosity(Dev d, Pass p, const
             for (int n = 0; n < 6; ++n) {
                 float value = center;
                 if (in_grid(d, add3(c, nbr_off(n)))) {
-                    const uint32_t ni = uint32_t(axis) * d.pool_cells + nbr_index(d, index, c, n);
+                    const uint32_t ni = uint32_t(axis) * d.pool_cells + nbr_index_cta(index, c, n);
                     if ((d.face_flags[ni] & FACE_VALID) != 0u) value = src[ni];
                 }
                 sum = sum + value;
@@ -384,7 +412,7 @@ __global__ void __launch_bounds__(GRID_THREADS) k_rbgs(Dev d, float* __restrict_
         for (int n = 0; n < 6; ++n) {
             const int3 nb = add3(c, nbr_off(n));
             if (!in_grid(d, nb)) continue;
-            const uint32_t ni = nbr_index(d, index, c, n);
+            const uint32_t ni = nbr_index_cta(index, c, n);
             if (type_of(d.cell_type[ni]) == CELL_FLUID) sum = sum + pres[ni];
         }
         if (diag > 0.0f) {
@@ -411,10 +439,10 @@ __global__ void __launch_bounds__(GRID_THREADS) k_project(Dev d, Pass p, float* 
                 const int3 ca = add3(c, nbr_off(2 * axis));
                 float pa, pb;
                 if (type_of(a) == CELL_FLUID && type_of(b) == CELL_FLUID) {
-                    pa = d.pressure[nbr_index(d, index, c, 2 * axis)];
+                    pa = d.pressure[nbr_index_cta(index, c, 2 * axis)];
                     pb = d.pressure[index];
                 } else if (type_of(a) == CELL_FLUID) {
-                    pa = d.pressure[nbr_index(d, index, c, 2 * axis)];
+                    pa = d.pressure[nbr_index_cta(index, c, 2 * axis)];
                     pb = pa - pa * air_face_weight(d, p, cell_density(d, p, ca), c);
                 } else {
                     pb = d.pressure[index];
@@ -681,7 +709,7 @@ __global__ void __launch_bounds__(GRID_THREADS) k_density_displacement(Dev d, fl
             if (type_of(a) == CELL_SOLID || type_of(b) == CELL_SOLID) {
                 value = 0.0f;
             } else {
-                const float qa = type_of(a) == CELL_FLUID ? d.density_q[nbr_index(d, index, c, 2 * axis)] : 0.0f;
+                const float qa = type_of(a) == CELL_FLUID ? d.density_q[nbr_index_cta(index, c, 2 * axis)] : 0.0f;
                 const float qb = type_of(b) == CELL_FLUID ? d.density_q[index] : 0.0f;
                 value = -(qb - qa);
             }
@@ -705,13 +733,21 @@ __global__ void __launch_bounds__(GRID_THREADS) k_extrapolate(Dev d, const float
             const uint32_t flags = d.face_flags[f];
             const float center = src[f];
             if ((flags & known) != 0u) { dst[f] = center; continue; }
+            // all six neighbours' flags and values are loaded before any is tested (an out-of-grid
+            // neighbour reads the null slot and is then skipped)
+            uint32_t nf[6];
+            float nv[6];
+#pragma unroll
+            for (int n = 0; n < 6; ++n) {
+                const uint32_t ni = uint32_t(axis) * d.pool_cells + nbr_index_cta(index, c, n);
+                nf[n] = d.face_flags[ni];
+                nv[n] = src[ni];
+            }
             float sum = 0.0f, count = 0.0f;
 #pragma unroll
             for (int n = 0; n < 6; ++n) {
                 if (!in_grid(d, add3(c, nbr_off(n)))) continue;
-                const uint32_t ni = uint32_t(axis) * d.pool_cells + nbr_index(d, index, c, n);
-                const uint32_t nf = d.face_flags[ni];
-                if ((nf & known) != 0u && (nf & FACE_SOLID) == 0u) { sum = sum + src[ni]; count = count + 1.0f; }
+                if ((nf[n] & known) != 0u && (nf[n] & FACE_SOLID) == 0u) { sum = sum + nv[n]; count = count + 1.0f; }
             }
             if (count > 0.0f) {
                 dst[f] = sum / count;
