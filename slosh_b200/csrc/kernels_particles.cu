@@ -153,16 +153,68 @@ __global__ void __launch_bounds__(P2G_THREADS) k_p2g(Dev d, Pass p, const slosh_
     const long long nodes_ll = (long long)ndim.x * ndim.y * ndim.z;
     const long long cells_ll = (long long)cdim.x * cdim.y * cdim.z;
     const bool tiled = nodes_ll <= P2G_TILE_NODES && cells_ll <= P2G_TILE_CELLS;
-    const int nodes = tiled ? int(nodes_ll) : 0;
-    const int ncells = tiled ? int(cells_ll) : 0;
-    if (tiled) {
-        for (int t = threadIdx.x; t < 6 * nodes; t += P2G_THREADS) tile[(t / nodes) * P2G_TILE_NODES + (t % nodes)] = 0;
+    const float inv_h = d.inv_h, h = d.h;
+    const uint32_t tf = d.total_faces;
+    if (!tiled) {  // uniform: the box does not fit, every contribution goes to global memory
+        for (int k = 0; k < P2G_PER_THREAD; ++k) {
+            const uint32_t i = first + uint32_t(k);
+            if (i >= n) break;
+            float4 ra, rb;
+            uint4 rc;
+            load_particle_raw(particles, i, ra, rb, rc);
+            if (is_dead_age(ra.w)) continue;
+            const ParticleF part = unpack_particle(ra, rb, rc);
+            const int3 cell = p2g_cell(d, part.pos);
+#pragma unroll
+            for (int axis = 0; axis < 3; ++axis) {
+                const float3 cp = p.use_apic ? (axis == 0 ? part.cx : (axis == 1 ? part.cy : part.cz)) : make_float3(0.0f, 0.0f, 0.0f);
+                const float up = compf(part.vel, axis);
+                const float ox = axis == 0 ? 0.0f : 0.5f, oy = axis == 1 ? 0.0f : 0.5f, oz = axis == 2 ? 0.0f : 0.5f;
+                const float gx = part.pos.x * inv_h - ox, gy = part.pos.y * inv_h - oy, gz = part.pos.z * inv_h - oz;
+                const int3 base = make_int3(int(floorf(gx)), int(floorf(gy)), int(floorf(gz)));
+                const float fx = gx - float(base.x), fy = gy - float(base.y), fz = gz - float(base.z);
+#pragma unroll
+                for (int o = 0; o < 8; ++o) {
+                    const int oix = o & 1, oiy = (o >> 1) & 1, oiz = (o >> 2) & 1;
+                    const int3 node = make_int3(base.x + oix, base.y + oiy, base.z + oiz);
+                    if (!in_grid(d, node)) continue;
+                    const float w3x = oix ? fx : 1.0f - fx, w3y = oiy ? fy : 1.0f - fy, w3z = oiz ? fz : 1.0f - fz;
+                    const float w = w3x * w3y * w3z;
+                    if (w <= 0.0f) continue;
+                    const float3 xn = make_float3((float(node.x) + ox) * h, (float(node.y) + oy) * h, (float(node.z) + oz) * h);
+                    const int mom = __float2int_rn(w * (up + dot3(cp, sub3(xn, part.pos))) * P2G_FIXED_SCALE);
+                    const int wt = __float2int_rn(w * P2G_FIXED_SCALE);
+                    const uint32_t ci = cell_index(d, node);
+                    if (!is_null_cell(ci)) {
+                        const uint32_t f = uint32_t(axis) * d.pool_cells + ci;
+                        atomicAdd(d.accum + f, mom);
+                        atomicAdd(d.accum + tf + f, wt);
+                    }
+                }
+            }
+            const uint32_t ci = cell_index(d, cell);
+            if (!is_null_cell(ci)) atomicAdd(d.cell_count + ci, 1);
+        }
+        return;
+    }
+    const int nodes = int(nodes_ll);
+    const int ncells = int(cells_ll);
+    {
+        const int n4 = (nodes + 3) >> 2;
+        const int4 z4 = make_int4(0, 0, 0, 0);
+#pragma unroll
+        for (int q = 0; q < 6; ++q)
+            for (int t = threadIdx.x; t < n4; t += P2G_THREADS) reinterpret_cast<int4*>(tile + q * P2G_TILE_NODES)[t] = z4;
         for (int t = threadIdx.x; t < ncells; t += P2G_THREADS) ctile[t] = 0;
     }
     __syncthreads();
 
-    const float inv_h = d.inv_h, h = d.h;
-    const uint32_t tf = d.total_faces;
+    // Per particle and MAC component the 8 stencil nodes share their per-axis factors: the weights
+    // (1 - f, f), the node offsets x_n - x_p and their products with the APIC row, the in-grid tests
+    // and the tile index, so only the products and sums that differ per node are formed per node. The
+    // arithmetic per node is the same sequence of float operations as (w3x * w3y * w3z) and
+    // w * (u_p + dot(c_p, x_n - x_p)) * scale, hence bit-identical contributions.
+    const int sy = ndim.x, sz = ndim.x * ndim.y;
     for (int k = 0; k < P2G_PER_THREAD; ++k) {
         const uint32_t i = first + uint32_t(k);
         if (i >= n) break;
@@ -180,52 +232,58 @@ __global__ void __launch_bounds__(P2G_THREADS) k_p2g(Dev d, Pass p, const slosh_
             const float gx = part.pos.x * inv_h - ox, gy = part.pos.y * inv_h - oy, gz = part.pos.z * inv_h - oz;
             const int3 base = make_int3(int(floorf(gx)), int(floorf(gy)), int(floorf(gz)));
             const float fx = gx - float(base.x), fy = gy - float(base.y), fz = gz - float(base.z);
+            const float wx[2] = {1.0f - fx, fx}, wy[2] = {1.0f - fy, fy}, wz[2] = {1.0f - fz, fz};
+            float px[2], py[2], pz[2];
+            bool inx[2], iny[2], inz[2];
 #pragma unroll
-            for (int o = 0; o < 8; ++o) {
-                const int oix = o & 1, oiy = (o >> 1) & 1, oiz = (o >> 2) & 1;
-                const int3 node = make_int3(base.x + oix, base.y + oiy, base.z + oiz);
-                if (!in_grid(d, node)) continue;
-                const float w3x = oix ? fx : 1.0f - fx, w3y = oiy ? fy : 1.0f - fy, w3z = oiz ? fz : 1.0f - fz;
-                const float w = w3x * w3y * w3z;
-                if (w <= 0.0f) continue;
-                const float3 xn = make_float3((float(node.x) + ox) * h, (float(node.y) + oy) * h, (float(node.z) + oz) * h);
-                const int mom = __float2int_rn(w * (up + dot3(cp, sub3(xn, part.pos))) * P2G_FIXED_SCALE);
-                const int wt = __float2int_rn(w * P2G_FIXED_SCALE);
-                if (tiled) {
-                    const int t = (node.x - origin.x) + ndim.x * ((node.y - origin.y) + ndim.y * (node.z - origin.z));
-                    atomicAdd(tile + (2 * axis) * P2G_TILE_NODES + t, mom);
-                    atomicAdd(tile + (2 * axis + 1) * P2G_TILE_NODES + t, wt);
-                } else {
-                    const uint32_t ci = cell_index(d, node);
-                    if (!is_null_cell(ci)) {
-                        const uint32_t f = uint32_t(axis) * d.pool_cells + ci;
-                        atomicAdd(d.accum + f, mom);
-                        atomicAdd(d.accum + tf + f, wt);
-                    }
+            for (int j = 0; j < 2; ++j) {
+                px[j] = cp.x * ((float(base.x + j) + ox) * h - part.pos.x);
+                py[j] = cp.y * ((float(base.y + j) + oy) * h - part.pos.y);
+                pz[j] = cp.z * ((float(base.z + j) + oz) * h - part.pos.z);
+                inx[j] = unsigned(base.x + j) < unsigned(d.grid.x);
+                iny[j] = unsigned(base.y + j) < unsigned(d.grid.y);
+                inz[j] = unsigned(base.z + j) < unsigned(d.grid.z);
+            }
+            const int tb = (base.x - origin.x) + sy * (base.y - origin.y) + sz * (base.z - origin.z);
+            int* tm = tile + (2 * axis) * P2G_TILE_NODES + tb;
+            int* tw = tile + (2 * axis + 1) * P2G_TILE_NODES + tb;
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                const int oiy = b & 1, oiz = b >> 1;
+                if (!(iny[oiy] && inz[oiz])) continue;
+                const float wyz = wy[oiy];
+                const float pyz = py[oiy];
+                const int to = oiy * sy + oiz * sz;
+#pragma unroll
+                for (int oix = 0; oix < 2; ++oix) {
+                    if (!inx[oix]) continue;
+                    const float w = wx[oix] * wyz * wz[oiz];
+                    if (w <= 0.0f) continue;
+                    const int mom = __float2int_rn(w * (up + (px[oix] + pyz + pz[oiz])) * P2G_FIXED_SCALE);
+                    const int wt = __float2int_rn(w * P2G_FIXED_SCALE);
+                    atomicAdd(tm + to + oix, mom);
+                    atomicAdd(tw + to + oix, wt);
                 }
             }
         }
-        if (tiled) {
-            atomicAdd(ctile + (cell.x - mn.x) + cdim.x * ((cell.y - mn.y) + cdim.y * (cell.z - mn.z)), 1);
-        } else {
-            const uint32_t ci = cell_index(d, cell);
-            if (!is_null_cell(ci)) atomicAdd(d.cell_count + ci, 1);
-        }
+        atomicAdd(ctile + (cell.x - mn.x) + cdim.x * ((cell.y - mn.y) + cdim.y * (cell.z - mn.z)), 1);
     }
-    if (!tiled) return;  // uniform
     __syncthreads();
-    // Flush: one global add per non-zero tile entry.
-    for (int t = threadIdx.x; t < 6 * nodes; t += P2G_THREADS) {
-        const int q = t / nodes, l = t - q * nodes;
-        const int v = tile[q * P2G_TILE_NODES + l];
-        if (v == 0) continue;
-        const int lx = l % ndim.x, ly = (l / ndim.x) % ndim.y, lz = l / (ndim.x * ndim.y);
+    // Flush: per tile node one cell lookup, then one global add per non-zero quantity.
+    for (int l = threadIdx.x; l < nodes; l += P2G_THREADS) {
+        const int lz = l / sz, r = l - lz * sz, ly = r / sy, lx = r - ly * sy;
         const int3 node = make_int3(origin.x + lx, origin.y + ly, origin.z + lz);
         if (!in_grid(d, node)) continue;
+        int v[6];
+        bool any = false;
+#pragma unroll
+        for (int q = 0; q < 6; ++q) { v[q] = tile[q * P2G_TILE_NODES + l]; any |= v[q] != 0; }
+        if (!any) continue;
         const uint32_t ci = cell_index(d, node);
         if (is_null_cell(ci)) continue;
-        const int axis = q >> 1;
-        atomicAdd(d.accum + (q & 1) * d.total_faces + uint32_t(axis) * d.pool_cells + ci, v);
+#pragma unroll
+        for (int q = 0; q < 6; ++q)
+            if (v[q] != 0) atomicAdd(d.accum + (q & 1) * tf + uint32_t(q >> 1) * d.pool_cells + ci, v[q]);
     }
     for (int t = threadIdx.x; t < ncells; t += P2G_THREADS) {
         const int v = ctile[t];
