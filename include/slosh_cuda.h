@@ -403,6 +403,65 @@ SLOSH_API slosh_status slosh_build_surface(void* ctx, const slosh_surface_params
 SLOSH_API slosh_status slosh_surface_device_ptrs(void* ctx, void** field_f16, void** positions, void** normals, void** tangents,
                                                  void** indices);
 
+/* ---- learned warm start (extension; no counterpart in the reference) ----------------------------
+ * A 3-D convolutional U-Net (4 levels, 16/32/64/64 channels, 3x3x3 kernels, BF16 weights and
+ * activations, FP32 accumulation) maps (divergence / scale, fluid mask, solid mask) on the dense grid
+ * to pressure / scale, scale = max |divergence| over the fluid cells. With settings.warm_start =
+ * SLOSH_WARM_START_LEARNED and a network attached, the pressure solve of every substep starts from the
+ * network's guess on the fluid cells (zero elsewhere) and still runs to the same stopping test; without
+ * a network LEARNED starts from zero. Training pairs come from the plain solver (capture after a
+ * substep). Parameters: per convolution W[27][cout][cin] (tap = (dz+1) 9 + (dy+1) 3 + (dx+1)) then
+ * bias[cout], in network order; then the head's 16 weights and its bias. */
+typedef struct slosh_unet_config_t {
+    uint32_t dim[3];      /* grid (x, y, z), each a multiple of 8 and tileable into 128-voxel boxes per level */
+    uint32_t batch;       /* samples per training step (slots) */
+    uint32_t seed;        /* He-normal initialisation */
+    float learning_rate;  /* Adam */
+    float beta1, beta2, eps;
+} slosh_unet_config_t;
+SLOSH_API void slosh_unet_config_default(slosh_unet_config_t* out);
+SLOSH_API slosh_status slosh_unet_create(const slosh_unet_config_t* config, int32_t device, void** out_net);
+SLOSH_API void slosh_unet_destroy(void* net);
+SLOSH_API const char* slosh_unet_last_error(void);
+SLOSH_API uint64_t slosh_unet_num_params(void* net);
+SLOSH_API slosh_status slosh_unet_get_params(void* net, float* host, uint64_t count);
+SLOSH_API slosh_status slosh_unet_set_params(void* net, const float* host, uint64_t count);  /* also resets Adam */
+/* Sample `slot` from host arrays: input [D][H][W][16] BF16 bits (channels as above, 3..15 zero),
+ * target [D][H][W] (pressure / scale, 0 outside the fluid; may be NULL), its fluid voxel count. */
+SLOSH_API slosh_status slosh_unet_set_sample(void* net, uint32_t slot, const uint16_t* input_bf16, const float* target,
+                                             uint32_t fluid_voxels);
+/* Sample `slot` from a simulation context: its divergence, cell types and current pressure (the
+ * solution of the last substep's solve), on the device. */
+SLOSH_API slosh_status slosh_unet_capture_sample(void* net, void* sim_ctx, uint32_t slot);
+/* Forward pass over all slots; host_guess [B][D][H][W] (pressure / scale) may be NULL. */
+SLOSH_API slosh_status slosh_unet_forward(void* net, float* host_guess);
+/* After slosh_unet_forward: loss and parameter gradients (host_grads [num_params] may be NULL). */
+SLOSH_API slosh_status slosh_unet_backward(void* net, float* out_loss, float* host_grads);
+/* Forward, backward and one Adam step. */
+SLOSH_API slosh_status slosh_unet_train_step(void* net, float* out_loss);
+SLOSH_API uint64_t slosh_unet_launch_count(void* net);
+/* Attaches (or with NULL detaches) the network used when warm_start = LEARNED; the network's grid
+ * must equal the context's and its slot 0 is overwritten by each solve. */
+SLOSH_API slosh_status slosh_set_warm_start_network(void* ctx, void* net);
+/* One 3x3x3 convolution through the network's kernels (test entry): y = relu(conv(x) + bias) as BF16,
+ * the data gradient dx (per K-block, BF16) of dz = dy, dW [27][cout][cin] and db (FP32). Arrays are
+ * dense [batch][z][y][x][channels]; block channels and cout are 16, 32 or 64. */
+typedef struct slosh_conv_test_t {
+    uint32_t dim[3], batch;
+    uint32_t nblocks;
+    uint32_t cin[2];
+    uint32_t cout;
+    const uint16_t* x[2];
+    const float* w;
+    const float* bias;
+    const uint16_t* dy;
+    uint16_t* y;
+    uint16_t* dx[2];
+    float* dw;
+    float* db;
+} slosh_conv_test_t;
+SLOSH_API slosh_status slosh_unet_conv_test(const slosh_conv_test_t* t);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

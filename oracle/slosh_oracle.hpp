@@ -2162,7 +2162,9 @@ public:
 
     void substep(int step) {
         const bool last = step == substeps - 1;
-        P.warm_start_scale = prev_dt > 0.0f ? P.dt / prev_dt : 1.0f;
+        // PREVIOUS: MarkCellsCS rescales the last solution by dt / dt_prev; ZERO and LEARNED start
+        // from zero (LEARNED then takes the network's guess).
+        P.warm_start_scale = S.warm_start == uint32_t(SLOSH_WARM_START_PREVIOUS) ? (prev_dt > 0.0f ? P.dt / prev_dt : 1.0f) : 0.0f;
         prev_dt = P.dt;
         P.frame_seed = uint32_t(sim_frame * 16ull + uint64_t(step));
         // Brick pool

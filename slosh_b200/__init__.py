@@ -54,6 +54,21 @@ SIGNATURES = {
     "slosh_surface_params_default": ([C.POINTER(SurfaceParams)], None),
     "slosh_build_surface": ([_VP, C.POINTER(SurfaceParams), C.POINTER(SurfaceInfo)], C.c_int),
     "slosh_surface_device_ptrs": ([_VP, C.POINTER(_VP), C.POINTER(_VP), C.POINTER(_VP), C.POINTER(_VP), C.POINTER(_VP)], C.c_int),
+    "slosh_unet_config_default": ([C.POINTER(_abi.UnetConfig)], None),
+    "slosh_unet_create": ([C.POINTER(_abi.UnetConfig), C.c_int32, C.POINTER(_VP)], C.c_int),
+    "slosh_unet_destroy": ([_VP], None),
+    "slosh_unet_last_error": ([], C.c_char_p),
+    "slosh_unet_num_params": ([_VP], C.c_uint64),
+    "slosh_unet_get_params": ([_VP, C.c_void_p, C.c_uint64], C.c_int),
+    "slosh_unet_set_params": ([_VP, C.c_void_p, C.c_uint64], C.c_int),
+    "slosh_unet_set_sample": ([_VP, C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint32], C.c_int),
+    "slosh_unet_capture_sample": ([_VP, _VP, C.c_uint32], C.c_int),
+    "slosh_unet_forward": ([_VP, C.c_void_p], C.c_int),
+    "slosh_unet_backward": ([_VP, C.POINTER(C.c_float), C.c_void_p], C.c_int),
+    "slosh_unet_train_step": ([_VP, C.POINTER(C.c_float)], C.c_int),
+    "slosh_unet_launch_count": ([_VP], C.c_uint64),
+    "slosh_set_warm_start_network": ([_VP, _VP], C.c_int),
+    "slosh_unet_conv_test": ([C.POINTER(_abi.ConvTest)], C.c_int),
 }
 PHASES = ("sort", "pool", "p2g", "grid", "pressure", "project", "density", "extrapolate", "g2p")
 

@@ -198,3 +198,16 @@ def frame_input(settings, emits=(), colliders=(), manipulators=(), delta_time=1.
     fi.paused = 1 if paused else 0
     fi._keep = (ea, ca, ma)
     return fi
+
+
+class UnetConfig(C.Structure):
+    """slosh_unet_config_t: the learned warm-start network's grid, batch, seed and Adam settings."""
+    _fields_ = [("dim", C.c_uint32 * 3), ("batch", C.c_uint32), ("seed", C.c_uint32), ("learning_rate", C.c_float),
+                ("beta1", C.c_float), ("beta2", C.c_float), ("eps", C.c_float)]
+
+
+class ConvTest(C.Structure):
+    """slosh_conv_test_t: one convolution's host arrays for slosh_unet_conv_test."""
+    _fields_ = [("dim", C.c_uint32 * 3), ("batch", C.c_uint32), ("nblocks", C.c_uint32), ("cin", C.c_uint32 * 2),
+                ("cout", C.c_uint32), ("x", C.c_void_p * 2), ("w", C.c_void_p), ("bias", C.c_void_p), ("dy", C.c_void_p),
+                ("y", C.c_void_p), ("dx", C.c_void_p * 2), ("dw", C.c_void_p), ("db", C.c_void_p)]

@@ -11,8 +11,8 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libslosh_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
-SOURCES = ["driver.cu", "kernels_grid.cu", "kernels_particles.cu", "kernels_mg.cu", "kernels_sort.cu", "sort_static.cu", "kernels_surface.cu"]
-HEADERS = ["common.cuh", "kernels.h"]
+SOURCES = ["driver.cu", "kernels_grid.cu", "kernels_particles.cu", "kernels_mg.cu", "kernels_sort.cu", "sort_static.cu", "kernels_surface.cu", "kernels_unet.cu", "unet.cu"]
+HEADERS = ["common.cuh", "kernels.h", "tc.cuh", "unet.h"]
 FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17", "--fmad=false",
     "-Xcompiler", "-fPIC,-ffp-contract=off,-fvisibility=hidden,-O2", "-Xptxas", "-O3",

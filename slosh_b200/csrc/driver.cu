@@ -23,10 +23,18 @@
 #include <cstdlib>
 #include <cstring>
 #include <new>
+#include <stdexcept>
 #include <string>
 #include <vector>
 
 #include "kernels.h"
+
+namespace slosh {
+namespace unet {
+struct Net;
+int warm_start(Net* net, const Dev& d, const float* divergence, float* pressure, cudaStream_t s);  // unet.cu
+}  // namespace unet
+}  // namespace slosh
 
 namespace slosh {
 namespace {
@@ -111,6 +119,7 @@ bool layout_equals(const slosh_settings_t& a, const slosh_settings_t& b) {
 
 struct Ctx {
     int device = 0;
+    slosh::unet::Net* warm_net = nullptr;  // learned warm start (not owned)
     int num_sms = 148;
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
@@ -721,7 +730,9 @@ struct Ctx {
     // ---- one substep (Step_RenderThread :564-713) ----
     void substep(int step) {
         const bool last = step == substeps - 1;
-        P.warm_start_scale = prev_dt > 0.0f ? P.dt / prev_dt : 1.0f;
+        // Warm start of the pressure solve: the previous solution rescaled by dt / dt_prev
+        // (MarkCellsCS), or a zero initial guess (ZERO, and LEARNED before the network's guess).
+        P.warm_start_scale = S.warm_start == uint32_t(SLOSH_WARM_START_PREVIOUS) ? (prev_dt > 0.0f ? P.dt / prev_dt : 1.0f) : 0.0f;
         prev_dt = P.dt;
         P.frame_seed = uint32_t(sim_frame * 16ull + uint64_t(step));
         const Dev d = dev();
@@ -754,6 +765,8 @@ struct Ctx {
         }
         {
             PhaseScope ps(this, 4);
+            if (S.warm_start == uint32_t(SLOSH_WARM_START_LEARNED) && warm_net)
+                count(slosh::unet::warm_start(warm_net, d, divergence, pressure, stream));
             if (S.pressure_solver == SLOSH_SOLVER_MGPCG) {
                 const int coarse = clampi_h(S.mg_coarse_iterations, 1, 200);
                 if (S.tolerance > 0.0f) mgpcg(pressure, divergence, 0, S.tolerance, S.max_iterations, coarse, 0);
@@ -1031,6 +1044,12 @@ slosh_status guarded(Fn fn) {
     } catch (const std::bad_alloc&) {
         g_error = "host allocation failed";
         return SLOSH_ERR_OUT_OF_MEMORY;
+    } catch (const std::invalid_argument& e) {
+        g_error = e.what();
+        return SLOSH_ERR_INVALID_ARG;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return SLOSH_ERR_CUDA;
     } catch (...) {
         g_error = "unknown error";
         return SLOSH_ERR_CUDA;
@@ -1051,6 +1070,22 @@ void set_last_error(const char* message) { g_error = message ? message : ""; }
 }  // namespace slosh
 
 using namespace slosh;
+
+namespace slosh {
+namespace unet {
+// The simulation state the warm-start network reads and writes (unet.cu).
+void* sim_ctx_dev(void* ctx, Dev* out, float** divergence, float** pressure, cudaStream_t* stream) {
+    if (!ctx) return nullptr;
+    Ctx* c = static_cast<Ctx*>(ctx);
+    if (!c->allocated) return nullptr;
+    *out = c->dev();
+    *divergence = c->divergence;
+    *pressure = c->pressure;
+    *stream = c->stream;
+    return ctx;
+}
+}  // namespace unet
+}  // namespace slosh
 
 extern "C" {
 
@@ -1317,6 +1352,14 @@ SLOSH_API void slosh_surface_params_default(slosh_surface_params_t* out) {
     out->build_mesh = 1u;
     out->max_vertices = 1u << 22;
     out->max_indices = 1u << 24;
+}
+
+SLOSH_API slosh_status slosh_set_warm_start_network(void* ctx, void* net) {
+    return guarded([&]() -> slosh_status {
+        Ctx* c = as_ctx(ctx);
+        c->warm_net = static_cast<slosh::unet::Net*>(net);
+        return SLOSH_OK;
+    });
 }
 
 SLOSH_API slosh_status slosh_build_surface(void* ctx, const slosh_surface_params_t* params, slosh_surface_info_t* out) {

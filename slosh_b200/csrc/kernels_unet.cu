@@ -1,0 +1,680 @@
+// Kernels of the learned warm start (sm_100a): TMA + tcgen05 implicit-GEMM convolution and weight
+// gradient, pooling / upsampling and their gradients, the 1x1 head with the masked MSE loss, Adam,
+// and the dense input / guess exchange with the sparse brick pool. Layouts and forms: unet.h.
+#include "tc.cuh"
+#include "unet.h"
+
+namespace slosh {
+namespace unet {
+namespace {
+
+using namespace tc;
+
+__device__ __forceinline__ float bf(bf16 v) { return __bfloat162float(v); }
+
+// Tile t of the volume: its origin and batch entry.
+struct TileOrigin {
+    int x0, y0, z0, b;
+    uint64_t v0;  // linear voxel of row 0 (rows are consecutive voxels)
+};
+__device__ __forceinline__ TileOrigin tile_origin(const Vol& v, uint32_t t) {
+    const uint32_t tx = v.W / v.bx, ty = v.H / v.by, tz = v.D / v.bz;
+    TileOrigin o;
+    o.x0 = int((t % tx) * v.bx);
+    t /= tx;
+    o.y0 = int((t % ty) * v.by);
+    t /= ty;
+    o.z0 = int((t % tz) * v.bz);
+    o.b = int(t / tz);
+    o.v0 = ((uint64_t(o.b) * v.D + uint64_t(o.z0)) * v.H + uint64_t(o.y0)) * v.W + uint64_t(o.x0);
+    return o;
+}
+__device__ __forceinline__ void tap_offset(uint32_t tap, int& dx, int& dy, int& dz) {
+    dx = int(tap % 3u) - 1;
+    dy = int((tap / 3u) % 3u) - 1;
+    dz = int(tap / 9u) - 1;
+}
+__device__ __forceinline__ uint8_t* align1024(uint8_t* p) { return p + ((1024u - (smem_u32(p) & 1023u)) & 1023u); }
+__device__ __forceinline__ uint32_t tmem_cols(uint32_t n) { return n <= 32u ? 32u : (n <= 64u ? 64u : (n <= 128u ? 128u : 256u)); }
+
+// ---- implicit-GEMM convolution -----------------------------------------------------------------------
+// Warp 0 lane 0 produces (TMA), warp 1 lane 0 issues the MMAs, all four warps run the epilogue: row r
+// of the tile (TMEM lane r) is thread r. Stage s holds A (128 rows x C of one tap and K-block) at
+// stage offset 0 and B (N rows x C) at a_region; each is a K-major operand with the swizzle of its
+// row length (2 C bytes): 8-row groups 16 C bytes apart (SBO), the K = 16 steps 32 bytes apart.
+__global__ void __launch_bounds__(128) k_conv3d(const __grid_constant__ ConvArgs a, uint32_t stage_bytes, uint32_t a_region) {
+    extern __shared__ uint8_t dsm[];
+    __shared__ __align__(8) uint64_t full[CONV_STAGES], empty[CONV_STAGES], done;
+    __shared__ uint32_t tmem_slot;
+    uint8_t* base = align1024(dsm);
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    const TileOrigin o = tile_origin(a.vol, blockIdx.x);
+    const uint32_t ncols = tmem_cols(a.n);
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < CONV_STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(&done, 1);
+        fence_mbar_init();
+        for (uint32_t k = 0; k < a.nblocks; ++k) {
+            prefetch_map(&a.act[k]);
+            prefetch_map(&a.wgt[k]);
+        }
+    }
+    if (warp == 0) tmem_alloc(&tmem_slot, ncols);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_slot;
+    const uint32_t niter = 27u * a.nblocks;
+
+    if (warp == 0 && lane == 0) {
+        for (uint32_t it = 0; it < niter; ++it) {
+            const uint32_t s = it % CONV_STAGES;
+            if (it >= uint32_t(CONV_STAGES) && !mbar_wait(&empty[s], ((it / CONV_STAGES) - 1u) & 1u, a.error, 1u)) break;
+            const uint32_t tap = it / a.nblocks, blk = it % a.nblocks, cb = a.cb[blk];
+            int dx, dy, dz;
+            tap_offset(tap, dx, dy, dz);
+            uint8_t* sa = base + s * stage_bytes;
+            mbar_arrive_expect_tx(&full[s], cb * 256u + cb * a.n * 2u);
+            tma_load_5d(sa, &a.act[blk], 0, o.x0 + dx, o.y0 + dy, o.z0 + dz, o.b, &full[s]);
+            tma_load_2d(sa + a_region, &a.wgt[blk], 0, int(tap * a.n), &full[s]);
+        }
+    } else if (warp == 1 && lane == 0) {
+        const uint32_t idesc = idesc_bf16_f32(128u, a.n, 0u, 0u);
+        for (uint32_t it = 0; it < niter; ++it) {
+            const uint32_t s = it % CONV_STAGES;
+            if (!mbar_wait(&full[s], (it / CONV_STAGES) & 1u, a.error, 2u)) break;
+            tc_fence_after();
+            const uint32_t cb = a.cb[it % a.nblocks];
+            const uint32_t row = cb * 2u, layout = swizzle_of_row_bytes(row);
+            const uint32_t sa = smem_u32(base + s * stage_bytes), sb = sa + a_region;
+            for (uint32_t k = 0; k < cb / 16u; ++k)
+                mma_bf16(tmem, smem_desc(sa + 32u * k, 16u, 8u * row, layout), smem_desc(sb + 32u * k, 16u, 8u * row, layout), idesc,
+                         (it | k) != 0u ? 1u : 0u);
+            mma_commit(&empty[s]);
+        }
+        mma_commit(&done);
+    }
+    const bool ok = mbar_wait(&done, 0u, a.error, 4u);
+    __syncwarp();
+    tc_fence_after();
+    if (ok) {
+        const uint32_t r = warp * 32u + lane;
+        const uint64_t v = o.v0 + r;
+        for (uint32_t c0 = 0; c0 < a.n; c0 += 16u) {
+            float acc[16];
+            tmem_ld16(tmem + ((warp * 32u) << 16) + c0, acc);
+            if (a.bias)
+#pragma unroll
+                for (int j = 0; j < 16; ++j) acc[j] = acc[j] + a.bias[c0 + uint32_t(j)];
+            if (a.relu)
+#pragma unroll
+                for (int j = 0; j < 16; ++j) acc[j] = fmaxf(acc[j], 0.0f);
+            const uint32_t oi = c0 < a.oc[0] ? 0u : 1u;
+            const uint32_t cc = oi == 0u ? c0 : c0 - a.oc[0];
+            const uint64_t e = v * a.oc[oi] + cc;
+            uint4* dst = reinterpret_cast<uint4*>(a.out[oi] + e);
+            if (a.accumulate) {
+                const uint4 w0 = dst[0], w1 = dst[1];
+                const bf16* old0 = reinterpret_cast<const bf16*>(&w0);
+                const bf16* old1 = reinterpret_cast<const bf16*>(&w1);
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    acc[j] = acc[j] + bf(old0[j]);
+                    acc[8 + j] = acc[8 + j] + bf(old1[j]);
+                }
+            }
+            if (a.mask[oi]) {
+                const uint4* mp = reinterpret_cast<const uint4*>(a.mask[oi] + e);
+                const uint4 m0 = mp[0], m1 = mp[1];
+                const bf16* mk0 = reinterpret_cast<const bf16*>(&m0);
+                const bf16* mk1 = reinterpret_cast<const bf16*>(&m1);
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    if (!(bf(mk0[j]) > 0.0f)) acc[j] = 0.0f;
+                    if (!(bf(mk1[j]) > 0.0f)) acc[8 + j] = 0.0f;
+                }
+            }
+            uint4 w[2];
+            bf16* wb = reinterpret_cast<bf16*>(w);
+#pragma unroll
+            for (int j = 0; j < 16; ++j) wb[j] = __float2bfloat16_rn(acc[j]);
+            dst[0] = w[0];
+            dst[1] = w[1];
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        tmem_dealloc(tmem, ncols);
+    }
+}
+
+// ---- weight gradient ------------------------------------------------------------------------------------
+// CTA (chunk, group): taps g*T .. g*T+T-1 (T = 128 / c) over the chunk's voxel tiles. Stage s: A =
+// T regions of 128 voxel rows x c (tap t's shifted input), B = 128 voxel rows x n (dZ). Both are
+// MN-major: A's MN atoms (c channels, one per tap) are 256 c bytes apart (LBO), 8-voxel groups 16 c
+// bytes apart (SBO); B has one atom, 8-voxel groups 16 n bytes apart. K = 16 voxels per MMA.
+__global__ void __launch_bounds__(128) k_wgrad(const __grid_constant__ WgradArgs a, uint32_t stage_bytes, uint32_t a_region) {
+    extern __shared__ uint8_t dsm[];
+    __shared__ __align__(8) uint64_t full[WGRAD_STAGES], empty[WGRAD_STAGES], done;
+    __shared__ uint32_t tmem_slot;
+    uint8_t* base = align1024(dsm);
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    const uint32_t T = 128u / a.c, g = blockIdx.y, chunk = blockIdx.x;
+    const uint32_t tiles = a.vol.tiles();
+    const uint32_t t_begin = chunk * a.tiles_per_chunk;
+    const uint32_t t_end = min(tiles, t_begin + a.tiles_per_chunk);
+    const uint32_t ncols = tmem_cols(a.n);
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < WGRAD_STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(&done, 1);
+        fence_mbar_init();
+        prefetch_map(&a.act);
+        prefetch_map(&a.grad);
+    }
+    if (warp == 0) tmem_alloc(&tmem_slot, ncols);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_slot;
+    const uint32_t niter = t_end > t_begin ? t_end - t_begin : 0u;
+    const uint32_t region = 256u * a.c;  // one tap's 128 rows x c channels
+
+    if (warp == 0 && lane == 0) {
+        for (uint32_t it = 0; it < niter; ++it) {
+            const uint32_t s = it % WGRAD_STAGES;
+            if (it >= uint32_t(WGRAD_STAGES) && !mbar_wait(&empty[s], ((it / WGRAD_STAGES) - 1u) & 1u, a.error, 8u)) break;
+            const TileOrigin o = tile_origin(a.vol, t_begin + it);
+            uint8_t* sa = base + s * stage_bytes;
+            uint32_t taps = 0;
+            for (uint32_t t = 0; t < T; ++t)
+                if (g * T + t < 27u) ++taps;
+            mbar_arrive_expect_tx(&full[s], taps * region + 256u * a.n);
+            for (uint32_t t = 0; t < T; ++t) {
+                const uint32_t tap = g * T + t;
+                if (tap >= 27u) break;
+                int dx, dy, dz;
+                tap_offset(tap, dx, dy, dz);
+                tma_load_5d(sa + t * region, &a.act, 0, o.x0 + dx, o.y0 + dy, o.z0 + dz, o.b, &full[s]);
+            }
+            tma_load_5d(sa + a_region, &a.grad, 0, o.x0, o.y0, o.z0, o.b, &full[s]);
+        }
+    } else if (warp == 1 && lane == 0) {
+        const uint32_t idesc = idesc_bf16_f32(128u, a.n, 1u, 1u);
+        const uint32_t la = swizzle_of_row_bytes(2u * a.c), lb = swizzle_of_row_bytes(2u * a.n);
+        for (uint32_t it = 0; it < niter; ++it) {
+            const uint32_t s = it % WGRAD_STAGES;
+            if (!mbar_wait(&full[s], (it / WGRAD_STAGES) & 1u, a.error, 16u)) break;
+            tc_fence_after();
+            const uint32_t sa = smem_u32(base + s * stage_bytes), sb = sa + a_region;
+#pragma unroll
+            for (uint32_t k = 0; k < 8u; ++k)
+                mma_bf16(tmem, smem_desc(sa + k * 32u * a.c, region, 16u * a.c, la), smem_desc(sb + k * 32u * a.n, 256u * a.n, 16u * a.n, lb),
+                         idesc, (it | k) != 0u ? 1u : 0u);
+            mma_commit(&empty[s]);
+        }
+        mma_commit(&done);
+    }
+    const bool ok = mbar_wait(&done, 0u, a.error, 32u);
+    __syncwarp();
+    tc_fence_after();
+    if (ok) {
+        const uint32_t m = warp * 32u + lane;
+        const uint32_t tap = g * T + m / a.c, ci = m % a.c;
+        for (uint32_t c0 = 0; c0 < a.n; c0 += 16u) {
+            float acc[16];
+            tmem_ld16(tmem + ((warp * 32u) << 16) + c0, acc);
+            if (tap < 27u) {
+                float* dst = a.partial + ((uint64_t(chunk) * 27u + tap) * a.n + c0) * a.c + ci;
+#pragma unroll
+                for (int j = 0; j < 16; ++j) dst[uint64_t(j) * a.c] = niter ? acc[j] : 0.0f;
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        tmem_dealloc(tmem, ncols);
+    }
+}
+
+// out[i] = sum over chunks of partial[chunk][i], in chunk order.
+__global__ void k_reduce_chunks(const float* __restrict__ partial, float* __restrict__ out, uint32_t chunks, uint32_t count) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    float s = 0.0f;
+    for (uint32_t c = 0; c < chunks; ++c) s = s + partial[uint64_t(c) * count + i];
+    out[i] = s;
+}
+
+// Weight gradient of one K-block: out[(tap n + co) cin + off + cl] = sum over chunks of
+// partial[chunk][tap][co][cl], in chunk order.
+__global__ void k_reduce_wgrad(const float* __restrict__ partial, float* __restrict__ out, uint32_t chunks, uint32_t n, uint32_t cb,
+                               uint32_t cin, uint32_t off) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t count = 27u * n * cb;
+    if (i >= count) return;
+    float s = 0.0f;
+    for (uint32_t c = 0; c < chunks; ++c) s = s + partial[uint64_t(c) * count + i];
+    const uint32_t cl = i % cb, row = i / cb;
+    out[row * cin + off + cl] = s;
+}
+
+// Bias gradient partials: chunk c sums channel j over its voxel range (thread j + n * q takes voxels
+// q, q + 256 / n, ...; the per-thread sums are added in thread order).
+__global__ void k_bias_partial(const bf16* __restrict__ g, uint32_t n, uint64_t voxels, uint64_t per_chunk, float* __restrict__ partial) {
+    __shared__ float s_sum[256];
+    const uint32_t q = threadIdx.x / n, j = threadIdx.x % n, lanes = 256u / n;
+    const uint64_t v0 = uint64_t(blockIdx.x) * per_chunk;
+    const uint64_t v1 = min(voxels, v0 + per_chunk);
+    float s = 0.0f;
+    if (q < lanes)
+        for (uint64_t v = v0 + q; v < v1; v += lanes) s = s + bf(g[v * n + j]);
+    s_sum[threadIdx.x] = s;
+    __syncthreads();
+    if (threadIdx.x < n) {
+        float t = 0.0f;
+        for (uint32_t k = 0; k < lanes; ++k) t = t + s_sum[k * n + threadIdx.x];
+        partial[uint64_t(blockIdx.x) * n + threadIdx.x] = t;
+    }
+}
+
+// ---- pooling and upsampling (8 channels per thread) ----------------------------------------------------
+struct V8 {
+    float f[8];
+};
+__device__ __forceinline__ V8 ld8(const bf16* p) {
+    const uint4 w = *reinterpret_cast<const uint4*>(p);
+    const bf16* b = reinterpret_cast<const bf16*>(&w);
+    V8 v;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) v.f[j] = bf(b[j]);
+    return v;
+}
+__device__ __forceinline__ void st8(bf16* p, const V8& v) {
+    uint4 w;
+    bf16* b = reinterpret_cast<bf16*>(&w);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) b[j] = __float2bfloat16_rn(v.f[j]);
+    *reinterpret_cast<uint4*>(p) = w;
+}
+__device__ __forceinline__ void mask8(V8& v, const bf16* m) {
+    const V8 mv = ld8(m);
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+        if (!(mv.f[j] > 0.0f)) v.f[j] = 0.0f;
+}
+// Linear voxel of the fine child o (x fastest) of coarse voxel (b, z, y, x).
+__device__ __forceinline__ uint64_t child_of(const Vol& f, uint32_t b, uint32_t z, uint32_t y, uint32_t x, int o) {
+    return ((uint64_t(b) * f.D + 2u * z + uint32_t((o >> 2) & 1)) * f.H + 2u * y + uint32_t((o >> 1) & 1)) * f.W + 2u * x + uint32_t(o & 1);
+}
+__device__ __forceinline__ bool coarse_coord(const Vol& f, uint64_t i, uint32_t& b, uint32_t& z, uint32_t& y, uint32_t& x) {
+    const uint32_t W = f.W / 2u, H = f.H / 2u, D = f.D / 2u;
+    x = uint32_t(i % W);
+    i /= W;
+    y = uint32_t(i % H);
+    i /= H;
+    z = uint32_t(i % D);
+    b = uint32_t(i / D);
+    return b < f.B;
+}
+__global__ void k_pool(const bf16* __restrict__ in, bf16* __restrict__ out, Vol f, uint32_t c) {
+    const uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const uint32_t g8 = c / 8u;
+    uint32_t b, z, y, x;
+    if (!coarse_coord(f, t / g8, b, z, y, x)) return;
+    const uint32_t cg = uint32_t(t % g8) * 8u;
+    V8 s;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) s.f[j] = 0.0f;
+#pragma unroll
+    for (int o = 0; o < 8; ++o) {
+        const V8 v = ld8(in + child_of(f, b, z, y, x, o) * c + cg);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) s.f[j] = s.f[j] + v.f[j];
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j) s.f[j] = s.f[j] * 0.125f;
+    st8(out + (t / g8) * c + cg, s);
+}
+__global__ void k_pool_bwd(const bf16* __restrict__ gout, bf16* __restrict__ gin, Vol f, uint32_t c, uint32_t accumulate,
+                           const bf16* __restrict__ mask) {
+    const uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const uint32_t g8 = c / 8u;
+    uint32_t b, z, y, x;
+    if (!coarse_coord(f, t / g8, b, z, y, x)) return;
+    const uint32_t cg = uint32_t(t % g8) * 8u;
+    const V8 gv = ld8(gout + (t / g8) * c + cg);
+#pragma unroll
+    for (int o = 0; o < 8; ++o) {
+        const uint64_t e = child_of(f, b, z, y, x, o) * c + cg;
+        V8 v;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) v.f[j] = gv.f[j] * 0.125f;
+        if (accumulate) {
+            const V8 old = ld8(gin + e);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) v.f[j] = old.f[j] + v.f[j];
+        }
+        if (mask) mask8(v, mask + e);
+        st8(gin + e, v);
+    }
+}
+__global__ void k_upsample(const bf16* __restrict__ in, bf16* __restrict__ out, Vol f, uint32_t c) {
+    const uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const uint32_t g8 = c / 8u;
+    uint32_t b, z, y, x;
+    if (!coarse_coord(f, t / g8, b, z, y, x)) return;
+    const uint32_t cg = uint32_t(t % g8) * 8u;
+    const uint4 w = *reinterpret_cast<const uint4*>(in + (t / g8) * c + cg);
+#pragma unroll
+    for (int o = 0; o < 8; ++o) *reinterpret_cast<uint4*>(out + child_of(f, b, z, y, x, o) * c + cg) = w;
+}
+__global__ void k_upsample_bwd(const bf16* __restrict__ gout, bf16* __restrict__ gin, Vol f, uint32_t c, const bf16* __restrict__ mask) {
+    const uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const uint32_t g8 = c / 8u;
+    uint32_t b, z, y, x;
+    if (!coarse_coord(f, t / g8, b, z, y, x)) return;
+    const uint32_t cg = uint32_t(t % g8) * 8u;
+    V8 s;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) s.f[j] = 0.0f;
+#pragma unroll
+    for (int o = 0; o < 8; ++o) {
+        const V8 v = ld8(gout + child_of(f, b, z, y, x, o) * c + cg);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) s.f[j] = s.f[j] + v.f[j];
+    }
+    const uint64_t e = (t / g8) * c + cg;
+    if (mask) mask8(s, mask + e);
+    st8(gin + e, s);
+}
+
+// ---- head (16 -> 1), loss and its gradients ------------------------------------------------------------
+// head_w = [w0..w15, bias]. Chunk partials per CTA: [17 head gradients, loss]; the CTA's 256 threads
+// take voxels v0 + t, v0 + t + 256, ... and their sums are folded in thread order.
+constexpr uint32_t HEAD_THREADS = 256;
+__global__ void __launch_bounds__(HEAD_THREADS) k_head(const bf16* __restrict__ d0, const bf16* __restrict__ input,
+                                                       const float* __restrict__ hw, float* __restrict__ out, const float* __restrict__ target,
+                                                       const uint32_t* __restrict__ nfluid, bf16* __restrict__ g_d0, float* __restrict__ partial,
+                                                       uint64_t voxels, uint64_t per_chunk) {
+    __shared__ float s_part[HEAD_THREADS][18];
+    float w[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) w[j] = hw[j];
+    const float bias = hw[16];
+    const float inv_n = target ? 1.0f / float(max(nfluid[0], 1u)) : 0.0f;
+    float acc[18];
+#pragma unroll
+    for (int j = 0; j < 18; ++j) acc[j] = 0.0f;
+    const uint64_t v0 = uint64_t(blockIdx.x) * per_chunk;
+    const uint64_t v1 = min(voxels, v0 + per_chunk);
+    for (uint64_t v = v0 + threadIdx.x; v < v1; v += HEAD_THREADS) {
+        const V8 a = ld8(d0 + v * 16u), b = ld8(d0 + v * 16u + 8u);
+        float h[16];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            h[j] = a.f[j];
+            h[8 + j] = b.f[j];
+        }
+        float y = 0.0f;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) y = y + w[j] * h[j];
+        y = y + bias;
+        if (out) out[v] = y;
+        if (!target) continue;
+        const bool fluid = bf(input[v * IN_CHANNELS + 1u]) > 0.5f;
+        const float diff = fluid ? y - target[v] : 0.0f;
+        const float dy = 2.0f * diff * inv_n;
+        V8 ga, gb;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            ga.f[j] = h[j] > 0.0f ? dy * w[j] : 0.0f;
+            gb.f[j] = h[8 + j] > 0.0f ? dy * w[8 + j] : 0.0f;
+        }
+        st8(g_d0 + v * 16u, ga);
+        st8(g_d0 + v * 16u + 8u, gb);
+#pragma unroll
+        for (int j = 0; j < 16; ++j) acc[j] = acc[j] + dy * h[j];
+        acc[16] = acc[16] + dy;
+        acc[17] = acc[17] + diff * diff * inv_n;
+    }
+    if (!target) return;
+#pragma unroll
+    for (int j = 0; j < 18; ++j) s_part[threadIdx.x][j] = acc[j];
+    __syncthreads();
+    if (threadIdx.x < 18) {
+        float s = 0.0f;
+        for (uint32_t t = 0; t < HEAD_THREADS; ++t) s = s + s_part[t][threadIdx.x];
+        partial[uint64_t(blockIdx.x) * 18u + threadIdx.x] = s;
+    }
+}
+
+// ---- Adam ----------------------------------------------------------------------------------------------
+__global__ void k_adam(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m, float* __restrict__ v, uint64_t count,
+                       float lr, float b1, float b2, float eps, float c1, float c2) {
+    const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.0f - b1) * gi;
+    const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    p[i] = p[i] - lr * (mi * c1) / (sqrtf(vi * c2) + eps);
+}
+
+// ---- BF16 weight copies ----------------------------------------------------------------------------------
+struct ConvWeightArgs {
+    const float* w;
+    uint32_t n, cin, nblocks;
+    uint32_t cb[2];
+    bf16* fwd[2];
+    bf16* dgrad;
+};
+__global__ void k_conv_weights(ConvWeightArgs a) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t total = 27u * a.n * a.cin;
+    if (i >= total) return;
+    const uint32_t ci = i % a.cin, co = (i / a.cin) % a.n, tap = i / (a.cin * a.n);
+    const bf16 v = __float2bfloat16_rn(a.w[i]);
+    const uint32_t blk = (a.nblocks > 1u && ci >= a.cb[0]) ? 1u : 0u;
+    const uint32_t cl = blk ? ci - a.cb[0] : ci;
+    a.fwd[blk][(tap * a.n + co) * a.cb[blk] + cl] = v;
+    a.dgrad[((26u - tap) * a.cin + ci) * a.n + co] = v;
+}
+
+// ---- exchange with the simulation's brick pool -------------------------------------------------------
+__device__ __forceinline__ uint32_t float_order_key(float f) { return __float_as_uint(fabsf(f)); }
+// Pass 1: max |divergence| over fluid cells and the fluid count of the dense grid.
+__global__ void k_pack_scan(Dev d, const float* __restrict__ div, uint32_t* __restrict__ meta, uint32_t slot) {
+    const uint32_t W = uint32_t(d.grid.x), H = uint32_t(d.grid.y), D = uint32_t(d.grid.z);
+    const uint64_t n = uint64_t(W) * H * D;
+    uint32_t kmax = 0u, cnt = 0u;
+    for (uint64_t v = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; v < n; v += uint64_t(gridDim.x) * blockDim.x) {
+        const int3 c = make_int3(int(v % W), int((v / W) % H), int(v / (uint64_t(W) * H)));
+        const uint32_t ci = cell_index(d, c);
+        if (is_null_cell(ci) || type_of(d.cell_type[ci]) != CELL_FLUID) continue;
+        kmax = max(kmax, float_order_key(div[ci]));
+        ++cnt;
+    }
+    kmax = __reduce_max_sync(0xFFFFFFFFu, kmax);
+    cnt = __reduce_add_sync(0xFFFFFFFFu, cnt);
+    if ((threadIdx.x & 31u) == 0u) {
+        if (kmax) atomicMax(meta + 2u * slot, kmax);
+        if (cnt) atomicAdd(meta + 2u * slot + 1u, cnt);
+    }
+}
+__device__ __forceinline__ float slot_scale(const uint32_t* meta, uint32_t slot) {
+    const float s = __uint_as_float(meta[2u * slot]);
+    return s > 0.0f ? s : 1.0f;
+}
+// Pass 2: the dense input (and target) of the slot.
+__global__ void k_pack(Dev d, const float* __restrict__ div, const float* __restrict__ pressure, bf16* __restrict__ input,
+                       float* __restrict__ target, const uint32_t* __restrict__ meta, uint32_t slot) {
+    const uint32_t W = uint32_t(d.grid.x), H = uint32_t(d.grid.y), D = uint32_t(d.grid.z);
+    const uint64_t n = uint64_t(W) * H * D;
+    const uint64_t v = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    const float scale = slot_scale(meta, slot);
+    const int3 c = make_int3(int(v % W), int((v / W) % H), int(v / (uint64_t(W) * H)));
+    const uint32_t ci = cell_index(d, c);
+    const bool border = c.x == 0 || c.y == 0 || c.z == 0 || c.x == d.grid.x - 1 || c.y == d.grid.y - 1 || c.z == d.grid.z - 1;
+    uint32_t type = border ? CELL_SOLID : CELL_AIR;
+    float dv = 0.0f, pv = 0.0f;
+    if (!is_null_cell(ci)) {
+        type = type_of(d.cell_type[ci]);
+        if (type == CELL_FLUID) {
+            dv = div[ci] / scale;
+            if (pressure) pv = pressure[ci] / scale;
+        }
+    }
+    uint4 w[2] = {make_uint4(0u, 0u, 0u, 0u), make_uint4(0u, 0u, 0u, 0u)};
+    bf16* wb = reinterpret_cast<bf16*>(w);
+    wb[0] = __float2bfloat16_rn(dv);
+    wb[1] = __float2bfloat16_rn(type == CELL_FLUID ? 1.0f : 0.0f);
+    wb[2] = __float2bfloat16_rn(type == CELL_SOLID ? 1.0f : 0.0f);
+    uint4* dst = reinterpret_cast<uint4*>(input + (uint64_t(slot) * n + v) * IN_CHANNELS);
+    dst[0] = w[0];
+    dst[1] = w[1];
+    if (target) target[uint64_t(slot) * n + v] = pv;
+}
+__global__ void k_scatter_guess(Dev d, const float* __restrict__ guess, const uint32_t* __restrict__ meta, float* __restrict__ pressure) {
+    const uint32_t W = uint32_t(d.grid.x), H = uint32_t(d.grid.y), D = uint32_t(d.grid.z);
+    const uint64_t n = uint64_t(W) * H * D;
+    const uint64_t v = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    const int3 c = make_int3(int(v % W), int((v / W) % H), int(v / (uint64_t(W) * H)));
+    const uint32_t ci = cell_index(d, c);
+    if (is_null_cell(ci) || type_of(d.cell_type[ci]) != CELL_FLUID) return;
+    pressure[ci] = guess[v] * slot_scale(meta, 0u);
+}
+
+uint32_t blocks_for(uint64_t n, uint32_t threads) { return uint32_t((n + threads - 1u) / threads); }
+
+}  // namespace
+
+size_t conv_smem_bytes(uint32_t cb_max, uint32_t n) {
+    const size_t a_region = 256u * cb_max;
+    const size_t b_region = (size_t(n) * cb_max * 2u + 1023u) / 1024u * 1024u;
+    return CONV_STAGES * (a_region + b_region) + 1024u;
+}
+size_t wgrad_smem_bytes(uint32_t c, uint32_t n) {
+    (void)c;
+    const size_t a_region = 128u * 128u * 2u;  // T taps x 128 rows x c channels, T c = 128
+    const size_t b_region = (256u * size_t(n) + 1023u) / 1024u * 1024u;
+    return WGRAD_STAGES * (a_region + b_region) + 1024u;
+}
+
+int launch_conv(const ConvArgs& a, cudaStream_t s) {
+    uint32_t cbmax = a.cb[0];
+    if (a.nblocks > 1u) cbmax = a.cb[0] > a.cb[1] ? a.cb[0] : a.cb[1];
+    const uint32_t a_region = 256u * cbmax;
+    const uint32_t b_region = (a.n * cbmax * 2u + 1023u) / 1024u * 1024u;
+    const size_t smem = conv_smem_bytes(cbmax, a.n);
+    static bool configured = false;
+    if (!configured) {
+        cudaFuncSetAttribute(k_conv3d, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        configured = true;
+    }
+    k_conv3d<<<a.vol.tiles(), 128, smem, s>>>(a, a_region + b_region, a_region);
+    return 1;
+}
+int launch_wgrad(const WgradArgs& a, uint32_t chunks, cudaStream_t s) {
+    const uint32_t a_region = 128u * 128u * 2u;
+    const uint32_t b_region = (256u * a.n + 1023u) / 1024u * 1024u;
+    const size_t smem = wgrad_smem_bytes(a.c, a.n);
+    static bool configured = false;
+    if (!configured) {
+        cudaFuncSetAttribute(k_wgrad, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+        configured = true;
+    }
+    const uint32_t T = 128u / a.c;
+    k_wgrad<<<dim3(chunks, (27u + T - 1u) / T), 128, smem, s>>>(a, a_region + b_region, a_region);
+    return 1;
+}
+int launch_reduce_chunks(const float* partial, float* out, uint32_t chunks, uint32_t count, cudaStream_t s) {
+    k_reduce_chunks<<<blocks_for(count, 256), 256, 0, s>>>(partial, out, chunks, count);
+    return 1;
+}
+int launch_reduce_wgrad(const float* partial, float* out, uint32_t chunks, uint32_t n, uint32_t cb, uint32_t cin, uint32_t off,
+                        cudaStream_t s) {
+    k_reduce_wgrad<<<blocks_for(27ull * n * cb, 256), 256, 0, s>>>(partial, out, chunks, n, cb, cin, off);
+    return 1;
+}
+int launch_bias_grad(const bf16* g, uint32_t n, uint64_t voxels, float* partial, uint32_t chunks, float* out, cudaStream_t s) {
+    const uint64_t per = (voxels + chunks - 1u) / chunks;
+    k_bias_partial<<<chunks, 256, 0, s>>>(g, n, voxels, per, partial);
+    k_reduce_chunks<<<1, 256, 0, s>>>(partial, out, chunks, n);
+    return 2;
+}
+int launch_pool(const bf16* in, bf16* out, Vol f, uint32_t c, cudaStream_t s) {
+    const uint64_t n = f.voxels() / 8u * (c / 8u);
+    k_pool<<<blocks_for(n, 256), 256, 0, s>>>(in, out, f, c);
+    return 1;
+}
+int launch_pool_bwd(const bf16* gout, bf16* gin, Vol f, uint32_t c, uint32_t accumulate, const bf16* mask, cudaStream_t s) {
+    const uint64_t n = f.voxels() / 8u * (c / 8u);
+    k_pool_bwd<<<blocks_for(n, 256), 256, 0, s>>>(gout, gin, f, c, accumulate, mask);
+    return 1;
+}
+int launch_upsample(const bf16* in, bf16* out, Vol f, uint32_t c, cudaStream_t s) {
+    const uint64_t n = f.voxels() / 8u * (c / 8u);
+    k_upsample<<<blocks_for(n, 256), 256, 0, s>>>(in, out, f, c);
+    return 1;
+}
+int launch_upsample_bwd(const bf16* gout, bf16* gin, Vol f, uint32_t c, const bf16* mask, cudaStream_t s) {
+    const uint64_t n = f.voxels() / 8u * (c / 8u);
+    k_upsample_bwd<<<blocks_for(n, 256), 256, 0, s>>>(gout, gin, f, c, mask);
+    return 1;
+}
+int launch_head(const bf16* d0, const bf16* input, const float* head_w, float* out, const float* target, const uint32_t* nfluid,
+                bf16* g_d0, float* partial, uint32_t chunks, float* head_grad, float* loss, uint64_t voxels, cudaStream_t s) {
+    const uint64_t per = (voxels + chunks - 1u) / chunks;
+    k_head<<<chunks, HEAD_THREADS, 0, s>>>(d0, input, head_w, out, target, nfluid, g_d0, partial, voxels, per);
+    if (!target) return 1;
+    k_reduce_chunks<<<1, 32, 0, s>>>(partial, head_grad, chunks, 18u);  // head_grad[0..16] gradients, [17] the loss
+    return 2;
+}
+int launch_adam(float* p, const float* g, float* m, float* v, uint64_t count, float lr, float b1, float b2, float eps, float c1,
+                float c2, cudaStream_t s) {
+    k_adam<<<blocks_for(count, 256), 256, 0, s>>>(p, g, m, v, count, lr, b1, b2, eps, c1, c2);
+    return 1;
+}
+int launch_conv_weights(const float* w, uint32_t n, uint32_t cin, const uint32_t* cb, uint32_t nblocks, bf16* const* fwd, bf16* dgrad,
+                        cudaStream_t s) {
+    ConvWeightArgs a;
+    a.w = w;
+    a.n = n;
+    a.cin = cin;
+    a.nblocks = nblocks;
+    a.cb[0] = cb[0];
+    a.cb[1] = nblocks > 1u ? cb[1] : 0u;
+    a.fwd[0] = fwd[0];
+    a.fwd[1] = nblocks > 1u ? fwd[1] : nullptr;
+    a.dgrad = dgrad;
+    k_conv_weights<<<blocks_for(27ull * n * cin, 256), 256, 0, s>>>(a);
+    return 1;
+}
+int launch_pack_input(const Dev& d, const float* divergence, const float* pressure, bf16* input, float* target, uint32_t* meta,
+                      uint32_t slot, cudaStream_t s) {
+    const uint64_t n = uint64_t(d.grid.x) * d.grid.y * d.grid.z;
+    k_pack_scan<<<592, 256, 0, s>>>(d, divergence, meta, slot);
+    k_pack<<<blocks_for(n, 256), 256, 0, s>>>(d, divergence, pressure, input, target, meta, slot);
+    return 2;
+}
+int launch_scatter_guess(const Dev& d, const float* guess, const uint32_t* meta, float* pressure, cudaStream_t s) {
+    const uint64_t n = uint64_t(d.grid.x) * d.grid.y * d.grid.z;
+    k_scatter_guess<<<blocks_for(n, 256), 256, 0, s>>>(d, guess, meta, pressure);
+    return 1;
+}
+
+}  // namespace unet
+}  // namespace slosh

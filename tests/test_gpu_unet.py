@@ -1,0 +1,113 @@
+"""GPU parity of the learned warm start's kernels and network against the numpy oracle
+(oracle/unet_oracle.py): single convolutions (forward, data and weight gradients, bias gradient) for
+every channel configuration the network uses, the whole network's output, loss and parameter
+gradients, and the warm start inside a simulation.
+
+Tolerances: the GPU accumulates in FP32 on the tensor cores in its own order, the oracle in FP64; both
+round activations and activation gradients to BF16 at the same points. A convolution output may
+therefore differ by one BF16 rounding step (2^-8 relative); weight gradients (FP32 sums of BF16
+products) agree to 1e-3 of their scale; through the 14 layers of the network, rounding flips
+compound, so the network is compared by relative L2 error and direction."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+from oracle import unet_oracle as U  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ws():
+    from slosh_b200 import warmstart
+    return warmstart
+
+
+def _bits(x):
+    return U.bf16_bits(np.asarray(x, np.float32))
+
+
+CONFIGS = [
+    ([16], 16), ([16], 32), ([32], 32), ([32], 64), ([64], 64),
+    ([64, 64], 64), ([64, 32], 32), ([32, 16], 16),
+]
+VOLUMES = [((16, 8, 8), 1), ((8, 8, 8), 2), ((128, 2, 2), 1)]
+
+
+@pytest.mark.parametrize("cins,cout", CONFIGS)
+@pytest.mark.parametrize("dim,batch", VOLUMES)
+def test_conv_kernels_match_oracle(ws, cins, cout, dim, batch):
+    rng = np.random.default_rng(sum(cins) * 7 + cout + dim[0] + batch)
+    W, H, D = dim
+    xs = [U.bf16(rng.standard_normal((batch, D, H, W, c)).astype(np.float32)) for c in cins]
+    cin = sum(cins)
+    w = (rng.standard_normal((27, cout, cin)) * np.sqrt(2.0 / (27 * cin))).astype(np.float32)
+    b = (rng.standard_normal(cout) * 0.1).astype(np.float32)
+    dy = U.bf16(rng.standard_normal((batch, D, H, W, cout)).astype(np.float32))
+    y_bits, dx_bits, dw, db = ws.conv_test([_bits(x) for x in xs], w, b, _bits(dy), dim, batch)
+    wq = U.bf16(w)
+    y_ref = U.conv3d(xs, wq, b, relu=True, round_out=False)
+    y = U.from_bits(y_bits)
+    # one BF16 rounding of the FP32 result (relative 2^-8) plus FP32 accumulation order
+    assert np.all(np.abs(y - y_ref) <= np.abs(y_ref) * 2.0 ** -7 + 1e-3), np.abs(y - y_ref).max()
+    dx_ref = U.conv3d_dgrad(dy, wq, cins)
+    for k in range(len(cins)):
+        dx = U.from_bits(dx_bits[k])
+        assert np.all(np.abs(dx - dx_ref[k]) <= np.abs(dx_ref[k]) * 2.0 ** -7 + 1e-3), (k, np.abs(dx - dx_ref[k]).max())
+    dw_ref, db_ref = U.conv3d_wgrad(xs, dy)
+    scale = np.abs(dw_ref).max()
+    assert np.abs(dw - dw_ref).max() <= 1e-3 * scale + 1e-4, np.abs(dw - dw_ref).max() / scale
+    assert np.allclose(db, db_ref, rtol=1e-4, atol=1e-3)
+
+
+def _problem(seed, dim):
+    rng = np.random.default_rng(seed)
+    W, H, D = dim
+    inp = np.zeros((1, D, H, W, U.IN_CHANNELS), np.float32)
+    zz, yy, xx = np.meshgrid(np.arange(D), np.arange(H), np.arange(W), indexing="ij")
+    fluid = (yy < H // 2) & (xx > 0) & (xx < W - 1) & (zz > 0) & (zz < D - 1) & (yy > 0)
+    solid = (xx == 0) | (yy == 0) | (zz == 0) | (xx == W - 1) | (yy == H - 1) | (zz == D - 1)
+    inp[0, ..., 0] = U.bf16(np.where(fluid, rng.uniform(-1, 1, fluid.shape), 0.0).astype(np.float32))
+    inp[0, ..., 1] = fluid
+    inp[0, ..., 2] = solid
+    target = np.where(fluid, np.sin(xx * 0.3) * np.cos(zz * 0.2) * (H // 2 - yy) / H, 0.0).astype(np.float32)
+    return inp, target[None]
+
+
+def test_network_forward_and_gradients_match_oracle(ws):
+    dim = (64, 32, 32)
+    net = ws.WarmStartNet(dim=dim, batch=1, seed=11)
+    p = net.params()
+    inp, target = _problem(3, dim)
+    net.set_sample(0, _bits(inp[0]), target[0])
+    guess = net.forward()
+    loss, grads = net.backward()
+    ref = U.Network(p)
+    lref, gref, yref = ref.loss_and_grads(inp, target)
+    err = np.linalg.norm(guess - yref) / np.linalg.norm(yref)
+    assert err < 2e-2, err
+    assert abs(loss - lref) <= 2e-2 * lref, (loss, lref)
+    lay, head_off, n = U.layout()
+    for i, (w_off, b_off, cout, cins) in enumerate(lay):
+        g, r = grads[w_off:b_off + cout], gref[w_off:b_off + cout]
+        rel = np.linalg.norm(g - r) / np.linalg.norm(r)
+        cos = float(g @ r) / (np.linalg.norm(g) * np.linalg.norm(r))
+        assert rel < 0.15 and cos > 0.99, (i, rel, cos)
+    gh, rh = grads[head_off:], gref[head_off:]
+    assert np.linalg.norm(gh - rh) <= 2e-2 * np.linalg.norm(rh)
+    net.close()
+
+
+def test_training_reduces_loss(ws):
+    dim = (64, 32, 32)
+    net = ws.WarmStartNet(dim=dim, batch=2, seed=12, learning_rate=2e-3)
+    samples = [_problem(s, dim) for s in range(2)]
+    for k, (inp, tg) in enumerate(samples):
+        net.set_sample(k, _bits(inp[0]), tg[0])
+    first = net.train_step()
+    for _ in range(60):
+        last = net.train_step()
+    assert np.isfinite(last) and last < 0.5 * first, (first, last)
+    net.close()
