@@ -26,6 +26,8 @@ import sys
 import threading
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -396,8 +398,26 @@ def run_tanks(args):
     h1 = [sim.transfer_bytes() for sim in sims]
     clk = clocks.stop()
     seq_total, seq_dev_ms, seq_wall_ms = timed(False)
-    rows = gather_tank_stats([(k, sim.results().substeps, sim.results().last_solve_iterations, sim.results().fluid_cells)
-                              for k, sim in zip(mine, sims)])
+
+    # Per-tank substep latency: one more frame of every tank with phase events on the tanks' own
+    # streams (outside the timed region); a tank's latency is its frame's device time / its substeps,
+    # batched (sharing the GPU with the other tanks) and one tank at a time.
+    def latencies(batched):
+        for sim in sims:
+            sim.enable_phase_timing(True)
+        if batched:
+            S.step_frames(sims, nxt)
+        else:
+            for sim, fi in zip(sims, nxt):
+                sim.step_frame(fi)
+        out = [sum(sim.phase_ms().values()) / max(sim.results().substeps, 1) for sim in sims]
+        for sim in sims:
+            sim.enable_phase_timing(False)
+        return out
+    lat_b = latencies(True)
+    lat_s = latencies(False)
+    rows = gather_tank_stats([(k, sim.results().substeps, sim.results().last_solve_iterations, sim.results().fluid_cells, lb, ls)
+                              for k, sim, lb, ls in zip(mine, sims, lat_b, lat_s)], width=6)
     for sim in sims:
         sim.close()
     if rank == 0:
@@ -414,6 +434,10 @@ def run_tanks(args):
                        "l2": "inputs larger than L2 (1.3 GB of particles)"},
             "sequential": {"value": seq_total / (seq_dev_ms * 1e-3), "ms_per_step": seq_dev_ms / args.steps},
             "tank_iterations_mean": statistics.mean(r[2] for r in rows) if rows else None,
+            "tank_substep_latency_ms": {
+                "batched_p50": float(np.percentile([r[4] for r in rows], 50)), "batched_p99": float(np.percentile([r[4] for r in rows], 99)),
+                "sequential_p50": float(np.percentile([r[5] for r in rows], 50)),
+                "sequential_p99": float(np.percentile([r[5] for r in rows], 99))},
             "clocks": clk,
             "e2e": {"value": total / (wall_ms * 1e-3), "unit": "substeps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": None, "roofline": None, "cpu_baseline": None,
@@ -424,12 +448,45 @@ def run_tanks(args):
         dist.destroy_process_group()
 
 
+def run_warm_start(args):
+    """Learned warm start at 128^3: held-out randomised scenes (seeds 90000+), the first frame's pressure
+    solve from a zero guess and from the trained network's guess (weights slosh_b200/warmstart_128.npz,
+    trained on 20k MGPCG pairs by slosh_b200.train_warmstart); --steps scenes (default 200 here)."""
+    world, rank, local = dist_setup(args.gpus)
+    import torch
+    from slosh_b200 import train_warmstart as TW
+    torch.cuda.set_device(local)
+    if rank != 0:
+        return
+    path = os.path.join(ROOT, "slosh_b200", "warmstart_128.npz")
+    if not os.path.exists(path):
+        print(json.dumps({"metric": "pressure-solve ms at 128^3, learned warm start", "unavailable": "no trained weights"}))
+        return
+    scenes = args.steps if args.steps != 10 else 200
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev = TW.evaluate(TW.load_weights(path), scenes=scenes, n=128)
+    clk = clocks.stop()
+    line = {
+        "metric": "pressure-solve ms at 128^3 to 1e-6, learned warm start (zero guess beside it)",
+        "value": ev["pressure_ms_learned"], "unit": "ms", "n_gpus": 1, "steps": scenes, "warmup": 0,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "bf16 network, f32 solve", "data": "synthetic",
+        "config": {"workload": "warm_start_128", "grid": [128, 128, 128], "scenes": scenes, "scene_seeds": "90000+",
+                   "network": "3-D U-Net, 4 levels, 16/32/64/64 channels, 3x3x3, BF16/FP32-accumulate",
+                   "solver": "MGPCG", "tolerance": 1e-6},
+        "evaluation": ev, "clocks": clk, "gpu_launches": None, "roofline": None, "cpu_baseline": None,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
     elif args.workload.startswith("tanks"):
         run_tanks(args)
+    elif args.workload == "warm_start_128":
+        run_warm_start(args)
     else:
         run_slosh(args)
 

@@ -57,7 +57,10 @@ __device__ __forceinline__ bool inside3(int3 c, int3 dim) {
     return c.x >= 0 && c.y >= 0 && c.z >= 0 && c.x < dim.x && c.y < dim.y && c.z < dim.z;
 }
 __device__ __forceinline__ bool is_red(int3 c) { return (uint32_t(c.x + c.y + c.z) & 1u) == 0u; }
-__device__ __forceinline__ bool solve_done(const MGState& m) { return *(volatile uint32_t*)(m.ctl + 3) != 0u; }
+// The iteration kernels carry no "solve finished" test: they are only ever issued while the solve runs
+// (the graph's WHILE node runs its body while PCGInit / UpdatePR set the condition; the host loop reads
+// the done flag before issuing each iteration), so a test would only put a dependent load in front of
+// every kernel.
 
 // Level-0 stencil (ghost-fluid diagonal DiagF + epsilon, sum of fluid neighbours of buf).
 __device__ __forceinline__ void stencil0(const Dev& d, const float* buf, uint32_t i, int3 c, float& diag, float& sum) {
@@ -552,7 +555,6 @@ __device__ __forceinline__ Nb6 load_black(const Dev& d, const MGState& m, uint32
 // Red sweep with rho = r . z over all cells (red: the new value, black: the current z). Cells the sweep
 // does not update are stored back unchanged (each cell belongs to one warp's brick).
 __global__ void __launch_bounds__(GRID_THREADS, 3) k_smooth0(Dev d, MGState m) {
-    if (solve_done(m)) return;
     w4_pass<1, 1>(d, m, 1,
         [&](const Geo& g, const uint32_t* ns) { return load_sweep(d, m, g, ns); },
         [&](const Geo& g, const SweepQ& v, double* v0, double*) {
@@ -581,7 +583,6 @@ __global__ void __launch_bounds__(GRID_THREADS, 3) k_smooth0(Dev d, MGState m) {
 
 // Black sweep (no dot product).
 __global__ void __launch_bounds__(GRID_THREADS) k_smooth0_black(Dev d, MGState m) {
-    if (solve_done(m)) return;
     w0_black<4>(d, m, [](uint32_t, uint32_t) {},
         [&](uint32_t i, uint32_t l, const uint32_t* ns) { return load_black(d, m, i, l, ns); },
         [&](uint32_t i, uint32_t, const Nb6& v) {
@@ -598,7 +599,6 @@ __global__ void __launch_bounds__(GRID_THREADS) k_smooth0_black(Dev d, MGState m
 // x_c where the parent is fluid and 0 elsewhere) in shared memory. Adding +0 instead of skipping the
 // addition changes at most the sign of a zero z_n, which the neighbour sum (started at +0) absorbs.
 __global__ void __launch_bounds__(GRID_THREADS) k_prolong_smooth0(Dev d, MGState m) {
-    if (solve_done(m)) return;
     constexpr int WARPS = GRID_THREADS / 32;
     __shared__ float s_cx[WARPS][216];
     const MGLevel C = m.lv[1];
@@ -643,7 +643,6 @@ __global__ void __launch_bounds__(GRID_THREADS) k_prolong_smooth0(Dev d, MGState
 
 // Levels 1..3 through the active-brick footprints, with the per-solve stencil words.
 __global__ void k_smooth_fp(Dev d, MGState m, int l, uint32_t parity) {
-    if (solve_done(m)) return;
     const MGLevel L = m.lv[l];
     const uint32_t dx = uint32_t(L.dim.x), dxy = uint32_t(L.dim.x * L.dim.y);
     const uint32_t want = parity == 0u ? CW_RED : 0u;
@@ -658,7 +657,6 @@ __global__ void k_smooth_fp(Dev d, MGState m, int l, uint32_t parity) {
 }
 // Restriction l -> l + 1 over level l + 1's footprint: b_c = (sum of the fluid children's residuals) / 4.
 __global__ void k_restrict_fp(Dev d, MGState m, int l) {
-    if (solve_done(m)) return;
     const MGLevel F = m.lv[l], C = m.lv[l + 1];
     const uint32_t fdx = uint32_t(F.dim.x), fdxy = uint32_t(F.dim.x * F.dim.y);
     const uint32_t flast = F.cells - 1u;
@@ -692,7 +690,6 @@ __global__ void k_restrict_fp(Dev d, MGState m, int l) {
 }
 // Prolongation l + 1 -> l fused with the black sweep of level l (see k_prolong_smooth0).
 __global__ void k_prolong_smooth_fp(Dev d, MGState m, int l) {
-    if (solve_done(m)) return;
     const MGLevel F = m.lv[l], C = m.lv[l + 1];
     const uint32_t dx = uint32_t(F.dim.x), dxy = uint32_t(F.dim.x * F.dim.y);
     const uint32_t last = F.cells - 1u, clast = C.cells - 1u;
@@ -726,7 +723,6 @@ __global__ void k_prolong_smooth_fp(Dev d, MGState m, int l) {
 // memory, then sum each of the 64 coarse cells' fluid children in child order (x fastest), as the
 // per-coarse-cell loop does.
 __global__ void __launch_bounds__(GRID_THREADS) k_restrict0(Dev d, MGState m) {
-    if (solve_done(m)) return;
     constexpr int WARPS = GRID_THREADS / 32;
     __shared__ float s_res[WARPS][BRICK_CELLS];
     __shared__ uint8_t s_fluid[WARPS][BRICK_CELLS];
@@ -888,7 +884,6 @@ __device__ __forceinline__ void s_coarse_solve(const SLevel L, int iterations) {
     __syncthreads();
 }
 __global__ void __launch_bounds__(1024) k_vcycle_tail(MGState m, int tail, int iterations) {
-    if (solve_done(m)) return;
     extern __shared__ __align__(16) unsigned char s_tail[];
     const int nl = m.num_levels;
     SLevel S[SLOSH_MAX_MG_LEVELS];
@@ -1006,7 +1001,6 @@ __global__ void __launch_bounds__(1024) k_vcycle_tail(MGState m, int tail, int i
 
 // ---- the coarse solve directly on level 0 (grids of <= 512 cells have a single level) --------------------
 __global__ void __launch_bounds__(1024) k_coarse_solve0(Dev d, MGState m, int iterations) {
-    if (solve_done(m)) return;
     const MGLevel L = m.lv[0];
     for (int it = 0; it < iterations; ++it) {
         for (uint32_t colour = 0; colour < 2u; ++colour) {
@@ -1031,7 +1025,6 @@ __global__ void __launch_bounds__(1024) k_coarse_solve0(Dev d, MGState m, int it
 __device__ __forceinline__ float* dir_buf(const MGState& m, uint32_t parity) { return parity ? m.dvec2 : m.dvec; }
 
 __global__ void __launch_bounds__(GRID_THREADS, 3) k_apply_a(Dev d, MGState m) {
-    if (solve_done(m)) return;
     const uint32_t it = m.ctl[0];
     const bool first = it == 0u;
     const float beta = first ? 0.0f : ratio_f(m.scalars[0], m.scalars[3]);
@@ -1081,7 +1074,6 @@ __global__ void __launch_bounds__(GRID_THREADS, 3) k_apply_a(Dev d, MGState m) {
 
 // ---- PCGUpdatePRCS: p += alpha d, r -= alpha q, red pre-smooth; ||r||^2 and the loop decision -------------
 __global__ void __launch_bounds__(GRID_THREADS, 3) k_update_pr(Dev d, MGState m, float* __restrict__ p, unsigned long long handle) {
-    if (solve_done(m)) return;
     const float alpha = ratio_f(m.scalars[0], m.scalars[2]);
     const float* dcur = dir_buf(m, (m.ctl[0] + 1u) & 1u);
     struct V {

@@ -38,118 +38,161 @@ __device__ __forceinline__ uint8_t* align1024(uint8_t* p) { return p + ((1024u -
 __device__ __forceinline__ uint32_t tmem_cols(uint32_t n) { return n <= 32u ? 32u : (n <= 64u ? 64u : (n <= 128u ? 128u : 256u)); }
 
 // ---- implicit-GEMM convolution -----------------------------------------------------------------------
-// Warp 0 lane 0 produces (TMA), warp 1 lane 0 issues the MMAs, all four warps run the epilogue: row r
-// of the tile (TMEM lane r) is thread r. Stage s holds A (128 rows x C of one tap and K-block) at
-// stage offset 0 and B (N rows x C) at a_region; each is a K-major operand with the swizzle of its
-// row length (2 C bytes): 8-row groups 16 C bytes apart (SBO), the K = 16 steps 32 bytes apart.
-__global__ void __launch_bounds__(128) k_conv3d(const __grid_constant__ ConvArgs a, uint32_t stage_bytes, uint32_t a_region) {
+// Persistent and warp-specialised: CTA b takes tiles b, b + gridDim.x, ...; warp 0 (one lane) loads with
+// TMA, warp 1 (one lane) issues the MMAs, warps 2-5 run the epilogue (warp w reads TMEM lanes 32 (w % 4)
+// .. +31, so tile row r = 32 (w % 4) + lane is that thread's voxel). The stage ring runs across tiles;
+// the accumulator is double-buffered in TMEM (2 x N columns), so one tile's epilogue overlaps the next
+// tile's loads and MMAs; several such CTAs share an SM. Stage s holds A (128 rows x C of one tap and K-block) at stage offset 0 and B
+// (N rows x C) at a_region; both are K-major with the swizzle of their row length (2 C bytes): 8-row
+// groups 16 C bytes apart (SBO), the K = 16 steps 32 bytes apart.
+constexpr int CONV_THREADS = 192;
+constexpr int CONV_MAX_STAGES = 8;
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__global__ void __launch_bounds__(CONV_THREADS) k_conv3d(const __grid_constant__ ConvArgs a, uint32_t stage_bytes, uint32_t a_region,
+                                                        uint32_t stages) {
     extern __shared__ uint8_t dsm[];
-    __shared__ __align__(8) uint64_t full[CONV_STAGES], empty[CONV_STAGES], done;
+    __shared__ __align__(8) uint64_t full[CONV_MAX_STAGES], empty[CONV_MAX_STAGES], acc_full[2], acc_empty[2];
     __shared__ uint32_t tmem_slot;
     uint8_t* base = align1024(dsm);
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-    const TileOrigin o = tile_origin(a.vol, blockIdx.x);
     const uint32_t ncols = tmem_cols(a.n);
+    const uint32_t tiles = a.vol.tiles();
     if (threadIdx.x == 0) {
-        for (int s = 0; s < CONV_STAGES; ++s) {
+        for (uint32_t s = 0; s < stages; ++s) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], 1);
         }
-        mbar_init(&done, 1);
+        for (int k = 0; k < 2; ++k) {
+            mbar_init(&acc_full[k], 1);
+            mbar_init(&acc_empty[k], 128);
+        }
         fence_mbar_init();
         for (uint32_t k = 0; k < a.nblocks; ++k) {
             prefetch_map(&a.act[k]);
             prefetch_map(&a.wgt[k]);
         }
     }
-    if (warp == 0) tmem_alloc(&tmem_slot, ncols);
+    if (warp == 0) tmem_alloc(&tmem_slot, 2u * ncols);
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = tmem_slot;
     const uint32_t niter = 27u * a.nblocks;
 
-    if (warp == 0 && lane == 0) {
-        for (uint32_t it = 0; it < niter; ++it) {
-            const uint32_t s = it % CONV_STAGES;
-            if (it >= uint32_t(CONV_STAGES) && !mbar_wait(&empty[s], ((it / CONV_STAGES) - 1u) & 1u, a.error, 1u)) break;
-            const uint32_t tap = it / a.nblocks, blk = it % a.nblocks, cb = a.cb[blk];
-            int dx, dy, dz;
-            tap_offset(tap, dx, dy, dz);
-            uint8_t* sa = base + s * stage_bytes;
-            mbar_arrive_expect_tx(&full[s], cb * 256u + cb * a.n * 2u);
-            tma_load_5d(sa, &a.act[blk], 0, o.x0 + dx, o.y0 + dy, o.z0 + dz, o.b, &full[s]);
-            tma_load_2d(sa + a_region, &a.wgt[blk], 0, int(tap * a.n), &full[s]);
+    if (warp == 0) {
+        if (lane == 0) {
+            uint32_t g = 0;
+            bool ok = true;
+            for (uint32_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
+                const TileOrigin o = tile_origin(a.vol, t);
+                for (uint32_t it = 0; it < niter; ++it, ++g) {
+                    const uint32_t s = g % stages;
+                    if (g >= stages && !mbar_wait(&empty[s], ((g / stages) - 1u) & 1u, a.error, 1u)) {
+                        ok = false;
+                        break;
+                    }
+                    const uint32_t tap = it / a.nblocks, blk = it % a.nblocks, cb = a.cb[blk];
+                    int dx, dy, dz;
+                    tap_offset(tap, dx, dy, dz);
+                    uint8_t* sa = base + s * stage_bytes;
+                    mbar_arrive_expect_tx(&full[s], cb * 256u + cb * a.n * 2u);
+                    tma_load_5d(sa, &a.act[blk], 0, o.x0 + dx, o.y0 + dy, o.z0 + dz, o.b, &full[s]);
+                    tma_load_2d(sa + a_region, &a.wgt[blk], 0, int(tap * a.n), &full[s]);
+                }
+            }
         }
-    } else if (warp == 1 && lane == 0) {
-        const uint32_t idesc = idesc_bf16_f32(128u, a.n, 0u, 0u);
-        for (uint32_t it = 0; it < niter; ++it) {
-            const uint32_t s = it % CONV_STAGES;
-            if (!mbar_wait(&full[s], (it / CONV_STAGES) & 1u, a.error, 2u)) break;
+    } else if (warp == 1) {
+        if (lane == 0) {
+            const uint32_t idesc = idesc_bf16_f32(128u, a.n, 0u, 0u);
+            uint32_t g = 0, tl = 0;
+            bool ok = true;
+            for (uint32_t t = blockIdx.x; t < tiles && ok; t += gridDim.x, ++tl) {
+                const uint32_t acc = tl & 1u;
+                if (tl >= 2u && !mbar_wait(&acc_empty[acc], ((tl >> 1) - 1u) & 1u, a.error, 2u)) break;
+                tc_fence_after();
+                const uint32_t dcol = tmem + acc * ncols;
+                for (uint32_t it = 0; it < niter; ++it, ++g) {
+                    const uint32_t s = g % stages;
+                    if (!mbar_wait(&full[s], (g / stages) & 1u, a.error, 2u)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t cb = a.cb[it % a.nblocks];
+                    const uint32_t row = cb * 2u, layout = swizzle_of_row_bytes(row);
+                    const uint32_t sa = smem_u32(base + s * stage_bytes), sb = sa + a_region;
+                    for (uint32_t k = 0; k < cb / 16u; ++k)
+                        mma_bf16(dcol, smem_desc(sa + 32u * k, 16u, 8u * row, layout), smem_desc(sb + 32u * k, 16u, 8u * row, layout),
+                                 idesc, (it | k) != 0u ? 1u : 0u);
+                    mma_commit(&empty[s]);
+                }
+                mma_commit(&acc_full[acc]);
+            }
+        }
+    } else {
+        const uint32_t q = warp & 3u;  // TMEM lane quarter of this warp
+        const uint32_t r = q * 32u + lane;
+        uint32_t tl = 0;
+        for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x, ++tl) {
+            const uint32_t acc = tl & 1u;
+            const bool ok = __all_sync(0xFFFFFFFFu, mbar_wait(&acc_full[acc], (tl >> 1) & 1u, a.error, 4u));
             tc_fence_after();
-            const uint32_t cb = a.cb[it % a.nblocks];
-            const uint32_t row = cb * 2u, layout = swizzle_of_row_bytes(row);
-            const uint32_t sa = smem_u32(base + s * stage_bytes), sb = sa + a_region;
-            for (uint32_t k = 0; k < cb / 16u; ++k)
-                mma_bf16(tmem, smem_desc(sa + 32u * k, 16u, 8u * row, layout), smem_desc(sb + 32u * k, 16u, 8u * row, layout), idesc,
-                         (it | k) != 0u ? 1u : 0u);
-            mma_commit(&empty[s]);
+            if (!ok) break;
+            const TileOrigin o = tile_origin(a.vol, t);
+            const uint64_t v = o.v0 + r;
+            for (uint32_t c0 = 0; c0 < a.n; c0 += 16u) {
+                float x[16];
+                tmem_ld16(tmem + acc * ncols + ((q * 32u) << 16) + c0, x);
+                if (a.bias)
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) x[j] = x[j] + a.bias[c0 + uint32_t(j)];
+                if (a.relu)
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) x[j] = fmaxf(x[j], 0.0f);
+                const uint32_t oi = c0 < a.oc[0] ? 0u : 1u;
+                const uint32_t cc = oi == 0u ? c0 : c0 - a.oc[0];
+                const uint64_t e = v * a.oc[oi] + cc;
+                uint4* dst = reinterpret_cast<uint4*>(a.out[oi] + e);
+                if (a.accumulate) {
+                    const uint4 w0 = dst[0], w1 = dst[1];
+                    const bf16* old0 = reinterpret_cast<const bf16*>(&w0);
+                    const bf16* old1 = reinterpret_cast<const bf16*>(&w1);
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        x[j] = x[j] + bf(old0[j]);
+                        x[8 + j] = x[8 + j] + bf(old1[j]);
+                    }
+                }
+                if (a.mask[oi]) {
+                    const uint4* mp = reinterpret_cast<const uint4*>(a.mask[oi] + e);
+                    const uint4 m0 = mp[0], m1 = mp[1];
+                    const bf16* mk0 = reinterpret_cast<const bf16*>(&m0);
+                    const bf16* mk1 = reinterpret_cast<const bf16*>(&m1);
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        if (!(bf(mk0[j]) > 0.0f)) x[j] = 0.0f;
+                        if (!(bf(mk1[j]) > 0.0f)) x[8 + j] = 0.0f;
+                    }
+                }
+                uint4 w[2];
+                bf16* wb = reinterpret_cast<bf16*>(w);
+#pragma unroll
+                for (int j = 0; j < 16; ++j) wb[j] = __float2bfloat16_rn(x[j]);
+                dst[0] = w[0];
+                dst[1] = w[1];
+            }
+            tc_fence_before();
+            mbar_arrive(&acc_empty[acc]);
         }
-        mma_commit(&done);
     }
-    const bool ok = mbar_wait(&done, 0u, a.error, 4u);
     __syncwarp();
-    tc_fence_after();
-    if (ok) {
-        const uint32_t r = warp * 32u + lane;
-        const uint64_t v = o.v0 + r;
-        for (uint32_t c0 = 0; c0 < a.n; c0 += 16u) {
-            float acc[16];
-            tmem_ld16(tmem + ((warp * 32u) << 16) + c0, acc);
-            if (a.bias)
-#pragma unroll
-                for (int j = 0; j < 16; ++j) acc[j] = acc[j] + a.bias[c0 + uint32_t(j)];
-            if (a.relu)
-#pragma unroll
-                for (int j = 0; j < 16; ++j) acc[j] = fmaxf(acc[j], 0.0f);
-            const uint32_t oi = c0 < a.oc[0] ? 0u : 1u;
-            const uint32_t cc = oi == 0u ? c0 : c0 - a.oc[0];
-            const uint64_t e = v * a.oc[oi] + cc;
-            uint4* dst = reinterpret_cast<uint4*>(a.out[oi] + e);
-            if (a.accumulate) {
-                const uint4 w0 = dst[0], w1 = dst[1];
-                const bf16* old0 = reinterpret_cast<const bf16*>(&w0);
-                const bf16* old1 = reinterpret_cast<const bf16*>(&w1);
-#pragma unroll
-                for (int j = 0; j < 8; ++j) {
-                    acc[j] = acc[j] + bf(old0[j]);
-                    acc[8 + j] = acc[8 + j] + bf(old1[j]);
-                }
-            }
-            if (a.mask[oi]) {
-                const uint4* mp = reinterpret_cast<const uint4*>(a.mask[oi] + e);
-                const uint4 m0 = mp[0], m1 = mp[1];
-                const bf16* mk0 = reinterpret_cast<const bf16*>(&m0);
-                const bf16* mk1 = reinterpret_cast<const bf16*>(&m1);
-#pragma unroll
-                for (int j = 0; j < 8; ++j) {
-                    if (!(bf(mk0[j]) > 0.0f)) acc[j] = 0.0f;
-                    if (!(bf(mk1[j]) > 0.0f)) acc[8 + j] = 0.0f;
-                }
-            }
-            uint4 w[2];
-            bf16* wb = reinterpret_cast<bf16*>(w);
-#pragma unroll
-            for (int j = 0; j < 16; ++j) wb[j] = __float2bfloat16_rn(acc[j]);
-            dst[0] = w[0];
-            dst[1] = w[1];
-        }
-    }
     tc_fence_before();
     __syncthreads();
     if (warp == 0) {
         tc_fence_after();
-        tmem_dealloc(tmem, ncols);
+        tmem_dealloc(tmem, 2u * ncols);
     }
 }
 
@@ -546,7 +589,61 @@ __global__ void k_pack(Dev d, const float* __restrict__ div, const float* __rest
     dst[1] = w[1];
     if (target) target[uint64_t(slot) * n + v] = pv;
 }
-__global__ void k_scatter_guess(Dev d, const float* __restrict__ guess, const uint32_t* __restrict__ meta, float* __restrict__ pressure) {
+// Energy-optimal scale of the guess g (the network's output on the dense grid): with x0 = beta g, beta =
+// (g . b) / (g . A g) minimises the A-norm error ||x0 - x||_A over the line through g, so the solve never
+// starts worse (in that norm) than from zero. A and b are level 0 of the solve: (A g)_i = (diag_i +
+// DiagEpsilon) g_i - sum of g over the fluid neighbours, b_i = -div_i, over the fluid cells. Chunk c of
+// the dense voxels gives partial[2c] = sum g.b, partial[2c + 1] = sum g.Ag (FP64, threads folded in order).
+constexpr uint32_t ENERGY_THREADS = 256;
+__global__ void __launch_bounds__(ENERGY_THREADS) k_energy_partial(Dev d, const float* __restrict__ guess, const bf16* __restrict__ input,
+                                                                   const float* __restrict__ div, double* __restrict__ partial,
+                                                                   uint64_t per_chunk) {
+    __shared__ double s_gb[ENERGY_THREADS], s_gag[ENERGY_THREADS];
+    const uint32_t W = uint32_t(d.grid.x), H = uint32_t(d.grid.y), D = uint32_t(d.grid.z);
+    const uint64_t n = uint64_t(W) * H * D;
+    const uint64_t v0 = uint64_t(blockIdx.x) * per_chunk;
+    const uint64_t v1 = min(n, v0 + per_chunk);
+    double gb = 0.0, gag = 0.0;
+    auto fluid = [&](uint64_t v) { return bf(input[v * IN_CHANNELS + 1u]) > 0.5f; };
+    for (uint64_t v = v0 + threadIdx.x; v < v1; v += ENERGY_THREADS) {
+        if (!fluid(v)) continue;
+        const int3 c = make_int3(int(v % W), int((v / W) % H), int(v / (uint64_t(W) * H)));
+        const uint32_t ci = cell_index(d, c);
+        const float g = guess[v];
+        float nb = 0.0f;
+        const uint64_t sx = 1u, sy = W, sz = uint64_t(W) * H;
+        if (c.x > 0 && fluid(v - sx)) nb = nb + guess[v - sx];
+        if (c.x + 1 < d.grid.x && fluid(v + sx)) nb = nb + guess[v + sx];
+        if (c.y > 0 && fluid(v - sy)) nb = nb + guess[v - sy];
+        if (c.y + 1 < d.grid.y && fluid(v + sy)) nb = nb + guess[v + sy];
+        if (c.z > 0 && fluid(v - sz)) nb = nb + guess[v - sz];
+        if (c.z + 1 < d.grid.z && fluid(v + sz)) nb = nb + guess[v + sz];
+        const float ag = (d.cell_diag[ci] + DIAG_EPSILON) * g - nb;
+        gb += double(g) * double(-div[ci]);
+        gag += double(g) * double(ag);
+    }
+    s_gb[threadIdx.x] = gb;
+    s_gag[threadIdx.x] = gag;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0, b = 0.0;
+        for (uint32_t t = 0; t < ENERGY_THREADS; ++t) {
+            a += s_gb[t];
+            b += s_gag[t];
+        }
+        partial[2u * blockIdx.x] = a;
+        partial[2u * blockIdx.x + 1u] = b;
+    }
+}
+__global__ void k_energy_finish(const double* __restrict__ partial, uint32_t chunks, float* __restrict__ beta) {
+    double a = 0.0, b = 0.0;
+    for (uint32_t c = 0; c < chunks; ++c) {
+        a += partial[2u * c];
+        b += partial[2u * c + 1u];
+    }
+    *beta = b > 0.0 ? float(a / b) : 0.0f;
+}
+__global__ void k_scatter_guess(Dev d, const float* __restrict__ guess, const float* __restrict__ beta, float* __restrict__ pressure) {
     const uint32_t W = uint32_t(d.grid.x), H = uint32_t(d.grid.y), D = uint32_t(d.grid.z);
     const uint64_t n = uint64_t(W) * H * D;
     const uint64_t v = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -554,17 +651,20 @@ __global__ void k_scatter_guess(Dev d, const float* __restrict__ guess, const ui
     const int3 c = make_int3(int(v % W), int((v / W) % H), int(v / (uint64_t(W) * H)));
     const uint32_t ci = cell_index(d, c);
     if (is_null_cell(ci) || type_of(d.cell_type[ci]) != CELL_FLUID) return;
-    pressure[ci] = guess[v] * slot_scale(meta, 0u);
+    pressure[ci] = guess[v] * beta[0];
 }
 
 uint32_t blocks_for(uint64_t n, uint32_t threads) { return uint32_t((n + threads - 1u) / threads); }
+uint32_t tmem_cols_host(uint32_t n) { return n <= 32u ? 32u : (n <= 64u ? 64u : (n <= 128u ? 128u : 256u)); }
 
 }  // namespace
 
 size_t conv_smem_bytes(uint32_t cb_max, uint32_t n) {
     const size_t a_region = 256u * cb_max;
     const size_t b_region = (size_t(n) * cb_max * 2u + 1023u) / 1024u * 1024u;
-    return CONV_STAGES * (a_region + b_region) + 1024u;
+    size_t stages = (48u * 1024u) / (a_region + b_region);
+    stages = stages < 3u ? 3u : (stages > size_t(CONV_MAX_STAGES) ? size_t(CONV_MAX_STAGES) : stages);
+    return stages * (a_region + b_region) + 1024u;
 }
 size_t wgrad_smem_bytes(uint32_t c, uint32_t n) {
     (void)c;
@@ -578,13 +678,30 @@ int launch_conv(const ConvArgs& a, cudaStream_t s) {
     if (a.nblocks > 1u) cbmax = a.cb[0] > a.cb[1] ? a.cb[0] : a.cb[1];
     const uint32_t a_region = 256u * cbmax;
     const uint32_t b_region = (a.n * cbmax * 2u + 1023u) / 1024u * 1024u;
-    const size_t smem = conv_smem_bytes(cbmax, a.n);
-    static bool configured = false;
-    if (!configured) {
-        cudaFuncSetAttribute(k_conv3d, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-        configured = true;
+    const uint32_t stage = a_region + b_region;
+    // The loads are L2-latency bound, so what counts is the number of stages in flight per SM: 3-8
+    // stages in about 48 KB per CTA, and as many persistent CTAs per SM as shared memory (227 KB),
+    // TMEM (512 columns, two accumulators per CTA) and threads (2048) allow.
+    uint32_t stages = (48u * 1024u) / stage;
+    stages = stages < 3u ? 3u : (stages > uint32_t(CONV_MAX_STAGES) ? uint32_t(CONV_MAX_STAGES) : stages);
+    const size_t smem = size_t(stages) * stage + 1024u;
+    static int num_sms = 0;
+    if (!num_sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev);
+        if (num_sms <= 0) num_sms = 148;
+        cudaFuncSetAttribute(k_conv3d, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
     }
-    k_conv3d<<<a.vol.tiles(), 128, smem, s>>>(a, a_region + b_region, a_region);
+    const uint32_t tiles = a.vol.tiles();
+    uint32_t per_sm = uint32_t((227u * 1024u) / (smem + 1024u));
+    const uint32_t by_tmem = 512u / (2u * tmem_cols_host(a.n));
+    if (per_sm > by_tmem) per_sm = by_tmem;
+    if (per_sm > 2048u / CONV_THREADS) per_sm = 2048u / CONV_THREADS;
+    if (per_sm < 1u) per_sm = 1u;
+    uint32_t grid = uint32_t(num_sms) * per_sm;
+    if (grid > tiles) grid = tiles;
+    k_conv3d<<<grid, CONV_THREADS, smem, s>>>(a, stage, a_region, stages);
     return 1;
 }
 int launch_wgrad(const WgradArgs& a, uint32_t chunks, cudaStream_t s) {
@@ -670,10 +787,13 @@ int launch_pack_input(const Dev& d, const float* divergence, const float* pressu
     k_pack<<<blocks_for(n, 256), 256, 0, s>>>(d, divergence, pressure, input, target, meta, slot);
     return 2;
 }
-int launch_scatter_guess(const Dev& d, const float* guess, const uint32_t* meta, float* pressure, cudaStream_t s) {
+int launch_scatter_guess(const Dev& d, const float* guess, const bf16* input, const float* divergence, double* partial, uint32_t chunks,
+                         float* beta, float* pressure, cudaStream_t s) {
     const uint64_t n = uint64_t(d.grid.x) * d.grid.y * d.grid.z;
-    k_scatter_guess<<<blocks_for(n, 256), 256, 0, s>>>(d, guess, meta, pressure);
-    return 1;
+    k_energy_partial<<<chunks, ENERGY_THREADS, 0, s>>>(d, guess, input, divergence, partial, (n + chunks - 1u) / chunks);
+    k_energy_finish<<<1, 1, 0, s>>>(partial, chunks, beta);
+    k_scatter_guess<<<blocks_for(n, 256), 256, 0, s>>>(d, guess, beta, pressure);
+    return 3;
 }
 
 }  // namespace unet

@@ -143,6 +143,8 @@ struct Net {
     uint32_t* nfluid = nullptr;  // total fluid voxels of the batch
     uint32_t* error = nullptr;
     float *wpartial = nullptr, *bpartial = nullptr, *hpartial = nullptr, *head_grad = nullptr;
+    double* energy = nullptr;  // warm-start scale partials
+    float* beta = nullptr;     // warm-start scale of the last guess
     uint32_t head_chunks = 0, bias_chunks = 0;
     uint64_t step = 0;
     uint64_t launches = 0;
@@ -185,6 +187,7 @@ struct Net {
     }
 
     Net(const slosh_unet_config_t& config, int dev) : cfg(config), device(dev) {
+        if (device < 0) UCK(cudaGetDevice(&device));  // -1: the calling thread's current device
         UCK(cudaSetDevice(device));
         UCK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
         const uint32_t W = cfg.dim[0], H = cfg.dim[1], D = cfg.dim[2], B = cfg.batch ? cfg.batch : 1u;
@@ -237,6 +240,8 @@ struct Net {
         head_chunks = 592;
         hpartial = dmalloc<float>(size_t(head_chunks) * 18u);
         head_grad = dmalloc<float>(18);
+        energy = dmalloc<double>(2u * 592u);
+        beta = dmalloc<float>(1);
         init_params();
     }
     ~Net() {
@@ -251,7 +256,7 @@ struct Net {
             cudaFree(c.wd);
         }
         for (void* p : {(void*)params, (void*)grads, (void*)adam_m, (void*)adam_v, (void*)target, (void*)guess, (void*)meta, (void*)nfluid,
-                        (void*)error, (void*)wpartial, (void*)bpartial, (void*)hpartial, (void*)head_grad})
+                        (void*)error, (void*)wpartial, (void*)bpartial, (void*)hpartial, (void*)head_grad, (void*)energy, (void*)beta})
             cudaFree(p);
         cudaStreamDestroy(stream);
     }
@@ -445,7 +450,7 @@ int warm_start(Net* net, const Dev& d, const float* divergence, float* pressure,
     const uint64_t before = net->launches;
     net->forward();
     n += int(net->launches - before);
-    n += launch_scatter_guess(d, net->guess, net->meta, pressure, s);
+    n += launch_scatter_guess(d, net->guess, net->T[size_t(net->t_in)].act, divergence, net->energy, 592u, net->beta, pressure, s);
     net->stream = keep;
     return n;
 }

@@ -98,8 +98,10 @@ int launch_conv_weights(const float* w, uint32_t n, uint32_t cin, const uint32_t
 // bits, meta[2 slot + 1] = fluid voxel count (accumulated; the caller clears it).
 int launch_pack_input(const Dev& d, const float* divergence, const float* pressure, bf16* input, float* target, uint32_t* meta,
                       uint32_t slot, cudaStream_t s);
-// pressure[fluid cells] = guess[v] * scale of slot 0.
-int launch_scatter_guess(const Dev& d, const float* guess, const uint32_t* meta, float* pressure, cudaStream_t s);
+// Initial pressure from slot 0's guess: pressure[fluid cells] = beta * guess[v], beta = (g . b) / (g . A g)
+// of the solve's level-0 system (energy-optimal scale, deterministic FP64 sums over `chunks` chunks).
+int launch_scatter_guess(const Dev& d, const float* guess, const bf16* input, const float* divergence, double* partial, uint32_t chunks,
+                         float* beta, float* pressure, cudaStream_t s);
 
 }  // namespace unet
 }  // namespace slosh

@@ -35,9 +35,10 @@ def lpt_partition(costs, parts):
     return [sorted(p) for p in plan]
 
 
-def gather_tank_stats(stats, device=None):
-    """All-gather of per-tank result rows (tank index, substeps, last solve iterations, fluid cells) from
-    every rank, as one list sorted by tank index; a single process returns its own rows."""
+def gather_tank_stats(stats, device=None, width=4):
+    """All-gather of per-tank result rows (tank index, substeps, last solve iterations, fluid cells, and
+    any further per-tank figures up to `width` columns) from every rank, as one list sorted by tank
+    index; a single process returns its own rows."""
     rows = [tuple(float(v) for v in r) for r in stats]
     if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
         return sorted(rows)
@@ -46,7 +47,6 @@ def gather_tank_stats(stats, device=None):
     n = torch.tensor([len(rows)], dtype=torch.int64, device=dev)
     counts = [torch.zeros_like(n) for _ in range(world)]
     dist.all_gather(counts, n)
-    width = 4
     cap = int(max(int(c.item()) for c in counts))
     mine = torch.zeros((max(cap, 1), width), dtype=torch.float64, device=dev)
     if rows:

