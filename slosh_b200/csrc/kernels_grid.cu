@@ -36,16 +36,24 @@ __device__ __forceinline__ uint32_t nbr_index_cta(uint32_t index, int3 c, int n)
     const uint32_t local = index & (BRICK_CELLS - 1u);
     return cta_nbr_slots()[n] * BRICK_CELLS + (plus ? local - 7u * stride : local + 7u * stride);
 }
+// Neighbour n of cell (c, index): from the CTA's neighbour slots (for_active_cells<true>) or through
+// the brick table (for_active_cells<false>).
+template <bool kSlots = true>
+__device__ __forceinline__ uint32_t nbr_at(const Dev& d, uint32_t index, int3 c, int n) {
+    return kSlots ? nbr_index_cta(index, c, n) : nbr_index(d, index, c, n);
+}
 // In-grid neighbour n of cell (c, index); out-of-grid neighbours resolve into the null brick.
+template <bool kSlots = true>
 __device__ __forceinline__ uint32_t nidx(const Dev& d, uint32_t index, int3 c, int n) {
     const int3 nb = add3(c, nbr_off(n));
     if (!in_grid(d, nb)) return local_index_of(nb);
-    return nbr_index_cta(index, c, n);
+    return nbr_at<kSlots>(d, index, c, n);
 }
+template <bool kSlots = true>
 __device__ __forceinline__ uint32_t ntype(const Dev& d, uint32_t index, int3 c, int n) {
     const int3 nb = add3(c, nbr_off(n));
     if (!in_grid(d, nb)) return CELL_SOLID;
-    return d.cell_type[nbr_index_cta(index, c, n)];
+    return d.cell_type[nbr_at<kSlots>(d, index, c, n)];
 }
 
 // CellDensity (Slosh.usf:211-224).
@@ -84,23 +92,28 @@ __device__ __forceinline__ bool touches_air(const Dev& d, uint32_t index, int3 c
     return t;
 }
 
-// Visits the in-grid cells of the active bricks: fn(index, c). fn must not contain CTA barriers; every
-// thread of the CTA must call it (it loads the brick's neighbour slots between two barriers).
-template <class Fn>
+// Visits the in-grid cells of the active bricks: fn(index, c); one brick per CTA iteration. With kSlots
+// the brick's six face-neighbour slots are first loaded into shared memory (between two barriers), so
+// nbr_index_cta resolves neighbours across the brick's faces without brick-table reads; then fn must not
+// contain CTA barriers and every thread must call it. Passes with little work per brick (one colour of
+// a sweep, no neighbours at all) take kSlots = false: no barriers, neighbours through the brick table.
+template <bool kSlots, class Fn>
 __device__ __forceinline__ void for_active_cells(const Dev& d, Fn fn) {
     const uint32_t active = d.active_bricks[0];
     uint32_t* ns = cta_nbr_slots();
     for (uint32_t e = blockIdx.x; e < active; e += gridDim.x) {
         const uint32_t brick = d.active_bricks[1u + e];
         const int3 bc = brick_coord_of(d, brick);
-        __syncthreads();  // the previous brick's cells are done with the neighbour slots
-        if (threadIdx.x < 6u) {
-            const int3 nb = add3(bc, nbr_off(int(threadIdx.x)));
-            const bool in = nb.x >= 0 && nb.y >= 0 && nb.z >= 0 && nb.x < d.brick_dim.x && nb.y < d.brick_dim.y && nb.z < d.brick_dim.z;
-            ns[threadIdx.x] = in ? __ldg(d.brick_table + brick_index_of(d, nb)) : 0u;
+        if (kSlots) {
+            __syncthreads();  // the previous brick's cells are done with the neighbour slots
+            if (threadIdx.x < 6u) {
+                const int3 nb = add3(bc, nbr_off(int(threadIdx.x)));
+                const bool in = nb.x >= 0 && nb.y >= 0 && nb.z >= 0 && nb.x < d.brick_dim.x && nb.y < d.brick_dim.y && nb.z < d.brick_dim.z;
+                ns[threadIdx.x] = in ? __ldg(d.brick_table + brick_index_of(d, nb)) : 0u;
+            }
         }
         const uint32_t slot = __ldg(d.brick_table + brick);
-        __syncthreads();
+        if (kSlots) __syncthreads();
 #pragma unroll
         for (int k = 0; k < 2; ++k) {
             const uint32_t l = threadIdx.x + uint32_t(k) * 256u;
@@ -271,7 +284,7 @@ __global__ void k_clear_new_slots(Dev d) {  // ClearNewSlotsCS
 // just before the count-based fluid marking, gives the same types in one pass over the cells.
 __global__ void __launch_bounds__(GRID_THREADS) k_mark_cells(Dev d, Pass p) {
     uint32_t fluid = 0;
-    for_active_cells(d, [&](uint32_t index, int3 c) {
+    for_active_cells<false>(d, [&](uint32_t index, int3 c) {
         uint32_t packed = CELL_AIR;
         if (c.x == 0 || c.y == 0 || c.z == 0 || c.x == d.grid.x - 1 || c.y == d.grid.y - 1 || c.z == d.grid.z - 1) {
             packed = CELL_SOLID;
@@ -303,7 +316,7 @@ __global__ void __launch_bounds__(GRID_THREADS) k_mark_cells(Dev d, Pass p) {
 // ---- NormalizeFace ------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(GRID_THREADS) k_normalize(Dev d, Pass p, float* __restrict__ vel) {
     const uint32_t tf = d.total_faces;
-    for_active_cells(d, [&](uint32_t index, int3 c) {
+    for_active_cells<true>(d, [&](uint32_t index, int3 c) {
         const uint32_t b = d.cell_type[index];
 #pragma unroll
         for (int axis = 0; axis < 3; ++axis) {
@@ -345,7 +358,7 @@ __global__ void __launch_bounds__(GRID_THREADS) k_normalize(Dev d, Pass p, float
 __global__ void __launch_bounds__(GRID_THREADS) k_viscosity(Dev d, Pass p, const float* __restrict__ ustar,
                                                             const float* __restrict__ src, float* __restrict__ dst) {
     const float alpha = p.viscosity_alpha;
-    for_active_cells(d, [&](uint32_t index, int3 c) {
+    for_active_cells<true>(d, [&](uint32_t index, int3 c) {
 #pragma unroll
         for (int axis = 0; axis < 3; ++axis) {
             const uint32_t f = uint32_t(axis) * d.pool_cells + index;
@@ -368,7 +381,7 @@ __global__ void __launch_bounds__(GRID_THREADS) k_viscosity(Dev d, Pass p, const
 
 // ---- DivergenceCS --------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(GRID_THREADS) k_divergence(Dev d, Pass p, const float* __restrict__ vel) {
-    for_active_cells(d, [&](uint32_t index, int3 c) {
+    for_active_cells<true>(d, [&](uint32_t index, int3 c) {
         d.cell_count[index] = 0;
         if (type_of(d.cell_type[index]) != CELL_FLUID) {
             d.divergence[index] = 0.0f;
@@ -403,7 +416,7 @@ __global__ void __launch_bounds__(GRID_THREADS) k_divergence(Dev d, Pass p, cons
 // ---- PressureRBGSCS: one SOR colour sweep ----------------------------------------------------------------
 __global__ void __launch_bounds__(GRID_THREADS) k_rbgs(Dev d, float* __restrict__ pres, const float* __restrict__ rhs,
                                                        uint32_t parity, float omega) {
-    for_active_cells(d, [&](uint32_t index, int3 c) {
+    for_active_cells<false>(d, [&](uint32_t index, int3 c) {
         if (type_of(d.cell_type[index]) != CELL_FLUID) return;
         if ((uint32_t(c.x + c.y + c.z) & 1u) != parity) return;
         float sum = 0.0f;
@@ -412,7 +425,7 @@ __global__ void __launch_bounds__(GRID_THREADS) k_rbgs(Dev d, float* __restrict_
         for (int n = 0; n < 6; ++n) {
             const int3 nb = add3(c, nbr_off(n));
             if (!in_grid(d, nb)) continue;
-            const uint32_t ni = nbr_index_cta(index, c, n);
+            const uint32_t ni = nbr_at<false>(d, index, c, n);
             if (type_of(d.cell_type[ni]) == CELL_FLUID) sum = sum + pres[ni];
         }
         if (diag > 0.0f) {
@@ -425,7 +438,7 @@ __global__ void __launch_bounds__(GRID_THREADS) k_rbgs(Dev d, float* __restrict_
 
 // ---- ProjectFace (its two-way coupling terms are accumulated by k_coupling_faces after the pass) ---------
 __global__ void __launch_bounds__(GRID_THREADS) k_project(Dev d, Pass p, float* __restrict__ vel) {
-    for_active_cells(d, [&](uint32_t index, int3 c) {
+    for_active_cells<true>(d, [&](uint32_t index, int3 c) {
         const uint32_t b = d.cell_type[index];
 #pragma unroll
         for (int axis = 0; axis < 3; ++axis) {
@@ -527,7 +540,7 @@ __device__ void accumulate_contact(const Dev& d, const Pass& p, uint32_t solid_p
 // The coupling terms of ProjectFace (Slosh.usf:1004-1029), on the projected field after the projection
 // pass (the reference samples the wetted-face velocity while the same pass writes it).
 __global__ void __launch_bounds__(GRID_THREADS) k_coupling_faces(Dev d, Pass p, const float* __restrict__ vel) {
-    for_active_cells(d, [&](uint32_t index, int3 c) {
+    for_active_cells<false>(d, [&](uint32_t index, int3 c) {
         const uint32_t b = d.cell_type[index];
 #pragma unroll
         for (int axis = 0; axis < 3; ++axis) {
@@ -583,7 +596,7 @@ __device__ bool body_surface_pressure(const Dev& d, int3 c, float& p_hat) {
 }
 // CouplingForceCS, Slosh.usf:1127-1216.
 __global__ void __launch_bounds__(GRID_THREADS) k_coupling_force(Dev d, Pass p) {
-    for_active_cells(d, [&](uint32_t index, int3 c) {
+    for_active_cells<false>(d, [&](uint32_t index, int3 c) {
         const uint32_t packed = d.cell_type[index];
         const uint32_t type = type_of(packed);
         if (type == CELL_AIR) return;
@@ -633,7 +646,7 @@ __global__ void __launch_bounds__(GRID_THREADS) k_coupling_force(Dev d, Pass p) 
 }
 // SubmergedCS, Slosh.usf:1316-1370.
 __global__ void __launch_bounds__(GRID_THREADS) k_submerged(Dev d) {
-    for_active_cells(d, [&](uint32_t index, int3 c) {
+    for_active_cells<false>(d, [&](uint32_t index, int3 c) {
         const uint32_t packed = d.cell_type[index];
         const uint32_t id = collider_of(packed);
         if (type_of(packed) != CELL_SOLID || id == 0u) return;
@@ -668,7 +681,7 @@ __global__ void __launch_bounds__(GRID_THREADS) k_submerged(Dev d) {
 
 // ---- ResidualCS ------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(GRID_THREADS) k_residual(Dev d, Pass p, const float* __restrict__ vel) {
-    for_active_cells(d, [&](uint32_t index, int3 c) {
+    for_active_cells<true>(d, [&](uint32_t index, int3 c) {
         if (type_of(d.cell_type[index]) != CELL_FLUID) return;
         float div = 0.0f;
 #pragma unroll
@@ -688,7 +701,7 @@ __global__ void __launch_bounds__(GRID_THREADS) k_residual(Dev d, Pass p, const 
 
 // ---- DensityProjectionRhsCS -------------------------------------------------------------------------------
 __global__ void __launch_bounds__(GRID_THREADS) k_density_rhs(Dev d, Pass p) {
-    for_active_cells(d, [&](uint32_t index, int3 c) {
+    for_active_cells<true>(d, [&](uint32_t index, int3 c) {
         d.density_q[index] = 0.0f;
         if (type_of(d.cell_type[index]) != CELL_FLUID) { d.density_rhs[index] = 0.0f; return; }
         float dev = cell_density_interior(d, p, index, c) - 1.0f;
@@ -699,7 +712,7 @@ __global__ void __launch_bounds__(GRID_THREADS) k_density_rhs(Dev d, Pass p) {
 
 // ---- DensityDisplacementFace -----------------------------------------------------------------------------
 __global__ void __launch_bounds__(GRID_THREADS) k_density_displacement(Dev d, float* __restrict__ dst) {
-    for_active_cells(d, [&](uint32_t index, int3 c) {
+    for_active_cells<true>(d, [&](uint32_t index, int3 c) {
         const uint32_t b = d.cell_type[index];
 #pragma unroll
         for (int axis = 0; axis < 3; ++axis) {
@@ -726,7 +739,7 @@ __global__ void __launch_bounds__(GRID_THREADS) k_extrapolate(Dev d, const float
     uint32_t known = FACE_VALID;
     for (uint32_t it = 0; it < iteration; ++it) known |= 1u << (FACE_EXTRAP_SHIFT + it);
     const uint32_t new_bit = 1u << (FACE_EXTRAP_SHIFT + iteration);
-    for_active_cells(d, [&](uint32_t index, int3 c) {
+    for_active_cells<true>(d, [&](uint32_t index, int3 c) {
 #pragma unroll
         for (int axis = 0; axis < 3; ++axis) {
             const uint32_t f = uint32_t(axis) * d.pool_cells + index;

@@ -149,16 +149,17 @@ __device__ double final_reduce(const double* partials, uint32_t n, DotSmem& sm) 
 
 // Visits the cells of level l (1..3) that lie in the active bricks' footprints: fn(ci, c). Levels
 // whose cells are coarser than a brick are scanned densely.
+// Thread t0 of `stride` threads takes footprint cells t0, t0 + stride, ...
 template <class Fn>
-__device__ __forceinline__ void for_footprint(const Dev& d, const MGLevel& L, int l, Fn fn) {
+__device__ __forceinline__ void for_footprint_span(const Dev& d, const MGLevel& L, int l, uint32_t t0, uint32_t stride, Fn fn) {
     if (l > 3) {
-        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < L.cells; i += gridDim.x * blockDim.x) fn(i, coord3(i, L.dim));
+        for (uint32_t i = t0; i < L.cells; i += stride) fn(i, coord3(i, L.dim));
         return;
     }
     const int side = 8 >> l;
     const uint32_t per = uint32_t(side * side * side);
     const uint32_t count = d.active_bricks[0];
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;; t += gridDim.x * blockDim.x) {
+    for (uint32_t t = t0;; t += stride) {
         const uint32_t e = t / per, lc = t % per;
         // The brick index is loaded before the bound is known (clamped into the list), so it overlaps
         // the load of the active count.
@@ -169,6 +170,10 @@ __device__ __forceinline__ void for_footprint(const Dev& d, const MGLevel& L, in
                                  bc.z * side + int(lc / uint32_t(side * side)));
         if (inside3(c, L.dim)) fn(lin3(c, L.dim), c);
     }
+}
+template <class Fn>
+__device__ __forceinline__ void for_footprint(const Dev& d, const MGLevel& L, int l, Fn fn) {
+    for_footprint_span(d, L, l, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x, fn);
 }
 
 // ---- level-0 stencil words ------------------------------------------------------------------------
@@ -641,81 +646,88 @@ __global__ void __launch_bounds__(GRID_THREADS) k_prolong_smooth0(Dev d, MGState
         });
 }
 
-// Levels 1..3 through the active-brick footprints, with the per-solve stencil words.
-__global__ void k_smooth_fp(Dev d, MGState m, int l, uint32_t parity) {
-    const MGLevel L = m.lv[l];
+// Levels 1..3 through the active-brick footprints, with the per-solve stencil words; each pass is a
+// per-cell body and a grid-wide kernel over the level's footprint.
+// Sweep of one colour (want = CW_RED: red cells, 0: black cells) at cell i of level L.
+__device__ __forceinline__ void smooth_fp_cell(const MGLevel& L, uint32_t i, uint32_t want) {
     const uint32_t dx = uint32_t(L.dim.x), dxy = uint32_t(L.dim.x * L.dim.y);
-    const uint32_t want = parity == 0u ? CW_RED : 0u;
-    const uint32_t last = L.cells - 1u;
-    for_footprint(d, L, l, [&](uint32_t i, int3) {
-        const uint32_t w = L.word[i];
-        const float b = lv_ld(L.b, i, L.prec);
-        const float sum = word_sum_g(L.x, L.prec, w, i, dx, dxy, last);
-        if (!(w & CW_FLUID) || (w & CW_RED) != want) return;
-        lv_st(L.x, i, L.prec, (b + sum) / word_diag(w));
-    });
+    const uint32_t w = L.word[i];
+    const float b = lv_ld(L.b, i, L.prec);
+    const float sum = word_sum_g(L.x, L.prec, w, i, dx, dxy, L.cells - 1u);
+    if (!(w & CW_FLUID) || (w & CW_RED) != want) return;
+    lv_st(L.x, i, L.prec, (b + sum) / word_diag(w));
 }
-// Restriction l -> l + 1 over level l + 1's footprint: b_c = (sum of the fluid children's residuals) / 4.
-__global__ void k_restrict_fp(Dev d, MGState m, int l) {
-    const MGLevel F = m.lv[l], C = m.lv[l + 1];
+// Restriction F -> C at coarse cell ci: b_c = (sum of the fluid children's residuals) / 4.
+__device__ __forceinline__ void restrict_fp_cell(const MGLevel& F, const MGLevel& C, uint32_t ci, int3 c) {
     const uint32_t fdx = uint32_t(F.dim.x), fdxy = uint32_t(F.dim.x * F.dim.y);
     const uint32_t flast = F.cells - 1u;
-    for_footprint(d, C, l + 1, [&](uint32_t ci, int3 c) {
-        // Every child's word, b, x and neighbours are loaded before any of them is tested.
-        const uint32_t cw = C.word[ci];
-        float res[8];
-        uint32_t fl = 0u;
+    // Every child's word, b, x and neighbours are loaded before any of them is tested.
+    const uint32_t cw = C.word[ci];
+    float res[8];
+    uint32_t fl = 0u;
 #pragma unroll
-        for (int o = 0; o < 8; ++o) {
-            const int3 f = make_int3(c.x * 2 + (o & 1), c.y * 2 + ((o >> 1) & 1), c.z * 2 + ((o >> 2) & 1));
-            const bool in = inside3(f, F.dim);
-            const uint32_t fi = in ? lin3(f, F.dim) : 0u;
-            const uint32_t w = F.word[fi];
-            const float r = lv_ld(F.b, fi, F.prec) - (word_diag(w) * lv_ld(F.x, fi, F.prec) - word_sum_g(F.x, F.prec, w, fi, fdx, fdxy, flast));
-            res[o] = 0.0f;
-            if (in && (w & CW_FLUID)) {
-                fl |= 1u << o;
-                res[o] = r;
-            }
+    for (int o = 0; o < 8; ++o) {
+        const int3 f = make_int3(c.x * 2 + (o & 1), c.y * 2 + ((o >> 1) & 1), c.z * 2 + ((o >> 2) & 1));
+        const bool in = inside3(f, F.dim);
+        const uint32_t fi = in ? lin3(f, F.dim) : 0u;
+        const uint32_t w = F.word[fi];
+        const float r = lv_ld(F.b, fi, F.prec) - (word_diag(w) * lv_ld(F.x, fi, F.prec) - word_sum_g(F.x, F.prec, w, fi, fdx, fdxy, flast));
+        res[o] = 0.0f;
+        if (in && (w & CW_FLUID)) {
+            fl |= 1u << o;
+            res[o] = r;
         }
-        if (!(cw & CW_FLUID)) { lv_st(C.b, ci, C.prec, 0.0f); lv_st(C.x, ci, C.prec, 0.0f); return; }
-        float sum = 0.0f;
+    }
+    if (!(cw & CW_FLUID)) { lv_st(C.b, ci, C.prec, 0.0f); lv_st(C.x, ci, C.prec, 0.0f); return; }
+    float sum = 0.0f;
 #pragma unroll
-        for (int o = 0; o < 8; ++o)
-            if ((fl >> o) & 1u) sum = sum + res[o];
-        const float bb = 0.25f * sum;
-        lv_st(C.b, ci, C.prec, bb);
-        lv_st(C.x, ci, C.prec, (cw & CW_RED) ? bb / word_diag(cw) : 0.0f);
-    });
+    for (int o = 0; o < 8; ++o)
+        if ((fl >> o) & 1u) sum = sum + res[o];
+    const float bb = 0.25f * sum;
+    lv_st(C.b, ci, C.prec, bb);
+    lv_st(C.x, ci, C.prec, (cw & CW_RED) ? bb / word_diag(cw) : 0.0f);
 }
-// Prolongation l + 1 -> l fused with the black sweep of level l (see k_prolong_smooth0).
-__global__ void k_prolong_smooth_fp(Dev d, MGState m, int l) {
-    const MGLevel F = m.lv[l], C = m.lv[l + 1];
+// Prolongation C -> F fused with the black sweep of F (see k_prolong_smooth0) at fine cell i.
+__device__ __forceinline__ void prolong_smooth_fp_cell(const MGLevel& F, const MGLevel& C, uint32_t i, int3 c) {
     const uint32_t dx = uint32_t(F.dim.x), dxy = uint32_t(F.dim.x * F.dim.y);
     const uint32_t last = F.cells - 1u, clast = C.cells - 1u;
-    for_footprint(d, F, l, [&](uint32_t i, int3 c) {
-        // The neighbours' x and their parents' words and x are loaded before the word is tested
-        // (indices clamped into the levels; values of non-fluid neighbours are not used).
-        const uint32_t w = F.word[i];
-        const float b = lv_ld(F.b, i, F.prec);
-        const uint32_t off[6] = {i - 1u, i + 1u, i - dx, i + dx, i - dxy, i + dxy};
-        float v[6];
+    // The neighbours' x and their parents' words and x are loaded before the word is tested
+    // (indices clamped into the levels; values of non-fluid neighbours are not used).
+    const uint32_t w = F.word[i];
+    const float b = lv_ld(F.b, i, F.prec);
+    const uint32_t off[6] = {i - 1u, i + 1u, i - dx, i + dx, i - dxy, i + dxy};
+    float v[6];
 #pragma unroll
-        for (int n = 0; n < 6; ++n) {
-            const int3 nb = add3(c, nbr_off(n));
-            const uint32_t pi = min(lin3(make_int3(nb.x / 2, nb.y / 2, nb.z / 2), C.dim), clast);
-            const float xn = lv_ld(F.x, min(off[n], last), F.prec);
-            const uint32_t pw = C.word[pi];
-            const float px = lv_ld(C.x, pi, C.prec);
-            v[n] = (pw & CW_FLUID) ? q_prec(xn + px, F.prec) : xn;  // the prolonged value as it would be stored
-        }
-        if (!(w & CW_FLUID) || (w & CW_RED)) return;
-        float sum = 0.0f;
+    for (int n = 0; n < 6; ++n) {
+        const int3 nb = add3(c, nbr_off(n));
+        const uint32_t pi = min(lin3(make_int3(nb.x / 2, nb.y / 2, nb.z / 2), C.dim), clast);
+        const float xn = lv_ld(F.x, min(off[n], last), F.prec);
+        const uint32_t pw = C.word[pi];
+        const float px = lv_ld(C.x, pi, C.prec);
+        v[n] = (pw & CW_FLUID) ? q_prec(xn + px, F.prec) : xn;  // the prolonged value as it would be stored
+    }
+    if (!(w & CW_FLUID) || (w & CW_RED)) return;
+    float sum = 0.0f;
 #pragma unroll
-        for (int n = 0; n < 6; ++n)
-            if ((w >> n) & 1u) sum = sum + v[n];
-        lv_st(F.x, i, F.prec, (b + sum) / word_diag(w));
-    });
+    for (int n = 0; n < 6; ++n)
+        if ((w >> n) & 1u) sum = sum + v[n];
+    lv_st(F.x, i, F.prec, (b + sum) / word_diag(w));
+}
+
+__global__ void k_smooth_fp(Dev d, MGState m, int l, uint32_t parity) {
+    const MGLevel L = m.lv[l];
+    const uint32_t want = parity == 0u ? CW_RED : 0u;
+    for_footprint(d, L, l, [&](uint32_t i, int3) { smooth_fp_cell(L, i, want); });
+}
+// Restriction l -> l + 1 over level l + 1's footprint.
+__global__ void k_restrict_fp(Dev d, MGState m, int l) {
+    const MGLevel F = m.lv[l], C = m.lv[l + 1];
+    for_footprint(d, C, l + 1, [&](uint32_t ci, int3 c) { restrict_fp_cell(F, C, ci, c); });
+}
+// Prolongation l + 1 -> l fused with the black sweep of level l.
+__global__ void k_prolong_smooth_fp(Dev d, MGState m, int l) {
+    const MGLevel F = m.lv[l], C = m.lv[l + 1];
+    for_footprint(d, F, l, [&](uint32_t i, int3 c) { prolong_smooth_fp_cell(F, C, i, c); });
 }
 
 // ---- MGRestrictCS level 0 -> 1 over the 4^3 level-1 cells of every active brick (SparseCoarse) -----------
