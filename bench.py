@@ -54,6 +54,11 @@ def parse():
     # tanks_64: 64 independent tanks (32^3-128^3), LPT-partitioned over the ranks; each step is one frame of
     # every tank, overlapped on the device by slosh_step_frames, and the same frames are then timed sequentially
     ap.add_argument("--tanks", type=int, default=64)
+    # autotune the brick passes' CTAs per SM (slosh_autotune) during warm-up: candidates 2-16, one timed
+    # frame each; results do not depend on the choice
+    ap.add_argument("--autotune", action="store_true")
+    # fixed CTAs per SM of the brick passes (0: the library default)
+    ap.add_argument("--ctas-per-sm", type=int, default=0)
     return ap.parse_args()
 
 
@@ -233,9 +238,16 @@ def run_slosh(args):
     stream = torch.cuda.Stream()
     sim.set_stream(stream.cuda_stream)
     sim.set_emit_seed(sc["seed"])
+    if args.ctas_per_sm > 0:
+        sim.set_ctas_per_sm(args.ctas_per_sm)
     cols = sc.get("colliders", [])
     sim.step_frame(A.frame_input(sc["settings"], emits=sc["emits"], colliders=cols))  # scene creation (frame 1)
     fi = A.frame_input(sc["settings"], colliders=cols)
+    tuned = None
+    if args.autotune:
+        r = sim.autotune(fi, frames=1)
+        tuned = {"ctas_per_sm": int(r.best_ctas_per_sm), "brick_ctas": int(r.brick_ctas),
+                 "ms_per_substep": {int(r.ctas_per_sm[k]): round(float(r.ms_per_substep[k]), 4) for k in range(r.num_candidates)}}
     for _ in range(max(args.warmup, 3) - 1):
         sim.step_frame(fi)
     sim.enable_phase_timing(True)
@@ -306,7 +318,7 @@ def run_slosh(args):
         "config": {"workload": sc["name"], "grid": list(sc["settings"].grid_dim), "particles": n_particles,
                    "solver": "MGPCG" if args.solver == "mgpcg" else "RBGS omega 1.9 x200", "tolerance": 1e-6 if args.solver == "mgpcg" else None, "transfer": "APIC", "cfl": 1.0, "frame_dt": 1.0 / 120.0,
                    "sort_interval": 4, "parallelism": f"replicas{world}", "step": "one frame of CFL substeps",
-                   "mg_coarse_storage": args.precision,
+                   "mg_coarse_storage": args.precision, "autotune": tuned,
                    "l2": f"inputs larger than L2 (particles {48.0 * n_particles / 1e9:.2f} GB)"},
         "substeps": total_substeps,
         "particle_updates_per_s": total_substeps * n_particles / (dev_ms * 1e-3),
@@ -361,6 +373,12 @@ def run_tanks(args):
         streams.append(st)
     S.step_frames(sims, [A.frame_input(tanks[k]["settings"], emits=tanks[k]["emits"]) for k in mine])
     nxt = [A.frame_input(tanks[k]["settings"]) for k in mine]
+    tuned = None
+    if args.autotune:  # each tank alone, one timed frame per candidate
+        tuned = {}
+        for sim, fi in zip(sims, nxt):
+            r = sim.autotune(fi, frames=1)
+            tuned[int(r.best_ctas_per_sm)] = tuned.get(int(r.best_ctas_per_sm), 0) + 1
     for _ in range(max(args.warmup, 3) - 1):
         S.step_frames(sims, nxt)
 
@@ -430,6 +448,7 @@ def run_tanks(args):
             "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"tanks_{args.tanks}", "tanks": args.tanks, "particles": particles, "solver": "MGPCG",
+                       "autotune_ctas_per_sm_counts": tuned,
                        "tolerance": 1e-6, "step": "one frame of every tank", "parallelism": f"lpt{world}",
                        "l2": "inputs larger than L2 (1.3 GB of particles)"},
             "sequential": {"value": seq_total / (seq_dev_ms * 1e-3), "ms_per_step": seq_dev_ms / args.steps},

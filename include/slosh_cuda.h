@@ -313,6 +313,19 @@ SLOSH_API slosh_status slosh_step_frame(void* ctx, const slosh_frame_input_t* in
  * `count` independent contexts. All frames are enqueued on the contexts' own streams before any is
  * waited for, so small tanks overlap on the device. statuses (optional, count entries) receives each
  * context's frame status; the return value is the first non-OK one. */
+/* Autotuner of the brick passes' launch shape (extension): steps `frames` frames of `input` for each
+ * candidate number of CTAs per SM (2, 4, 8, 12, 16; capped at one CTA per pool brick), times them on the
+ * device and leaves the context on the fastest per substep. The simulation advances by those frames;
+ * results never depend on the shape (every brick pass is a grid-stride loop). Default: 8 per SM. */
+typedef struct slosh_autotune_result_t {
+    uint32_t num_candidates;
+    uint32_t ctas_per_sm[8];
+    float ms_per_substep[8];
+    uint32_t best_ctas_per_sm;
+    uint32_t brick_ctas;        /* the chosen grid of the brick passes */
+} slosh_autotune_result_t;
+SLOSH_API slosh_status slosh_autotune(void* ctx, const slosh_frame_input_t* input, uint32_t frames, slosh_autotune_result_t* out);
+SLOSH_API slosh_status slosh_set_ctas_per_sm(void* ctx, uint32_t ctas_per_sm);
 SLOSH_API slosh_status slosh_step_frames(void* const* ctxs, const slosh_frame_input_t* inputs, uint32_t count,
                                          slosh_status* statuses);
 /* Split form of slosh_step_frame for per-substep harnesses: begin_frame does the frame prologue

@@ -54,6 +54,8 @@ SIGNATURES = {
     "slosh_surface_params_default": ([C.POINTER(SurfaceParams)], None),
     "slosh_build_surface": ([_VP, C.POINTER(SurfaceParams), C.POINTER(SurfaceInfo)], C.c_int),
     "slosh_surface_device_ptrs": ([_VP, C.POINTER(_VP), C.POINTER(_VP), C.POINTER(_VP), C.POINTER(_VP), C.POINTER(_VP)], C.c_int),
+    "slosh_autotune": ([_VP, C.POINTER(FrameInput), C.c_uint32, C.POINTER(_abi.AutotuneResult)], C.c_int),
+    "slosh_set_ctas_per_sm": ([_VP, C.c_uint32], C.c_int),
     "slosh_unet_config_default": ([C.POINTER(_abi.UnetConfig)], None),
     "slosh_unet_create": ([C.POINTER(_abi.UnetConfig), C.c_int32, C.POINTER(_VP)], C.c_int),
     "slosh_unet_destroy": ([_VP], None),
@@ -254,6 +256,17 @@ class Simulation:
 
     def launch_count(self):
         return int(self._lib.slosh_launch_count(self._ctx))
+
+    # ---- launch-shape autotuner ----
+    def autotune(self, fi, frames=2):
+        """Times `frames` frames of fi per candidate CTAs-per-SM count of the brick passes and keeps the
+        fastest (slosh_autotune); the simulation advances by those frames. Returns the result struct."""
+        r = _abi.AutotuneResult()
+        _check(self._lib.slosh_autotune(self._ctx, C.byref(fi), int(frames), C.byref(r)))
+        return r
+
+    def set_ctas_per_sm(self, n):
+        _check(self._lib.slosh_set_ctas_per_sm(self._ctx, int(n)))
 
     def transfer_bytes(self):
         h2d, d2h = C.c_uint64(), C.c_uint64()

@@ -211,3 +211,9 @@ class ConvTest(C.Structure):
     _fields_ = [("dim", C.c_uint32 * 3), ("batch", C.c_uint32), ("nblocks", C.c_uint32), ("cin", C.c_uint32 * 2),
                 ("cout", C.c_uint32), ("x", C.c_void_p * 2), ("w", C.c_void_p), ("bias", C.c_void_p), ("dy", C.c_void_p),
                 ("y", C.c_void_p), ("dx", C.c_void_p * 2), ("dw", C.c_void_p), ("db", C.c_void_p)]
+
+
+class AutotuneResult(C.Structure):
+    """slosh_autotune_result_t: per candidate CTAs-per-SM count, the device ms per substep."""
+    _fields_ = [("num_candidates", C.c_uint32), ("ctas_per_sm", C.c_uint32 * 8), ("ms_per_substep", C.c_float * 8),
+                ("best_ctas_per_sm", C.c_uint32), ("brick_ctas", C.c_uint32)]

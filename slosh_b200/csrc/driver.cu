@@ -234,6 +234,24 @@ struct Ctx {
         for (void* p : v) cudaFree(p);
         v.clear();
     }
+    // CTAs of the brick passes: a multiple of the SM count, at most one per pool brick. The solve graphs
+    // hold the grid sizes, so a change re-captures them. Every brick pass is a grid-stride loop whose
+    // results do not depend on the grid size.
+    uint32_t ctas_per_sm = 8;
+    int brick_ctas_for(uint32_t per_sm) const {
+        return std::max(1, std::min<int>(int(num_pool_bricks > 1u ? num_pool_bricks - 1u : 1u), num_sms * int(per_sm)));
+    }
+    void set_ctas_per_sm(uint32_t per_sm) {
+        per_sm = std::max(1u, std::min(per_sm, 32u));
+        ctas_per_sm = per_sm;
+        if (!allocated) return;
+        const int bc = brick_ctas_for(per_sm);
+        if (bc != shape.brick_ctas) {
+            CK(cudaStreamSynchronize(stream));
+            destroy_graphs();
+            shape.brick_ctas = bc;
+        }
+    }
     void destroy_graphs() {
         for (auto& g : graphs) {
             if (g.exec) cudaGraphExecDestroy(g.exec);
@@ -397,9 +415,8 @@ struct Ctx {
         total_emitted = 0;
         prev_dt = 0.0f;
         last_max_speed = 0.0f;
-        int brick_ctas = std::max(1, std::min<int>(int(num_pool_bricks - 1u), num_sms * 8));
-        shape.brick_ctas = brick_ctas;
         shape.num_sms = num_sms;
+        shape.brick_ctas = brick_ctas_for(ctas_per_sm);
         allocated = true;
     }
     void zero_all() {
@@ -1217,6 +1234,73 @@ SLOSH_API slosh_status slosh_step_frame(void* ctx, const slosh_frame_input_t* in
         for (int s = 0; s < n; ++s) c->substep(s);
         c->end_frame();
         return frame_status(c);
+    });
+}
+
+// Autotuner of the brick-pass launch shape: steps `frames` frames of `input` per candidate CTAs-per-SM
+// count, times them on the device (events on the context's stream), and leaves the context on the
+// fastest per substep. The simulation advances by all these frames; results do not depend on the shape.
+SLOSH_API slosh_status slosh_autotune(void* ctx, const slosh_frame_input_t* input, uint32_t frames, slosh_autotune_result_t* out) {
+    return guarded([&]() -> slosh_status {
+        Ctx* c = as_ctx(ctx);
+        if (!input) throw StatusError{SLOSH_ERR_INVALID_ARG, "input is NULL"};
+        const uint32_t cand[] = {2u, 4u, 8u, 12u, 16u};
+        const uint32_t nc = uint32_t(sizeof(cand) / sizeof(cand[0]));
+        slosh_autotune_result_t r;
+        std::memset(&r, 0, sizeof(r));
+        cudaEvent_t e0, e1;
+        CK(cudaEventCreate(&e0));
+        CK(cudaEventCreate(&e1));
+        float best = 0.0f;
+        slosh_status worst = SLOSH_OK;
+        try {
+            for (uint32_t k = 0; k < nc; ++k) {
+                c->set_ctas_per_sm(cand[k]);
+                // one untimed frame captures the solve graphs of this shape
+                int n = c->begin_frame(*input);
+                for (int sidx = 0; sidx < n; ++sidx) c->substep(sidx);
+                c->end_frame();
+                CK(cudaEventRecord(e0, c->stream));
+                int substeps = 0;
+                for (uint32_t f = 0; f < std::max(frames, 1u); ++f) {
+                    n = c->begin_frame(*input);
+                    for (int sidx = 0; sidx < n; ++sidx) c->substep(sidx);
+                    c->end_frame();
+                    substeps += n;
+                    const slosh_status st = frame_status(c);
+                    if (st != SLOSH_OK && worst == SLOSH_OK) worst = st;
+                }
+                CK(cudaEventRecord(e1, c->stream));
+                CK(cudaEventSynchronize(e1));
+                float ms = 0.0f;
+                CK(cudaEventElapsedTime(&ms, e0, e1));
+                const float per = substeps > 0 ? ms / float(substeps) : ms;
+                r.ctas_per_sm[k] = cand[k];
+                r.ms_per_substep[k] = per;
+                if (k == 0 || per < best) {
+                    best = per;
+                    r.best_ctas_per_sm = cand[k];
+                }
+            }
+        } catch (...) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            throw;
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        r.num_candidates = nc;
+        c->set_ctas_per_sm(r.best_ctas_per_sm);
+        r.brick_ctas = uint32_t(c->shape.brick_ctas);
+        if (out) *out = r;
+        return worst == SLOSH_OK ? SLOSH_OK : worst;
+    });
+}
+SLOSH_API slosh_status slosh_set_ctas_per_sm(void* ctx, uint32_t ctas_per_sm) {
+    return guarded([&]() -> slosh_status {
+        if (ctas_per_sm == 0u) throw StatusError{SLOSH_ERR_INVALID_ARG, "ctas_per_sm must be positive"};
+        as_ctx(ctx)->set_ctas_per_sm(ctas_per_sm);
+        return SLOSH_OK;
     });
 }
 

@@ -170,3 +170,26 @@ def test_coarse_storage_precision(slosh, oracle_mod, mode, n):
     run_frames(g, o, sc, frames=2)
     r = g.results()
     assert r.last_solve_rel_residual <= 1e-6
+
+
+def test_launch_shape_does_not_change_results(slosh):
+    """The brick passes' grid size (CTAs per SM, chosen by slosh_autotune) changes only speed: a scene
+    stepped with 2 and with 16 CTAs per SM ends bit-identical; the autotuner reports every candidate
+    and keeps one of them."""
+    sc = scenes.dam_break_sphere(slosh.settings_default, n=96)
+    runs = []
+    for per_sm in (2, 16):
+        sim = slosh.Simulation(sc["settings"])
+        sim.set_emit_seed(sc["seed"])
+        sim.set_ctas_per_sm(per_sm)
+        sim.step_frame(A.frame_input(sc["settings"], emits=sc["emits"]))
+        for _ in range(2):
+            sim.step_frame(A.frame_input(sc["settings"]))
+        runs.append((sim.particles().view(np.uint32).copy(), sim.read("PRESSURE").view(np.uint32).copy()))
+        if per_sm == 16:
+            r = sim.autotune(A.frame_input(sc["settings"]), frames=1)
+            assert r.num_candidates == 5 and r.best_ctas_per_sm in list(r.ctas_per_sm)[:5]
+            assert all(r.ms_per_substep[k] > 0 for k in range(5))
+        sim.close()
+    assert np.array_equal(runs[0][0], runs[1][0])
+    assert np.array_equal(runs[0][1], runs[1][1])
