@@ -417,6 +417,7 @@ struct Ctx {
         last_max_speed = 0.0f;
         shape.num_sms = num_sms;
         shape.brick_ctas = brick_ctas_for(ctas_per_sm);
+        shape.mg_ctas = brick_ctas_for(4u);
         allocated = true;
     }
     void zero_all() {

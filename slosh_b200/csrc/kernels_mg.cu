@@ -1198,8 +1198,8 @@ int launch_mg_build_type(const Dev& d, const MGState& m, int l, cudaStream_t s) 
 }
 int launch_pcg_init(const Dev& d, const MGState& m, const float* p, const float* div, unsigned long long handle, const Shape& sh,
                     cudaStream_t s) {
-    k_pcg_words<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, m);
-    k_pcg_init<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, m, p, div, handle);
+    k_pcg_words<<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m);
+    k_pcg_init<<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m, p, div, handle);
     return 2;
 }
 
@@ -1223,7 +1223,7 @@ int launch_vcycle(const Dev& d, const MGState& m, int coarse_iterations, const S
     const int nl = m.num_levels;
     if (nl == 1) {
         k_coarse_solve0<<<1, 1024, 0, s>>>(d, m, coarse_iterations);
-        k_smooth0<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, m);
+        k_smooth0<<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m);
         return 2;
     }
     const int tail = mg_tail_level(m);
@@ -1234,10 +1234,10 @@ int launch_vcycle(const Dev& d, const MGState& m, int coarse_iterations, const S
         return int(std::max<uint64_t>(1, std::min<uint64_t>(uint64_t(sh.brick_ctas), (cells + 255u) / 256u)));
     };
     int n = 0;
-    k_smooth0_black<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, m);
+    k_smooth0_black<<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m);
     ++n;
     for (int l = 0; l < tail; ++l) {
-        if (l == 0) k_restrict0<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, m);
+        if (l == 0) k_restrict0<<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m);
         else k_restrict_fp<<<fp_blocks(l + 1), 256, 0, s>>>(d, m, l);
         ++n;
         if (l + 1 < tail) {  // the tail kernel does its own first smoothing sweep
@@ -1249,8 +1249,8 @@ int launch_vcycle(const Dev& d, const MGState& m, int coarse_iterations, const S
     ++n;
     for (int l = tail - 1; l >= 0; --l) {
         if (l == 0) {
-            k_prolong_smooth0<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, m);
-            k_smooth0<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, m);
+            k_prolong_smooth0<<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m);
+            k_smooth0<<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m);
         } else {
             k_prolong_smooth_fp<<<fp_blocks(l), 256, 0, s>>>(d, m, l);
             k_smooth_fp<<<fp_blocks(l), 256, 0, s>>>(d, m, l, 0u);
@@ -1260,16 +1260,16 @@ int launch_vcycle(const Dev& d, const MGState& m, int coarse_iterations, const S
     return n;
 }
 int launch_pcg_apply_a(const Dev& d, const MGState& m, const Shape& sh, cudaStream_t s) {
-    k_apply_a<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, m);
+    k_apply_a<<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m);
     return 1;
 }
 int launch_pcg_update_pr(const Dev& d, const MGState& m, float* p, unsigned long long handle, const Shape& sh, cudaStream_t s) {
-    k_update_pr<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, m, p, handle);
+    k_update_pr<<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m, p, handle);
     return 1;
 }
 int launch_pcg_update_d(const Dev&, const MGState&, const Shape&, cudaStream_t) { return 0; }  // fused into ApplyA
 int launch_true_residual(const Dev& d, const MGState& m, const float* p, const float* div, const Shape& sh, cudaStream_t s) {
-    k_true_residual<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, m, p, div);
+    k_true_residual<<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m, p, div);
     return 1;
 }
 
