@@ -28,7 +28,6 @@ namespace unet {
 
 typedef __nv_bfloat16 bf16;
 
-constexpr int CONV_STAGES = 4;
 constexpr int WGRAD_STAGES = 4;
 constexpr uint32_t IN_CHANNELS = 16;  // divergence, fluid, solid, zero padding to the MMA's K of 16
 

@@ -107,3 +107,35 @@ def test_network_bf16_storage_is_close_to_exact():
     assert abs(l1 - l2) <= 0.01 * l2
     assert np.linalg.norm(g1 - g2) <= 0.25 * np.linalg.norm(g2)
     assert float(g1 @ g2) >= 0.95 * np.linalg.norm(g1) * np.linalg.norm(g2)
+
+
+def test_shipped_weights_match_the_layout():
+    """The trained weights in the package have the network's parameter count, finite values, and BF16-
+    rounded convolution weights exactly where the oracle's layout puts them."""
+    from slosh_b200 import train_warmstart as TW
+    lay, head_off, n = U.layout()
+    path = os.path.join(os.path.dirname(__file__), "..", "slosh_b200", "warmstart_128.npz")
+    p = TW.load_weights(path)
+    assert p.shape == (n,) and np.all(np.isfinite(p))
+    mask = TW.conv_weight_mask(n)
+    want = np.zeros(n, bool)
+    for (w_off, b_off, cout, cins) in lay:
+        want[w_off:b_off] = True
+    assert np.array_equal(mask, want)
+    assert np.array_equal(U.bf16(p[mask]), p[mask])
+
+
+def test_random_scenes_are_seeded():
+    """The warm-start scene generator is a pure function of its seed (held-out seeds never repeat training
+    ones), with 1-4 boxes inside the domain and 0-3 spheres."""
+    import slosh_b200 as S
+    from slosh_b200 import warmstart as W
+    a = W.random_scene(S.settings_default, 10001, 128)
+    b = W.random_scene(S.settings_default, 10001, 128)
+    assert [list(e.cell_min) + list(e.cell_dims) + list(e.velocity) for e in a[1]] == \
+           [list(e.cell_min) + list(e.cell_dims) + list(e.velocity) for e in b[1]]
+    for seed in range(10000, 10040):
+        s, emits, cols = W.random_scene(S.settings_default, seed, 128)
+        assert 1 <= len(emits) <= 4 and 0 <= len(cols) <= 3
+        for e in emits:
+            assert min(e.cell_min) >= 1 and all(m + d <= 127 for m, d in zip(e.cell_min, e.cell_dims))
