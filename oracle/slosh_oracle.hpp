@@ -1,5 +1,6 @@
 // TEST INFRASTRUCTURE -- not part of the product. Only tests/, __graft_entry__.smoke() and the
-// cpu_baseline leg of bench.py load this code, and only as the checker.
+// cpu_baseline leg of bench.py load this code, and only as the reference the GPU results are compared
+// with (or, in bench.py, as the timed CPU baseline).
 //
 // CPU oracle of the Slosh FLIP/APIC simulation substep: a statement-by-statement restatement of the
 // reference's HLSL kernels and of the C++ schedule that dispatches them (paths relative to the

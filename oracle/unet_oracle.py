@@ -1,5 +1,5 @@
-"""CPU oracle of the learned warm-start network (test infrastructure only: the tests import it as
-the checker; nothing in the product path calls it).
+"""CPU oracle of the learned warm-start network (test infrastructure only: the tests and smoke() compare
+the GPU results with it; nothing in the product path calls it).
 
 A numpy restatement of the U-Net the library trains and runs on the GPU (slosh_b200/csrc/unet.cu):
 the same layers, parameter layout and BF16 storage points, with FP64 accumulation. The network is
