@@ -1,7 +1,7 @@
 """TEST INFRASTRUCTURE -- Python handle on the CPU oracle (liboracle.so, built from slosh_oracle.hpp).
 
-Only tests/, __graft_entry__.smoke() and the cpu_baseline leg of bench.py use this module, as the
-checker. Its calls mirror the product's C ABI so a parity test drives both sides the same way.
+Only tests/, __graft_entry__.smoke() and the cpu_baseline leg of bench.py use this module: as the
+reference the GPU results are compared with, or as the timed CPU baseline. Its calls mirror the product's C ABI so a parity test drives both sides the same way.
 """
 import ctypes as C
 import os
