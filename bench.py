@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--autotune", action="store_true")
     # fixed CTAs per SM of the brick passes (0: the library default)
     ap.add_argument("--ctas-per-sm", type=int, default=0)
+    # fixed CTAs per SM of the level-0 MGPCG passes (0: the library default)
+    ap.add_argument("--mg-ctas-per-sm", type=int, default=0)
     return ap.parse_args()
 
 
@@ -240,6 +242,8 @@ def run_slosh(args):
     sim.set_emit_seed(sc["seed"])
     if args.ctas_per_sm > 0:
         sim.set_ctas_per_sm(args.ctas_per_sm)
+    if args.mg_ctas_per_sm > 0:
+        sim.set_mg_ctas_per_sm(args.mg_ctas_per_sm)
     cols = sc.get("colliders", [])
     sim.step_frame(A.frame_input(sc["settings"], emits=sc["emits"], colliders=cols))  # scene creation (frame 1)
     fi = A.frame_input(sc["settings"], colliders=cols)

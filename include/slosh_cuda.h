@@ -326,6 +326,8 @@ typedef struct slosh_autotune_result_t {
 } slosh_autotune_result_t;
 SLOSH_API slosh_status slosh_autotune(void* ctx, const slosh_frame_input_t* input, uint32_t frames, slosh_autotune_result_t* out);
 SLOSH_API slosh_status slosh_set_ctas_per_sm(void* ctx, uint32_t ctas_per_sm);
+/* CTAs per SM of the level-0 MGPCG passes (one warp per brick; default 3); results do not depend on it. */
+SLOSH_API slosh_status slosh_set_mg_ctas_per_sm(void* ctx, uint32_t ctas_per_sm);
 SLOSH_API slosh_status slosh_step_frames(void* const* ctxs, const slosh_frame_input_t* inputs, uint32_t count,
                                          slosh_status* statuses);
 /* Split form of slosh_step_frame for per-substep harnesses: begin_frame does the frame prologue

@@ -56,6 +56,7 @@ SIGNATURES = {
     "slosh_surface_device_ptrs": ([_VP, C.POINTER(_VP), C.POINTER(_VP), C.POINTER(_VP), C.POINTER(_VP), C.POINTER(_VP)], C.c_int),
     "slosh_autotune": ([_VP, C.POINTER(FrameInput), C.c_uint32, C.POINTER(_abi.AutotuneResult)], C.c_int),
     "slosh_set_ctas_per_sm": ([_VP, C.c_uint32], C.c_int),
+    "slosh_set_mg_ctas_per_sm": ([_VP, C.c_uint32], C.c_int),
     "slosh_unet_config_default": ([C.POINTER(_abi.UnetConfig)], None),
     "slosh_unet_create": ([C.POINTER(_abi.UnetConfig), C.c_int32, C.POINTER(_VP)], C.c_int),
     "slosh_unet_destroy": ([_VP], None),
@@ -267,6 +268,9 @@ class Simulation:
 
     def set_ctas_per_sm(self, n):
         _check(self._lib.slosh_set_ctas_per_sm(self._ctx, int(n)))
+
+    def set_mg_ctas_per_sm(self, n):
+        _check(self._lib.slosh_set_mg_ctas_per_sm(self._ctx, int(n)))
 
     def transfer_bytes(self):
         h2d, d2h = C.c_uint64(), C.c_uint64()

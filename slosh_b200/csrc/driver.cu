@@ -241,6 +241,18 @@ struct Ctx {
     int brick_ctas_for(uint32_t per_sm) const {
         return std::max(1, std::min<int>(int(num_pool_bricks > 1u ? num_pool_bricks - 1u : 1u), num_sms * int(per_sm)));
     }
+    uint32_t mg_ctas_per_sm = 3;  // = the CTAs of these 80-register kernels resident per SM: one wave
+    void set_mg_ctas_per_sm(uint32_t per_sm) {
+        per_sm = std::max(1u, std::min(per_sm, 32u));
+        mg_ctas_per_sm = per_sm;
+        if (!allocated) return;
+        const int bc = brick_ctas_for(per_sm);
+        if (bc != shape.mg_ctas) {
+            CK(cudaStreamSynchronize(stream));
+            destroy_graphs();
+            shape.mg_ctas = bc;
+        }
+    }
     void set_ctas_per_sm(uint32_t per_sm) {
         per_sm = std::max(1u, std::min(per_sm, 32u));
         ctas_per_sm = per_sm;
@@ -417,7 +429,7 @@ struct Ctx {
         last_max_speed = 0.0f;
         shape.num_sms = num_sms;
         shape.brick_ctas = brick_ctas_for(ctas_per_sm);
-        shape.mg_ctas = brick_ctas_for(4u);
+        shape.mg_ctas = brick_ctas_for(mg_ctas_per_sm);
         allocated = true;
     }
     void zero_all() {
@@ -1295,6 +1307,13 @@ SLOSH_API slosh_status slosh_autotune(void* ctx, const slosh_frame_input_t* inpu
         r.brick_ctas = uint32_t(c->shape.brick_ctas);
         if (out) *out = r;
         return worst == SLOSH_OK ? SLOSH_OK : worst;
+    });
+}
+SLOSH_API slosh_status slosh_set_mg_ctas_per_sm(void* ctx, uint32_t ctas_per_sm) {
+    return guarded([&]() -> slosh_status {
+        if (ctas_per_sm == 0u) throw StatusError{SLOSH_ERR_INVALID_ARG, "ctas_per_sm must be positive"};
+        as_ctx(ctx)->set_mg_ctas_per_sm(ctas_per_sm);
+        return SLOSH_OK;
     });
 }
 SLOSH_API slosh_status slosh_set_ctas_per_sm(void* ctx, uint32_t ctas_per_sm) {

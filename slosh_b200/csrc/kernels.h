@@ -13,7 +13,7 @@ namespace slosh {
 // shape never depends on the (device-resident) active count.
 struct Shape {
     int brick_ctas;     // CTAs of a brick pass (multiple of the SM count)
-    int mg_ctas;        // CTAs of the level-0 MGPCG passes (one warp per brick; 4 per SM measured best)
+    int mg_ctas;        // CTAs of the level-0 MGPCG passes (one warp per brick; 3 per SM measured best)
     int particle_ctas;  // upper bound for particle passes is computed per call
     int num_sms;
 };
