@@ -424,6 +424,9 @@ struct Ctx {
         for (uint32_t sl = 1; sl <= pool_slots; ++sl) free_init[sl] = sl;
         CK(cudaMemcpy(free_slots, free_init.data(), sizeof(uint32_t) * num_pool_bricks, cudaMemcpyHostToDevice));
         CK(cudaMemset(slot_brick, 0xFF, sizeof(uint32_t) * num_pool_bricks));
+        // The clears above run on the legacy default stream, which the context's non-blocking streams do
+        // not wait for: finish them before any frame work is issued.
+        CK(cudaDeviceSynchronize());
         total_emitted = 0;
         prev_dt = 0.0f;
         last_max_speed = 0.0f;
@@ -478,6 +481,7 @@ struct Ctx {
         CK(cudaMemset(particles[0], 0, size_t(cap) * sizeof(slosh_particle_t)));
         if (num_particles)
             CK(cudaMemcpy(particles[0], keep.data(), sizeof(slosh_particle_t) * num_particles, cudaMemcpyHostToDevice));
+        CK(cudaDeviceSynchronize());  // the clear (default stream) before the frame's emission (context stream)
     }
 
     Dev dev() const {

@@ -242,6 +242,8 @@ struct Net {
         head_grad = dmalloc<float>(18);
         energy = dmalloc<double>(2u * 592u);
         beta = dmalloc<float>(1);
+        // dmalloc clears on the legacy default stream, which `stream` (non-blocking) does not wait for
+        UCK(cudaDeviceSynchronize());
         init_params();
     }
     ~Net() {
@@ -422,7 +424,8 @@ struct Net {
         uint32_t e = 0;
         UCK(cudaMemcpy(&e, error, 4, cudaMemcpyDeviceToHost));
         if (e) {
-            UCK(cudaMemset(error, 0, 4));
+            UCK(cudaMemsetAsync(error, 0, 4, stream));
+            UCK(cudaStreamSynchronize(stream));
             throw std::runtime_error("tensor-core pipeline wait timed out (error bits " + std::to_string(e) + ")");
         }
     }
@@ -611,7 +614,7 @@ SLOSH_API slosh_status slosh_unet_conv_test(const slosh_conv_test_t* t) {
         auto alloc = [&](size_t bytes) {
             void* p = nullptr;
             UCK(cudaMalloc(&p, bytes + 16));
-            UCK(cudaMemset(p, 0, bytes + 16));
+            UCK(cudaMemsetAsync(p, 0, bytes + 16, s));  // on the work stream, so it is ordered before the uploads
             owned.push_back(p);
             return p;
         };
