@@ -659,15 +659,7 @@ uint32_t tmem_cols_host(uint32_t n) { return n <= 32u ? 32u : (n <= 64u ? 64u : 
 
 }  // namespace
 
-size_t conv_smem_bytes(uint32_t cb_max, uint32_t n) {
-    const size_t a_region = 256u * cb_max;
-    const size_t b_region = (size_t(n) * cb_max * 2u + 1023u) / 1024u * 1024u;
-    size_t stages = (48u * 1024u) / (a_region + b_region);
-    stages = stages < 3u ? 3u : (stages > size_t(CONV_MAX_STAGES) ? size_t(CONV_MAX_STAGES) : stages);
-    return stages * (a_region + b_region) + 1024u;
-}
-size_t wgrad_smem_bytes(uint32_t c, uint32_t n) {
-    (void)c;
+static size_t wgrad_smem_bytes(uint32_t n) {
     const size_t a_region = 128u * 128u * 2u;  // T taps x 128 rows x c channels, T c = 128
     const size_t b_region = (256u * size_t(n) + 1023u) / 1024u * 1024u;
     return WGRAD_STAGES * (a_region + b_region) + 1024u;
@@ -707,7 +699,7 @@ int launch_conv(const ConvArgs& a, cudaStream_t s) {
 int launch_wgrad(const WgradArgs& a, uint32_t chunks, cudaStream_t s) {
     const uint32_t a_region = 128u * 128u * 2u;
     const uint32_t b_region = (256u * a.n + 1023u) / 1024u * 1024u;
-    const size_t smem = wgrad_smem_bytes(a.c, a.n);
+    const size_t smem = wgrad_smem_bytes(a.n);
     static bool configured = false;
     if (!configured) {
         cudaFuncSetAttribute(k_wgrad, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
@@ -753,7 +745,7 @@ int launch_upsample_bwd(const bf16* gout, bf16* gin, Vol f, uint32_t c, const bf
     return 1;
 }
 int launch_head(const bf16* d0, const bf16* input, const float* head_w, float* out, const float* target, const uint32_t* nfluid,
-                bf16* g_d0, float* partial, uint32_t chunks, float* head_grad, float* loss, uint64_t voxels, cudaStream_t s) {
+                bf16* g_d0, float* partial, uint32_t chunks, float* head_grad, uint64_t voxels, cudaStream_t s) {
     const uint64_t per = (voxels + chunks - 1u) / chunks;
     k_head<<<chunks, HEAD_THREADS, 0, s>>>(d0, input, head_w, out, target, nfluid, g_d0, partial, voxels, per);
     if (!target) return 1;

@@ -313,7 +313,7 @@ struct Net {
             after_conv(i);
         }
         launches += launch_head(T[size_t(t_d0)].act, T[size_t(t_in)].act, params + head_off, guess, nullptr, nullptr, nullptr, nullptr,
-                                head_chunks, nullptr, nullptr, vol[0].voxels(), stream);
+                                head_chunks, nullptr, vol[0].voxels(), stream);
     }
     // The resampling step that follows convolution i in the forward order.
     void after_conv(size_t i) {
@@ -381,7 +381,7 @@ struct Net {
     float backward_and_grads() {
         UCK(cudaMemsetAsync(grads, 0, num_params * 4, stream));
         launches += launch_head(T[size_t(t_d0)].act, T[size_t(t_in)].act, params + head_off, guess, target, nfluid, T[size_t(t_d0)].grad,
-                                hpartial, head_chunks, head_grad, nullptr, vol[0].voxels(), stream);
+                                hpartial, head_chunks, head_grad, vol[0].voxels(), stream);
         UCK(cudaMemcpyAsync(grads + head_off, head_grad, 17 * 4, cudaMemcpyDeviceToDevice, stream));
         const uint32_t wr[2] = {0u, 0u};
         // convolutions in reverse; the gradient of every ReLU tensor is masked by its last contribution

@@ -5,12 +5,13 @@
 // 16, 32 or 64 per tensor (a 128-channel convolution input is two tensors, a "K-block" each).
 //
 // Kernel forms (kernels_unet.cu):
-//   k_conv3d   implicit-GEMM 3x3x3 convolution, stride 1, zero padding 1: a CTA computes 128 output
-//              voxels x N channels; per (tap, K-block) TMA loads the 128 shifted input rows and the
-//              tap's N x C weights into swizzled shared memory and one thread issues tcgen05.mma
-//              (M = 128, K = 16) into a TMEM accumulator; the epilogue adds the bias, applies ReLU,
-//              splits the channels over one or two output tensors, optionally adds to them and masks
-//              them (ReLU backward). With flipped, transposed weights it is also the data gradient.
+//   k_conv3d   implicit-GEMM 3x3x3 convolution, stride 1, zero padding 1, persistent: a CTA takes
+//              tiles of 128 output voxels x N channels in turn; per (tap, K-block) TMA loads the 128
+//              shifted input rows and the tap's N x C weights into swizzled shared memory and one
+//              thread issues tcgen05.mma (M = 128, K = 16) into one of two TMEM accumulators; four
+//              epilogue warps add the bias, apply ReLU, split the channels over one or two output
+//              tensors, optionally add to them and mask them (ReLU backward) while the next tile's
+//              loads and MMAs run. With flipped, transposed weights it is also the data gradient.
 //   k_wgrad    weight gradient dW[tap][n][c] = sum_v X[v + tap][c] dZ[v][n] as tcgen05.mma with both
 //              operands MN-major: M = 128 rows are (tap, c) pairs of 128 / C taps, N = output
 //              channels, K = 128 voxels per stage; per-chunk partials are summed in chunk order.
@@ -67,8 +68,6 @@ struct alignas(64) WgradArgs {
     uint32_t* error;
 };
 
-size_t conv_smem_bytes(uint32_t cb_max, uint32_t n);
-size_t wgrad_smem_bytes(uint32_t c, uint32_t n);
 int launch_conv(const ConvArgs& a, cudaStream_t s);
 int launch_wgrad(const WgradArgs& a, uint32_t chunks, cudaStream_t s);
 int launch_reduce_chunks(const float* partial, float* out, uint32_t chunks, uint32_t count, cudaStream_t s);
@@ -83,7 +82,7 @@ int launch_upsample_bwd(const bf16* gout, bf16* gin, Vol fine, uint32_t c, const
 // the head's gradients and the gradient of the decoder tensor (ReLU-masked): head_grad[0..16] =
 // d loss / d (w0..w15, bias), head_grad[17] = the loss.
 int launch_head(const bf16* d0, const bf16* input, const float* head_w, float* out, const float* target, const uint32_t* nfluid,
-                bf16* g_d0, float* partial, uint32_t chunks, float* head_grad, float* loss, uint64_t voxels, cudaStream_t s);
+                bf16* g_d0, float* partial, uint32_t chunks, float* head_grad, uint64_t voxels, cudaStream_t s);
 int launch_adam(float* p, const float* g, float* m, float* v, uint64_t count, float lr, float b1, float b2, float eps, float c1,
                 float c2, cudaStream_t s);
 // BF16 weight copies of one convolution from its FP32 master [27][n][cin]: the forward K-blocks
