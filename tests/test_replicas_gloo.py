@@ -75,7 +75,9 @@ def _tanks_main(rank, world, port, queue):
     plan = lpt_partition(costs, world)
     mine = [(i, 10 + i, 20 + rank, 100 * i) for i in plan[rank]]
     rows = gather_tank_stats(mine)
-    queue.put((rank, plan, rows))
+    # the benchmark's rows carry two more columns (batched and sequential substep latency)
+    wide = gather_tank_stats([(i, 10 + i, 20 + rank, 100 * i, 0.5 + i, 0.25 * (rank + 1)) for i in plan[rank]], width=6)
+    queue.put((rank, plan, rows, wide))
     dist.barrier()
     dist.destroy_process_group()
 
@@ -102,9 +104,12 @@ def test_two_rank_tank_batch_stats():
         p.join(timeout=180)
         assert p.exitcode == 0
     out = sorted(q.get(timeout=5) for _ in range(2))
-    (_, plan0, rows0), (_, plan1, rows1) = out
+    (_, plan0, rows0, wide0), (_, plan1, rows1, wide1) = out
     assert plan0 == plan1
     assert rows0 == rows1
+    assert wide0 == wide1 and all(len(r) == 6 for r in wide0)
+    assert [int(r[0]) for r in wide0] == list(range(7))
+    assert all(r[4] == 0.5 + r[0] and r[5] == 0.25 * (int(r[2]) - 19) for r in wide0)
     assert [int(r[0]) for r in rows0] == list(range(7))
     owner = {i: r for r, p in enumerate(plan0) for i in p}
     assert all(int(row[2]) == 20 + owner[int(row[0])] for row in rows0)
