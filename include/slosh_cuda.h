@@ -346,10 +346,15 @@ SLOSH_API slosh_status slosh_sort_particles(void* ctx);
  * the current device, enqueued on cuda_stream (NULL = default stream) without waiting for it.
  * Scratch is one static device array per device, sized for SLOSH_STATIC_SORT_MAX_PARTICLES particles
  * and SLOSH_STATIC_SORT_MAX_KEYS sort keys (grids up to 256^3); larger inputs return
- * SLOSH_ERR_CAPACITY. The first call on a device resolves that array's address (make it before any
- * stream capture starts on the device). Overlapping calls on one device race on the shared scratch:
- * order them. particles_out must not alias particles_in; perm_out (count words), key_offsets_out
- * (sort-key count words) and live_count_out (1 word) are optional device outputs. */
+ * SLOSH_ERR_CAPACITY. The array's address differs per CUDA context; each call looks up the current
+ * context's and resolves it on the first call in that context. That first call also loads the library's
+ * device code into the context if CUDA has not loaded it yet (lazy module loading is the default), which
+ * commits about 7.4 MB of device memory for the scratch, and it is the only call that allocates: make it
+ * at start-up, before any stream capture begins in that context (CUDA_MODULE_LOADING=EAGER moves the
+ * load to context creation). Once loaded, the scratch stays resident on that device until the process
+ * exits. Overlapping calls on one device race on the shared scratch: order them. particles_out must not
+ * alias particles_in; perm_out (count words), key_offsets_out (sort-key count words) and live_count_out
+ * (1 word) are optional device outputs. */
 #define SLOSH_STATIC_SORT_MAX_PARTICLES 262144u
 #define SLOSH_STATIC_SORT_MAX_KEYS (262144u + 1u)
 SLOSH_API slosh_status slosh_sort_particles_static(const slosh_particle_t* particles_in, slosh_particle_t* particles_out,

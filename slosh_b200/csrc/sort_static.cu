@@ -15,10 +15,16 @@
 //   * a tool that re-sorts a particle snapshot without creating a simulation context (whose creation
 //     allocates the whole brick pool).
 //
-// Set-up: the first call on a device resolves the scratch's address on that device with
-// cudaGetSymbolAddress (which loads this library's device code there if it is not loaded yet) and caches
-// it; every later call on that device reuses the cached pointer. Make the first call on each device
-// before any stream capture starts on it.
+// Set-up: a __device__ array has its own address in every CUDA context, so the address is resolved per
+// context. Each call looks up the current context's unique ID (cuCtxGetId, fetched through
+// cudaGetDriverEntryPoint, so the library needs no link against the driver library) in a small cache; on a
+// miss it resolves the array's address with cudaGetSymbolAddress in that context and caches it. A host that
+// runs in its own context (cuCtxCreate, an engine's or a green context), or that resets a device and starts
+// again, therefore gets the address of its current context, never a stale one. The first call in a context
+// also loads this library's device code there if it is not loaded yet (CUDA loads modules lazily by default),
+// which commits the static scratch and the code on that device: that first call allocates, every later one
+// does not. Make it during start-up, before any stream capture begins in that context; with
+// CUDA_MODULE_LOADING=EAGER the load happens when the context is created instead.
 //
 // Races: there is one scratch per device. Calls that overlap on a device -- two streams, or two host
 // threads, with nothing ordering them -- race on it and corrupt each other's results. Issue them on one
@@ -26,6 +32,8 @@
 //
 // What must start at zero: only the per-key counts, which launch_sort clears on the stream at the start of
 // every call; every other scratch word is written before it is read within the call.
+#include <cuda.h>  // CUcontext and CUresult only: the driver calls are fetched at run time
+
 #include <cmath>
 #include <cstdio>
 #include <mutex>
@@ -53,24 +61,71 @@ constexpr size_t kScratchWords = 5 * kParticleWords + 2 * kKeyWords + kTileHistW
 
 static __device__ __align__(256) uint32_t g_sort_scratch[kScratchWords];
 
-constexpr int kMaxDevices = 64;
+// Scratch addresses per CUDA context, keyed by the context's process-unique ID (IDs are never reused, so an
+// entry can go stale only by its context being destroyed, and then no call can run in it again).
+struct ScratchEntry {
+    unsigned long long context_id;
+    uint32_t* ptr;
+};
+constexpr size_t kMaxCachedContexts = 64;
 std::mutex g_setup_mutex;
-uint32_t* g_scratch_ptr[kMaxDevices] = {};
+ScratchEntry g_scratch_cache[kMaxCachedContexts] = {};
+size_t g_scratch_entries = 0, g_scratch_next = 0;  // filled entries; next slot to overwrite when full
 
-// Address of g_sort_scratch on the current device, resolved once per device.
-cudaError_t scratch_on_current_device(uint32_t** out) {
-    int device = 0;
-    cudaError_t e = cudaGetDevice(&device);
-    if (e != cudaSuccess) return e;
-    if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
+using CtxGetCurrentFn = CUresult(CUDAAPI*)(CUcontext*);
+using CtxGetIdFn = CUresult(CUDAAPI*)(CUcontext, unsigned long long*);
+CtxGetCurrentFn g_ctx_get_current = nullptr;
+CtxGetIdFn g_ctx_get_id = nullptr;
+
+// ID of the context current on this thread, or 0 when none is current. Call with g_setup_mutex held.
+cudaError_t current_context_id(unsigned long long* id) {
+    *id = 0;
+    if (!g_ctx_get_current || !g_ctx_get_id) {
+        void* f0 = nullptr;
+        void* f1 = nullptr;
+        cudaDriverEntryPointQueryResult q0 = cudaDriverEntryPointSymbolNotFound, q1 = cudaDriverEntryPointSymbolNotFound;
+        cudaError_t e = cudaGetDriverEntryPoint("cuCtxGetCurrent", &f0, cudaEnableDefault, &q0);
+        if (e != cudaSuccess) return e;
+        e = cudaGetDriverEntryPoint("cuCtxGetId", &f1, cudaEnableDefault, &q1);
+        if (e != cudaSuccess) return e;
+        if (q0 != cudaDriverEntryPointSuccess || q1 != cudaDriverEntryPointSuccess || !f0 || !f1) return cudaErrorSymbolNotFound;
+        g_ctx_get_current = reinterpret_cast<CtxGetCurrentFn>(f0);
+        g_ctx_get_id = reinterpret_cast<CtxGetIdFn>(f1);
+    }
+    CUcontext ctx = nullptr;
+    if (g_ctx_get_current(&ctx) != CUDA_SUCCESS) return cudaErrorDeviceUninitialized;
+    if (!ctx) return cudaSuccess;
+    if (g_ctx_get_id(ctx, id) != CUDA_SUCCESS) return cudaErrorDeviceUninitialized;
+    return cudaSuccess;
+}
+
+// Address of g_sort_scratch in the current context, resolved once per context.
+cudaError_t scratch_in_current_context(uint32_t** out) {
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_ptr[device]) {
-        void* p = nullptr;
+    unsigned long long id = 0;
+    cudaError_t e = current_context_id(&id);
+    if (e != cudaSuccess) return e;
+    void* p = nullptr;
+    if (id == 0) {
+        // No context is current yet: resolving the symbol makes the current device's primary context current.
         e = cudaGetSymbolAddress(&p, g_sort_scratch);
         if (e != cudaSuccess) return e;
-        g_scratch_ptr[device] = static_cast<uint32_t*>(p);
+        e = current_context_id(&id);
+        if (e != cudaSuccess) return e;
+        if (id == 0) return cudaErrorDeviceUninitialized;
     }
-    *out = g_scratch_ptr[device];
+    for (size_t k = 0; k < g_scratch_entries; ++k)
+        if (g_scratch_cache[k].context_id == id) {
+            *out = g_scratch_cache[k].ptr;
+            return cudaSuccess;
+        }
+    if (!p) {
+        e = cudaGetSymbolAddress(&p, g_sort_scratch);
+        if (e != cudaSuccess) return e;
+    }
+    const size_t k = g_scratch_entries < kMaxCachedContexts ? g_scratch_entries++ : (g_scratch_next++ % kMaxCachedContexts);
+    g_scratch_cache[k] = ScratchEntry{id, static_cast<uint32_t*>(p)};
+    *out = g_scratch_cache[k].ptr;
     return cudaSuccess;
 }
 
@@ -130,8 +185,8 @@ SLOSH_API slosh_status slosh_sort_particles_static(const slosh_particle_t* parti
             return fail(SLOSH_ERR_INVALID_ARG, std::string(fn) + names[k] + " is not device memory of the current device");
 
     uint32_t* base = nullptr;
-    e = scratch_on_current_device(&base);
-    if (e != cudaSuccess) return fail(SLOSH_ERR_CUDA, std::string(fn) + "cudaGetSymbolAddress: " + cudaGetErrorString(e));
+    e = scratch_in_current_context(&base);
+    if (e != cudaSuccess) return fail(SLOSH_ERR_CUDA, std::string(fn) + "resolving the static scratch: " + cudaGetErrorString(e));
 
     SortBuffers b{};
     uint32_t* w = base;

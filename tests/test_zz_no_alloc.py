@@ -4,7 +4,10 @@ It must give exactly what the context's sort (slosh_sort_particles) gives on the
 sorted records, permutation, per-key offsets and live count, all integer or copied bytes, so the bar
 is bit-exact -- on two calls in a row (the second smaller than the first, so stale scratch from the
 first call would show), and it must refuse inputs above its static scratch size before touching the
-device. This file is collected last so that the GPU test also runs after every other test."""
+device. Calls after the first in a context must not allocate device memory: neither the device's free
+memory nor torch's allocator may change across them. With the optional outputs left NULL the scratch
+stands in for them, and an empty input gives a live count of 0. This file is collected last so that
+the GPU test also runs after every other test."""
 import ctypes as C
 
 import numpy as np
@@ -65,7 +68,11 @@ def test_static_sort_matches_context_sort(slosh):
     d_off = torch.empty(num_keys, dtype=torch.int32, device=dev)
     d_live = torch.empty(1, dtype=torch.int32, device=dev)
     stream = torch.cuda.current_stream(dev)
-    for seed, n in ((11, n_max), (12, 70001)):
+
+    def sort_static(n, perm, off, live):
+        slosh.sort_particles_static(d_in.data_ptr(), d_out.data_ptr(), n, GRID, CELL, perm, off, live, stream.cuda_stream)
+
+    for call, (seed, n) in enumerate(((11, n_max), (12, 70001))):
         p = _particles(seed, n)
         sim.upload_particles(p)
         sim.sort_particles()
@@ -80,13 +87,33 @@ def test_static_sort_matches_context_sort(slosh):
         d_off.fill_(-1)
         d_live.fill_(-1)
         torch.cuda.synchronize(dev)
-        slosh.sort_particles_static(d_in.data_ptr(), d_out.data_ptr(), n, GRID, CELL, d_perm.data_ptr(),
-                                    d_off.data_ptr(), d_live.data_ptr(), stream.cuda_stream)
+        free0, alloc0 = torch.cuda.mem_get_info(dev)[0], torch.cuda.memory_allocated(dev)
+        sort_static(n, d_perm.data_ptr(), d_off.data_ptr(), d_live.data_ptr())
         torch.cuda.synchronize(dev)
+        if call > 0:  # the first call in this context may load the library's device code; later ones allocate nothing
+            assert torch.cuda.mem_get_info(dev)[0] == free0, "device free memory changed across the call"
+            assert torch.cuda.memory_allocated(dev) == alloc0
         got = d_out[: n * 48].cpu().numpy().view(A.PARTICLE_DTYPE)
         assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), f"records differ (seed {seed})"
         assert np.array_equal(d_perm[:n].cpu().numpy().view(np.uint32), want_perm)
         assert np.array_equal(d_off.cpu().numpy().view(np.uint32), want_off)
         assert int(d_live.item()) == want_live
         assert want_live == int((p["age"] >= 0).sum())
+
+        # the optional outputs left NULL: the records alone, through the scratch's own copies
+        d_out.fill_(0xCD)
+        torch.cuda.synchronize(dev)
+        sort_static(n, 0, 0, 0)
+        torch.cuda.synchronize(dev)
+        got = d_out[: n * 48].cpu().numpy().view(A.PARTICLE_DTYPE)
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), f"records differ without optional outputs (seed {seed})"
+
+    # an empty input: nothing to move, a live count of 0 and all-zero key offsets
+    d_live.fill_(-1)
+    d_off.fill_(-1)
+    torch.cuda.synchronize(dev)
+    sort_static(0, 0, d_off.data_ptr(), d_live.data_ptr())
+    torch.cuda.synchronize(dev)
+    assert int(d_live.item()) == 0
+    assert not d_off.any().item()
     sim.close()
