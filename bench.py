@@ -33,6 +33,19 @@ sys.path.insert(0, ROOT)
 
 METRIC = "FLIP substeps/s at 256^3 ~16M particles; pressure-solve ms to 1e-6 rel residual"
 HBM_FALLBACK_GBS = 6650.0
+# The preconditioner the GPU arm runs by default: the reference's MGPCG (same V-cycle, same stopping test)
+# with each coarse-grid correction scaled by 1.7, which makes up for the piecewise-constant prolongation.
+# `--mg-correction 1` runs the reference's V-cycle exactly.
+PRECOND = {"mg_correction_scale": 1.7, "mg_smoothing_sweeps": 1, "pcg_flexible": 0, "mg_coarse_iterations": 16}
+
+
+def apply_precond(settings, args):
+    settings.mg_correction_scale = args.mg_correction
+    settings.mg_smoothing_sweeps = args.mg_sweeps
+    settings.pcg_flexible = args.pcg_flexible
+    settings.mg_coarse_iterations = args.mg_coarse_iterations
+    return {"mg_correction_scale": args.mg_correction, "mg_smoothing_sweeps": args.mg_sweeps,
+            "pcg_flexible": bool(args.pcg_flexible), "mg_coarse_iterations": args.mg_coarse_iterations}
 
 
 def parse():
@@ -47,6 +60,8 @@ def parse():
                     help="dam_break_sphere_<n> (n multiple of 8, 32..256), dam_break_64, boxes_512 (512x256x256, 34.5M particles, "
                          "3 static spheres) or tanks_64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    # skip the second timed run with the reference's V-cycle (reported as "reference_vcycle")
+    ap.add_argument("--no-reference-vcycle", action="store_true")
     # mgpcg: MGPCG to a relative residual of 1e-6 (the benchmark); rbgs: red-black SOR, omega 1.9, 200 iterations
     ap.add_argument("--solver", choices=["mgpcg", "rbgs"], default="mgpcg")
     # storage of the V-cycle's coarse levels (precision_mode); the CG vectors and level 0 stay FP32
@@ -61,6 +76,12 @@ def parse():
     ap.add_argument("--ctas-per-sm", type=int, default=0)
     # fixed CTAs per SM of the level-0 MGPCG passes (0: the library default)
     ap.add_argument("--mg-ctas-per-sm", type=int, default=0)
+    # multigrid preconditioner: scale of each coarse-grid correction (1 = the reference's V-cycle),
+    # red-black sweep pairs per smoothing, flexible PCG, coarsest-level iterations
+    ap.add_argument("--mg-correction", type=float, default=PRECOND["mg_correction_scale"])
+    ap.add_argument("--mg-sweeps", type=int, default=PRECOND["mg_smoothing_sweeps"])
+    ap.add_argument("--pcg-flexible", type=int, default=PRECOND["pcg_flexible"])
+    ap.add_argument("--mg-coarse-iterations", type=int, default=PRECOND["mg_coarse_iterations"])
     return ap.parse_args()
 
 
@@ -178,6 +199,9 @@ def cpu_baseline_sample(workload, solver="mgpcg"):
 
 
 def run_reference(args):
+    """The reference path's CPU restatement on all host cores, over the same window as the GPU arm: the
+    emission frame and max(W, 3) - 1 more frames untimed (the GPU arm's warm-up), then `steps` substeps of
+    the frames that follow, timed one by one. The reference runs its own V-cycle (correction scale 1)."""
     world, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
     if rank != 0:
         return
@@ -188,54 +212,93 @@ def run_reference(args):
     sc = make_scene(args.workload, O.settings_default, args.solver)
     o = O.Oracle(sc["settings"])
     o.set_emit_seed(sc["seed"])
-    fi = A.frame_input(sc["settings"], emits=sc["emits"], colliders=sc.get("colliders", []))
-    fi_next = A.frame_input(sc["settings"], colliders=sc.get("colliders", []))
+    cols = sc.get("colliders", [])
+    o.step_frame(A.frame_input(sc["settings"], emits=sc["emits"], colliders=cols))  # frame 1: scene creation
+    fi = A.frame_input(sc["settings"], colliders=cols)
+    warm_frames = max(args.warmup, 3) - 1
+    for _ in range(warm_frames):
+        o.step_frame(fi)
     pending = []
+    iters = []
+    state = {"open": False}
 
     def next_substep():
-        nonlocal fi
         if not pending:
-            if getattr(next_substep, "open", False):
+            if state["open"]:
                 o.end_frame()
             n, _ = o.begin_frame(fi)
-            fi = fi_next
             pending.extend(range(n))
-            next_substep.open = True
+            state["open"] = True
         o.substep(pending.pop(0))
+        iters.append(o.results().last_solve_iterations)
 
-    for _ in range(args.warmup):
-        next_substep()
-    t0 = time.perf_counter()
+    el = 0.0
     for _ in range(args.steps):
+        t0 = time.perf_counter()
         next_substep()
-    el = time.perf_counter() - t0
+        el += time.perf_counter() - t0
     value = args.steps / el
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "substeps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * el / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": sc["name"], "grid": list(sc["settings"].grid_dim), "particles": sc["particles"],
-                   "solver": "MGPCG" if args.solver == "mgpcg" else "RBGS omega 1.9 x200", "tolerance": 1e-6 if args.solver == "mgpcg" else None, "step": "one substep"},
+                   "solver": "MGPCG" if args.solver == "mgpcg" else "RBGS omega 1.9 x200",
+                   "tolerance": 1e-6 if args.solver == "mgpcg" else None, "transfer": "APIC", "cfl": 1.0,
+                   "frame_dt": 1.0 / 120.0, "sort_interval": 4, "parallelism": "host threads",
+                   "step": "one substep (the GPU arm's step is one frame; both report substeps/s)",
+                   "window": f"frames 1-{warm_frames + 1} untimed, then {args.steps} substeps from frame {warm_frames + 2}",
+                   "preconditioner": {"mg_correction_scale": 1.0, "mg_smoothing_sweeps": 1, "pcg_flexible": False,
+                                      "mg_coarse_iterations": 16}},
+        "pressure_iterations_mean": statistics.mean(iters) if iters else None,
         "cpu_baseline": {"value": value, "unit": "substeps/s", "cores": cores, "kind": "port",
-                         "sample": f"{args.steps} substeps of {sc['name']} after {args.warmup} warm-up substeps"},
+                         "sample": f"{args.steps} substeps of {sc['name']} from frame {warm_frames + 2}, C++ oracle with OpenMP"},
         "e2e": {"value": value, "unit": "substeps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    o.close()
     print(json.dumps(line), flush=True)
 
 
-def run_slosh(args):
-    world, rank, local = dist_setup(args.gpus)
+def _timed_frames(sim, fi, steps, stream, phases):
+    """Steps `steps` frames on the simulation's stream: device time (CUDA events on that stream), host
+    wall time around the public calls, and per-frame solver statistics."""
     import torch
+    out = {"phase": {k: 0.0 for k in phases}, "substeps": 0, "iters": [], "rels": [], "trues": [], "active": 0}
+    l0 = sim.launch_count()
+    h0, d0 = sim.transfer_bytes()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ev0.record(stream)
+    for _ in range(steps):
+        sim.step_frame(fi)
+        r = sim.results()
+        out["substeps"] += r.substeps
+        out["iters"].append(r.last_solve_iterations)
+        out["rels"].append(r.last_solve_rel_residual)
+        out["trues"].append(r.last_solve_true_rel_residual)
+        out["active"] = max(out["active"], int(r.raw_stats[7]))
+        for k, v in sim.phase_ms().items():
+            out["phase"][k] += v
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    out["wall_ms"] = (time.perf_counter() - t0) * 1000.0
+    out["dev_ms"] = ev0.elapsed_time(ev1)
+    out["launches"] = sim.launch_count() - l0
+    h1, d1 = sim.transfer_bytes()
+    out["h2d"], out["d2h"] = h1 - h0, d1 - d0
+    return out
 
-    import slosh_b200 as S
-    from slosh_b200 import _abi as A
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
+
+def _scene_sim(args, S, A, local, settings_fn=None):
+    """The workload's simulation on its own stream, stepped through the emission frame (frame 1)."""
+    import torch
     sc = make_scene(args.workload, S.settings_default, args.solver)
     sc["settings"].precision_mode = {"fp32": A.PRECISION_FP32, "fp16": A.PRECISION_FP16_STORAGE,
                                      "bf16": A.PRECISION_BF16_STORAGE}[args.precision]
+    precond = apply_precond(sc["settings"], args)
+    if settings_fn:
+        precond = settings_fn(sc["settings"], precond)
     sim = S.Simulation(sc["settings"], device=local)
     stream = torch.cuda.Stream()
     sim.set_stream(stream.cuda_stream)
@@ -246,7 +309,21 @@ def run_slosh(args):
         sim.set_mg_ctas_per_sm(args.mg_ctas_per_sm)
     cols = sc.get("colliders", [])
     sim.step_frame(A.frame_input(sc["settings"], emits=sc["emits"], colliders=cols))  # scene creation (frame 1)
-    fi = A.frame_input(sc["settings"], colliders=cols)
+    return sc, sim, stream, A.frame_input(sc["settings"], colliders=cols), precond
+
+
+def run_slosh(args):
+    world, rank, local = dist_setup(args.gpus)
+    import torch
+
+    import slosh_b200 as S
+    from slosh_b200 import _abi as A
+    from slosh_b200.replicas import reduce_run
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    sc, sim, stream, fi, precond = _scene_sim(args, S, A, local)
     tuned = None
     if args.autotune:
         r = sim.autotune(fi, frames=1)
@@ -260,38 +337,37 @@ def run_slosh(args):
         dist.barrier()
     clocks = ClockSampler(local)
     clocks.start()
-    l0 = sim.launch_count()
-    h0, d0 = sim.transfer_bytes()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    phase = {k: 0.0 for k in S.PHASES}
-    substeps = 0
-    iters = []
-    rels = []
-    active = 0
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    ev0.record(stream)
-    for _ in range(args.steps):
-        sim.step_frame(fi)
-        r = sim.results()
-        substeps += r.substeps
-        iters.append(r.last_solve_iterations)
-        rels.append(r.last_solve_rel_residual)
-        active = max(active, int(r.raw_stats[7]))
-        for k, v in sim.phase_ms().items():
-            phase[k] += v
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    t1 = time.perf_counter()
+    run = _timed_frames(sim, fi, args.steps, stream, S.PHASES)
     clk = clocks.stop()
-    dev_ms = ev0.elapsed_time(ev1)
-    wall_ms = (t1 - t0) * 1000.0
-    launches = sim.launch_count() - l0
-    h1, d1 = sim.transfer_bytes()
-    from slosh_b200.replicas import reduce_run
-    total_substeps, dev_ms, wall_ms = reduce_run(substeps, dev_ms, wall_ms)
+    sim.close()
+    substeps, phase, iters, rels, trues, active = (run["substeps"], run["phase"], run["iters"], run["rels"], run["trues"],
+                                                   run["active"])
+    launches = run["launches"]
+    total_substeps, dev_ms, wall_ms = reduce_run(substeps, run["dev_ms"], run["wall_ms"])
+    # The same workload with the reference's V-cycle (correction scale 1, one sweep pair, plain PCG), timed
+    # the same way on a fresh simulation: what the preconditioner options change.
+    ref_vc = None
+    if args.solver == "mgpcg" and not args.no_reference_vcycle:
+        def ref_settings(st, _):
+            st.mg_correction_scale, st.mg_smoothing_sweeps, st.pcg_flexible = 1.0, 1, 0
+            return None
+        _, sim2, stream2, fi2, _ = _scene_sim(args, S, A, local, ref_settings)
+        for _ in range(max(args.warmup, 3) - 1):
+            sim2.step_frame(fi2)
+        sim2.enable_phase_timing(True)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        run2 = _timed_frames(sim2, fi2, args.steps, stream2, S.PHASES)
+        sim2.close()
+        t2, dev2, _ = reduce_run(run2["substeps"], run2["dev_ms"], run2["wall_ms"])
+        ref_vc = {"value": t2 / (dev2 * 1e-3), "unit": "substeps/s",
+                  "pressure_solve_ms": run2["phase"]["pressure"] / max(run2["substeps"], 1),
+                  "pressure_iterations_mean": statistics.mean(run2["iters"]) if run2["iters"] else None,
+                  "pressure_rel_residual_max": max(run2["rels"]) if run2["rels"] else None,
+                  "preconditioner": {"mg_correction_scale": 1.0, "mg_smoothing_sweeps": 1, "pcg_flexible": False,
+                                     "mg_coarse_iterations": args.mg_coarse_iterations}}
     if rank != 0:
-        sim.close()
         if dist:
             dist.barrier()
             dist.destroy_process_group()
@@ -322,24 +398,25 @@ def run_slosh(args):
         "config": {"workload": sc["name"], "grid": list(sc["settings"].grid_dim), "particles": n_particles,
                    "solver": "MGPCG" if args.solver == "mgpcg" else "RBGS omega 1.9 x200", "tolerance": 1e-6 if args.solver == "mgpcg" else None, "transfer": "APIC", "cfl": 1.0, "frame_dt": 1.0 / 120.0,
                    "sort_interval": 4, "parallelism": f"replicas{world}", "step": "one frame of CFL substeps",
-                   "mg_coarse_storage": args.precision, "autotune": tuned,
+                   "mg_coarse_storage": args.precision, "preconditioner": precond, "autotune": tuned,
                    "l2": f"inputs larger than L2 (particles {48.0 * n_particles / 1e9:.2f} GB)"},
         "substeps": total_substeps,
         "particle_updates_per_s": total_substeps * n_particles / (dev_ms * 1e-3),
         "pressure_solve_ms": phase["pressure"] / max(substeps, 1),
         "pressure_iterations_mean": statistics.mean(iters) if iters else None,
         "pressure_rel_residual_max": (max(rels) if rels else None) if args.solver == "mgpcg" else None,
+        "pressure_true_rel_residual_max": max(trues) if trues else None,
+        "reference_vcycle": ref_vc,
         "phase_ms_per_substep": {k: v / max(substeps, 1) for k, v in phase.items()},
         "clocks": clk,
         "e2e": {"value": total_substeps / (wall_ms * 1e-3), "unit": "substeps/s",
-                "h2d_bytes_per_step": (h1 - h0) // args.steps, "d2h_bytes_per_step": (d1 - d0) // args.steps},
+                "h2d_bytes_per_step": run["h2d"] // args.steps, "d2h_bytes_per_step": run["d2h"] // args.steps},
         "gpu_launches": launches,
         "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
                      "algorithmic_bytes_per_launch": algo[dom]},
     }
     if world == 1 and not args.no_cpu_baseline:
-        sim.close()
         torch.cuda.synchronize()
         try:
             line["cpu_baseline"] = cpu_baseline_sample(args.workload, args.solver)

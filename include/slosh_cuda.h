@@ -38,7 +38,7 @@ extern "C" {
 #define SLOSH_API __attribute__((visibility("default")))
 #endif
 
-#define SLOSH_ABI_VERSION 1u
+#define SLOSH_ABI_VERSION 2u
 
 /* Limits, SloshTypes.h:93-110. The particle cap is raised above the reference's 16,777,216. */
 #define SLOSH_MAX_COLLIDERS 64u
@@ -118,6 +118,16 @@ typedef struct slosh_settings_t {
     int32_t max_iterations; /* iteration cap when tolerance > 0 */
     uint32_t precision_mode;/* SLOSH_PRECISION_* of the V-cycle storage */
     uint32_t warm_start;    /* SLOSH_WARM_START_* */
+    /* Multigrid preconditioner (extensions; the defaults are the reference's V-cycle). */
+    float mg_correction_scale;   /* every restriction multiplies the reference's 1/4 by this factor, which
+                                    scales each level's coarse-grid correction; 1 = the reference. Values
+                                    of 1.5-1.9 make up for the piecewise-constant prolongation and roughly
+                                    halve the PCG iterations on 256^3 grids. Clamped to [0.5, 1.95]. */
+    int32_t mg_smoothing_sweeps; /* red-black sweep pairs in each pre- and post-smoothing of every level
+                                    above the coarsest; 1 = the reference. Clamped to [1, 4]. */
+    uint32_t pcg_flexible;       /* 1: flexible PCG, beta = r_k.(z_k - z_{k-1}) / rho_{k-1} (Polak-Ribiere),
+                                    robust to a preconditioner that is not exactly linear (FP16/BF16
+                                    storage); 0: beta = rho_k / rho_{k-1} (the reference) */
 } slosh_settings_t;
 
 /* FSloshParticleGPU (SloshTypes.h:84-91): Pos, Age (negative or NaN = dead), Vel,

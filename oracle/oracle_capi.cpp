@@ -323,7 +323,7 @@ ORACLE_API int oracle_copy_state(void* dst, void* src) {
             cv(d.mg[l].x, s.mg[l].x); cv(d.mg[l].b, s.mg[l].b);
         }
         cv(d.pcg_r, s.pcg_r); cv(d.pcg_z, s.pcg_z); cv(d.pcg_d, s.pcg_d); cv(d.pcg_q, s.pcg_q);
-        std::copy(s.scalars, s.scalars + 4, d.scalars);
+        std::copy(s.scalars, s.scalars + 5, d.scalars);
         d.cur = s.cur; d.substeps = s.substeps; d.frame_dt_sub = s.frame_dt_sub;
         d.density_projection_this_frame = s.density_projection_this_frame;
         d.last_disp_index = s.last_disp_index;

@@ -322,6 +322,9 @@ inline void settings_default(slosh_settings_t* s) {  // SloshTypes.h:113-160
     s->max_iterations = 200;
     s->precision_mode = SLOSH_PRECISION_FP32;
     s->warm_start = SLOSH_WARM_START_PREVIOUS;
+    s->mg_correction_scale = 1.0f;
+    s->mg_smoothing_sweeps = 1;
+    s->pcg_flexible = 0u;
 }
 
 // Step_RenderThread's clamps (SloshProxy.cpp:344-347). The grid and particle caps are raised above
@@ -431,6 +434,9 @@ struct PassParams {
     float coupling_scale = 1024.0f, density_relaxation = 0;
     uint32_t use_apic = 1, smooth_coupling = 1, ghost_fluid = 1, num_colliders = 0, num_manipulators = 0;
     uint32_t precision_mode = SLOSH_PRECISION_FP32;  // storage of the coarse MG levels
+    float restrict_scale = 0.25f;  // factor of the restriction's fluid-child sum: 0.25 x mg_correction_scale
+    int mg_sweeps = 1;             // red-black sweep pairs per pre- and post-smoothing (mg_smoothing_sweeps)
+    uint32_t pcg_flexible = 0;     // flexible (Polak-Ribiere) beta
     uint32_t frame_seed = 0;
 };
 
@@ -682,7 +688,7 @@ public:
     };
     std::vector<Level> mg;                 // mg[0] is unused storage-wise (level 0 lives in the pool)
     std::vector<R> pcg_r, pcg_z, pcg_d, pcg_q;
-    double scalars[4] = {0, 0, 0, 0};       // rho, scratch, d.Ad, previous rho
+    double scalars[5] = {0, 0, 0, 0, 0};    // rho, scratch, d.Ad, previous rho, r.z_prev (flexible PCG)
     double bb = 0.0, rr = 0.0;              // ||b||^2, ||r||^2 of the current solve
     int32_t last_solve_iterations = 0;
     float last_solve_rel_residual = 0.0f, last_solve_true_rel_residual = 0.0f;
@@ -747,7 +753,7 @@ public:
         pcg_z.assign(L.pool_cells, R(0));
         pcg_d.assign(L.pool_cells, R(0));
         pcg_q.assign(L.pool_cells, R(0));
-        std::fill(scalars, scalars + 4, 0.0);
+        std::fill(scalars, scalars + 5, 0.0);
         total_emitted = 0;
         prev_dt = 0.0f;
         last_max_speed = 0.0f;
@@ -1344,7 +1350,7 @@ public:
                     sum = sum + (bf[fi] - (diag * xf[fi] - nbsum));
                 }
             }
-            R b = R(0.25f) * sum;
+            R b = R(P.restrict_scale) * sum;
             cl.b[ci] = store_q(l + 1, b);
             R cdiag = R(DIAG_EPSILON);
             for (int n = 0; n < 6; ++n) {
@@ -1406,25 +1412,38 @@ public:
         }
     }
 
-    // VCycle, SloshProxy.cpp:904-959. Returns rho = r.z.
+    // VCycle, SloshProxy.cpp:904-959. Returns rho = r.z. Every level above the coarsest is pre-smoothed
+    // by P.mg_sweeps red-black pairs (the first red half is the red initialisation its producer wrote)
+    // and post-smoothed by P.mg_sweeps black-red pairs; the reference is one pair.
     double vcycle(int coarse_iterations) {
         const int nl = L.num_levels;
         if (nl == 1) {
             mg_coarse_solve(0, coarse_iterations);
             return mg_smooth(0, 0u, true);
         }
-        mg_smooth(0, 1u, false);
+        const int sweeps = P.mg_sweeps;
+        auto pre_smooth = [&](int l) {
+            mg_smooth(l, 1u, false);
+            for (int k = 1; k < sweeps; ++k) {
+                mg_smooth(l, 0u, false);
+                mg_smooth(l, 1u, false);
+            }
+        };
+        pre_smooth(0);
         for (int l = 0; l < nl - 1; ++l) {
             mg_restrict(l);
-            if (l + 1 < nl - 1) mg_smooth(l + 1, 1u, false);
+            if (l + 1 < nl - 1) pre_smooth(l + 1);
         }
         mg_coarse_solve(nl - 1, coarse_iterations);
         double rho = 0.0;
         for (int l = nl - 2; l >= 0; --l) {
             mg_prolong(l);
-            mg_smooth(l, 1u, false);
-            double d = mg_smooth(l, 0u, l == 0);
-            if (l == 0) rho = d;
+            for (int k = 0; k < sweeps; ++k) {
+                mg_smooth(l, 1u, false);
+                const bool last = k == sweeps - 1;
+                double d = mg_smooth(l, 0u, l == 0 && last);
+                if (l == 0 && last) rho = d;
+            }
         }
         return rho;
     }
@@ -1484,6 +1503,13 @@ public:
             scalars[2] = dq;
             // PCGUpdatePRCS (+ ||r||^2)
             const R alpha = R(ratio_f(scalars[0], scalars[2]));
+            if (P.pcg_flexible) {  // r_{k+1} . z_k with the new residual, before z is overwritten
+                scalars[4] = level0_dot([&](uint32_t i, I3) -> double {
+                    if (type_of(cell_type[i]) != CELL_FLUID) return 0.0;
+                    R ri = pcg_r[i] - alpha * pcg_q[i];
+                    return double(ri * pcg_z[i]);
+                });
+            }
             rr = level0_dot([&](uint32_t i, I3 c) -> double {
                 if (type_of(cell_type[i]) != CELL_FLUID) return 0.0;
                 p[i] = p[i] + alpha * pcg_d[i];
@@ -1508,9 +1534,11 @@ public:
         return done;
     }
     // PCGUpdateDCS: d = z + beta d. The first direction is d = z exactly (the reference computes
-    // z + 0 * d; the two differ only in the sign of a zero or a non-finite stale d).
+    // z + 0 * d; the two differ only in the sign of a zero or a non-finite stale d). Flexible PCG
+    // subtracts r_k.z_{k-1} (scalars[4]) from rho_k, in FP64, before the ratio.
     void update_d(bool first) {
-        const R beta = first ? R(0) : R(ratio_f(scalars[0], scalars[3]));
+        const double num = P.pcg_flexible ? scalars[0] - scalars[4] : scalars[0];
+        const R beta = first ? R(0) : R(ratio_f(num, scalars[3]));
         for_active_cells([&](uint32_t i, I3) {
             if (type_of(cell_type[i]) != CELL_FLUID) return;
             pcg_d[i] = first ? pcg_z[i] : pcg_z[i] + beta * pcg_d[i];
@@ -1862,30 +1890,53 @@ public:
 
     // ---- G2P + advection: GatherComponent, SampleVelocityComponent, AdvectParticle, G2PAdvectCS,
     //      Slosh.usf:1376-1678 ------------------------------------------------------------------------
+    // Trilinear interpolation of the 8 stencil values u[o] (o = x + 2 y + 4 z) as lerps with fused
+    // multiply-adds, x then y then z, and the three partial derivatives from the same differences:
+    // mathematically the reference's sum_o w_o u_o and sum_o sign_o (w3 w3) inv_h u_o (Slosh.usf:1376-1443),
+    // rounded in this order on both sides of the parity (the HLSL fixes no order either: its compiler may
+    // fuse a multiply-add).
+    struct Lerp3 {
+        R val, gx, gy, gz;
+    };
+    static Lerp3 lerp3(const R u[8], R fx, R fy, R fz, R inv_h, bool grad) {
+        const R d00 = u[1] - u[0], d10 = u[3] - u[2], d01 = u[5] - u[4], d11 = u[7] - u[6];
+        const R a00 = std::fma(fx, d00, u[0]), a10 = std::fma(fx, d10, u[2]);
+        const R a01 = std::fma(fx, d01, u[4]), a11 = std::fma(fx, d11, u[6]);
+        const R e0 = a10 - a00, e1 = a11 - a01;
+        const R b0 = std::fma(fy, e0, a00), b1 = std::fma(fy, e1, a01);
+        const R g = b1 - b0;
+        Lerp3 r{std::fma(fz, g, b0), R(0), R(0), R(0)};
+        if (grad) {
+            r.gz = g * inv_h;
+            r.gy = std::fma(fz, e1 - e0, e0) * inv_h;
+            const R c0 = std::fma(fy, d10 - d00, d00), c1 = std::fma(fy, d11 - d01, d01);
+            r.gx = std::fma(fz, c1 - c0, c0) * inv_h;
+        }
+        return r;
+    }
     void gather_component(int axis, V3<R> xp, const std::vector<R>& v, R& unew, R& delta_sum, R& delta_weight, V3<R>& grad) const {
         const R inv_h = R(P.inv_cell_size);
         V3<R> off{axis == 0 ? R(0) : R(0.5f), axis == 1 ? R(0) : R(0.5f), axis == 2 ? R(0) : R(0.5f)};
         V3<R> g{xp.x * inv_h - off.x, xp.y * inv_h - off.y, xp.z * inv_h - off.z};
         I3 base{int(std::floor(g.x)), int(std::floor(g.y)), int(std::floor(g.z))};
         V3<R> fr{g.x - R(base.x), g.y - R(base.y), g.z - R(base.z)};
-        unew = R(0); delta_sum = R(0); delta_weight = R(0); grad = {R(0), R(0), R(0)};
+        delta_sum = R(0); delta_weight = R(0);
+        R u[8];
         for (uint32_t o = 0; o < 8u; ++o) {
             I3 oi{int(o & 1u), int((o >> 1u) & 1u), int((o >> 2u) & 1u)};
             I3 node{clampi(base.x + oi.x, 0, L.grid.x - 1), clampi(base.y + oi.y, 0, L.grid.y - 1), clampi(base.z + oi.z, 0, L.grid.z - 1)};
-            V3<R> w3{oi.x ? fr.x : R(1) - fr.x, oi.y ? fr.y : R(1) - fr.y, oi.z ? fr.z : R(1) - fr.z};
-            R w = w3.x * w3.y * w3.z;
-            V3<R> sign{oi.x ? R(1) : R(-1), oi.y ? R(1) : R(-1), oi.z ? R(1) : R(-1)};
-            V3<R> gw{sign.x * (w3.y * w3.z) * inv_h, sign.y * (w3.x * w3.z) * inv_h, sign.z * (w3.x * w3.y) * inv_h};
             uint32_t f = face_index(axis, node);
-            R u = v[f];
-            unew = unew + w * u;
-            if (P.use_apic != 0u) {
-                grad = grad + gw * u;
-            } else if ((face_flags[f] & FACE_HAS_WEIGHT) != 0u) {
-                delta_sum = delta_sum + w * (u - vel_old[f]);
+            u[o] = v[f];
+            if (P.use_apic == 0u && (face_flags[f] & FACE_HAS_WEIGHT) != 0u) {
+                V3<R> w3{oi.x ? fr.x : R(1) - fr.x, oi.y ? fr.y : R(1) - fr.y, oi.z ? fr.z : R(1) - fr.z};
+                R w = w3.x * w3.y * w3.z;
+                delta_sum = delta_sum + w * (u[o] - vel_old[f]);
                 delta_weight = delta_weight + w;
             }
         }
+        const Lerp3 l = lerp3(u, fr.x, fr.y, fr.z, inv_h, P.use_apic != 0u);
+        unew = l.val;
+        grad = {l.gx, l.gy, l.gz};
     }
     R sample_velocity_component(int axis, V3<R> xp, R fallback, bool check_known, const std::vector<R>& v) const {
         const uint32_t known = FACE_VALID | (0xFFFFFFFFu << FACE_EXTRAP_SHIFT);
@@ -1894,17 +1945,15 @@ public:
         V3<R> g{xp.x * inv_h - off.x, xp.y * inv_h - off.y, xp.z * inv_h - off.z};
         I3 base{int(std::floor(g.x)), int(std::floor(g.y)), int(std::floor(g.z))};
         V3<R> fr{g.x - R(base.x), g.y - R(base.y), g.z - R(base.z)};
-        R u = R(0);
+        R u[8];
         for (uint32_t o = 0; o < 8u; ++o) {
             I3 oi{int(o & 1u), int((o >> 1u) & 1u), int((o >> 2u) & 1u)};
             I3 node{clampi(base.x + oi.x, 0, L.grid.x - 1), clampi(base.y + oi.y, 0, L.grid.y - 1), clampi(base.z + oi.z, 0, L.grid.z - 1)};
-            V3<R> w3{oi.x ? fr.x : R(1) - fr.x, oi.y ? fr.y : R(1) - fr.y, oi.z ? fr.z : R(1) - fr.z};
             uint32_t f = face_index(axis, node);
-            R uf = v[f];
-            if (check_known && (face_flags[f] & known) == 0u) uf = fallback;
-            u = u + w3.x * w3.y * w3.z * uf;
+            u[o] = v[f];
+            if (check_known && (face_flags[f] & known) == 0u) u[o] = fallback;
         }
-        return u;
+        return lerp3(u, fr.x, fr.y, fr.z, inv_h, false).val;
     }
     V3<R> sample_density_displacement(V3<R> xp, const std::vector<R>& disp) const {
         const R inv_h = R(P.inv_cell_size);
@@ -1914,14 +1963,13 @@ public:
             V3<R> g{xp.x * inv_h - off.x, xp.y * inv_h - off.y, xp.z * inv_h - off.z};
             I3 base{int(std::floor(g.x)), int(std::floor(g.y)), int(std::floor(g.z))};
             V3<R> fr{g.x - R(base.x), g.y - R(base.y), g.z - R(base.z)};
-            R value = R(0);
+            R u[8];
             for (uint32_t o = 0; o < 8u; ++o) {
                 I3 oi{int(o & 1u), int((o >> 1u) & 1u), int((o >> 2u) & 1u)};
                 I3 node{clampi(base.x + oi.x, 0, L.grid.x - 1), clampi(base.y + oi.y, 0, L.grid.y - 1), clampi(base.z + oi.z, 0, L.grid.z - 1)};
-                V3<R> w3{oi.x ? fr.x : R(1) - fr.x, oi.y ? fr.y : R(1) - fr.y, oi.z ? fr.z : R(1) - fr.z};
-                value = value + w3.x * w3.y * w3.z * disp[face_index(axis, node)];
+                u[o] = disp[face_index(axis, node)];
             }
-            out[axis] = value;
+            out[axis] = lerp3(u, fr.x, fr.y, fr.z, inv_h, false).val;
         }
         R len = length(out);
         V3<R> d = len > R(0.5f) ? out * (R(0.5f) / len) : out;
@@ -2120,6 +2168,9 @@ public:
         P.warm_start_scale = 1.0f;
         P.smooth_coupling = s.smooth_coupling_force ? 1u : 0u;
         P.precision_mode = s.precision_mode <= uint32_t(SLOSH_PRECISION_BF16_STORAGE) ? s.precision_mode : uint32_t(SLOSH_PRECISION_FP32);
+        P.restrict_scale = 0.25f * clampr(s.mg_correction_scale, 0.5f, 1.95f);
+        P.mg_sweeps = clampi(s.mg_smoothing_sweeps, 1, 4);
+        P.pcg_flexible = s.pcg_flexible ? 1u : 0u;
         P.ghost_fluid = s.ghost_fluid ? 1u : 0u;
         const int interval = clampi(s.density_projection_interval, 1, 8);
         P.density_relaxation = 1.0f - std::pow(1.0f - clampr(s.density_relaxation, 0.0f, 1.0f), float(interval));

@@ -73,7 +73,8 @@ class Settings(C.Structure):
         ("extrapolation_layers", C.c_int32), ("min_substeps", C.c_int32), ("max_substeps", C.c_int32),
         ("max_frame_dt", C.c_float), ("cfl", C.c_float), ("max_speed", C.c_float),
         ("tolerance", C.c_float), ("max_iterations", C.c_int32), ("precision_mode", C.c_uint32),
-        ("warm_start", C.c_uint32),
+        ("warm_start", C.c_uint32), ("mg_correction_scale", C.c_float), ("mg_smoothing_sweeps", C.c_int32),
+        ("pcg_flexible", C.c_uint32),
     ]
 
 

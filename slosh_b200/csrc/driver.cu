@@ -100,6 +100,9 @@ slosh_settings_t defaults() {
     s.max_iterations = 200;
     s.precision_mode = SLOSH_PRECISION_FP32;
     s.warm_start = SLOSH_WARM_START_PREVIOUS;
+    s.mg_correction_scale = 1.0f;
+    s.mg_smoothing_sweeps = 1;
+    s.pcg_flexible = 0u;
     return s;
 }
 
@@ -406,7 +409,7 @@ struct Ctx {
         mg.nbr_slots = dalloc<uint32_t>(8 * size_t(num_pool_bricks), false);
         mg.q = dalloc<float>(pc, false);
         mg.partials = dalloc<double>(2 * size_t(num_pool_bricks), false);
-        mg.scalars = dalloc<double>(8, false);
+        mg.scalars = dalloc<double>(16, false);
         mg.counters = dalloc<uint32_t>(8, false);
         mg.ctl = dalloc<uint32_t>(8, false);
         {
@@ -463,7 +466,7 @@ struct Ctx {
             CK(cudaMemset(mg.lv[l].b, 0, level_cells[l] * 4));
             CK(cudaMemset(mg.lv[l].word, 0, level_cells[l] * 2));
         }
-        CK(cudaMemset(mg.scalars, 0, 8 * sizeof(double)));
+        CK(cudaMemset(mg.scalars, 0, 16 * sizeof(double)));
         CK(cudaMemset(mg.counters, 0, 8 * 4));
         CK(cudaMemset(mg.ctl, 0, 8 * 4));
         CK(cudaMemset(mg.partials, 0, 2 * size_t(num_pool_bricks) * sizeof(double)));
@@ -726,6 +729,17 @@ struct Ctx {
                 destroy_graphs();
                 mg_prec = prec;
                 for (int l = 1; l < mg.num_levels; ++l) mg.lv[l].prec = prec;
+            }
+            // preconditioner options (the solve graphs hold the MGState by value)
+            const float restrict_scale = 0.25f * clampf_h(s.mg_correction_scale, 0.5f, 1.95f);
+            const int sweeps = clampi_h(s.mg_smoothing_sweeps, 1, 4);
+            const uint32_t flexible = s.pcg_flexible ? 1u : 0u;
+            if (restrict_scale != mg.restrict_scale || sweeps != mg.sweeps || flexible != mg.flexible) {
+                CK(cudaStreamSynchronize(stream));
+                destroy_graphs();
+                mg.restrict_scale = restrict_scale;
+                mg.sweeps = sweeps;
+                mg.flexible = flexible;
             }
         }
         ++sim_frame;

@@ -87,7 +87,8 @@ struct MGState {
     float* dvec;
     float* q;
     double* partials;     // one per brick entry, two dots (capacity 2 x num_pool_bricks)
-    double* scalars;      // [0] rho, [2] d.Ad, [3] previous rho, [4] ||b||^2, [5] ||r||^2, [6..7] true residual, [8] tol
+    double* scalars;      // [0] rho, [2] d.Ad, [3] previous rho, [4] ||b||^2, [5] ||r||^2, [6..7] true residual, [8] tol,
+                          // [9] r.z_prev (flexible PCG)
     uint32_t* counters;   // last-CTA counters, one per reduction kind
     uint32_t* ctl;        // [0] completed iterations, [1] limit, [2] tolerance mode, [3] done, [4] frame: a solve hit its limit
     uint8_t* word;        // level-0 stencil word per pool cell (fluid neighbours, fluid, red)
@@ -96,6 +97,9 @@ struct MGState {
     uint32_t* tail_list;  // per tail level: red fluid cells, then black fluid cells (dense indices)
     uint32_t* tail_meta;  // per level: [red offset, red count, black offset, black count]
     unsigned char* tail_image;  // per solve: the tail kernel's shared memory minus x and b (mg_tail_smem bytes)
+    float restrict_scale;       // factor of the restriction's fluid-child sum: 0.25 x mg_correction_scale
+    int sweeps;                 // red-black sweep pairs per pre- and post-smoothing (mg_smoothing_sweeps)
+    uint32_t flexible;          // flexible PCG: UpdatePR also reduces r_{k+1}.z_k into scalars[9]
 };
 int launch_mg_words(const MGState& m, int l, cudaStream_t s);
 int launch_mg_tail_lists(const MGState& m, cudaStream_t s);

@@ -18,11 +18,13 @@
 //   * the small coarse levels (<= 4096 cells) run as one single-CTA kernel (descent, coarse solve,
 //     ascent with block barriers between passes).
 #include <algorithm>
+#include <cstdlib>
 
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
 #include "kernels.h"
+#include "tc.cuh"
 
 namespace slosh {
 
@@ -557,10 +559,12 @@ __device__ __forceinline__ Nb6 load_black(const Dev& d, const MGState& m, uint32
     return v;
 }
 
-// Red sweep with rho = r . z over all cells (red: the new value, black: the current z). Cells the sweep
-// does not update are stored back unchanged (each cell belongs to one warp's brick).
+// Red sweep; with DOT also rho = r . z over all cells (red: the new value, black: the current z), which
+// shifts rho. Cells the sweep does not update are stored back unchanged (each cell belongs to one warp's
+// brick).
+template <bool DOT>
 __global__ void __launch_bounds__(GRID_THREADS, 3) k_smooth0(Dev d, MGState m) {
-    w4_pass<1, 1>(d, m, 1,
+    w4_pass<DOT ? 1 : 0, 1>(d, m, 1,
         [&](const Geo& g, const uint32_t* ns) { return load_sweep(d, m, g, ns); },
         [&](const Geo& g, const SweepQ& v, double* v0, double*) {
             const X2 x = partner(v.z);
@@ -657,8 +661,9 @@ __device__ __forceinline__ void smooth_fp_cell(const MGLevel& L, uint32_t i, uin
     if (!(w & CW_FLUID) || (w & CW_RED) != want) return;
     lv_st(L.x, i, L.prec, (b + sum) / word_diag(w));
 }
-// Restriction F -> C at coarse cell ci: b_c = (sum of the fluid children's residuals) / 4.
-__device__ __forceinline__ void restrict_fp_cell(const MGLevel& F, const MGLevel& C, uint32_t ci, int3 c) {
+// Restriction F -> C at coarse cell ci: b_c = scale x (sum of the fluid children's residuals), scale = 1/4 in
+// the reference (times mg_correction_scale).
+__device__ __forceinline__ void restrict_fp_cell(const MGLevel& F, const MGLevel& C, uint32_t ci, int3 c, float scale) {
     const uint32_t fdx = uint32_t(F.dim.x), fdxy = uint32_t(F.dim.x * F.dim.y);
     const uint32_t flast = F.cells - 1u;
     // Every child's word, b, x and neighbours are loaded before any of them is tested.
@@ -683,7 +688,7 @@ __device__ __forceinline__ void restrict_fp_cell(const MGLevel& F, const MGLevel
 #pragma unroll
     for (int o = 0; o < 8; ++o)
         if ((fl >> o) & 1u) sum = sum + res[o];
-    const float bb = 0.25f * sum;
+    const float bb = scale * sum;
     lv_st(C.b, ci, C.prec, bb);
     lv_st(C.x, ci, C.prec, (cw & CW_RED) ? bb / word_diag(cw) : 0.0f);
 }
@@ -722,7 +727,7 @@ __global__ void k_smooth_fp(Dev d, MGState m, int l, uint32_t parity) {
 // Restriction l -> l + 1 over level l + 1's footprint.
 __global__ void k_restrict_fp(Dev d, MGState m, int l) {
     const MGLevel F = m.lv[l], C = m.lv[l + 1];
-    for_footprint(d, C, l + 1, [&](uint32_t ci, int3 c) { restrict_fp_cell(F, C, ci, c); });
+    for_footprint(d, C, l + 1, [&](uint32_t ci, int3 c) { restrict_fp_cell(F, C, ci, c, m.restrict_scale); });
 }
 // Prolongation l + 1 -> l fused with the black sweep of level l.
 __global__ void k_prolong_smooth_fp(Dev d, MGState m, int l) {
@@ -782,12 +787,475 @@ __global__ void __launch_bounds__(GRID_THREADS) k_restrict0(Dev d, MGState m) {
                 const uint32_t fl = uint32_t((2 * cl.x + (o & 1)) + 8 * ((2 * cl.y + ((o >> 1) & 1)) + 8 * (2 * cl.z + ((o >> 2) & 1))));
                 if (s_fluid[warp][fl]) sum = sum + s_res[warp][fl];
             }
-            const float bb = 0.25f * sum;
+            const float bb = m.restrict_scale * sum;
             lv_st(C.b, ci, C.prec, bb);
             lv_st(C.x, ci, C.prec, (cw & CW_RED) ? bb / word_diag(cw) : 0.0f);
         }
         __syncwarp();
     }
+}
+
+__device__ __forceinline__ float* dir_buf(const MGState& m, uint32_t parity) { return parity ? m.dvec2 : m.dvec; }
+__device__ __forceinline__ const float* dir_buf_c(const MGState& m, uint32_t parity) { return parity ? m.dvec2 : m.dvec; }
+
+// ---- level-0 passes from a shared-memory stage of the brick (bulk async copies) ---------------------------
+// One warp per active brick, as above, but before computing the warp copies everything its pass reads into
+// a per-warp stage in shared memory, so a brick costs one round trip to L2 instead of one per round of
+// dependent loads:
+//   * per "face" array (one read with neighbours): the brick's 512 cells, then its six neighbour faces of 64
+//     cells each at 512 + 64 n (n = -x, +x, -y, +y, -z, +z; index y + 8 z, x + 8 z, x + 8 y in the face);
+//   * per "body" array: the brick's 512 cells; and the 512 stencil bytes.
+// Bodies (2 KB, 512 B), the +-y faces (8 rows of 32 B) and the +-z faces (one 256-byte plane) are 1-D bulk
+// copies (cp.async.bulk, no multicast) that complete on the warp's mbarrier; the +-x faces are strided
+// columns and are read by plain loads issued alongside. A missing neighbour is the all-zero null slot 0.
+// The stage of a warp is reused brick after brick; its mbarrier phase alternates.
+constexpr int ST_WARPS = 4;  // warps (bricks in flight) per CTA of a staged pass
+constexpr uint32_t ST_FACE = 896u;  // floats of a staged face array: body + 6 x 64
+template <int NF, int NB>
+struct __align__(16) WarpStage {
+    float f[NF > 0 ? NF : 1][ST_FACE];
+    float b[NB > 0 ? NB : 1][BRICK_CELLS];
+    uint8_t word[BRICK_CELLS];
+    uint64_t bar;
+    uint64_t pad;
+};
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(tc::smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(tc::smem_u32(bar))
+                 : "memory");
+}
+// Issues the copies of one brick into S (all lanes of the warp); stage_wait then waits for them.
+template <int NF, int NB>
+__device__ __forceinline__ void stage_issue(WarpStage<NF, NB>& S, const float* const* fa, const float* const* ba, const uint8_t* word,
+                                            uint32_t slot, const uint32_t* ns, uint32_t lane) {
+    constexpr uint32_t bytes = uint32_t(NF) * 3072u + uint32_t(NB) * 2048u + 512u;
+    constexpr int NC = NF * 19 + NB + 1;
+    // the stage's previous contents were read by generic loads: order them before the async-proxy writes
+    __syncwarp();
+    tc::fence_async_shared();
+    if (lane == 0) tc::mbar_arrive_expect_tx(&S.bar, bytes);
+    __syncwarp();
+    for (int c = int(lane); c < NC; c += 32) {
+        if (c < NF * 19) {
+            const int f = c / 19, q = c - 19 * f;
+            const float* a = fa[f];
+            if (q == 0) bulk_load(S.f[f], a + size_t(slot) * BRICK_CELLS, 2048u, &S.bar);
+            else if (q <= 8) bulk_load(S.f[f] + 640 + 8 * (q - 1), a + size_t(ns[2]) * BRICK_CELLS + 56 + 64 * (q - 1), 32u, &S.bar);
+            else if (q <= 16) bulk_load(S.f[f] + 704 + 8 * (q - 9), a + size_t(ns[3]) * BRICK_CELLS + 64 * (q - 9), 32u, &S.bar);
+            else if (q == 17) bulk_load(S.f[f] + 768, a + size_t(ns[4]) * BRICK_CELLS + 448, 256u, &S.bar);
+            else bulk_load(S.f[f] + 832, a + size_t(ns[5]) * BRICK_CELLS, 256u, &S.bar);
+        } else if (c < NF * 19 + NB) {
+            const int b = c - NF * 19;
+            bulk_load(S.b[b], ba[b] + size_t(slot) * BRICK_CELLS, 2048u, &S.bar);
+        } else {
+            bulk_load(S.word, word + size_t(slot) * BRICK_CELLS, 512u, &S.bar);
+        }
+    }
+    // +-x faces: cells (7, y, z) of the -x brick and (0, y, z) of the +x brick, j = y + 8 z
+    if (NF > 0) {
+        float xv[NF > 0 ? NF : 1][4];
+#pragma unroll
+        for (int f = 0; f < NF; ++f)
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const uint32_t j = lane + 32u * uint32_t(k);
+                const uint32_t l = 8u * j;  // local index of (0, y, z)
+                xv[f][2 * k] = fa[f][size_t(ns[0]) * BRICK_CELLS + l + 7u];
+                xv[f][2 * k + 1] = fa[f][size_t(ns[1]) * BRICK_CELLS + l];
+            }
+#pragma unroll
+        for (int f = 0; f < NF; ++f)
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const uint32_t j = lane + 32u * uint32_t(k);
+                S.f[f][512u + j] = xv[f][2 * k];
+                S.f[f][576u + j] = xv[f][2 * k + 1];
+            }
+    }
+}
+// Waits for the stage's copies (phase `parity` of its mbarrier); false if the bounded wait gave up, which
+// records the error in *error (ctl[5]).
+template <int NF, int NB>
+__device__ __forceinline__ bool stage_wait(WarpStage<NF, NB>& S, uint32_t parity, uint32_t* error) {
+    const bool ok = tc::mbar_wait(&S.bar, parity, error, 1u);
+    __syncwarp();
+    return ok;
+}
+template <int NF, int NB>
+__device__ __forceinline__ bool stage_brick(WarpStage<NF, NB>& S, const float* const* fa, const float* const* ba, const uint8_t* word,
+                                            uint32_t slot, const uint32_t* ns, uint32_t lane, uint32_t parity, uint32_t* error) {
+    stage_issue<NF, NB>(S, fa, ba, word, slot, ns, lane);
+    return stage_wait<NF, NB>(S, parity, error);
+}
+// Neighbour n of local cell l of a staged face array.
+__device__ __forceinline__ float snbr(const float* F, uint32_t l, int n) {
+    const uint32_t x = l & 7u, y = (l >> 3) & 7u, z = l >> 6;
+    switch (n) {
+        case 0: return x > 0u ? F[l - 1u] : F[512u + y + 8u * z];
+        case 1: return x < 7u ? F[l + 1u] : F[576u + y + 8u * z];
+        case 2: return y > 0u ? F[l - 8u] : F[640u + x + 8u * z];
+        case 3: return y < 7u ? F[l + 8u] : F[704u + x + 8u * z];
+        case 4: return z > 0u ? F[l - 64u] : F[768u + x + 8u * y];
+        default: return z < 7u ? F[l + 64u] : F[832u + x + 8u * y];
+    }
+}
+__device__ __forceinline__ float4 sld4(const float* F, uint32_t l) { return *reinterpret_cast<const float4*>(F + l); }
+// A quad of a staged face array with its neighbours, as load_q6 reads it from global memory.
+__device__ __forceinline__ Q6 sq6(const float* F, const Geo& g) {
+    Q6 q;
+    q.c = sld4(F, g.l);
+    q.ym = sld4(F, g.y > 0u ? g.l - 8u : 640u + 4u * g.h + 8u * g.z);
+    q.yp = sld4(F, g.y < 7u ? g.l + 8u : 704u + 4u * g.h + 8u * g.z);
+    q.zm = sld4(F, g.z > 0u ? g.l - 64u : 768u + 4u * g.h + 8u * g.y);
+    q.zp = sld4(F, g.z < 7u ? g.l + 64u : 832u + 4u * g.h + 8u * g.y);
+    q.xb = F[(g.h == 0u ? 512u : 576u) + g.y + 8u * g.z];
+    return q;
+}
+__device__ __forceinline__ uint32_t sword4(const uint8_t* W, const Geo& g) { return *reinterpret_cast<const uint32_t*>(W + g.l); }
+
+// Final FP64 reduction over the brick partials for a CTA of T threads: the canonical tree of final_reduce
+// (lane t = 0..1023 adds partials t, t + 1024, ... in order; groups of 32 lanes fold with shfl_down; the
+// 32 group sums are added in order), with each thread owning lanes x + T k.
+template <int T>
+__device__ double final_reduce_t(const double* partials, uint32_t n, double* lanes, double* w32) {
+    constexpr int K = 1024 / T;
+    double acc[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) acc[k] = 0.0;
+    for (uint32_t base = 0; base < n; base += 1024u) {
+        double v[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const uint32_t e = base + threadIdx.x + uint32_t(T * k);
+            v[k] = e < n ? __ldcg(partials + e) : 0.0;
+        }
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+            if (base + threadIdx.x + uint32_t(T * k) < n) acc[k] = acc[k] + v[k];
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k) lanes[threadIdx.x + uint32_t(T * k)] = acc[k];
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        const int lw = warp + (T / 32) * k;
+        const double v = warp_fold(lanes[lw * 32 + lane]);
+        if (lane == 0) w32[lw] = v;
+    }
+    __syncthreads();
+    double total = 0.0;
+    if (threadIdx.x == 0) {
+        total = w32[0];
+        for (int w = 1; w < 32; ++w) total = total + w32[w];
+    }
+    return total;
+}
+
+// Staged pass over the active bricks: per brick the stage is filled, then rounds k = 0..3 of the half-row
+// layout call apply(S, g, v0, v1) (dot terms as in w4_pass); with NDOT > 0 the last CTA reduces the brick
+// partials and calls store(t0, t1) in thread 0. fa/ba name the face and body arrays.
+template <int NF, int NB, int NDOT, class Apply, class Store>
+__device__ __forceinline__ void st_pass(const Dev& d, const MGState& m, uint32_t counter, const float* const* fa, const float* const* ba,
+                                        Apply apply, Store store) {
+    extern __shared__ __align__(16) unsigned char st_smem[];
+    using Stg = WarpStage<NF, NB>;
+    __shared__ uint32_t s_last;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    Stg& S = reinterpret_cast<Stg*>(st_smem)[warp];
+    if (lane == 0) {
+        tc::mbar_init(&S.bar, 1u);
+        tc::fence_mbar_init();
+    }
+    __syncwarp();
+    const uint32_t active = d.active_bricks[0];
+    const uint32_t cap = d.num_pool_bricks;
+    uint32_t parity = 0u;
+    for (uint32_t e = blockIdx.x * ST_WARPS + warp; e < active; e += gridDim.x * ST_WARPS) {
+        const uint4 s0 = *reinterpret_cast<const uint4*>(m.nbr_slots + 8u * e);
+        const uint4 s1 = *reinterpret_cast<const uint4*>(m.nbr_slots + 8u * e + 4u);
+        const uint32_t ns[6] = {s0.x, s0.y, s0.z, s0.w, s1.x, s1.y};
+        const uint32_t base = s1.z * BRICK_CELLS;
+        if (!stage_brick<NF, NB>(S, fa, ba, m.word, s1.z, ns, lane, parity, m.ctl + 5)) break;
+        parity ^= 1u;
+        double acc0 = 0.0, acc1 = 0.0;
+#pragma unroll
+        for (uint32_t k = 0; k < 4u; ++k) {
+            const Geo g = geo_of(base, lane, k);
+            double v0[4] = {0.0, 0.0, 0.0, 0.0}, v1[4] = {0.0, 0.0, 0.0, 0.0};
+            apply(S, g, v0, v1);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                acc0 = acc0 + v0[j];
+                acc1 = acc1 + v1[j];
+            }
+        }
+        if (NDOT > 0) {
+            const double t0 = warp_fold(acc0);
+            if (lane == 0) m.partials[e] = t0;
+        }
+        if (NDOT > 1) {
+            const double t1 = warp_fold(acc1);
+            if (lane == 0) m.partials[cap + e] = t1;
+        }
+    }
+    if (NDOT == 0) return;
+    __syncwarp();
+    if (lane == 0) tc::mbar_inval(&S.bar);  // the stage memory is reused by the final reduction below
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = (atomicAdd(m.counters + counter, 1u) == gridDim.x - 1u) ? 1u : 0u;
+    __syncthreads();
+    if (s_last) {
+        __threadfence();
+        // the stages are free now: the reduction's lanes live in their shared memory
+        double* lanes = reinterpret_cast<double*>(st_smem);
+        double* w32 = lanes + 1024;
+        const double r0 = final_reduce_t<ST_WARPS * 32>(m.partials, active, lanes, w32);
+        __syncthreads();
+        double r1 = 0.0;
+        if (NDOT > 1) r1 = final_reduce_t<ST_WARPS * 32>(m.partials + cap, active, lanes, w32);
+        if (threadIdx.x == 0) {
+            store(r0, r1);
+            m.counters[counter] = 0u;
+        }
+    }
+}
+// Staged pass in the black-cell layout of w0_black: prep(S, brick, lane) once per brick, then each lane's 8
+// black cells through apply(S, i, l).
+template <int NF, int NB, class Prep, class Apply>
+__device__ __forceinline__ void st_black(const Dev& d, const MGState& m, const float* const* fa, const float* const* ba, Prep prep,
+                                         Apply apply) {
+    extern __shared__ __align__(16) unsigned char st_smem[];
+    using Stg = WarpStage<NF, NB>;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    Stg& S = reinterpret_cast<Stg*>(st_smem)[warp];
+    if (lane == 0) {
+        tc::mbar_init(&S.bar, 1u);
+        tc::fence_mbar_init();
+    }
+    __syncwarp();
+    const uint32_t active = d.active_bricks[0];
+    uint32_t parity = 0u;
+    for (uint32_t e = blockIdx.x * ST_WARPS + warp; e < active; e += gridDim.x * ST_WARPS) {
+        const uint4 s0 = *reinterpret_cast<const uint4*>(m.nbr_slots + 8u * e);
+        const uint4 s1 = *reinterpret_cast<const uint4*>(m.nbr_slots + 8u * e + 4u);
+        const uint32_t ns[6] = {s0.x, s0.y, s0.z, s0.w, s1.x, s1.y};
+        const uint32_t base = s1.z * BRICK_CELLS;
+        stage_issue<NF, NB>(S, fa, ba, m.word, s1.z, ns, lane);
+        prep(S, s1.w, lane);  // its loads overlap the copies
+        if (!stage_wait<NF, NB>(S, parity, m.ctl + 5)) break;
+        parity ^= 1u;
+#pragma unroll
+        for (uint32_t k = 0; k < 8u; ++k) {
+            const uint32_t l = black_local(lane, k);
+            apply(S, base + l, l);
+        }
+    }
+}
+template <int NF, int NB>
+constexpr size_t st_smem_bytes() {
+    const size_t stage = sizeof(WarpStage<NF, NB>) * ST_WARPS;
+    const size_t reduce = (1024 + 32) * sizeof(double);
+    return stage > reduce ? stage : reduce;
+}
+
+// k_smooth0 from a stage: z (face), r and the diagonal (bodies).
+template <bool DOT>
+__global__ void __launch_bounds__(ST_WARPS * 32) k_smooth0_st(Dev d, MGState m) {
+    const float* fa[1] = {m.z};
+    const float* ba[2] = {m.r, d.cell_diag};
+    st_pass<1, 2, DOT ? 1 : 0>(d, m, 1, fa, ba,
+        [&](WarpStage<1, 2>& S, const Geo& g, double* v0, double*) {
+            const Q6 z = sq6(S.f[0], g);
+            const float4 r = sld4(S.b[0], g.l), dg = sld4(S.b[1], g.l);
+            const uint32_t w4 = sword4(S.word, g);
+            const X2 x = partner(z);
+            float out[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const uint32_t w = word_of(w4, j);
+                const float zj = comp(z.c, j), rj = comp(r, j);
+                out[j] = zj;
+                if (!(w & W_FLUID)) continue;
+                if (w & W_RED) {
+                    float n[6];
+                    nbrs6(z, x, g.h, j, n);
+                    const float val = (rj + nb_sum(n, w)) / (comp(dg, j) + DIAG_EPSILON);
+                    out[j] = val;
+                    v0[j] = double(rj * val);
+                } else {
+                    v0[j] = double(rj * zj);
+                }
+            }
+            st4(m.z + g.i, out);
+        },
+        [&](double rho, double) { m.scalars[3] = m.scalars[0]; m.scalars[0] = rho; });
+}
+// Black sweep from a stage.
+__global__ void __launch_bounds__(ST_WARPS * 32) k_smooth0_black_st(Dev d, MGState m) {
+    const float* fa[1] = {m.z};
+    const float* ba[2] = {m.r, d.cell_diag};
+    st_black<1, 2>(d, m, fa, ba, [](WarpStage<1, 2>&, uint32_t, uint32_t) {},
+        [&](WarpStage<1, 2>& S, uint32_t i, uint32_t l) {
+            const uint32_t w = S.word[l];
+            if (!(w & W_FLUID)) return;
+            float n[6];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) n[k] = snbr(S.f[0], l, k);
+            m.z[i] = (S.b[0][l] + nb_sum(n, w)) / (S.b[1][l] + DIAG_EPSILON);
+        });
+}
+// k_prolong_smooth0 from a stage (the level-1 6^3 block is staged by plain loads as before).
+__global__ void __launch_bounds__(ST_WARPS * 32) k_prolong_smooth0_st(Dev d, MGState m) {
+    __shared__ float s_cx[ST_WARPS][216];
+    const MGLevel C = m.lv[1];
+    float* cx = s_cx[threadIdx.x >> 5];
+    const float* fa[1] = {m.z};
+    const float* ba[2] = {m.r, d.cell_diag};
+    st_black<1, 2>(d, m, fa, ba,
+        [&](WarpStage<1, 2>&, uint32_t brick, uint32_t lane) {
+            const int3 bc = brick_coord_of(d, brick);
+            __syncwarp();
+            float v[7];
+#pragma unroll
+            for (int r = 0; r < 7; ++r) {
+                const uint32_t j = lane + 32u * uint32_t(r);
+                const int3 c = make_int3(bc.x * 4 - 1 + int(j % 6u), bc.y * 4 - 1 + int((j / 6u) % 6u), bc.z * 4 - 1 + int(j / 36u));
+                v[r] = 0.0f;
+                if (j < 216u && inside3(c, C.dim)) {
+                    const uint32_t ci = lin3(c, C.dim);
+                    const float x = lv_ld(C.x, ci, C.prec);
+                    v[r] = (C.word[ci] & CW_FLUID) ? x : 0.0f;
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < 7; ++r) {
+                const uint32_t j = lane + 32u * uint32_t(r);
+                if (j < 216u) cx[j] = v[r];
+            }
+        },
+        [&](WarpStage<1, 2>& S, uint32_t i, uint32_t l) {
+            const uint32_t w = S.word[l];
+            if (!(w & W_FLUID)) return;
+            const int x = int(l & 7u), y = int((l >> 3) & 7u), z = int(l >> 6);
+            const int p = ((x >> 1) + 1) + 6 * ((y >> 1) + 1) + 36 * ((z >> 1) + 1);
+            const int px = (x & 1) ? 1 : 0, py = (y & 1) ? 6 : 0, pz = (z & 1) ? 36 : 0;
+            const int po[6] = {p - 1 + px, p + px, p - 6 + py, p + py, p - 36 + pz, p + pz};
+            float sum = 0.0f;
+#pragma unroll
+            for (int n = 0; n < 6; ++n)
+                if ((w >> n) & 1u) sum = sum + (snbr(S.f[0], l, n) + cx[po[n]]);
+            m.z[i] = (S.b[0][l] + sum) / (S.b[1][l] + DIAG_EPSILON);
+        });
+}
+// k_restrict0 from a stage: the brick's fine residuals into the warp's s_res, then the 64 coarse cells.
+__global__ void __launch_bounds__(ST_WARPS * 32) k_restrict0_st(Dev d, MGState m) {
+    __shared__ float s_res[ST_WARPS][BRICK_CELLS];
+    const MGLevel C = m.lv[1];
+    const uint32_t warp = threadIdx.x >> 5;
+    const float* fa[1] = {m.z};
+    const float* ba[2] = {m.r, d.cell_diag};
+    const float scale = m.restrict_scale;
+    extern __shared__ __align__(16) unsigned char st_smem[];
+    using Stg = WarpStage<1, 2>;
+    const uint32_t lane = threadIdx.x & 31u;
+    Stg& S = reinterpret_cast<Stg*>(st_smem)[warp];
+    if (lane == 0) {
+        tc::mbar_init(&S.bar, 1u);
+        tc::fence_mbar_init();
+    }
+    __syncwarp();
+    const uint32_t active = d.active_bricks[0];
+    uint32_t parity = 0u;
+    for (uint32_t e = blockIdx.x * ST_WARPS + warp; e < active; e += gridDim.x * ST_WARPS) {
+        const uint4 s0 = *reinterpret_cast<const uint4*>(m.nbr_slots + 8u * e);
+        const uint4 s1 = *reinterpret_cast<const uint4*>(m.nbr_slots + 8u * e + 4u);
+        const uint32_t ns[6] = {s0.x, s0.y, s0.z, s0.w, s1.x, s1.y};
+        if (!stage_brick<1, 2>(S, fa, ba, m.word, s1.z, ns, lane, parity, m.ctl + 5)) break;
+        parity ^= 1u;
+#pragma unroll
+        for (uint32_t k = 0; k < 4u; ++k) {
+            const Geo g = geo_of(0u, lane, k);
+            const Q6 z = sq6(S.f[0], g);
+            const float4 r = sld4(S.b[0], g.l), dg = sld4(S.b[1], g.l);
+            const uint32_t w4 = sword4(S.word, g);
+            const X2 x = partner(z);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const uint32_t w = word_of(w4, j);
+                float n[6];
+                nbrs6(z, x, g.h, j, n);
+                const float diag = comp(dg, j) + DIAG_EPSILON;
+                if (w & W_FLUID) s_res[warp][g.l + uint32_t(j)] = comp(r, j) - (diag * comp(z.c, j) - nb_sum(n, w));
+            }
+        }
+        __syncwarp();
+        const int3 bc = brick_coord_of(d, s1.w);
+#pragma unroll
+        for (uint32_t h = 0; h < 2u; ++h) {
+            const uint32_t lc = lane + 32u * h;
+            const int3 cl = make_int3(int(lc & 3u), int((lc >> 2) & 3u), int(lc >> 4));
+            const int3 c = make_int3(bc.x * 4 + cl.x, bc.y * 4 + cl.y, bc.z * 4 + cl.z);
+            if (!inside3(c, C.dim)) continue;
+            const uint32_t ci = lin3(c, C.dim);
+            const uint32_t cw = C.word[ci];
+            if (!(cw & CW_FLUID)) {
+                lv_st(C.b, ci, C.prec, 0.0f);
+                lv_st(C.x, ci, C.prec, 0.0f);
+                continue;
+            }
+            float sum = 0.0f;
+#pragma unroll
+            for (int o = 0; o < 8; ++o) {
+                const uint32_t fl = uint32_t((2 * cl.x + (o & 1)) + 8 * ((2 * cl.y + ((o >> 1) & 1)) + 8 * (2 * cl.z + ((o >> 2) & 1))));
+                if (S.word[fl] & W_FLUID) sum = sum + s_res[warp][fl];
+            }
+            const float bb = scale * sum;
+            lv_st(C.b, ci, C.prec, bb);
+            lv_st(C.x, ci, C.prec, (cw & CW_RED) ? bb / word_diag(cw) : 0.0f);
+        }
+    }
+}
+// k_apply_a from a stage: z and the previous direction (faces), the diagonal (body).
+__global__ void __launch_bounds__(ST_WARPS * 32) k_apply_a_st(Dev d, MGState m) {
+    const uint32_t it = m.ctl[0];
+    const bool first = it == 0u;
+    const float beta = first ? 0.0f : ratio_f(m.flexible ? m.scalars[0] - m.scalars[9] : m.scalars[0], m.scalars[3]);
+    const float* dold = dir_buf_c(m, it & 1u);
+    float* dnew = dir_buf(m, (it + 1u) & 1u);
+    const float* fa[2] = {m.z, dold};
+    const float* ba[1] = {d.cell_diag};
+    st_pass<2, 1, 1>(d, m, 2, fa, ba,
+        [&](WarpStage<2, 1>& S, const Geo& g, double* v0, double*) {
+            const Q6 vz = sq6(S.f[0], g), vd = sq6(S.f[1], g);
+            const float4 dg = sld4(S.b[0], g.l);
+            const uint32_t w4 = sword4(S.word, g);
+            const X2 xz = partner(vz), xd = partner(vd);
+            float dn[4], q[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const uint32_t w = word_of(w4, j);
+                dn[j] = 0.0f;
+                q[j] = 0.0f;
+                if (!(w & W_FLUID)) continue;
+                const float dj = first ? comp(vz.c, j) : comp(vz.c, j) + beta * comp(vd.c, j);
+                float nz[6], nd[6];
+                nbrs6(vz, xz, g.h, j, nz);
+                nbrs6(vd, xd, g.h, j, nd);
+                float sum = 0.0f;
+#pragma unroll
+                for (int n = 0; n < 6; ++n)
+                    if ((w >> n) & 1u) sum = sum + (first ? nz[n] : nz[n] + beta * nd[n]);
+                const float qi = (comp(dg, j) + DIAG_EPSILON) * dj - sum;
+                dn[j] = dj;
+                q[j] = qi;
+                v0[j] = double(dj * qi);
+            }
+            st4(dnew + g.i, dn);
+            st4(m.q + g.i, q);
+        },
+        [&](double dq, double) { m.scalars[2] = dq; });
 }
 
 // ---- the small coarse levels in one CTA: levels tail..nl-1 of the V-cycle --------------------------------
@@ -952,7 +1420,16 @@ __global__ void __launch_bounds__(1024) k_vcycle_tail(MGState m, int tail, int i
         }
     }
     __syncthreads();
-    if (tail < nl - 1) s_sweep(S[tail], 1u);
+    // pre-smoothing of a level: its black half (the red half is the restriction's initialisation), then
+    // m.sweeps - 1 more red-black pairs
+    auto pre_smooth = [&](const SLevel& L) {
+        s_sweep(L, 1u);
+        for (int k = 1; k < m.sweeps; ++k) {
+            s_sweep(L, 0u);
+            s_sweep(L, 1u);
+        }
+    };
+    if (tail < nl - 1) pre_smooth(S[tail]);
     for (int l = tail; l < nl - 1; ++l) {
         const SLevel F = S[l];
         const SLevel C = S[l + 1];
@@ -976,12 +1453,12 @@ __global__ void __launch_bounds__(1024) k_vcycle_tail(MGState m, int tail, int i
 #pragma unroll
             for (int o = 0; o < 8; ++o)
                 if ((fl >> o) & 1u) sum = sum + res[o];
-            const float bb = 0.25f * sum;
+            const float bb = m.restrict_scale * sum;
             C.b[ci] = q_prec(bb, C.prec);
             C.x[ci] = q_prec((C.word[ci] & CW_RED) ? bb / C.diag[ci] : 0.0f, C.prec);
         }
         __syncthreads();
-        if (l + 1 < nl - 1) s_sweep(C, 1u);
+        if (l + 1 < nl - 1) pre_smooth(C);
     }
     s_coarse_solve(S[nl - 1], iterations);
     for (int l = nl - 2; l >= tail; --l) {
@@ -994,8 +1471,10 @@ __global__ void __launch_bounds__(1024) k_vcycle_tail(MGState m, int tail, int i
             if (C.word[pi] & CW_FLUID) F.x[i] = q_prec(F.x[i] + C.x[pi], F.prec);
         }
         __syncthreads();
-        s_sweep(F, 1u);
-        s_sweep(F, 0u);
+        for (int k = 0; k < m.sweeps; ++k) {
+            s_sweep(F, 1u);
+            s_sweep(F, 0u);
+        }
     }
     {
         const uint32_t c16 = tail_pad4(m.lv[tail].cells) / 4u;
@@ -1034,12 +1513,12 @@ __global__ void __launch_bounds__(1024) k_coarse_solve0(Dev d, MGState m, int it
 // d is double-buffered by iteration parity (ctl[0] is the number of finished iterations): the pass reads
 // the previous direction from one buffer and writes the new one to the other, and forms each fluid
 // neighbour's new direction z_n + beta d_n itself (bit-identical to what that neighbour writes).
-__device__ __forceinline__ float* dir_buf(const MGState& m, uint32_t parity) { return parity ? m.dvec2 : m.dvec; }
 
 __global__ void __launch_bounds__(GRID_THREADS, 3) k_apply_a(Dev d, MGState m) {
     const uint32_t it = m.ctl[0];
     const bool first = it == 0u;
-    const float beta = first ? 0.0f : ratio_f(m.scalars[0], m.scalars[3]);
+    // flexible PCG: beta = (rho_k - r_k.z_{k-1}) / rho_{k-1}, the numerator formed in FP64
+    const float beta = first ? 0.0f : ratio_f(m.flexible ? m.scalars[0] - m.scalars[9] : m.scalars[0], m.scalars[3]);
     const float* dold = dir_buf(m, it & 1u);
     float* dnew = dir_buf(m, (it + 1u) & 1u);
     struct V {
@@ -1085,14 +1564,16 @@ __global__ void __launch_bounds__(GRID_THREADS, 3) k_apply_a(Dev d, MGState m) {
 }
 
 // ---- PCGUpdatePRCS: p += alpha d, r -= alpha q, red pre-smooth; ||r||^2 and the loop decision -------------
+// FLEX (flexible PCG) also reduces r_{k+1}.z_k with the z of the finished V-cycle, before it is overwritten.
+template <bool FLEX>
 __global__ void __launch_bounds__(GRID_THREADS, 3) k_update_pr(Dev d, MGState m, float* __restrict__ p, unsigned long long handle) {
     const float alpha = ratio_f(m.scalars[0], m.scalars[2]);
     const float* dcur = dir_buf(m, (m.ctl[0] + 1u) & 1u);
     struct V {
-        float4 p, d, r, q, dg;
+        float4 p, d, r, q, dg, z;
         uint32_t w;
     };
-    w4_pass<1, 2>(d, m, 3,
+    w4_pass<FLEX ? 2 : 1, 2>(d, m, 3,
         [&](const Geo& g, const uint32_t*) {
             V v;
             v.p = ld4(p + g.i);
@@ -1100,10 +1581,11 @@ __global__ void __launch_bounds__(GRID_THREADS, 3) k_update_pr(Dev d, MGState m,
             v.r = ld4(m.r + g.i);
             v.q = ld4(m.q + g.i);
             v.dg = ld4(d.cell_diag + g.i);
+            v.z = FLEX ? ld4(m.z + g.i) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
             v.w = quad_words(m, g);
             return v;
         },
-        [&](const Geo& g, const V& v, double* v0, double*) {
+        [&](const Geo& g, const V& v, double* v0, double* v1) {
             float po[4], ro[4], zo[4];
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
@@ -1117,13 +1599,15 @@ __global__ void __launch_bounds__(GRID_THREADS, 3) k_update_pr(Dev d, MGState m,
                 ro[j] = ri;
                 zo[j] = (w & W_RED) ? ri / (comp(v.dg, j) + DIAG_EPSILON) : 0.0f;
                 v0[j] = double(ri * ri);
+                if (FLEX) v1[j] = double(ri * comp(v.z, j));
             }
             st4(p + g.i, po);
             st4(m.r + g.i, ro);
             st4(m.z + g.i, zo);
         },
-        [&](double rr, double) {
+        [&](double rr, double rz) {
             m.scalars[5] = rr;
+            if (FLEX) m.scalars[9] = rz;
             const uint32_t it = m.ctl[0] + 1u;
             m.ctl[0] = it;
             const double bb = m.scalars[4];
@@ -1173,6 +1657,34 @@ __global__ void __launch_bounds__(GRID_THREADS) k_true_residual(Dev d, MGState m
 
 inline int blocks_for(uint32_t n, int threads) { return int((n + uint32_t(threads) - 1u) / uint32_t(threads)); }
 
+// Level-0 passes from shared-memory stages (default) or straight from global memory (SLOSH_MG_STAGED=0).
+bool mg_staged() {
+    static const int v = [] {
+        const char* e = std::getenv("SLOSH_MG_STAGED");
+        return (e && e[0] == '0') ? 0 : 1;
+    }();
+    return v != 0;
+}
+// Grid of a staged pass: every CTA resident at once (one wave), at most one warp per pool brick.
+template <class K>
+int st_grid(K kernel, size_t smem, const Dev& d, const Shape& sh) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, ST_WARPS * 32, smem) != cudaSuccess || per_sm < 1) {
+        cudaGetLastError();
+        per_sm = 1;
+    }
+    const int cap = int((d.num_pool_bricks + uint32_t(ST_WARPS) - 1u) / uint32_t(ST_WARPS));
+    return std::max(1, std::min(cap, per_sm * sh.num_sms));
+}
+#define ST_LAUNCH(kernel, NF, NB, d, m, sh, s)                                         \
+    do {                                                                           \
+        constexpr size_t smem_ = st_smem_bytes<NF, NB>();                          \
+        static int grid_ = 0;                                                      \
+        if (!grid_) grid_ = st_grid(kernel, smem_, d, sh);                          \
+        kernel<<<std::min(grid_, st_grid_cap(d)), ST_WARPS * 32, smem_, s>>>(d, m); \
+    } while (0)
+inline int st_grid_cap(const Dev& d) { return std::max(1, int((d.num_pool_bricks + uint32_t(ST_WARPS) - 1u) / uint32_t(ST_WARPS))); }
+
 }  // namespace
 
 int mg_tail_level(const MGState& m) {
@@ -1221,9 +1733,23 @@ int launch_mg_tail_lists(const MGState& m, cudaStream_t s) {
 // One V-cycle (SloshProxy.cpp:904-959), leaving rho = r.z in scalars[0] (previous rho in scalars[3]).
 int launch_vcycle(const Dev& d, const MGState& m, int coarse_iterations, const Shape& sh, cudaStream_t s) {
     const int nl = m.num_levels;
+    const bool staged = mg_staged();
+    auto smooth0_red = [&](bool dot) {
+        if (staged) {
+            if (dot) ST_LAUNCH(k_smooth0_st<true>, 1, 2, d, m, sh, s);
+            else ST_LAUNCH(k_smooth0_st<false>, 1, 2, d, m, sh, s);
+        } else {
+            if (dot) k_smooth0<true><<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m);
+            else k_smooth0<false><<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m);
+        }
+    };
+    auto smooth0_black = [&]() {
+        if (staged) ST_LAUNCH(k_smooth0_black_st, 1, 2, d, m, sh, s);
+        else k_smooth0_black<<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m);
+    };
     if (nl == 1) {
         k_coarse_solve0<<<1, 1024, 0, s>>>(d, m, coarse_iterations);
-        k_smooth0<<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m);
+        smooth0_red(true);
         return 2;
     }
     const int tail = mg_tail_level(m);
@@ -1233,26 +1759,55 @@ int launch_vcycle(const Dev& d, const MGState& m, int coarse_iterations, const S
         const uint64_t cells = l <= 3 ? uint64_t(d.num_pool_bricks - 1u) * side * side * side : uint64_t(m.lv[l].cells);
         return int(std::max<uint64_t>(1, std::min<uint64_t>(uint64_t(sh.brick_ctas), (cells + 255u) / 256u)));
     };
+    // Pre-smoothing: the black half of the first pair (the red half is the red initialisation written by
+    // UpdatePR or the restriction), then sweeps - 1 red-black pairs. Post-smoothing: sweeps black-red pairs,
+    // the first black half fused with the prolongation, the last red half of level 0 with rho = r.z.
+    const int sweeps = std::max(m.sweeps, 1);
     int n = 0;
-    k_smooth0_black<<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m);
+    smooth0_black();
     ++n;
+    for (int k = 1; k < sweeps; ++k) {
+        smooth0_red(false);
+        smooth0_black();
+        n += 2;
+    }
     for (int l = 0; l < tail; ++l) {
-        if (l == 0) k_restrict0<<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m);
-        else k_restrict_fp<<<fp_blocks(l + 1), 256, 0, s>>>(d, m, l);
+        if (l == 0) {
+            if (staged) ST_LAUNCH(k_restrict0_st, 1, 2, d, m, sh, s);
+            else k_restrict0<<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m);
+        } else {
+            k_restrict_fp<<<fp_blocks(l + 1), 256, 0, s>>>(d, m, l);
+        }
         ++n;
-        if (l + 1 < tail) {  // the tail kernel does its own first smoothing sweep
+        if (l + 1 < tail) {  // the tail kernel does its own pre-smoothing
             k_smooth_fp<<<fp_blocks(l + 1), 256, 0, s>>>(d, m, l + 1, 1u);
             ++n;
+            for (int k = 1; k < sweeps; ++k) {
+                k_smooth_fp<<<fp_blocks(l + 1), 256, 0, s>>>(d, m, l + 1, 0u);
+                k_smooth_fp<<<fp_blocks(l + 1), 256, 0, s>>>(d, m, l + 1, 1u);
+                n += 2;
+            }
         }
     }
     k_vcycle_tail<<<1, 1024, mg_tail_smem(m), s>>>(m, tail, coarse_iterations);
     ++n;
     for (int l = tail - 1; l >= 0; --l) {
         if (l == 0) {
-            k_prolong_smooth0<<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m);
-            k_smooth0<<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m);
+            if (staged) ST_LAUNCH(k_prolong_smooth0_st, 1, 2, d, m, sh, s);
+            else k_prolong_smooth0<<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m);
+            for (int k = 1; k < sweeps; ++k) {
+                smooth0_red(false);
+                smooth0_black();
+                n += 2;
+            }
+            smooth0_red(true);
         } else {
             k_prolong_smooth_fp<<<fp_blocks(l), 256, 0, s>>>(d, m, l);
+            for (int k = 1; k < sweeps; ++k) {
+                k_smooth_fp<<<fp_blocks(l), 256, 0, s>>>(d, m, l, 0u);
+                k_smooth_fp<<<fp_blocks(l), 256, 0, s>>>(d, m, l, 1u);
+                n += 2;
+            }
             k_smooth_fp<<<fp_blocks(l), 256, 0, s>>>(d, m, l, 0u);
         }
         n += 2;
@@ -1260,11 +1815,13 @@ int launch_vcycle(const Dev& d, const MGState& m, int coarse_iterations, const S
     return n;
 }
 int launch_pcg_apply_a(const Dev& d, const MGState& m, const Shape& sh, cudaStream_t s) {
-    k_apply_a<<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m);
+    if (mg_staged()) ST_LAUNCH(k_apply_a_st, 2, 1, d, m, sh, s);
+    else k_apply_a<<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m);
     return 1;
 }
 int launch_pcg_update_pr(const Dev& d, const MGState& m, float* p, unsigned long long handle, const Shape& sh, cudaStream_t s) {
-    k_update_pr<<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m, p, handle);
+    if (m.flexible) k_update_pr<true><<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m, p, handle);
+    else k_update_pr<false><<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m, p, handle);
     return 1;
 }
 int launch_pcg_update_d(const Dev&, const MGState&, const Shape&, cudaStream_t) { return 0; }  // fused into ApplyA

@@ -336,32 +336,50 @@ __device__ __forceinline__ void stencil_indices(const Dev& d, const Stencil& s, 
     }
 }
 
+// Trilinear interpolation of the 8 stencil values u[o] (o = x + 2 y + 4 z) as lerps with fused
+// multiply-adds, x then y then z, and (grad) the three partial derivatives from the same differences:
+// mathematically the reference's sum_o w_o u_o and sum_o sign_o (w3 w3) inv_h u_o (Slosh.usf:1376-1443),
+// in about a sixth of its operations. The oracle rounds in the same order.
+__device__ __forceinline__ float lerp3(const float (&u)[8], float fx, float fy, float fz, float inv_h, bool grad, float3* g3) {
+    const float d00 = u[1] - u[0], d10 = u[3] - u[2], d01 = u[5] - u[4], d11 = u[7] - u[6];
+    const float a00 = __fmaf_rn(fx, d00, u[0]), a10 = __fmaf_rn(fx, d10, u[2]);
+    const float a01 = __fmaf_rn(fx, d01, u[4]), a11 = __fmaf_rn(fx, d11, u[6]);
+    const float e0 = a10 - a00, e1 = a11 - a01;
+    const float b0 = __fmaf_rn(fy, e0, a00), b1 = __fmaf_rn(fy, e1, a01);
+    const float g = b1 - b0;
+    if (grad) {
+        g3->z = g * inv_h;
+        g3->y = __fmaf_rn(fz, e1 - e0, e0) * inv_h;
+        const float c0 = __fmaf_rn(fy, d10 - d00, d00), c1 = __fmaf_rn(fy, d11 - d01, d01);
+        g3->x = __fmaf_rn(fz, c1 - c0, c0) * inv_h;
+    }
+    return __fmaf_rn(fz, g, b0);
+}
+
 // GatherComponent (Slosh.usf:1376-1410).
 __device__ __forceinline__ void gather_component(const Dev& d, const Pass& p, int axis, float3 xp, const float* __restrict__ vel,
                                                  float& unew, float& dsum, float& dw, float3& grad) {
     const Stencil s = stencil_of(d, xp, axis);
     uint32_t idx[8];
     stencil_indices(d, s, axis, idx);
-    unew = 0.0f; dsum = 0.0f; dw = 0.0f;
+    dsum = 0.0f; dw = 0.0f;
     grad = make_float3(0.0f, 0.0f, 0.0f);
+    float u[8];
 #pragma unroll
-    for (int o = 0; o < 8; ++o) {
-        const int oix = o & 1, oiy = (o >> 1) & 1, oiz = (o >> 2) & 1;
-        const float w3x = oix ? s.fx : 1.0f - s.fx, w3y = oiy ? s.fy : 1.0f - s.fy, w3z = oiz ? s.fz : 1.0f - s.fz;
-        const float w = w3x * w3y * w3z;
-        const float sx = oix ? 1.0f : -1.0f, sy = oiy ? 1.0f : -1.0f, sz = oiz ? 1.0f : -1.0f;
-        const uint32_t f = idx[o];
-        const float u = vel[f];
-        unew = unew + w * u;
-        if (p.use_apic != 0u) {
-            grad.x = grad.x + sx * (w3y * w3z) * d.inv_h * u;
-            grad.y = grad.y + sy * (w3x * w3z) * d.inv_h * u;
-            grad.z = grad.z + sz * (w3x * w3y) * d.inv_h * u;
-        } else if ((d.face_flags[f] & FACE_HAS_WEIGHT) != 0u) {
-            dsum = dsum + w * (u - d.vel_old[f]);
+    for (int o = 0; o < 8; ++o) u[o] = vel[idx[o]];
+    if (p.use_apic == 0u) {
+#pragma unroll
+        for (int o = 0; o < 8; ++o) {
+            const uint32_t f = idx[o];
+            if ((d.face_flags[f] & FACE_HAS_WEIGHT) == 0u) continue;
+            const int oix = o & 1, oiy = (o >> 1) & 1, oiz = (o >> 2) & 1;
+            const float w3x = oix ? s.fx : 1.0f - s.fx, w3y = oiy ? s.fy : 1.0f - s.fy, w3z = oiz ? s.fz : 1.0f - s.fz;
+            const float w = w3x * w3y * w3z;
+            dsum = dsum + w * (u[o] - d.vel_old[f]);
             dw = dw + w;
         }
     }
+    unew = lerp3(u, s.fx, s.fy, s.fz, d.inv_h, p.use_apic != 0u, &grad);
 }
 // SampleVelocityComponent (Slosh.usf:1417-1443).
 __device__ __forceinline__ float sample_component(const Dev& d, int axis, float3 xp, float fallback, bool check,
@@ -370,17 +388,15 @@ __device__ __forceinline__ float sample_component(const Dev& d, int axis, float3
     const Stencil s = stencil_of(d, xp, axis);
     uint32_t idx[8];
     stencil_indices(d, s, axis, idx);
-    float u = 0.0f;
+    float u[8];
 #pragma unroll
-    for (int o = 0; o < 8; ++o) {
-        const int oix = o & 1, oiy = (o >> 1) & 1, oiz = (o >> 2) & 1;
-        const float w3x = oix ? s.fx : 1.0f - s.fx, w3y = oiy ? s.fy : 1.0f - s.fy, w3z = oiz ? s.fz : 1.0f - s.fz;
-        const uint32_t f = idx[o];
-        float uf = vel[f];
-        if (check && (d.face_flags[f] & known) == 0u) uf = fallback;
-        u = u + w3x * w3y * w3z * uf;
+    for (int o = 0; o < 8; ++o) u[o] = vel[idx[o]];
+    if (check) {
+#pragma unroll
+        for (int o = 0; o < 8; ++o)
+            if ((d.face_flags[idx[o]] & known) == 0u) u[o] = fallback;
     }
-    return u;
+    return lerp3(u, s.fx, s.fy, s.fz, d.inv_h, false, nullptr);
 }
 // SampleDensityDisplacement (Slosh.usf:830-854).
 __device__ __forceinline__ float3 sample_displacement(const Dev& d, float3 xp, const float* __restrict__ disp) {
@@ -390,14 +406,10 @@ __device__ __forceinline__ float3 sample_displacement(const Dev& d, float3 xp, c
         const Stencil s = stencil_of(d, xp, axis);
         uint32_t idx[8];
         stencil_indices(d, s, axis, idx);
-        float value = 0.0f;
+        float u[8];
 #pragma unroll
-        for (int o = 0; o < 8; ++o) {
-            const int oix = o & 1, oiy = (o >> 1) & 1, oiz = (o >> 2) & 1;
-            const float w3x = oix ? s.fx : 1.0f - s.fx, w3y = oiy ? s.fy : 1.0f - s.fy, w3z = oiz ? s.fz : 1.0f - s.fz;
-            value = value + w3x * w3y * w3z * disp[idx[o]];
-        }
-        out[axis] = value;
+        for (int o = 0; o < 8; ++o) u[o] = disp[idx[o]];
+        out[axis] = lerp3(u, s.fx, s.fy, s.fz, d.inv_h, false, nullptr);
     }
     const float3 v = make_float3(out[0], out[1], out[2]);
     const float len = len3(v);

@@ -101,16 +101,21 @@ def pair(slosh, oracle_mod, sc):
     return g, o
 
 
-def run_frames(g, o, sc, frames, check_every_substep=True, tol=1e-5):
+def run_frames(g, o, sc, frames, check_every_substep=True, tol=1e-5, substeps=None):
     """Steps GPU and oracle frame by frame (emits on the first frame; colliders and manipulators every
-    frame) and compares the whole state after every substep and the results after every frame."""
+    frame) and compares the whole state after every substep and the results after every frame. With
+    `substeps`, runs whole frames until at least that many substeps were compared (`frames` is then a cap)."""
     extra = dict(colliders=sc.get("colliders", []), manipulators=sc.get("manipulators", []))
     fi = A.frame_input(sc["settings"], emits=sc["emits"], **extra)
     reports = []
+    done = 0
     for f in range(frames):
+        if substeps is not None and done >= substeps:
+            break
         ng, dtg = g.begin_frame(fi)
         no, dto = o.begin_frame(fi)
         assert (ng, dtg) == (no, dto), f"frame {f}: substeps/dt differ {ng, dtg} vs {no, dto}"
+        done += ng
         for s in range(ng):
             g.substep(s)
             o.substep(s)
@@ -132,4 +137,6 @@ def run_frames(g, o, sc, frames, check_every_substep=True, tol=1e-5):
                 assert list(getattr(fg, name)) == list(getattr(fo, name)) if hasattr(getattr(fg, name), "__len__") \
                     else getattr(fg, name) == getattr(fo, name), f"frame {f} collider {k} {name}"
         fi = A.frame_input(sc["settings"], **extra)
+    if substeps is not None:
+        assert done >= substeps, f"only {done} substeps in {frames} frames"
     return reports

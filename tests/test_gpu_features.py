@@ -193,3 +193,26 @@ def test_launch_shape_does_not_change_results(slosh):
         sim.close()
     assert np.array_equal(runs[0][0], runs[1][0])
     assert np.array_equal(runs[0][1], runs[1][1])
+
+
+@pytest.mark.parametrize("scale,sweeps,flexible,mode", [
+    (1.7, 1, 0, A.PRECISION_FP32),
+    (1.7, 2, 1, A.PRECISION_FP32),
+    (1.0, 3, 1, A.PRECISION_FP32),
+    (1.9, 1, 1, A.PRECISION_BF16_STORAGE),
+])
+def test_preconditioner_options(slosh, oracle_mod, scale, sweeps, flexible, mode):
+    """The multigrid preconditioner's options (coarse-grid correction scale, red-black sweep pairs per
+    smoothing, flexible PCG, with FP32 and BF16 coarse storage) on a 96^3 sparse scene whose hierarchy uses
+    footprint levels, the shared-memory tail and the coarsest solve: bit-exact against the oracle run with
+    the same options, every solve to its tolerance."""
+    sc = scenes.dam_break_sphere(slosh.settings_default, n=96)
+    s = sc["settings"]
+    s.max_substeps = 16
+    s.mg_correction_scale = scale
+    s.mg_smoothing_sweeps = sweeps
+    s.pcg_flexible = flexible
+    s.precision_mode = mode
+    g, o = pair(slosh, oracle_mod, sc)
+    run_frames(g, o, sc, frames=2)
+    assert g.results().last_solve_rel_residual <= 1e-6

@@ -356,3 +356,33 @@ def test_bf16_conversion_matches_torch(oracle_mod):
     lib = oracle_mod.lib()
     got = np.array([lib.oracle_f32_to_bf16(float(v)) for v in x], dtype=np.uint16)
     assert np.array_equal(got, want)
+
+
+def test_overcorrected_vcycle_needs_fewer_iterations(oracle_mod):
+    """The piecewise-constant prolongation under-corrects smooth errors; scaling each coarse-grid correction
+    by 1.7 (mg_correction_scale) and a second red-black sweep pair (mg_smoothing_sweeps) must each reach the
+    same 1e-6 relative residual in fewer PCG iterations than the reference's V-cycle on the same scene,
+    and flexible PCG must not change the count of a linear preconditioner by more than one."""
+    from slosh_b200 import scenes
+    counts = {}
+    for key, (scale, sweeps, flex) in {"ref": (1.0, 1, 0), "scaled": (1.7, 1, 0), "two": (1.7, 2, 0),
+                                       "flex": (1.7, 1, 1)}.items():
+        sc = scenes.dam_break_sphere(oracle_mod.settings_default, n=48)
+        s = sc["settings"]
+        s.max_substeps = 16
+        s.mg_correction_scale, s.mg_smoothing_sweeps, s.pcg_flexible = scale, sweeps, flex
+        o = oracle_mod.Oracle(s)
+        o.set_emit_seed(sc["seed"])
+        fi = A.frame_input(s, emits=sc["emits"])
+        its = []
+        for _ in range(3):
+            o.step_frame(fi)
+            fi = A.frame_input(s)
+            r = o.results()
+            assert r.last_solve_rel_residual <= 1e-6
+            its.append(r.last_solve_iterations)
+        o.close()
+        counts[key] = its
+    assert sum(counts["scaled"]) < sum(counts["ref"]), counts
+    assert sum(counts["two"]) < sum(counts["scaled"]), counts
+    assert all(abs(a - b) <= 1 for a, b in zip(counts["flex"], counts["scaled"])), counts
