@@ -1055,6 +1055,11 @@ public:
     }
 
     // ---- P2GCS, Slosh.usf:401-563: fixed-point sums are order independent -------------------------------
+    // P2GCS (Slosh.usf:448-563): per MAC component the 8 stencil nodes receive w (u_p + C_p . (x_n - x_p)) and w
+    // in 2^20 fixed point. The per-node terms are formed from per-axis factors: with S = 2^20,
+    // wS = w_x ((w_y w_z) S) and the affine term (u_p + C_x dx) + (C_y dy + C_z dz), then
+    // mom = rn(wS term) and weight = rn(wS). Mathematically the reference's w (u + dot(C, x_n - x_p)) S and
+    // w S; the GPU rounds in the same order.
     void p2g() {
         const R inv_h = R(P.inv_cell_size), h = R(P.cell_size);
         const R scale = R(P2G_FIXED_SCALE);
@@ -1080,11 +1085,13 @@ public:
                     I3 node = base + oi;
                     if (!in_grid(node)) continue;
                     V3<R> w3{oi.x ? fr.x : R(1) - fr.x, oi.y ? fr.y : R(1) - fr.y, oi.z ? fr.z : R(1) - fr.z};
-                    R w = w3.x * w3.y * w3.z;
-                    if (w <= R(0)) continue;
+                    R ws = w3.x * ((w3.y * w3.z) * scale);
+                    if (ws <= R(0)) continue;
                     V3<R> xn{(R(node.x) + off.x) * h, (R(node.y) + off.y) * h, (R(node.z) + off.z) * h};
-                    int32_t mom = to_i32_rn<R>(w * (up + dot(cp, xn - p.pos)) * scale);
-                    int32_t wt = to_i32_rn<R>(w * scale);
+                    V3<R> dx = xn - p.pos;
+                    R term = (up + cp.x * dx.x) + (cp.y * dx.y + cp.z * dx.z);
+                    int32_t mom = to_i32_rn<R>(ws * term);
+                    int32_t wt = to_i32_rn<R>(ws);
                     uint32_t cidx = cell_index(node);
                     if (is_null_cell(cidx)) continue;
                     uint32_t f = uint32_t(axis) * L.pool_cells + cidx;

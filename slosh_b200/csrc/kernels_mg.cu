@@ -813,7 +813,7 @@ constexpr int ST_WARPS = 4;  // warps (bricks in flight) per CTA of a staged pas
 constexpr uint32_t ST_FACE = 896u;  // floats of a staged face array: body + 6 x 64
 template <int NF, int NB>
 struct __align__(16) WarpStage {
-    float f[NF > 0 ? NF : 1][ST_FACE];
+    float f[NF > 0 ? NF : 1][NF > 0 ? ST_FACE : 4u];
     float b[NB > 0 ? NB : 1][BRICK_CELLS];
     uint8_t word[BRICK_CELLS];
     uint64_t bar;
@@ -836,15 +836,20 @@ __device__ __forceinline__ void stage_issue(WarpStage<NF, NB>& S, const float* c
     if (lane == 0) tc::mbar_arrive_expect_tx(&S.bar, bytes);
     __syncwarp();
     for (int c = int(lane); c < NC; c += 32) {
-        if (c < NF * 19) {
-            const int f = c / 19, q = c - 19 * f;
-            const float* a = fa[f];
-            if (q == 0) bulk_load(S.f[f], a + size_t(slot) * BRICK_CELLS, 2048u, &S.bar);
-            else if (q <= 8) bulk_load(S.f[f] + 640 + 8 * (q - 1), a + size_t(ns[2]) * BRICK_CELLS + 56 + 64 * (q - 1), 32u, &S.bar);
-            else if (q <= 16) bulk_load(S.f[f] + 704 + 8 * (q - 9), a + size_t(ns[3]) * BRICK_CELLS + 64 * (q - 9), 32u, &S.bar);
-            else if (q == 17) bulk_load(S.f[f] + 768, a + size_t(ns[4]) * BRICK_CELLS + 448, 256u, &S.bar);
-            else bulk_load(S.f[f] + 832, a + size_t(ns[5]) * BRICK_CELLS, 256u, &S.bar);
-        } else if (c < NF * 19 + NB) {
+        if constexpr (NF > 0) {
+            if (c < NF * 19) {
+                const int f = c / 19, q = c - 19 * f;
+                const float* a = fa[f];
+                float* dst = &S.f[0][0] + size_t(f) * ST_FACE;
+                if (q == 0) bulk_load(dst, a + size_t(slot) * BRICK_CELLS, 2048u, &S.bar);
+                else if (q <= 8) bulk_load(dst + 640 + 8 * (q - 1), a + size_t(ns[2]) * BRICK_CELLS + 56 + 64 * (q - 1), 32u, &S.bar);
+                else if (q <= 16) bulk_load(dst + 704 + 8 * (q - 9), a + size_t(ns[3]) * BRICK_CELLS + 64 * (q - 9), 32u, &S.bar);
+                else if (q == 17) bulk_load(dst + 768, a + size_t(ns[4]) * BRICK_CELLS + 448, 256u, &S.bar);
+                else bulk_load(dst + 832, a + size_t(ns[5]) * BRICK_CELLS, 256u, &S.bar);
+                continue;
+            }
+        }
+        if (c < NF * 19 + NB) {
             const int b = c - NF * 19;
             bulk_load(S.b[b], ba[b] + size_t(slot) * BRICK_CELLS, 2048u, &S.bar);
         } else {
@@ -852,7 +857,7 @@ __device__ __forceinline__ void stage_issue(WarpStage<NF, NB>& S, const float* c
         }
     }
     // +-x faces: cells (7, y, z) of the -x brick and (0, y, z) of the +x brick, j = y + 8 z
-    if (NF > 0) {
+    if constexpr (NF > 0) {
         float xv[NF > 0 ? NF : 1][4];
 #pragma unroll
         for (int f = 0; f < NF; ++f)
@@ -1256,6 +1261,54 @@ __global__ void __launch_bounds__(ST_WARPS * 32) k_apply_a_st(Dev d, MGState m) 
             st4(m.q + g.i, q);
         },
         [&](double dq, double) { m.scalars[2] = dq; });
+}
+
+// k_update_pr from a stage: p, the current direction, r, q, the diagonal (and with FLEX the finished
+// V-cycle's z) as bodies.
+template <bool FLEX>
+__global__ void __launch_bounds__(ST_WARPS * 32) k_update_pr_st(Dev d, MGState m, float* __restrict__ p, unsigned long long handle) {
+    constexpr int NB = FLEX ? 6 : 5;
+    const float alpha = ratio_f(m.scalars[0], m.scalars[2]);
+    const float* dcur = dir_buf_c(m, (m.ctl[0] + 1u) & 1u);
+    const float* ba[6] = {p, dcur, m.r, m.q, d.cell_diag, m.z};
+    st_pass<0, NB, FLEX ? 2 : 1>(d, m, 3, nullptr, ba,
+        [&](WarpStage<0, NB>& S, const Geo& g, double* v0, double* v1) {
+            const float4 vp = sld4(S.b[0], g.l), vd = sld4(S.b[1], g.l), vr = sld4(S.b[2], g.l), vq = sld4(S.b[3], g.l);
+            const float4 dg = sld4(S.b[4], g.l);
+            const float4 vz = FLEX ? sld4(S.b[NB - 1], g.l) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            const uint32_t w4 = sword4(S.word, g);
+            float po[4], ro[4], zo[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const uint32_t w = word_of(w4, j);
+                po[j] = comp(vp, j);
+                ro[j] = comp(vr, j);
+                zo[j] = 0.0f;
+                if (!(w & W_FLUID)) continue;
+                po[j] = comp(vp, j) + alpha * comp(vd, j);
+                const float ri = comp(vr, j) - alpha * comp(vq, j);
+                ro[j] = ri;
+                zo[j] = (w & W_RED) ? ri / (comp(dg, j) + DIAG_EPSILON) : 0.0f;
+                v0[j] = double(ri * ri);
+                if (FLEX) v1[j] = double(ri * comp(vz, j));
+            }
+            st4(p + g.i, po);
+            st4(m.r + g.i, ro);
+            st4(m.z + g.i, zo);
+        },
+        [&](double rr, double rz) {
+            m.scalars[5] = rr;
+            if (FLEX) m.scalars[9] = rz;
+            const uint32_t it = m.ctl[0] + 1u;
+            m.ctl[0] = it;
+            const double bb = m.scalars[4];
+            const double rel = bb > 0.0 ? sqrt(rr / bb) : 0.0;
+            const bool converged = m.ctl[2] != 0u && rel <= m.scalars[8];
+            const bool more = it < m.ctl[1] && !converged;
+            if (!more) m.ctl[3] = 1u;
+            if (!more && m.ctl[2] != 0u && !converged) m.ctl[4] = 1u;  // stopped at the limit: sticky for the frame
+            if (handle) cudaGraphSetConditional(handle, more ? 1u : 0u);
+        });
 }
 
 // ---- the small coarse levels in one CTA: levels tail..nl-1 of the V-cycle --------------------------------
@@ -1676,13 +1729,17 @@ int st_grid(K kernel, size_t smem, const Dev& d, const Shape& sh) {
     const int cap = int((d.num_pool_bricks + uint32_t(ST_WARPS) - 1u) / uint32_t(ST_WARPS));
     return std::max(1, std::min(cap, per_sm * sh.num_sms));
 }
-#define ST_LAUNCH(kernel, NF, NB, d, m, sh, s)                                         \
-    do {                                                                           \
-        constexpr size_t smem_ = st_smem_bytes<NF, NB>();                          \
-        static int grid_ = 0;                                                      \
-        if (!grid_) grid_ = st_grid(kernel, smem_, d, sh);                          \
-        kernel<<<std::min(grid_, st_grid_cap(d)), ST_WARPS * 32, smem_, s>>>(d, m); \
+#define ST_LAUNCH_ARGS(kernel, NF, NB, d, sh, s, ...)                                              \
+    do {                                                                                            \
+        constexpr size_t smem_ = st_smem_bytes<NF, NB>();                                           \
+        static int grid_ = 0;                                                                       \
+        if (!grid_) {                                                                               \
+            if (smem_ > 48u * 1024u) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_)); \
+            grid_ = st_grid(kernel, smem_, d, sh);                                                  \
+        }                                                                                           \
+        kernel<<<std::min(grid_, st_grid_cap(d)), ST_WARPS * 32, smem_, s>>>(__VA_ARGS__);          \
     } while (0)
+#define ST_LAUNCH(kernel, NF, NB, d, m, sh, s) ST_LAUNCH_ARGS(kernel, NF, NB, d, sh, s, d, m)
 inline int st_grid_cap(const Dev& d) { return std::max(1, int((d.num_pool_bricks + uint32_t(ST_WARPS) - 1u) / uint32_t(ST_WARPS))); }
 
 }  // namespace
@@ -1820,8 +1877,14 @@ int launch_pcg_apply_a(const Dev& d, const MGState& m, const Shape& sh, cudaStre
     return 1;
 }
 int launch_pcg_update_pr(const Dev& d, const MGState& m, float* p, unsigned long long handle, const Shape& sh, cudaStream_t s) {
-    if (m.flexible) k_update_pr<true><<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m, p, handle);
-    else k_update_pr<false><<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m, p, handle);
+    if (mg_staged()) {
+        if (m.flexible) ST_LAUNCH_ARGS(k_update_pr_st<true>, 0, 6, d, sh, s, d, m, p, handle);
+        else ST_LAUNCH_ARGS(k_update_pr_st<false>, 0, 5, d, sh, s, d, m, p, handle);
+    } else if (m.flexible) {
+        k_update_pr<true><<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m, p, handle);
+    } else {
+        k_update_pr<false><<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m, p, handle);
+    }
     return 1;
 }
 int launch_pcg_update_d(const Dev&, const MGState&, const Shape&, cudaStream_t) { return 0; }  // fused into ApplyA

@@ -179,11 +179,13 @@ __global__ void __launch_bounds__(P2G_THREADS) k_p2g(Dev d, Pass p, const slosh_
                     const int3 node = make_int3(base.x + oix, base.y + oiy, base.z + oiz);
                     if (!in_grid(d, node)) continue;
                     const float w3x = oix ? fx : 1.0f - fx, w3y = oiy ? fy : 1.0f - fy, w3z = oiz ? fz : 1.0f - fz;
-                    const float w = w3x * w3y * w3z;
-                    if (w <= 0.0f) continue;
+                    const float ws = w3x * ((w3y * w3z) * P2G_FIXED_SCALE);
+                    if (ws <= 0.0f) continue;
                     const float3 xn = make_float3((float(node.x) + ox) * h, (float(node.y) + oy) * h, (float(node.z) + oz) * h);
-                    const int mom = __float2int_rn(w * (up + dot3(cp, sub3(xn, part.pos))) * P2G_FIXED_SCALE);
-                    const int wt = __float2int_rn(w * P2G_FIXED_SCALE);
+                    const float3 dx = sub3(xn, part.pos);
+                    const float term = (up + cp.x * dx.x) + (cp.y * dx.y + cp.z * dx.z);
+                    const int mom = __float2int_rn(ws * term);
+                    const int wt = __float2int_rn(ws);
                     const uint32_t ci = cell_index(d, node);
                     if (!is_null_cell(ci)) {
                         const uint32_t f = uint32_t(axis) * d.pool_cells + ci;
@@ -211,9 +213,10 @@ __global__ void __launch_bounds__(P2G_THREADS) k_p2g(Dev d, Pass p, const slosh_
 
     // Per particle and MAC component the 8 stencil nodes share their per-axis factors: the weights
     // (1 - f, f), the node offsets x_n - x_p and their products with the APIC row, the in-grid tests
-    // and the tile index, so only the products and sums that differ per node are formed per node. The
-    // arithmetic per node is the same sequence of float operations as (w3x * w3y * w3z) and
-    // w * (u_p + dot(c_p, x_n - x_p)) * scale, hence bit-identical contributions.
+    // and the tile index; per (y, z) pair (w_y w_z) 2^20 and C_y dy + C_z dz, per x u_p + C_x dx, so per
+    // node one product forms the scaled weight and one sum and one product the momentum:
+    // weight = rn(w_x ((w_y w_z) 2^20)), momentum = rn(that (u_p + C_x dx) + (C_y dy + C_z dz)) -- the
+    // oracle's order.
     const int sy = ndim.x, sz = ndim.x * ndim.y;
     for (int k = 0; k < P2G_PER_THREAD; ++k) {
         const uint32_t i = first + uint32_t(k);
@@ -247,20 +250,21 @@ __global__ void __launch_bounds__(P2G_THREADS) k_p2g(Dev d, Pass p, const slosh_
             const int tb = (base.x - origin.x) + sy * (base.y - origin.y) + sz * (base.z - origin.z);
             int* tm = tile + (2 * axis) * P2G_TILE_NODES + tb;
             int* tw = tile + (2 * axis + 1) * P2G_TILE_NODES + tb;
+            const float upx[2] = {up + px[0], up + px[1]};
 #pragma unroll
             for (int b = 0; b < 4; ++b) {
                 const int oiy = b & 1, oiz = b >> 1;
                 if (!(iny[oiy] && inz[oiz])) continue;
-                const float wyz = wy[oiy];
-                const float pyz = py[oiy];
+                const float wyzs = (wy[oiy] * wz[oiz]) * P2G_FIXED_SCALE;
+                const float pyz = py[oiy] + pz[oiz];
                 const int to = oiy * sy + oiz * sz;
 #pragma unroll
                 for (int oix = 0; oix < 2; ++oix) {
                     if (!inx[oix]) continue;
-                    const float w = wx[oix] * wyz * wz[oiz];
-                    if (w <= 0.0f) continue;
-                    const int mom = __float2int_rn(w * (up + (px[oix] + pyz + pz[oiz])) * P2G_FIXED_SCALE);
-                    const int wt = __float2int_rn(w * P2G_FIXED_SCALE);
+                    const float ws = wx[oix] * wyzs;
+                    if (ws <= 0.0f) continue;
+                    const int mom = __float2int_rn(ws * (upx[oix] + pyz));
+                    const int wt = __float2int_rn(ws);
                     atomicAdd(tm + to + oix, mom);
                     atomicAdd(tw + to + oix, wt);
                 }
