@@ -442,6 +442,9 @@ def run_tanks(args):
     if world > 1:
         import torch.distributed as dist
     tanks = scenes.tank_batch(S.settings_default, count=args.tanks)
+    precond = None
+    for t in tanks:
+        precond = apply_precond(t["settings"], args)
     plan = lpt_partition([t["cost"] for t in tanks], world)
     mine = plan[rank]
     sims, streams = [], []
@@ -529,6 +532,7 @@ def run_tanks(args):
             "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"tanks_{args.tanks}", "tanks": args.tanks, "particles": particles, "solver": "MGPCG",
+                       "preconditioner": precond,
                        "autotune_ctas_per_sm_counts": tuned,
                        "tolerance": 1e-6, "step": "one frame of every tank", "parallelism": f"lpt{world}",
                        "l2": "inputs larger than L2 (1.3 GB of particles)"},

@@ -1552,13 +1552,23 @@ public:
         });
     }
     // ||b - A p|| / ||b|| with the level-0 operator (diagnostic of a finished solve).
+    // The residual is evaluated in FP64 from the stored (FP32) solution and operator -- diag_f + 1e-4 as the
+    // solve forms it, the fluid neighbours in neighbour order -- so it measures the solution, not the
+    // cancellation of an FP32 evaluation of A p.
     double true_rel_residual(const std::vector<R>& p, const std::vector<R>& div) {
         double num = level0_dot([&](uint32_t i, I3 c) -> double {
             if (type_of(cell_type[i]) != CELL_FLUID) return 0.0;
             R diag, sum;
             stencil(0, p, c, i, &cell_diag, diag, sum);
-            R r = -div[i] - (diag * p[i] - sum);
-            return double(r * r);
+            double nsum = 0.0;
+            for (int n = 0; n < 6; ++n) {
+                I3 nb = c + neighbour_offset(n);
+                if (!inside(nb, mg[0].dim)) continue;
+                uint32_t ni = level_index(0, nb);
+                if ((level_type_raw(0, ni) & CELL_TYPE_MASK) == CELL_FLUID) nsum = nsum + double(p[ni]);
+            }
+            double r = -double(div[i]) - (double(diag) * double(p[i]) - nsum);
+            return r * r;
         });
         double den = level0_dot([&](uint32_t i, I3) -> double {
             if (type_of(cell_type[i]) != CELL_FLUID) return 0.0;

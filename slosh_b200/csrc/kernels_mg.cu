@@ -735,6 +735,76 @@ __global__ void k_prolong_smooth_fp(Dev d, MGState m, int l) {
     for_footprint(d, F, l, [&](uint32_t i, int3 c) { prolong_smooth_fp_cell(F, C, i, c); });
 }
 
+// ---- levels 1 .. tail-1 of a V-cycle in two cooperative launches ------------------------------------------
+// The footprint passes of the descent (pre-smoothing, restriction) and of the ascent (prolongation with the
+// first black half, the remaining half-sweeps) are each run by one grid of co-resident CTAs (a cooperative
+// launch), with a grid-wide barrier between consecutive passes instead of a kernel boundary. The barrier is
+// a counter and a generation word in device memory (counters[6], counters[7]); every wait is bounded and
+// records ctl[5] |= 2 when it gives up.
+__device__ __forceinline__ void grid_barrier(const MGState& m) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile uint32_t* gen = m.counters + 7;
+        const uint32_t g = *gen;
+        __threadfence();
+        if (atomicAdd(m.counters + 6, 1u) == gridDim.x - 1u) {
+            m.counters[6] = 0u;
+            __threadfence();
+            atomicAdd(m.counters + 7, 1u);
+        } else {
+            uint32_t it = 0;
+            while (*gen == g) {
+                if (++it > (1u << 24)) {
+                    atomicOr(m.ctl + 5, 2u);
+                    break;
+                }
+                __nanosleep(20);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+template <class Fn>
+__device__ __forceinline__ void coop_footprint(const Dev& d, const MGLevel& L, int l, Fn fn) {
+    for_footprint_span(d, L, l, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x, fn);
+}
+// Descent: for l = 1 .. tail - 1, pre-smoothing of level l (its black half, then sweeps - 1 red-black pairs)
+// and the restriction l -> l + 1; level 1 holds the restriction from level 0 on entry.
+__global__ void __launch_bounds__(1024) k_coarse_descent(Dev d, MGState m, int tail) {
+    const int sweeps = max(m.sweeps, 1);
+    bool first = true;
+    for (int l = 1; l < tail; ++l) {
+        const MGLevel L = m.lv[l];
+        for (int k = 0; k < 2 * sweeps - 1; ++k) {
+            const uint32_t want = (k & 1) ? CW_RED : 0u;  // black, red, black, ...
+            if (!first) grid_barrier(m);
+            first = false;
+            coop_footprint(d, L, l, [&](uint32_t i, int3) { smooth_fp_cell(L, i, want); });
+        }
+        const MGLevel C = m.lv[l + 1];
+        grid_barrier(m);
+        coop_footprint(d, C, l + 1, [&](uint32_t ci, int3 c) { restrict_fp_cell(L, C, ci, c, m.restrict_scale); });
+    }
+}
+// Ascent: for l = tail - 1 .. 1, the prolongation l + 1 -> l fused with the black half, then the red half and
+// sweeps - 1 more black-red pairs.
+__global__ void __launch_bounds__(1024) k_coarse_ascent(Dev d, MGState m, int tail) {
+    const int sweeps = max(m.sweeps, 1);
+    bool first = true;
+    for (int l = tail - 1; l >= 1; --l) {
+        const MGLevel F = m.lv[l], C = m.lv[l + 1];
+        if (!first) grid_barrier(m);
+        first = false;
+        coop_footprint(d, F, l, [&](uint32_t i, int3 c) { prolong_smooth_fp_cell(F, C, i, c); });
+        for (int k = 1; k < 2 * sweeps; ++k) {
+            const uint32_t want = (k & 1) ? CW_RED : 0u;  // red, black, red, ...
+            grid_barrier(m);
+            coop_footprint(d, F, l, [&](uint32_t i, int3) { smooth_fp_cell(F, i, want); });
+        }
+    }
+}
+
 // ---- MGRestrictCS level 0 -> 1 over the 4^3 level-1 cells of every active brick (SparseCoarse) -----------
 // One warp per brick: the lanes form the fine residuals of the brick's 512 cells in warp-private shared
 // memory, then sum each of the 64 coarse cells' fluid children in child order (x fastest), as the
@@ -805,9 +875,9 @@ __device__ __forceinline__ const float* dir_buf_c(const MGState& m, uint32_t par
 //   * per "face" array (one read with neighbours): the brick's 512 cells, then its six neighbour faces of 64
 //     cells each at 512 + 64 n (n = -x, +x, -y, +y, -z, +z; index y + 8 z, x + 8 z, x + 8 y in the face);
 //   * per "body" array: the brick's 512 cells; and the 512 stencil bytes.
-// Bodies (2 KB, 512 B), the +-y faces (8 rows of 32 B) and the +-z faces (one 256-byte plane) are 1-D bulk
-// copies (cp.async.bulk, no multicast) that complete on the warp's mbarrier; the +-x faces are strided
-// columns and are read by plain loads issued alongside. A missing neighbour is the all-zero null slot 0.
+// Bodies (2 KB, 512 B) and the +-z faces (one 256-byte plane each) are 1-D bulk copies (cp.async.bulk, no
+// multicast) that complete on the warp's mbarrier; the +-x and +-y faces are strided in the neighbour
+// brick and are read by plain loads issued alongside. A missing neighbour is the all-zero null slot 0.
 // The stage of a warp is reused brick after brick; its mbarrier phase alternates.
 constexpr int ST_WARPS = 4;  // warps (bricks in flight) per CTA of a staged pass
 constexpr uint32_t ST_FACE = 896u;  // floats of a staged face array: body + 6 x 64
@@ -828,8 +898,8 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t b
 template <int NF, int NB>
 __device__ __forceinline__ void stage_issue(WarpStage<NF, NB>& S, const float* const* fa, const float* const* ba, const uint8_t* word,
                                             uint32_t slot, const uint32_t* ns, uint32_t lane) {
-    constexpr uint32_t bytes = uint32_t(NF) * 3072u + uint32_t(NB) * 2048u + 512u;
-    constexpr int NC = NF * 19 + NB + 1;
+    constexpr uint32_t bytes = uint32_t(NF) * 2560u + uint32_t(NB) * 2048u + 512u;
+    constexpr int NC = NF * 3 + NB + 1;
     // the stage's previous contents were read by generic loads: order them before the async-proxy writes
     __syncwarp();
     tc::fence_async_shared();
@@ -837,44 +907,49 @@ __device__ __forceinline__ void stage_issue(WarpStage<NF, NB>& S, const float* c
     __syncwarp();
     for (int c = int(lane); c < NC; c += 32) {
         if constexpr (NF > 0) {
-            if (c < NF * 19) {
-                const int f = c / 19, q = c - 19 * f;
+            if (c < NF * 3) {
+                const int f = c / 3, q = c - 3 * f;
                 const float* a = fa[f];
                 float* dst = &S.f[0][0] + size_t(f) * ST_FACE;
                 if (q == 0) bulk_load(dst, a + size_t(slot) * BRICK_CELLS, 2048u, &S.bar);
-                else if (q <= 8) bulk_load(dst + 640 + 8 * (q - 1), a + size_t(ns[2]) * BRICK_CELLS + 56 + 64 * (q - 1), 32u, &S.bar);
-                else if (q <= 16) bulk_load(dst + 704 + 8 * (q - 9), a + size_t(ns[3]) * BRICK_CELLS + 64 * (q - 9), 32u, &S.bar);
-                else if (q == 17) bulk_load(dst + 768, a + size_t(ns[4]) * BRICK_CELLS + 448, 256u, &S.bar);
+                else if (q == 1) bulk_load(dst + 768, a + size_t(ns[4]) * BRICK_CELLS + 448, 256u, &S.bar);
                 else bulk_load(dst + 832, a + size_t(ns[5]) * BRICK_CELLS, 256u, &S.bar);
                 continue;
             }
         }
-        if (c < NF * 19 + NB) {
-            const int b = c - NF * 19;
+        if (c < NF * 3 + NB) {
+            const int b = c - NF * 3;
             bulk_load(S.b[b], ba[b] + size_t(slot) * BRICK_CELLS, 2048u, &S.bar);
         } else {
             bulk_load(S.word, word + size_t(slot) * BRICK_CELLS, 512u, &S.bar);
         }
     }
-    // +-x faces: cells (7, y, z) of the -x brick and (0, y, z) of the +x brick, j = y + 8 z
+    // +-x faces: cells (7, y, z) of the -x brick and (0, y, z) of the +x brick (j = y + 8 z); +-y faces:
+    // cells (x, 7, z) of the -y brick and (x, 0, z) of the +y brick (j = x + 8 z). Plain loads, all issued
+    // before any is stored.
     if constexpr (NF > 0) {
-        float xv[NF > 0 ? NF : 1][4];
+        float xv[NF > 0 ? NF : 1][8];
 #pragma unroll
         for (int f = 0; f < NF; ++f)
 #pragma unroll
             for (int k = 0; k < 2; ++k) {
                 const uint32_t j = lane + 32u * uint32_t(k);
-                const uint32_t l = 8u * j;  // local index of (0, y, z)
-                xv[f][2 * k] = fa[f][size_t(ns[0]) * BRICK_CELLS + l + 7u];
-                xv[f][2 * k + 1] = fa[f][size_t(ns[1]) * BRICK_CELLS + l];
+                const uint32_t lx = 8u * j;                      // local index of (0, y, z), j = y + 8 z
+                const uint32_t ly = (j & 7u) + 64u * (j >> 3);   // local index of (x, 0, z), j = x + 8 z
+                xv[f][4 * k] = fa[f][size_t(ns[0]) * BRICK_CELLS + lx + 7u];
+                xv[f][4 * k + 1] = fa[f][size_t(ns[1]) * BRICK_CELLS + lx];
+                xv[f][4 * k + 2] = fa[f][size_t(ns[2]) * BRICK_CELLS + ly + 56u];
+                xv[f][4 * k + 3] = fa[f][size_t(ns[3]) * BRICK_CELLS + ly];
             }
 #pragma unroll
         for (int f = 0; f < NF; ++f)
 #pragma unroll
             for (int k = 0; k < 2; ++k) {
                 const uint32_t j = lane + 32u * uint32_t(k);
-                S.f[f][512u + j] = xv[f][2 * k];
-                S.f[f][576u + j] = xv[f][2 * k + 1];
+                S.f[f][512u + j] = xv[f][4 * k];
+                S.f[f][576u + j] = xv[f][4 * k + 1];
+                S.f[f][640u + j] = xv[f][4 * k + 2];
+                S.f[f][704u + j] = xv[f][4 * k + 3];
             }
     }
 }
@@ -1673,7 +1748,7 @@ __global__ void __launch_bounds__(GRID_THREADS, 3) k_update_pr(Dev d, MGState m,
         });
 }
 
-// ---- ||b - A p||^2 and ||b||^2 of a finished solve (diagnostic) ---------------------------------------------
+// ---- ||b - A p||^2 (FP64 evaluation) and ||b||^2 of a finished solve (diagnostic) -------------------------
 __global__ void __launch_bounds__(GRID_THREADS) k_true_residual(Dev d, MGState m, const float* __restrict__ p,
                                                                 const float* __restrict__ div) {
     struct V {
@@ -1700,8 +1775,14 @@ __global__ void __launch_bounds__(GRID_THREADS) k_true_residual(Dev d, MGState m
                 float n[6];
                 nbrs6(v.p, x, g.h, j, n);
                 const float b = -comp(v.dv, j);
-                const float r = b - (diag * comp(v.p.c, j) - nb_sum(n, w));
-                v0[j] = double(r * r);
+                // evaluated in FP64 from the stored solution, so it measures the solution rather than the
+                // cancellation of an FP32 evaluation of A p
+                double nsum = 0.0;
+#pragma unroll
+                for (int k = 0; k < 6; ++k)
+                    if ((w >> k) & 1u) nsum = nsum + double(n[k]);
+                const double r = double(b) - (double(diag) * double(comp(v.p.c, j)) - nsum);
+                v0[j] = r * r;
                 v1[j] = double(b * b);
             }
         },
@@ -1717,6 +1798,39 @@ bool mg_staged() {
         return (e && e[0] == '0') ? 0 : 1;
     }();
     return v != 0;
+}
+// Levels 1 .. tail-1 as two cooperative launches (default) or one launch per pass (SLOSH_MG_COOP=0).
+bool mg_coop() {
+    static const int v = [] {
+        const char* e = std::getenv("SLOSH_MG_COOP");
+        return (e && e[0] == '0') ? 0 : 1;
+    }();
+    return v != 0;
+}
+// Cooperative launch of a coarse pass kernel on every SM's co-resident CTAs.
+template <class K>
+cudaError_t coop_launch(K kernel, const Dev& d, const MGState& m, int tail, const Shape& sh, cudaStream_t s) {
+    static int per_sm = 0;
+    if (!per_sm) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 1024, 0) != cudaSuccess || per_sm < 1) {
+            cudaGetLastError();
+            per_sm = 1;
+        }
+    }
+    // about two level-1 footprint cells per thread, at most every co-resident CTA
+    const uint64_t cells1 = uint64_t(d.num_pool_bricks > 1u ? d.num_pool_bricks - 1u : 1u) * 64u;
+    const int want = int(std::min<uint64_t>((cells1 + 2047u) / 2048u, uint64_t(per_sm) * uint64_t(sh.num_sms)));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(unsigned(std::max(want, 1)));
+    cfg.blockDim = dim3(1024);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, d, m, tail);
 }
 // Grid of a staged pass: every CTA resident at once (one wave), at most one warp per pool brick.
 template <class K>
@@ -1828,10 +1942,16 @@ int launch_vcycle(const Dev& d, const MGState& m, int coarse_iterations, const S
         smooth0_black();
         n += 2;
     }
+    const bool coop = mg_coop() && tail > 1;
     for (int l = 0; l < tail; ++l) {
         if (l == 0) {
             if (staged) ST_LAUNCH(k_restrict0_st, 1, 2, d, m, sh, s);
             else k_restrict0<<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m);
+            if (coop) {  // pre-smoothing and restriction of levels 1 .. tail-1 in one launch
+                coop_launch(k_coarse_descent, d, m, tail, sh, s);
+                n += 2;
+                break;
+            }
         } else {
             k_restrict_fp<<<fp_blocks(l + 1), 256, 0, s>>>(d, m, l);
         }
@@ -1849,6 +1969,13 @@ int launch_vcycle(const Dev& d, const MGState& m, int coarse_iterations, const S
     k_vcycle_tail<<<1, 1024, mg_tail_smem(m), s>>>(m, tail, coarse_iterations);
     ++n;
     for (int l = tail - 1; l >= 0; --l) {
+        if (coop && l > 0) {
+            if (l == tail - 1) {  // levels tail-1 .. 1 in one launch
+                coop_launch(k_coarse_ascent, d, m, tail, sh, s);
+                ++n;
+            }
+            continue;
+        }
         if (l == 0) {
             if (staged) ST_LAUNCH(k_prolong_smooth0_st, 1, 2, d, m, sh, s);
             else k_prolong_smooth0<<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m);

@@ -7,6 +7,8 @@
 // Particles are 48-byte records read and written as three 16-byte vectors per thread. P2G accumulates
 // APIC momentum and weight as 2^20 fixed-point int32 (SloshCommon.ush:46-48), so the sums are exact
 // and independent of the order in which particles add them.
+#include <cstdlib>
+
 #include "kernels.h"
 
 namespace slosh {
@@ -107,8 +109,7 @@ __global__ void k_touch(Dev d, const slosh_particle_t* __restrict__ particles, u
 // memory with integer atomics, then adds each non-zero tile entry to global memory once. A CTA whose
 // box does not fit adds directly to global memory. Integer sums make both paths identical.
 constexpr int P2G_THREADS = 256;
-constexpr int P2G_PER_THREAD = 4;
-constexpr int P2G_CHUNK = P2G_THREADS * P2G_PER_THREAD;
+constexpr int P2G_PER_THREAD_DEFAULT = 4;
 constexpr int P2G_TILE_NODES = 2048;  // nodes per quantity (6 quantities) = 48 KB
 constexpr int P2G_TILE_CELLS = 1024;  // counted cells = 4 KB
 
@@ -117,7 +118,9 @@ __device__ __forceinline__ int3 p2g_cell(const Dev& d, float3 pos) {
                      clampi(int(floorf(pos.z * d.inv_h)), 0, d.grid.z - 1));
 }
 
+template <int P2G_PER_THREAD>
 __global__ void __launch_bounds__(P2G_THREADS) k_p2g(Dev d, Pass p, const slosh_particle_t* __restrict__ particles, uint32_t n) {
+    constexpr int P2G_CHUNK = P2G_THREADS * P2G_PER_THREAD;
     extern __shared__ int smem[];
     int* tile = smem;                          // [6][P2G_TILE_NODES]
     int* ctile = smem + 6 * P2G_TILE_NODES;    // [P2G_TILE_CELLS]
@@ -608,15 +611,26 @@ int launch_touch_particles(const Dev& d, const slosh_particle_t* particles, uint
     k_touch<<<(n + 255u) / 256u, 256, 0, s>>>(d, particles, n);
     return 1;
 }
-int launch_p2g(const Dev& d, const Pass& p, const slosh_particle_t* particles, uint32_t n, cudaStream_t s) {
-    if (n == 0) return 0;
+template <int PER>
+void launch_p2g_per(const Dev& d, const Pass& p, const slosh_particle_t* particles, uint32_t n, cudaStream_t s) {
     static bool configured = false;
     const int smem = (6 * P2G_TILE_NODES + P2G_TILE_CELLS) * int(sizeof(int));
     if (!configured) {
-        cudaFuncSetAttribute(k_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaFuncSetAttribute(k_p2g<PER>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         configured = true;
     }
-    k_p2g<<<(n + P2G_CHUNK - 1u) / P2G_CHUNK, P2G_THREADS, smem, s>>>(d, p, particles, n);
+    const uint32_t chunk = uint32_t(P2G_THREADS * PER);
+    k_p2g<PER><<<(n + chunk - 1u) / chunk, P2G_THREADS, smem, s>>>(d, p, particles, n);
+}
+int launch_p2g(const Dev& d, const Pass& p, const slosh_particle_t* particles, uint32_t n, cudaStream_t s) {
+    if (n == 0) return 0;
+    static const int per = [] {
+        const char* e = std::getenv("SLOSH_P2G_PER_THREAD");
+        return e ? std::atoi(e) : P2G_PER_THREAD_DEFAULT;
+    }();
+    if (per == 8) launch_p2g_per<8>(d, p, particles, n, s);
+    else if (per == 2) launch_p2g_per<2>(d, p, particles, n, s);
+    else launch_p2g_per<4>(d, p, particles, n, s);
     return 1;
 }
 int launch_g2p(const Dev& d, const Pass& p, slosh_particle_t* particles, uint32_t n, const float* vel, const float* disp,
