@@ -1,6 +1,8 @@
 // Kernels of the learned warm start (sm_100a): TMA + tcgen05 implicit-GEMM convolution and weight
 // gradient, pooling / upsampling and their gradients, the 1x1 head with the masked MSE loss, Adam,
 // and the dense input / guess exchange with the sparse brick pool. Layouts and forms: unet.h.
+#include <cstdlib>
+
 #include "tc.cuh"
 #include "unet.h"
 
@@ -142,6 +144,174 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv3d(const __grid_constant__
             if (!ok) break;
             const TileOrigin o = tile_origin(a.vol, t);
             const uint64_t v = o.v0 + r;
+            for (uint32_t c0 = 0; c0 < a.n; c0 += 16u) {
+                float x[16];
+                tmem_ld16(tmem + acc * ncols + ((q * 32u) << 16) + c0, x);
+                if (a.bias)
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) x[j] = x[j] + a.bias[c0 + uint32_t(j)];
+                if (a.relu)
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) x[j] = fmaxf(x[j], 0.0f);
+                const uint32_t oi = c0 < a.oc[0] ? 0u : 1u;
+                const uint32_t cc = oi == 0u ? c0 : c0 - a.oc[0];
+                const uint64_t e = v * a.oc[oi] + cc;
+                uint4* dst = reinterpret_cast<uint4*>(a.out[oi] + e);
+                if (a.accumulate) {
+                    const uint4 w0 = dst[0], w1 = dst[1];
+                    const bf16* old0 = reinterpret_cast<const bf16*>(&w0);
+                    const bf16* old1 = reinterpret_cast<const bf16*>(&w1);
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        x[j] = x[j] + bf(old0[j]);
+                        x[8 + j] = x[8 + j] + bf(old1[j]);
+                    }
+                }
+                if (a.mask[oi]) {
+                    const uint4* mp = reinterpret_cast<const uint4*>(a.mask[oi] + e);
+                    const uint4 m0 = mp[0], m1 = mp[1];
+                    const bf16* mk0 = reinterpret_cast<const bf16*>(&m0);
+                    const bf16* mk1 = reinterpret_cast<const bf16*>(&m1);
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        if (!(bf(mk0[j]) > 0.0f)) x[j] = 0.0f;
+                        if (!(bf(mk1[j]) > 0.0f)) x[8 + j] = 0.0f;
+                    }
+                }
+                uint4 w[2];
+                bf16* wb = reinterpret_cast<bf16*>(w);
+#pragma unroll
+                for (int j = 0; j < 16; ++j) wb[j] = __float2bfloat16_rn(x[j]);
+                dst[0] = w[0];
+                dst[1] = w[1];
+            }
+            tc_fence_before();
+            mbar_arrive(&acc_empty[acc]);
+        }
+    }
+    __syncwarp();
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        tmem_dealloc(tmem, 2u * ncols);
+    }
+}
+
+// ---- halo-box implicit-GEMM convolution ------------------------------------------------------------------
+// Tile = 8 (x) x 16 (y) x 1 (z) output voxels; TMEM row r = x + 8 y. Per tile and 8-channel plane of each
+// K-block, one TMA load brings the 10 x 18 x 3 halo box (zero-filled outside the volume) into shared memory
+// as [z][y][x][8 channels], 16 bytes per voxel: in the no-swizzle K-major layout every 8 consecutive x of
+// one (y, z) line are a contiguous 128-byte core matrix. The A operand of tap (dx, dy, dz) is the box shifted
+// by ((dz + 1) 18 + dy + 1) 160 + (dx + 1) 16 bytes: 8-row groups (the tile's y lines) 160 bytes apart (SBO),
+// the two planes of a K = 16 step one plane apart (LBO). The weights of all taps sit in shared memory as
+// [tap][plane][n][8 channels] (core matrices of 8 output channels, LBO = one plane of n rows, SBO = 128).
+// Warp 0 loads halo boxes (double-buffered across tiles), warp 1 issues the 27 x K / 16 MMAs of a tile, warps
+// 2-5 run the same epilogue as k_conv3d. Every wait is bounded.
+constexpr uint32_t HALO_X = 10u, HALO_Y = 18u, HALO_Z = 3u;
+constexpr uint32_t HALO_PLANE_BYTES = HALO_X * HALO_Y * HALO_Z * 16u;  // 8640
+constexpr uint32_t HALO_PLANE = 8704u;                                 // plane stride, a multiple of 128
+__global__ void __launch_bounds__(CONV_THREADS) k_conv3d_halo(const __grid_constant__ ConvArgs a, uint32_t wbytes, uint32_t hbytes) {
+    extern __shared__ uint8_t dsm[];
+    __shared__ __align__(8) uint64_t hfull[2], hempty[2], acc_full[2], acc_empty[2];
+    __shared__ uint32_t tmem_slot;
+    uint8_t* base = align1024(dsm);
+    uint8_t* wsm = base;
+    uint8_t* hsm = base + ((wbytes + 1023u) & ~1023u);
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    const uint32_t ncols = tmem_cols(a.n);
+    const uint32_t tiles = a.vol.tiles();
+    uint32_t planes[2] = {a.cb[0] / 8u, a.nblocks > 1u ? a.cb[1] / 8u : 0u};
+    const uint32_t wk1 = 27u * planes[0] * a.n * 16u;  // byte offset of K-block 1's weights
+    // weights [27][n][cb] -> [tap][plane][n][8], 16-byte chunks
+    for (uint32_t k = 0; k < a.nblocks; ++k) {
+        const uint32_t cb = a.cb[k], pk = planes[k];
+        const uint32_t chunks = 27u * a.n * pk;
+        const uint4* src = reinterpret_cast<const uint4*>(a.w_ptr[k]);
+        uint8_t* dst = wsm + (k ? wk1 : 0u);
+        for (uint32_t c = threadIdx.x; c < chunks; c += blockDim.x) {
+            const uint32_t p = c % pk, row = c / pk;  // row = tap n + nn
+            const uint32_t tap = row / a.n, nn = row % a.n;
+            *reinterpret_cast<uint4*>(dst + ((tap * pk + p) * a.n + nn) * 16u) = src[(size_t(row) * cb) / 8u + p];
+        }
+    }
+    fence_async_shared();  // the MMAs read the weights through the async proxy
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < 2; ++k) {
+            mbar_init(&hfull[k], 1);
+            mbar_init(&hempty[k], 1);
+            mbar_init(&acc_full[k], 1);
+            mbar_init(&acc_empty[k], 128);
+        }
+        fence_mbar_init();
+        for (uint32_t k = 0; k < a.nblocks; ++k) prefetch_map(&a.halo[k]);
+    }
+    if (warp == 0) tmem_alloc(&tmem_slot, 2u * ncols);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_slot;
+    const uint32_t ptotal = planes[0] + planes[1];
+
+    if (warp == 0) {
+        if (lane == 0) {
+            uint32_t tl = 0;
+            for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x, ++tl) {
+                const uint32_t hb = tl & 1u;
+                if (tl >= 2u && !mbar_wait(&hempty[hb], ((tl >> 1) - 1u) & 1u, a.error, 64u)) break;
+                const TileOrigin o = tile_origin(a.vol, t);
+                uint8_t* h = hsm + hb * hbytes;
+                mbar_arrive_expect_tx(&hfull[hb], ptotal * HALO_PLANE_BYTES);
+                uint32_t pl = 0;
+                for (uint32_t k = 0; k < a.nblocks; ++k)
+                    for (uint32_t p = 0; p < planes[k]; ++p, ++pl)
+                        tma_load_5d(h + pl * HALO_PLANE, &a.halo[k], int(8u * p), o.x0 - 1, o.y0 - 1, o.z0 - 1, o.b, &hfull[hb]);
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            const uint32_t idesc = idesc_bf16_f32(128u, a.n, 0u, 0u);
+            const uint32_t wsa = smem_u32(wsm), hsa = smem_u32(hsm);
+            uint32_t tl = 0;
+            for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x, ++tl) {
+                const uint32_t acc = tl & 1u, hb = tl & 1u;
+                if (tl >= 2u && !mbar_wait(&acc_empty[acc], ((tl >> 1) - 1u) & 1u, a.error, 2u)) break;
+                if (!mbar_wait(&hfull[hb], (tl >> 1) & 1u, a.error, 2u)) break;
+                tc_fence_after();
+                const uint32_t dcol = tmem + acc * ncols;
+                const uint32_t h = hsa + hb * hbytes;
+                uint32_t accumulate = 0u;
+                for (uint32_t tap = 0; tap < 27u; ++tap) {
+                    int dx, dy, dz;
+                    tap_offset(tap, dx, dy, dz);
+                    const uint32_t shift = (uint32_t(dz + 1) * HALO_Y + uint32_t(dy + 1)) * HALO_X * 16u + uint32_t(dx + 1) * 16u;
+                    uint32_t pl = 0;
+                    for (uint32_t k = 0; k < a.nblocks; ++k) {
+                        const uint32_t wb = wsa + (k ? wk1 : 0u) + tap * planes[k] * a.n * 16u;
+                        for (uint32_t ks = 0; ks < planes[k] / 2u; ++ks) {
+                            const uint64_t ad = smem_desc(h + (pl + 2u * ks) * HALO_PLANE + shift, HALO_PLANE, HALO_X * 16u, SWZ_NONE);
+                            const uint64_t bd = smem_desc(wb + 2u * ks * a.n * 16u, a.n * 16u, 128u, SWZ_NONE);
+                            mma_bf16(dcol, ad, bd, idesc, accumulate);
+                            accumulate = 1u;
+                        }
+                        pl += planes[k];
+                    }
+                }
+                mma_commit(&hempty[hb]);
+                mma_commit(&acc_full[acc]);
+            }
+        }
+    } else {
+        const uint32_t q = warp & 3u;  // TMEM lane quarter of this warp
+        const uint32_t r = q * 32u + lane;
+        uint32_t tl = 0;
+        for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x, ++tl) {
+            const uint32_t acc = tl & 1u;
+            const bool ok = __all_sync(0xFFFFFFFFu, mbar_wait(&acc_full[acc], (tl >> 1) & 1u, a.error, 4u));
+            tc_fence_after();
+            if (!ok) break;
+            const TileOrigin o = tile_origin(a.vol, t);
+            const uint64_t v = o.v0 + uint64_t(r >> 3) * a.vol.W + (r & 7u);
             for (uint32_t c0 = 0; c0 < a.n; c0 += 16u) {
                 float x[16];
                 tmem_ld16(tmem + acc * ncols + ((q * 32u) << 16) + c0, x);
@@ -665,7 +835,53 @@ static size_t wgrad_smem_bytes(uint32_t n) {
     return WGRAD_STAGES * (a_region + b_region) + 1024u;
 }
 
+// The halo-box form applies when every K-block has 16 or 32 channels, n <= 64, the weights of all taps fit
+// in 64 KB and the volume tiles into 8 x 16 x 1 boxes; SLOSH_CONV_HALO=0 turns it off.
+static bool conv_halo_enabled() {
+    static const int v = [] {
+        const char* e = std::getenv("SLOSH_CONV_HALO");
+        return (e && e[0] == '0') ? 0 : 1;
+    }();
+    return v != 0;
+}
+static int launch_conv_halo(const ConvArgs& in, cudaStream_t s) {
+    if (!conv_halo_enabled() || !in.in_ptr[0] || !in.w_ptr[0] || in.n > 64u || in.n % 16u) return 0;
+    uint32_t wbytes = 0, hbytes = 0;
+    for (uint32_t k = 0; k < in.nblocks; ++k) {
+        if ((in.cb[k] != 16u && in.cb[k] != 32u) || !in.in_ptr[k] || !in.w_ptr[k]) return 0;
+        wbytes += 27u * in.cb[k] * in.n * 2u;
+        hbytes += (in.cb[k] / 8u) * HALO_PLANE;
+    }
+    if (wbytes > 64u * 1024u || in.vol.W % 8u || in.vol.H % 16u) return 0;
+    ConvArgs a = in;
+    a.vol.bx = 8u;
+    a.vol.by = 16u;
+    a.vol.bz = 1u;
+    if (!halo_maps(a)) return 0;
+    const size_t smem = size_t((wbytes + 1023u) & ~1023u) + 2u * size_t(hbytes) + 1024u;
+    if (smem > 220u * 1024u) return 0;
+    static int num_sms = 0;
+    if (!num_sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev);
+        if (num_sms <= 0) num_sms = 148;
+        cudaFuncSetAttribute(k_conv3d_halo, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+    }
+    uint32_t per_sm = uint32_t((227u * 1024u) / (smem + 1024u));
+    const uint32_t by_tmem = 512u / (2u * tmem_cols_host(a.n));
+    if (per_sm > by_tmem) per_sm = by_tmem;
+    if (per_sm > 2048u / CONV_THREADS) per_sm = 2048u / CONV_THREADS;
+    if (per_sm < 1u) per_sm = 1u;
+    const uint32_t tiles = a.vol.tiles();
+    uint32_t grid = uint32_t(num_sms) * per_sm;
+    if (grid > tiles) grid = tiles;
+    k_conv3d_halo<<<grid, CONV_THREADS, smem, s>>>(a, wbytes, hbytes);
+    return 1;
+}
+
 int launch_conv(const ConvArgs& a, cudaStream_t s) {
+    if (launch_conv_halo(a, s)) return 1;
     uint32_t cbmax = a.cb[0];
     if (a.nblocks > 1u) cbmax = a.cb[0] > a.cb[1] ? a.cb[0] : a.cb[1];
     const uint32_t a_region = 256u * cbmax;

@@ -85,6 +85,17 @@ CUtensorMap wgt_map(const bf16* p, uint32_t C, uint32_t rows_per_tap) {
     if (r != CUDA_SUCCESS) throw std::runtime_error("tensor map (weights) rejected");
     return m;
 }
+// 5-D map of a dense NDHWC BF16 tensor with C channels whose box is the 10 x 18 x 3 halo of an 8 x 16 x 1
+// tile, 8 channels at a time, unswizzled (16 bytes per voxel in shared memory).
+bool halo_map(CUtensorMap* m, const bf16* p, uint32_t C, const Vol& v) {
+    const cuuint64_t dims[5] = {C, v.W, v.H, v.D, v.B};
+    const cuuint64_t strides[4] = {uint64_t(C) * 2u, uint64_t(C) * 2u * v.W, uint64_t(C) * 2u * v.W * v.H,
+                                   uint64_t(C) * 2u * v.W * v.H * v.D};
+    const cuuint32_t box[5] = {8u, 10u, 18u, 3u, 1u};
+    const cuuint32_t es[5] = {1u, 1u, 1u, 1u, 1u};
+    return encode_fn()(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<bf16*>(p), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                       CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
 Vol make_vol(uint32_t W, uint32_t H, uint32_t D, uint32_t B) {
     Vol v{W, H, D, B, 0, 0, 0};
     v.bx = W < 128u ? W : 128u;
@@ -127,6 +138,12 @@ uint32_t chunks_for(uint32_t tiles, uint32_t groups) {
 }
 
 }  // namespace
+
+bool halo_maps(ConvArgs& a) {
+    for (uint32_t k = 0; k < a.nblocks; ++k)
+        if (!a.in_ptr[k] || !halo_map(&a.halo[k], a.in_ptr[k], a.cb[k], a.vol)) return false;
+    return true;
+}
 
 struct Net {
     slosh_unet_config_t cfg{};
@@ -298,6 +315,8 @@ struct Net {
             a.act[k] = T[size_t(c.in[k])].map_act;
             a.wgt[k] = c.map_wf[k];
             a.cb[k] = c.cb[k];
+            a.in_ptr[k] = T[size_t(c.in[k])].act;
+            a.w_ptr[k] = c.wf[k];
         }
         a.vol = vol[T[size_t(c.out)].level];
         a.bias = params + c.b_off;
@@ -361,6 +380,8 @@ struct Net {
         a.wgt[0] = c.map_wd;
         a.cb[0] = c.n;
         a.n = c.cin;
+        a.in_ptr[0] = out.grad;
+        a.w_ptr[0] = c.wd;
         a.vol = vol[out.level];
         a.bias = nullptr;
         a.relu = 0;
@@ -647,6 +668,8 @@ SLOSH_API slosh_status slosh_unet_conv_test(const slosh_conv_test_t* t) {
                 a.act[k] = act_map(x[k], t->cin[k], v);
                 a.wgt[k] = wgt_map(wf[k], t->cin[k], n);
                 a.cb[k] = t->cin[k];
+                a.in_ptr[k] = x[k];
+                a.w_ptr[k] = wf[k];
             }
             a.vol = v;
             a.bias = b;
@@ -662,6 +685,8 @@ SLOSH_API slosh_status slosh_unet_conv_test(const slosh_conv_test_t* t) {
             g.wgt[0] = wgt_map(wd, n, cin);
             g.cb[0] = n;
             g.n = cin;
+            g.in_ptr[0] = dz;
+            g.w_ptr[0] = wd;
             g.vol = v;
             g.out[0] = dx[0];
             g.oc[0] = t->cin[0];

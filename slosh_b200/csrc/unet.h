@@ -12,6 +12,12 @@
 //              epilogue warps add the bias, apply ReLU, split the channels over one or two output
 //              tensors, optionally add to them and mask them (ReLU backward) while the next tile's
 //              loads and MMAs run. With flipped, transposed weights it is also the data gradient.
+//   k_conv3d_halo  the same convolution for the layers whose weights fit in shared memory (K-blocks of 16 or
+//              32 channels): a tile is an 8 x 16 x 1 box of voxels, and one TMA load per 8-channel plane brings
+//              its 10 x 18 x 3 halo box into shared memory in the no-swizzle core-matrix layout (16 bytes per
+//              voxel and plane); each of the 27 taps is then just an operand descriptor whose start address is
+//              shifted by the tap inside the halo box (8-row groups 160 bytes apart, planes one halo box apart).
+//              The weights of all taps stay in shared memory for the CTA's lifetime.
 //   k_wgrad    weight gradient dW[tap][n][c] = sum_v X[v + tap][c] dZ[v][n] as tcgen05.mma with both
 //              operands MN-major: M = 128 rows are (tap, c) pairs of 128 / C taps, N = output
 //              channels, K = 128 voxels per stage; per-chunk partials are summed in chunk order.
@@ -56,6 +62,11 @@ struct alignas(64) ConvArgs {
     const bf16* mask[2]; // multiply by (mask > 0) after the optional add
     uint32_t accumulate; // add to the outputs' current values
     uint32_t* error;
+    // for the halo-box form (k_conv3d_halo): the K-block inputs and weights as plain pointers; the
+    // launcher builds the halo tensor maps itself
+    const bf16* in_ptr[2];   // [B][D][H][W][cb]
+    const bf16* w_ptr[2];    // [27][n][cb]
+    CUtensorMap halo[2];     // 5-D (C, W, H, D, B), box (8, 10, 18, 3, 1), no swizzle (set by launch_conv)
 };
 
 struct alignas(64) WgradArgs {
@@ -69,6 +80,9 @@ struct alignas(64) WgradArgs {
 };
 
 int launch_conv(const ConvArgs& a, cudaStream_t s);
+// Halo tensor maps of a convolution's K-block inputs (box 8 channels x 10 x 18 x 3, no swizzle), for
+// k_conv3d_halo; false if a map is rejected.
+bool halo_maps(ConvArgs& a);
 int launch_wgrad(const WgradArgs& a, uint32_t chunks, cudaStream_t s);
 int launch_reduce_chunks(const float* partial, float* out, uint32_t chunks, uint32_t count, cudaStream_t s);
 int launch_reduce_wgrad(const float* partial, float* out, uint32_t chunks, uint32_t n, uint32_t cb, uint32_t cin, uint32_t off,

@@ -33,7 +33,9 @@ CONFIGS = [
     ([16], 16), ([16], 32), ([32], 32), ([32], 64), ([64], 64),
     ([64, 64], 64), ([64, 32], 32), ([32, 16], 16),
 ]
-VOLUMES = [((16, 8, 8), 1), ((8, 8, 8), 2), ((128, 2, 2), 1)]
+# the last two volumes tile into 8 x 16 x 1 boxes, so their 16/32-channel convolutions run the halo-box
+# kernel (one TMA halo load per tile, taps as descriptor offsets); the others the streamed-tap kernel
+VOLUMES = [((16, 8, 8), 1), ((8, 8, 8), 2), ((128, 2, 2), 1), ((16, 16, 4), 1), ((8, 32, 4), 2)]
 
 
 @pytest.mark.parametrize("cins,cout", CONFIGS)
