@@ -735,76 +735,6 @@ __global__ void k_prolong_smooth_fp(Dev d, MGState m, int l) {
     for_footprint(d, F, l, [&](uint32_t i, int3 c) { prolong_smooth_fp_cell(F, C, i, c); });
 }
 
-// ---- levels 1 .. tail-1 of a V-cycle in two cooperative launches ------------------------------------------
-// The footprint passes of the descent (pre-smoothing, restriction) and of the ascent (prolongation with the
-// first black half, the remaining half-sweeps) are each run by one grid of co-resident CTAs (a cooperative
-// launch), with a grid-wide barrier between consecutive passes instead of a kernel boundary. The barrier is
-// a counter and a generation word in device memory (counters[6], counters[7]); every wait is bounded and
-// records ctl[5] |= 2 when it gives up.
-__device__ __forceinline__ void grid_barrier(const MGState& m) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        volatile uint32_t* gen = m.counters + 7;
-        const uint32_t g = *gen;
-        __threadfence();
-        if (atomicAdd(m.counters + 6, 1u) == gridDim.x - 1u) {
-            m.counters[6] = 0u;
-            __threadfence();
-            atomicAdd(m.counters + 7, 1u);
-        } else {
-            uint32_t it = 0;
-            while (*gen == g) {
-                if (++it > (1u << 24)) {
-                    atomicOr(m.ctl + 5, 2u);
-                    break;
-                }
-                __nanosleep(20);
-            }
-        }
-        __threadfence();
-    }
-    __syncthreads();
-}
-template <class Fn>
-__device__ __forceinline__ void coop_footprint(const Dev& d, const MGLevel& L, int l, Fn fn) {
-    for_footprint_span(d, L, l, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x, fn);
-}
-// Descent: for l = 1 .. tail - 1, pre-smoothing of level l (its black half, then sweeps - 1 red-black pairs)
-// and the restriction l -> l + 1; level 1 holds the restriction from level 0 on entry.
-__global__ void __launch_bounds__(1024) k_coarse_descent(Dev d, MGState m, int tail) {
-    const int sweeps = max(m.sweeps, 1);
-    bool first = true;
-    for (int l = 1; l < tail; ++l) {
-        const MGLevel L = m.lv[l];
-        for (int k = 0; k < 2 * sweeps - 1; ++k) {
-            const uint32_t want = (k & 1) ? CW_RED : 0u;  // black, red, black, ...
-            if (!first) grid_barrier(m);
-            first = false;
-            coop_footprint(d, L, l, [&](uint32_t i, int3) { smooth_fp_cell(L, i, want); });
-        }
-        const MGLevel C = m.lv[l + 1];
-        grid_barrier(m);
-        coop_footprint(d, C, l + 1, [&](uint32_t ci, int3 c) { restrict_fp_cell(L, C, ci, c, m.restrict_scale); });
-    }
-}
-// Ascent: for l = tail - 1 .. 1, the prolongation l + 1 -> l fused with the black half, then the red half and
-// sweeps - 1 more black-red pairs.
-__global__ void __launch_bounds__(1024) k_coarse_ascent(Dev d, MGState m, int tail) {
-    const int sweeps = max(m.sweeps, 1);
-    bool first = true;
-    for (int l = tail - 1; l >= 1; --l) {
-        const MGLevel F = m.lv[l], C = m.lv[l + 1];
-        if (!first) grid_barrier(m);
-        first = false;
-        coop_footprint(d, F, l, [&](uint32_t i, int3 c) { prolong_smooth_fp_cell(F, C, i, c); });
-        for (int k = 1; k < 2 * sweeps; ++k) {
-            const uint32_t want = (k & 1) ? CW_RED : 0u;  // red, black, red, ...
-            grid_barrier(m);
-            coop_footprint(d, F, l, [&](uint32_t i, int3) { smooth_fp_cell(F, i, want); });
-        }
-    }
-}
-
 // ---- MGRestrictCS level 0 -> 1 over the 4^3 level-1 cells of every active brick (SparseCoarse) -----------
 // One warp per brick: the lanes form the fine residuals of the brick's 512 cells in warp-private shared
 // memory, then sum each of the 64 coarse cells' fluid children in child order (x fastest), as the
@@ -1791,46 +1721,16 @@ __global__ void __launch_bounds__(GRID_THREADS) k_true_residual(Dev d, MGState m
 
 inline int blocks_for(uint32_t n, int threads) { return int((n + uint32_t(threads) - 1u) / uint32_t(threads)); }
 
-// Level-0 passes from shared-memory stages (default) or straight from global memory (SLOSH_MG_STAGED=0).
+// Level-0 passes straight from global memory (default) or from shared-memory stages filled by bulk copies
+// (SLOSH_MG_STAGED=1). Both give identical results; the staged form measured slower on B200 (a 256^3 substep's
+// pressure solve 2.94 against 2.75 ms: fewer long-scoreboard stalls, but fewer resident warps and more
+// instructions), so it is kept as the measured alternative.
 bool mg_staged() {
     static const int v = [] {
         const char* e = std::getenv("SLOSH_MG_STAGED");
-        return (e && e[0] == '0') ? 0 : 1;
+        return (e && e[0] == '1') ? 1 : 0;
     }();
     return v != 0;
-}
-// Levels 1 .. tail-1 as two cooperative launches (default) or one launch per pass (SLOSH_MG_COOP=0).
-bool mg_coop() {
-    static const int v = [] {
-        const char* e = std::getenv("SLOSH_MG_COOP");
-        return (e && e[0] == '0') ? 0 : 1;
-    }();
-    return v != 0;
-}
-// Cooperative launch of a coarse pass kernel on every SM's co-resident CTAs.
-template <class K>
-cudaError_t coop_launch(K kernel, const Dev& d, const MGState& m, int tail, const Shape& sh, cudaStream_t s) {
-    static int per_sm = 0;
-    if (!per_sm) {
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 1024, 0) != cudaSuccess || per_sm < 1) {
-            cudaGetLastError();
-            per_sm = 1;
-        }
-    }
-    // about two level-1 footprint cells per thread, at most every co-resident CTA
-    const uint64_t cells1 = uint64_t(d.num_pool_bricks > 1u ? d.num_pool_bricks - 1u : 1u) * 64u;
-    const int want = int(std::min<uint64_t>((cells1 + 2047u) / 2048u, uint64_t(per_sm) * uint64_t(sh.num_sms)));
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(unsigned(std::max(want, 1)));
-    cfg.blockDim = dim3(1024);
-    cfg.dynamicSmemBytes = 0;
-    cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeCooperative;
-    attr[0].val.cooperative = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, kernel, d, m, tail);
 }
 // Grid of a staged pass: every CTA resident at once (one wave), at most one warp per pool brick.
 template <class K>
@@ -1942,16 +1842,10 @@ int launch_vcycle(const Dev& d, const MGState& m, int coarse_iterations, const S
         smooth0_black();
         n += 2;
     }
-    const bool coop = mg_coop() && tail > 1;
     for (int l = 0; l < tail; ++l) {
         if (l == 0) {
             if (staged) ST_LAUNCH(k_restrict0_st, 1, 2, d, m, sh, s);
             else k_restrict0<<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m);
-            if (coop) {  // pre-smoothing and restriction of levels 1 .. tail-1 in one launch
-                coop_launch(k_coarse_descent, d, m, tail, sh, s);
-                n += 2;
-                break;
-            }
         } else {
             k_restrict_fp<<<fp_blocks(l + 1), 256, 0, s>>>(d, m, l);
         }
@@ -1969,13 +1863,6 @@ int launch_vcycle(const Dev& d, const MGState& m, int coarse_iterations, const S
     k_vcycle_tail<<<1, 1024, mg_tail_smem(m), s>>>(m, tail, coarse_iterations);
     ++n;
     for (int l = tail - 1; l >= 0; --l) {
-        if (coop && l > 0) {
-            if (l == tail - 1) {  // levels tail-1 .. 1 in one launch
-                coop_launch(k_coarse_ascent, d, m, tail, sh, s);
-                ++n;
-            }
-            continue;
-        }
         if (l == 0) {
             if (staged) ST_LAUNCH(k_prolong_smooth0_st, 1, 2, d, m, sh, s);
             else k_prolong_smooth0<<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m);

@@ -4,6 +4,8 @@ manipulators and drains, sphere/box emission with velocity spread and speed jitt
 correction, warm start from zero, the dense (non-sparse) pool, red-black SOR on a sparse scene large
 enough to use every pool path, and two-way collider coupling (the per-collider integer accumulators and
 their decoded feedback)."""
+import os
+
 import numpy as np
 import pytest
 
@@ -216,3 +218,43 @@ def test_preconditioner_options(slosh, oracle_mod, scale, sweeps, flexible, mode
     g, o = pair(slosh, oracle_mod, sc)
     run_frames(g, o, sc, frames=2)
     assert g.results().last_solve_rel_residual <= 1e-6
+
+
+def test_staged_level0_passes_give_identical_results(slosh):
+    """The level-0 MGPCG passes can read their bricks from shared-memory stages filled by bulk async copies
+    (SLOSH_MG_STAGED=1, read once per process) instead of straight from global memory: a 96^3 scene stepped in a
+    child process with the staged passes must end bit-identical to the default passes here."""
+    import subprocess
+    import sys
+    code = (
+        "import sys, numpy as np\n"
+        "sys.path.insert(0, %r)\n"
+        "import slosh_b200 as S\n"
+        "from slosh_b200 import _abi as A, scenes\n"
+        "sc = scenes.dam_break_sphere(S.settings_default, n=96)\n"
+        "s = sc['settings']; s.max_substeps = 16; s.mg_correction_scale = 1.9; s.mg_smoothing_sweeps = 2\n"
+        "sim = S.Simulation(s); sim.set_emit_seed(sc['seed'])\n"
+        "sim.step_frame(A.frame_input(s, emits=sc['emits']))\n"
+        "for _ in range(2): sim.step_frame(A.frame_input(s))\n"
+        "np.save(sys.argv[1], np.concatenate([sim.particles().view(np.uint32).ravel(), sim.read('PRESSURE').view(np.uint32)]))\n"
+    ) % (os.path.dirname(os.path.dirname(os.path.abspath(__file__))),)
+    import tempfile
+    with tempfile.TemporaryDirectory() as tmp:
+        out = os.path.join(tmp, "staged.npy")
+        env = dict(os.environ, SLOSH_MG_STAGED="1")
+        r = subprocess.run([sys.executable, "-c", code, out], env=env, capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr[-2000:]
+        staged = np.load(out)
+    sc = scenes.dam_break_sphere(slosh.settings_default, n=96)
+    s = sc["settings"]
+    s.max_substeps = 16
+    s.mg_correction_scale = 1.9
+    s.mg_smoothing_sweeps = 2
+    sim = slosh.Simulation(s)
+    sim.set_emit_seed(sc["seed"])
+    sim.step_frame(A.frame_input(s, emits=sc["emits"]))
+    for _ in range(2):
+        sim.step_frame(A.frame_input(s))
+    plain = np.concatenate([sim.particles().view(np.uint32).ravel(), sim.read("PRESSURE").view(np.uint32)])
+    sim.close()
+    assert np.array_equal(staged, plain)
