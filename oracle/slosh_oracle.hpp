@@ -1340,6 +1340,15 @@ public:
         return 0.0;
     }
 
+    // Scale of the coarse levels with 16-bit storage (1 with FP32): a power of two bringing the level-0
+    // residual's norm (rr when the V-cycle starts) to about 1, applied by the restriction from level 0 and
+    // undone by the prolongation to level 0.
+    R coarse_scale() const {
+        if (P.precision_mode == SLOSH_PRECISION_FP32) return R(1);
+        int e = rr > 0.0 ? -std::ilogb(std::sqrt(rr)) : 0;
+        e = std::max(-60, std::min(60, e));
+        return R(std::ldexp(1.0f, e));
+    }
     void mg_restrict(int l) {  // MGRestrictCS: level l -> l + 1
         std::vector<R>& xf = level_x(l);
         std::vector<R>& bf = level_b(l);
@@ -1358,6 +1367,7 @@ public:
                 }
             }
             R b = R(P.restrict_scale) * sum;
+            if (l == 0) b = b * coarse_scale();
             cl.b[ci] = store_q(l + 1, b);
             R cdiag = R(DIAG_EPSILON);
             for (int n = 0; n < 6; ++n) {
@@ -1405,11 +1415,12 @@ public:
     void mg_prolong(int l) {  // MGProlongCS: level l + 1 -> l
         std::vector<R>& xf = level_x(l);
         Level& cl = mg[l + 1];
+        const R inv_scale = R(1) / coarse_scale();
         auto fine = [&](uint32_t i, I3 c) {
             if ((level_type_raw(l, i) & CELL_TYPE_MASK) != CELL_FLUID) return;
             I3 parent{c.x / 2, c.y / 2, c.z / 2};
             uint32_t pi = lin(parent, cl.dim);
-            if ((cl.type[pi] & CELL_TYPE_MASK) == CELL_FLUID) xf[i] = store_q(l, xf[i] + cl.x[pi]);
+            if ((cl.type[pi] & CELL_TYPE_MASK) == CELL_FLUID) xf[i] = store_q(l, xf[i] + (l == 0 ? cl.x[pi] * inv_scale : cl.x[pi]));
         };
         if (l == 0) {
             for_active_cells(fine);

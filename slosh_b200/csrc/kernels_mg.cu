@@ -51,6 +51,17 @@ __device__ __forceinline__ void lv_st(float* a, uint32_t i, uint32_t prec, float
     else reinterpret_cast<uint16_t*>(a)[i] = to_storage16(v, prec);
 }
 
+// Scale of the V-cycle's coarse levels with 16-bit storage: the restriction from level 0 multiplies by a power of
+// two that brings the level-0 residual's norm (||r||^2 in scalars[5] when a V-cycle starts) to about 1, and the
+// prolongation back to level 0 divides by it, so FP16's narrow exponent range holds the coarse values without
+// flushing small ones; the V-cycle is linear and a power of two scales exactly. 1 with FP32 storage.
+__device__ __forceinline__ float coarse_scale(const MGState& m) {
+    if (m.lv[1].prec == SLOSH_PRECISION_FP32) return 1.0f;
+    const double rr = m.scalars[5];
+    int e = rr > 0.0 ? -ilogb(sqrt(rr)) : 0;
+    e = max(-60, min(60, e));
+    return ldexpf(1.0f, e);
+}
 __device__ __forceinline__ uint32_t lin3(int3 c, int3 dim) { return uint32_t(c.x + dim.x * (c.y + dim.y * c.z)); }
 __device__ __forceinline__ int3 coord3(uint32_t i, int3 dim) {
     return make_int3(int(i % uint32_t(dim.x)), int((i / uint32_t(dim.x)) % uint32_t(dim.y)), int(i / uint32_t(dim.x * dim.y)));
@@ -611,6 +622,7 @@ __global__ void __launch_bounds__(GRID_THREADS) k_prolong_smooth0(Dev d, MGState
     constexpr int WARPS = GRID_THREADS / 32;
     __shared__ float s_cx[WARPS][216];
     const MGLevel C = m.lv[1];
+    const float ivs = 1.0f / coarse_scale(m);  // a power of two: exact
     float* cx = s_cx[threadIdx.x >> 5];
     w0_black<4>(d, m,
         [&](uint32_t brick, uint32_t lane) {
@@ -625,7 +637,7 @@ __global__ void __launch_bounds__(GRID_THREADS) k_prolong_smooth0(Dev d, MGState
                 if (j < 216u && inside3(c, C.dim)) {
                     const uint32_t ci = lin3(c, C.dim);
                     const float x = lv_ld(C.x, ci, C.prec);
-                    v[r] = (C.word[ci] & CW_FLUID) ? x : 0.0f;
+                    v[r] = (C.word[ci] & CW_FLUID) ? x * ivs : 0.0f;
                 }
             }
 #pragma unroll
@@ -744,6 +756,7 @@ __global__ void __launch_bounds__(GRID_THREADS) k_restrict0(Dev d, MGState m) {
     __shared__ float s_res[WARPS][BRICK_CELLS];
     __shared__ uint8_t s_fluid[WARPS][BRICK_CELLS];
     const MGLevel C = m.lv[1];
+    const float vs = coarse_scale(m);
     const uint32_t active = d.active_bricks[0];
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
     for (uint32_t e = blockIdx.x * wpb + warp; e < active; e += gridDim.x * wpb) {
@@ -787,7 +800,7 @@ __global__ void __launch_bounds__(GRID_THREADS) k_restrict0(Dev d, MGState m) {
                 const uint32_t fl = uint32_t((2 * cl.x + (o & 1)) + 8 * ((2 * cl.y + ((o >> 1) & 1)) + 8 * (2 * cl.z + ((o >> 2) & 1))));
                 if (s_fluid[warp][fl]) sum = sum + s_res[warp][fl];
             }
-            const float bb = m.restrict_scale * sum;
+            const float bb = (m.restrict_scale * sum) * vs;
             lv_st(C.b, ci, C.prec, bb);
             lv_st(C.x, ci, C.prec, (cw & CW_RED) ? bb / word_diag(cw) : 0.0f);
         }
@@ -1120,6 +1133,7 @@ __global__ void __launch_bounds__(ST_WARPS * 32) k_smooth0_black_st(Dev d, MGSta
 __global__ void __launch_bounds__(ST_WARPS * 32) k_prolong_smooth0_st(Dev d, MGState m) {
     __shared__ float s_cx[ST_WARPS][216];
     const MGLevel C = m.lv[1];
+    const float ivs = 1.0f / coarse_scale(m);  // a power of two: exact
     float* cx = s_cx[threadIdx.x >> 5];
     const float* fa[1] = {m.z};
     const float* ba[2] = {m.r, d.cell_diag};
@@ -1136,7 +1150,7 @@ __global__ void __launch_bounds__(ST_WARPS * 32) k_prolong_smooth0_st(Dev d, MGS
                 if (j < 216u && inside3(c, C.dim)) {
                     const uint32_t ci = lin3(c, C.dim);
                     const float x = lv_ld(C.x, ci, C.prec);
-                    v[r] = (C.word[ci] & CW_FLUID) ? x : 0.0f;
+                    v[r] = (C.word[ci] & CW_FLUID) ? x * ivs : 0.0f;
                 }
             }
 #pragma unroll
@@ -1167,6 +1181,7 @@ __global__ void __launch_bounds__(ST_WARPS * 32) k_restrict0_st(Dev d, MGState m
     const float* fa[1] = {m.z};
     const float* ba[2] = {m.r, d.cell_diag};
     const float scale = m.restrict_scale;
+    const float vs = coarse_scale(m);
     extern __shared__ __align__(16) unsigned char st_smem[];
     using Stg = WarpStage<1, 2>;
     const uint32_t lane = threadIdx.x & 31u;
@@ -1221,7 +1236,7 @@ __global__ void __launch_bounds__(ST_WARPS * 32) k_restrict0_st(Dev d, MGState m
                 const uint32_t fl = uint32_t((2 * cl.x + (o & 1)) + 8 * ((2 * cl.y + ((o >> 1) & 1)) + 8 * (2 * cl.z + ((o >> 2) & 1))));
                 if (S.word[fl] & W_FLUID) sum = sum + s_res[warp][fl];
             }
-            const float bb = scale * sum;
+            const float bb = (scale * sum) * vs;
             lv_st(C.b, ci, C.prec, bb);
             lv_st(C.x, ci, C.prec, (cw & CW_RED) ? bb / word_diag(cw) : 0.0f);
         }
