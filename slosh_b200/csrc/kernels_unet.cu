@@ -206,12 +206,13 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv3d(const __grid_constant__
 // by ((dz + 1) 18 + dy + 1) 160 + (dx + 1) 16 bytes: 8-row groups (the tile's y lines) 160 bytes apart (SBO),
 // the two planes of a K = 16 step one plane apart (LBO). The weights of all taps sit in shared memory as
 // [tap][plane][n][8 channels] (core matrices of 8 output channels, LBO = one plane of n rows, SBO = 128).
-// Warp 0 loads halo boxes (double-buffered across tiles), warp 1 issues the 27 x K / 16 MMAs of a tile, warps
-// 2-5 run the same epilogue as k_conv3d. Every wait is bounded.
+// Warp 0 loads halo boxes (nbuf = 1 or 2 buffers across tiles), warp 1 issues the 27 x K / 16 MMAs of a tile,
+// warps 2-5 run the same epilogue as k_conv3d. Every wait is bounded.
 constexpr uint32_t HALO_X = 10u, HALO_Y = 18u, HALO_Z = 3u;
 constexpr uint32_t HALO_PLANE_BYTES = HALO_X * HALO_Y * HALO_Z * 16u;  // 8640
 constexpr uint32_t HALO_PLANE = 8704u;                                 // plane stride, a multiple of 128
-__global__ void __launch_bounds__(CONV_THREADS) k_conv3d_halo(const __grid_constant__ ConvArgs a, uint32_t wbytes, uint32_t hbytes) {
+__global__ void __launch_bounds__(CONV_THREADS) k_conv3d_halo(const __grid_constant__ ConvArgs a, uint32_t wbytes, uint32_t hbytes,
+                                                             uint32_t nbuf) {
     extern __shared__ uint8_t dsm[];
     __shared__ __align__(8) uint64_t hfull[2], hempty[2], acc_full[2], acc_empty[2];
     __shared__ uint32_t tmem_slot;
@@ -257,8 +258,8 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv3d_halo(const __grid_const
         if (lane == 0) {
             uint32_t tl = 0;
             for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x, ++tl) {
-                const uint32_t hb = tl & 1u;
-                if (tl >= 2u && !mbar_wait(&hempty[hb], ((tl >> 1) - 1u) & 1u, a.error, 64u)) break;
+                const uint32_t hb = tl % nbuf;
+                if (tl >= nbuf && !mbar_wait(&hempty[hb], ((tl / nbuf) - 1u) & 1u, a.error, 64u)) break;
                 const TileOrigin o = tile_origin(a.vol, t);
                 uint8_t* h = hsm + hb * hbytes;
                 mbar_arrive_expect_tx(&hfull[hb], ptotal * HALO_PLANE_BYTES);
@@ -274,9 +275,9 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv3d_halo(const __grid_const
             const uint32_t wsa = smem_u32(wsm), hsa = smem_u32(hsm);
             uint32_t tl = 0;
             for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x, ++tl) {
-                const uint32_t acc = tl & 1u, hb = tl & 1u;
+                const uint32_t acc = tl & 1u, hb = tl % nbuf;
                 if (tl >= 2u && !mbar_wait(&acc_empty[acc], ((tl >> 1) - 1u) & 1u, a.error, 2u)) break;
-                if (!mbar_wait(&hfull[hb], (tl >> 1) & 1u, a.error, 2u)) break;
+                if (!mbar_wait(&hfull[hb], (tl / nbuf) & 1u, a.error, 2u)) break;
                 tc_fence_after();
                 const uint32_t dcol = tmem + acc * ncols;
                 const uint32_t h = hsa + hb * hbytes;
@@ -836,16 +837,20 @@ static size_t wgrad_smem_bytes(uint32_t n) {
 }
 
 // The halo-box form applies when every K-block has 16 or 32 channels, n <= 64, the weights of all taps fit
-// in 64 KB and the volume tiles into 8 x 16 x 1 boxes; SLOSH_CONV_HALO=0 turns it off.
-static bool conv_halo_enabled() {
+// in 64 KB, the volume tiles into 8 x 16 x 1 boxes and two halo buffers still leave three CTAs per SM (the
+// configurations where it measured faster than the streamed-tap kernel: 1.6-2x on the 16-channel 128^3 layers;
+// at one CTA per SM it was slower). SLOSH_CONV_HALO=0 turns it off; =2 also admits one-buffer configurations
+// of two CTAs per SM.
+static int conv_halo_mode() {
     static const int v = [] {
         const char* e = std::getenv("SLOSH_CONV_HALO");
-        return (e && e[0] == '0') ? 0 : 1;
+        return e ? std::atoi(e) : 1;
     }();
-    return v != 0;
+    return v;
 }
 static int launch_conv_halo(const ConvArgs& in, cudaStream_t s) {
-    if (!conv_halo_enabled() || !in.in_ptr[0] || !in.w_ptr[0] || in.n > 64u || in.n % 16u) return 0;
+    const int mode = conv_halo_mode();
+    if (mode == 0 || !in.in_ptr[0] || !in.w_ptr[0] || in.n > 64u || in.n % 16u) return 0;
     uint32_t wbytes = 0, hbytes = 0;
     for (uint32_t k = 0; k < in.nblocks; ++k) {
         if ((in.cb[k] != 16u && in.cb[k] != 32u) || !in.in_ptr[k] || !in.w_ptr[k]) return 0;
@@ -858,8 +863,14 @@ static int launch_conv_halo(const ConvArgs& in, cudaStream_t s) {
     a.vol.by = 16u;
     a.vol.bz = 1u;
     if (!halo_maps(a)) return 0;
-    const size_t smem = size_t((wbytes + 1023u) & ~1023u) + 2u * size_t(hbytes) + 1024u;
-    if (smem > 220u * 1024u) return 0;
+    uint32_t nbuf = 2u;
+    size_t smem = size_t((wbytes + 1023u) & ~1023u) + 2u * size_t(hbytes) + 1024u;
+    if ((227u * 1024u) / (smem + 1024u) < 3u) {
+        if (mode < 2) return 0;
+        nbuf = 1u;
+        smem = size_t((wbytes + 1023u) & ~1023u) + size_t(hbytes) + 1024u;
+        if ((227u * 1024u) / (smem + 1024u) < 2u) return 0;
+    }
     static int num_sms = 0;
     if (!num_sms) {
         int dev = 0;
@@ -876,7 +887,7 @@ static int launch_conv_halo(const ConvArgs& in, cudaStream_t s) {
     const uint32_t tiles = a.vol.tiles();
     uint32_t grid = uint32_t(num_sms) * per_sm;
     if (grid > tiles) grid = tiles;
-    k_conv3d_halo<<<grid, CONV_THREADS, smem, s>>>(a, wbytes, hbytes);
+    k_conv3d_halo<<<grid, CONV_THREADS, smem, s>>>(a, wbytes, hbytes, nbuf);
     return 1;
 }
 
