@@ -573,9 +573,9 @@ __device__ __forceinline__ Nb6 load_black(const Dev& d, const MGState& m, uint32
 // Red sweep; with DOT also rho = r . z over all cells (red: the new value, black: the current z), which
 // shifts rho. Cells the sweep does not update are stored back unchanged (each cell belongs to one warp's
 // brick).
-template <bool DOT, int B = 1>
-__global__ void __launch_bounds__(GRID_THREADS, B == 1 ? 3 : 2) k_smooth0(Dev d, MGState m) {
-    w4_pass<DOT ? 1 : 0, B>(d, m, 1,
+template <bool DOT>
+__global__ void __launch_bounds__(GRID_THREADS, 3) k_smooth0(Dev d, MGState m) {
+    w4_pass<DOT ? 1 : 0, 1>(d, m, 1,
         [&](const Geo& g, const uint32_t* ns) { return load_sweep(d, m, g, ns); },
         [&](const Geo& g, const SweepQ& v, double* v0, double*) {
             const X2 x = partner(v.z);
@@ -1587,8 +1587,7 @@ __global__ void __launch_bounds__(1024) k_coarse_solve0(Dev d, MGState m, int it
 // the previous direction from one buffer and writes the new one to the other, and forms each fluid
 // neighbour's new direction z_n + beta d_n itself (bit-identical to what that neighbour writes).
 
-template <int B = 1>
-__global__ void __launch_bounds__(GRID_THREADS, B == 1 ? 3 : 2) k_apply_a(Dev d, MGState m) {
+__global__ void __launch_bounds__(GRID_THREADS, 3) k_apply_a(Dev d, MGState m) {
     const uint32_t it = m.ctl[0];
     const bool first = it == 0u;
     // flexible PCG: beta = (rho_k - r_k.z_{k-1}) / rho_{k-1}, the numerator formed in FP64
@@ -1600,7 +1599,7 @@ __global__ void __launch_bounds__(GRID_THREADS, B == 1 ? 3 : 2) k_apply_a(Dev d,
         float4 dg;
         uint32_t w;
     };
-    w4_pass<1, B>(d, m, 2,
+    w4_pass<1, 1>(d, m, 2,
         [&](const Geo& g, const uint32_t* ns) {
             V v;
             v.z = load_q6(m.z, g, ns);
@@ -1741,14 +1740,6 @@ inline int blocks_for(uint32_t n, int threads) { return int((n + uint32_t(thread
 // (SLOSH_MG_STAGED=1). Both give identical results; the staged form measured slower on B200 (a 256^3 substep's
 // pressure solve 2.94 against 2.75 ms: fewer long-scoreboard stalls, but fewer resident warps and more
 // instructions), so it is kept as the measured alternative.
-// Rounds of a brick whose loads one warp issues together in k_smooth0 / k_apply_a (SLOSH_MG_BATCH = 1 or 2).
-int mg_batch() {
-    static const int v = [] {
-        const char* e = std::getenv("SLOSH_MG_BATCH");
-        return (e && e[0] == '2') ? 2 : 1;
-    }();
-    return v;
-}
 bool mg_staged() {
     static const int v = [] {
         const char* e = std::getenv("SLOSH_MG_STAGED");
@@ -1834,14 +1825,8 @@ int launch_vcycle(const Dev& d, const MGState& m, int coarse_iterations, const S
             if (dot) ST_LAUNCH(k_smooth0_st<true>, 1, 2, d, m, sh, s);
             else ST_LAUNCH(k_smooth0_st<false>, 1, 2, d, m, sh, s);
         } else {
-            if (mg_batch() == 2) {
-                const int g2 = std::min(sh.mg_ctas, 2 * sh.num_sms);  // the CTAs of these larger kernels resident at once
-                if (dot) k_smooth0<true, 2><<<g2, GRID_THREADS, 0, s>>>(d, m);
-                else k_smooth0<false, 2><<<g2, GRID_THREADS, 0, s>>>(d, m);
-            } else {
-                if (dot) k_smooth0<true><<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m);
-                else k_smooth0<false><<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m);
-            }
+            if (dot) k_smooth0<true><<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m);
+            else k_smooth0<false><<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m);
         }
     };
     auto smooth0_black = [&]() {
@@ -1917,8 +1902,7 @@ int launch_vcycle(const Dev& d, const MGState& m, int coarse_iterations, const S
 }
 int launch_pcg_apply_a(const Dev& d, const MGState& m, const Shape& sh, cudaStream_t s) {
     if (mg_staged()) ST_LAUNCH(k_apply_a_st, 2, 1, d, m, sh, s);
-    else if (mg_batch() == 2) k_apply_a<2><<<std::min(sh.mg_ctas, 2 * sh.num_sms), GRID_THREADS, 0, s>>>(d, m);
-    else k_apply_a<1><<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m);
+    else k_apply_a<<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m);
     return 1;
 }
 int launch_pcg_update_pr(const Dev& d, const MGState& m, float* p, unsigned long long handle, const Shape& sh, cudaStream_t s) {

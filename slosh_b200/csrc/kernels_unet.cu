@@ -839,8 +839,8 @@ static size_t wgrad_smem_bytes(uint32_t n) {
 // The halo-box form applies when every K-block has 16 or 32 channels, n <= 64, the weights of all taps fit
 // in 64 KB, the volume tiles into 8 x 16 x 1 boxes and two halo buffers still leave three CTAs per SM (the
 // configurations where it measured faster than the streamed-tap kernel: 1.6-2x on the 16-channel 128^3 layers;
-// at one CTA per SM it was slower). SLOSH_CONV_HALO=0 turns it off; =2 also admits one-buffer configurations
-// of two CTAs per SM.
+// at one CTA per SM it was slower, and a one-buffer form at two CTAs per SM gained nothing). SLOSH_CONV_HALO=0
+// turns it off.
 static int conv_halo_mode() {
     static const int v = [] {
         const char* e = std::getenv("SLOSH_CONV_HALO");
@@ -863,14 +863,9 @@ static int launch_conv_halo(const ConvArgs& in, cudaStream_t s) {
     a.vol.by = 16u;
     a.vol.bz = 1u;
     if (!halo_maps(a)) return 0;
-    uint32_t nbuf = 2u;
-    size_t smem = size_t((wbytes + 1023u) & ~1023u) + 2u * size_t(hbytes) + 1024u;
-    if ((227u * 1024u) / (smem + 1024u) < 3u) {
-        if (mode < 2) return 0;
-        nbuf = 1u;
-        smem = size_t((wbytes + 1023u) & ~1023u) + size_t(hbytes) + 1024u;
-        if ((227u * 1024u) / (smem + 1024u) < 2u) return 0;
-    }
+    const uint32_t nbuf = 2u;
+    const size_t smem = size_t((wbytes + 1023u) & ~1023u) + 2u * size_t(hbytes) + 1024u;
+    if ((227u * 1024u) / (smem + 1024u) < 3u) return 0;
     static int num_sms = 0;
     if (!num_sms) {
         int dev = 0;
