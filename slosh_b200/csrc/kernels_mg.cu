@@ -818,8 +818,8 @@ __device__ __forceinline__ const float* dir_buf_c(const MGState& m, uint32_t par
 //   * per "face" array (one read with neighbours): the brick's 512 cells, then its six neighbour faces of 64
 //     cells each at 512 + 64 n (n = -x, +x, -y, +y, -z, +z; index y + 8 z, x + 8 z, x + 8 y in the face);
 //   * per "body" array: the brick's 512 cells; and the 512 stencil bytes.
-// Bodies (2 KB, 512 B) and the +-z faces (one 256-byte plane each) are 1-D bulk copies (cp.async.bulk, no
-// multicast) that complete on the warp's mbarrier; the +-x and +-y faces are strided in the neighbour
+// Bodies (2 KB, 512 B) and the +-z faces (one 256-byte plane each) are 1-D bulk copies (cp.async.bulk, into this
+// CTA's own shared memory) that complete on the warp's mbarrier; the +-x and +-y faces are strided in the neighbour
 // brick and are read by plain loads issued alongside. A missing neighbour is the all-zero null slot 0.
 // The stage of a warp is reused brick after brick; its mbarrier phase alternates.
 constexpr int ST_WARPS = 4;  // warps (bricks in flight) per CTA of a staged pass

@@ -54,7 +54,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32
     return false;
 }
 
-// TMA tiled loads (no multicast): box at the given coordinates into shared memory, completing
+// TMA tiled loads, each into the issuing CTA's own shared memory: box at the given coordinates into shared memory, completing
 // `bytes` transaction bytes on bar. Out-of-range elements of the box are zero-filled.
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int c0, int c1, uint64_t* bar) {
     asm volatile(
