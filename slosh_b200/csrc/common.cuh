@@ -46,9 +46,6 @@ struct Dev {
     uint32_t* brick_want;
     uint32_t* new_slots;
     uint32_t* active_bricks;
-    // per active-brick entry e (rebuilt after every pool update): [8 e + 0..5] slots of the face-neighbour
-    // bricks -x, +x, -y, +y, -z, +z (0 outside the grid), [8 e + 6] own slot, [8 e + 7] brick index
-    const uint32_t* brick_entries;
     // cells
     uint32_t* cell_type;
     int32_t* cell_count;

@@ -505,7 +505,6 @@ struct Ctx {
         d.brick_want = brick_want;
         d.new_slots = new_slots;
         d.active_bricks = active_bricks;
-        d.brick_entries = mg.nbr_slots;
         d.cell_type = cell_type;
         d.cell_count = cell_count;
         d.pressure = pressure;
@@ -789,7 +788,6 @@ struct Ctx {
             PhaseScope ps(this, 1);
             count(launch_pool_update(d, stream));
             count(launch_clear_new_slots(d, shape, stream));
-            count(launch_brick_entries(d, mg.nbr_slots, shape, stream));
         }
         float* V[3] = {vel[vmap[0]], vel[vmap[1]], vel[vmap[2]]};
         {

@@ -21,8 +21,6 @@ struct Shape {
 // ---- brick pool (Slosh.usf:1719-1831) ----
 int launch_pool_update(const Dev& d, cudaStream_t s);
 int launch_clear_new_slots(const Dev& d, const Shape& sh, cudaStream_t s);
-// The active bricks' entries (face-neighbour slots, own slot, brick index) that the brick passes traverse.
-int launch_brick_entries(const Dev& d, uint32_t* entries, const Shape& sh, cudaStream_t s);
 
 // ---- grid passes ----
 int launch_mark_cells(const Dev& d, const Pass& p, const Shape& sh, cudaStream_t s);

@@ -92,65 +92,34 @@ __device__ __forceinline__ bool touches_air(const Dev& d, uint32_t index, int3 c
     return t;
 }
 
-// Visits the in-grid cells of the active bricks: fn(index, c); one brick per CTA iteration. The bricks come from
-// the entry table (d.brick_entries: neighbour slots, own slot, brick index), and the next brick's entry is loaded
-// while the current brick's cells run, so a brick costs no dependent table reads. With kSlots the brick's six
-// face-neighbour slots are placed in shared memory (between two barriers), so nbr_index_cta resolves neighbours
-// across the brick's faces without brick-table reads; then fn must not contain CTA barriers and every thread must
-// call it. Passes with little work per brick (one colour of a sweep, no neighbours at all) take kSlots = false: no
-// barriers, neighbours through the brick table.
+// Visits the in-grid cells of the active bricks: fn(index, c); one brick per CTA iteration. With kSlots
+// the brick's six face-neighbour slots are first loaded into shared memory (between two barriers), so
+// nbr_index_cta resolves neighbours across the brick's faces without brick-table reads; then fn must not
+// contain CTA barriers and every thread must call it. Passes with little work per brick (one colour of
+// a sweep, no neighbours at all) take kSlots = false: no barriers, neighbours through the brick table.
 template <bool kSlots, class Fn>
 __device__ __forceinline__ void for_active_cells(const Dev& d, Fn fn) {
     const uint32_t active = d.active_bricks[0];
     uint32_t* ns = cta_nbr_slots();
-    uint4 cur0 = make_uint4(0u, 0u, 0u, 0u), cur1 = make_uint4(0u, 0u, 0u, 0u);
-    if (blockIdx.x < active) {
-        cur0 = __ldg(reinterpret_cast<const uint4*>(d.brick_entries + 8u * blockIdx.x));
-        cur1 = __ldg(reinterpret_cast<const uint4*>(d.brick_entries + 8u * blockIdx.x + 4u));
-    }
     for (uint32_t e = blockIdx.x; e < active; e += gridDim.x) {
-        const uint32_t en = e + gridDim.x;
-        uint4 nx0 = make_uint4(0u, 0u, 0u, 0u), nx1 = make_uint4(0u, 0u, 0u, 0u);
-        if (en < active) {
-            nx0 = __ldg(reinterpret_cast<const uint4*>(d.brick_entries + 8u * en));
-            nx1 = __ldg(reinterpret_cast<const uint4*>(d.brick_entries + 8u * en + 4u));
-        }
-        const uint32_t slot = cur1.z, brick = cur1.w;
+        const uint32_t brick = d.active_bricks[1u + e];
         const int3 bc = brick_coord_of(d, brick);
         if (kSlots) {
             __syncthreads();  // the previous brick's cells are done with the neighbour slots
             if (threadIdx.x < 6u) {
-                const uint32_t t = threadIdx.x;
-                ns[t] = t == 0u ? cur0.x : (t == 1u ? cur0.y : (t == 2u ? cur0.z : (t == 3u ? cur0.w : (t == 4u ? cur1.x : cur1.y))));
+                const int3 nb = add3(bc, nbr_off(int(threadIdx.x)));
+                const bool in = nb.x >= 0 && nb.y >= 0 && nb.z >= 0 && nb.x < d.brick_dim.x && nb.y < d.brick_dim.y && nb.z < d.brick_dim.z;
+                ns[threadIdx.x] = in ? __ldg(d.brick_table + brick_index_of(d, nb)) : 0u;
             }
-            __syncthreads();
         }
+        const uint32_t slot = __ldg(d.brick_table + brick);
+        if (kSlots) __syncthreads();
 #pragma unroll
         for (int k = 0; k < 2; ++k) {
             const uint32_t l = threadIdx.x + uint32_t(k) * 256u;
             const int3 lc = local_coord_of(l);
             const int3 c = make_int3(bc.x * 8 + lc.x, bc.y * 8 + lc.y, bc.z * 8 + lc.z);
             if (in_grid(d, c)) fn(slot * BRICK_CELLS + l, c);
-        }
-        cur0 = nx0;
-        cur1 = nx1;
-    }
-}
-
-// Entry e of the active-brick table: its face-neighbour slots, own slot and brick index (one warp per entry).
-__global__ void k_brick_entries(Dev d, uint32_t* entries) {
-    const uint32_t active = d.active_bricks[0];
-    const uint32_t lane = threadIdx.x & 31u, wpb = blockDim.x >> 5;
-    for (uint32_t e = blockIdx.x * wpb + (threadIdx.x >> 5); e < active; e += gridDim.x * wpb) {
-        const uint32_t brick = d.active_bricks[1u + e];
-        if (lane < 6u) {
-            const int3 nb = add3(brick_coord_of(d, brick), nbr_off(int(lane)));
-            const bool in = nb.x >= 0 && nb.y >= 0 && nb.z >= 0 && nb.x < d.brick_dim.x && nb.y < d.brick_dim.y && nb.z < d.brick_dim.z;
-            entries[8u * e + lane] = in ? __ldg(d.brick_table + brick_index_of(d, nb)) : 0u;
-        } else if (lane == 6u) {
-            entries[8u * e + 6u] = __ldg(d.brick_table + brick);
-        } else if (lane == 7u) {
-            entries[8u * e + 7u] = brick;
         }
     }
 }
@@ -813,10 +782,6 @@ int launch_pool_update(const Dev& d, cudaStream_t s) {
         configured = smem;
     }
     k_pool_update<<<1, 1024, smem, s>>>(d);
-    return 1;
-}
-int launch_brick_entries(const Dev& d, uint32_t* entries, const Shape& sh, cudaStream_t s) {
-    k_brick_entries<<<sh.brick_ctas, 256, 0, s>>>(d, entries);
     return 1;
 }
 int launch_clear_new_slots(const Dev& d, const Shape& sh, cudaStream_t s) {
