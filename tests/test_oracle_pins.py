@@ -156,8 +156,9 @@ def test_p2g_weight_sums(oracle_mod):
         assert abs(fw[a].sum() - n) <= 8 * n / 2**20 + 1e-9
 
 
-def _assemble(o):
-    """Pressure system of the oracle's last solve, assembled from its own buffers (scipy CSR)."""
+def _assemble(o, fp64=False):
+    """Pressure system of the oracle's last solve, assembled from its own buffers (scipy CSR); with fp64 from the
+    FP64 oracle's double buffers (diagonal + double(1e-4f), as that oracle forms it)."""
     import scipy.sparse as sp
     L = o.layout()
     bd = np.array(list(L.brick_dim))
@@ -165,8 +166,8 @@ def _assemble(o):
     ab = o.read("ACTIVE_BRICKS")
     bt = o.read("BRICK_TABLE")
     ct = o.read("CELL_TYPE") & 3
-    diag = o.read("CELL_DIAG").astype(np.float64)
-    div = o.read("DIVERGENCE").astype(np.float64)
+    diag = (o.read_f64 if fp64 else o.read)("CELL_DIAG").astype(np.float64)
+    div = (o.read_f64 if fp64 else o.read)("DIVERGENCE").astype(np.float64)
     idx_of = {}
     cells = []
     for e in range(int(ab[0])):
@@ -185,7 +186,8 @@ def _assemble(o):
     rows, cols, vals = [], [], []
     b = np.zeros(len(cells))
     for k, (c, i) in enumerate(cells):
-        rows.append(k); cols.append(k); vals.append(float(np.float32(diag[i]) + np.float32(1e-4)))
+        rows.append(k); cols.append(k)
+        vals.append(float(diag[i] + np.float64(np.float32(1e-4))) if fp64 else float(np.float32(diag[i]) + np.float32(1e-4)))
         b[k] = -div[i]
         for d in ((1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1)):
             nb = (c[0] + d[0], c[1] + d[1], c[2] + d[2])
@@ -386,3 +388,35 @@ def test_overcorrected_vcycle_needs_fewer_iterations(oracle_mod):
     assert sum(counts["scaled"]) < sum(counts["ref"]), counts
     assert sum(counts["two"]) < sum(counts["scaled"]), counts
     assert all(abs(a - b) <= 1 for a, b in zip(counts["flex"], counts["scaled"])), counts
+
+
+@pytest.mark.parametrize("scale,sweeps,flexible", [(1.0, 1, 0), (1.9, 2, 1)])
+def test_mgpcg_matches_direct_solve_sparse_64(oracle_mod, scale, sweeps, flexible):
+    """The solve's mathematics pinned independently of any reduction order: the FP64 oracle's MGPCG on the sparse
+    64^3 dam break + falling sphere (ghost-fluid diagonals at the free surface, several MG levels through the
+    footprints and the shared tail), with the reference's V-cycle and with the tuned options, against scipy's
+    direct sparse solve of the same assembled system (diag_f + 1e-4 on the fluid cells, -1 per fluid neighbour)."""
+    import scipy.sparse.linalg as spla
+    sc = scenes.dam_break_sphere(oracle_mod.settings_default, n=64)
+    s = sc["settings"]
+    s.max_substeps = 16
+    s.mg_correction_scale, s.mg_smoothing_sweeps, s.pcg_flexible = scale, sweeps, flexible
+    o = oracle_mod.Oracle(s, fp64=True)
+    o.set_emit_seed(sc["seed"])
+    fi = A.frame_input(s, emits=sc["emits"])
+    for _ in range(2):
+        o.step_frame(fi)
+        fi = A.frame_input(s)
+    A_, b, idx = _assemble(o, fp64=True)
+    assert len(idx) > 30000
+    diag = A_.diagonal()
+    assert np.any(np.abs(diag - np.round(diag)) > 1e-3), "no ghost-fluid (fractional) diagonal in the system"
+    p = o.read_f64("PRESSURE")[idx]
+    exact = spla.spsolve(A_.tocsc(), b)
+    rel = np.linalg.norm(b - A_ @ p) / np.linalg.norm(b)
+    res = o.results()
+    assert res.last_solve_rel_residual <= 1e-6
+    # FP64: the true residual equals the recursive one (no FP32 floor)
+    assert rel <= 1.01e-6, rel
+    assert np.linalg.norm(p - exact) / np.linalg.norm(exact) < 1e-4
+    o.close()
