@@ -111,9 +111,20 @@ __global__ void k_touch(Dev d, const slosh_particle_t* __restrict__ particles, u
 // memory with integer atomics, then adds each non-zero tile entry to global memory once. A CTA whose
 // box does not fit adds directly to global memory. Integer sums make both paths identical.
 constexpr int P2G_THREADS = 256;
+#ifndef P2G_MINB_ONE
+#define P2G_MINB_ONE 6
+#endif
+#ifndef P2G_MINB_SMALL
+#define P2G_MINB_SMALL 5  // 48 registers, 5 CTAs per SM with the small tile
+#endif
 constexpr int P2G_PER_THREAD_DEFAULT = 2;  // measured: 2 per thread 0.975 ms, 4: 1.105, 8: 1.32 per 256^3 launch
-constexpr int P2G_TILE_NODES = 2048;  // nodes per quantity (6 quantities) = 48 KB
-constexpr int P2G_TILE_CELLS = 1024;  // counted cells = 4 KB
+// Tile capacity per CTA: nodes per quantity (6 quantities) and counted cells. A CTA of 2 particles per thread
+// (512 particles, about 64 cells) needs about a third of the larger tile; the smaller one halves the shared memory.
+template <int PER> struct P2GTile {
+    static constexpr int NODES = PER >= 4 ? 2048 : (PER == 2 ? 1024 : 512);
+    static constexpr int CELLS = PER >= 4 ? 1024 : (PER == 2 ? 512 : 256);
+    static constexpr int MINB = PER >= 4 ? 1 : (PER == 2 ? P2G_MINB_SMALL : P2G_MINB_ONE);
+};
 
 __device__ __forceinline__ int3 p2g_cell(const Dev& d, float3 pos) {
     return make_int3(clampi(int(floorf(pos.x * d.inv_h)), 0, d.grid.x - 1), clampi(int(floorf(pos.y * d.inv_h)), 0, d.grid.y - 1),
@@ -121,8 +132,11 @@ __device__ __forceinline__ int3 p2g_cell(const Dev& d, float3 pos) {
 }
 
 template <int P2G_PER_THREAD>
-__global__ void __launch_bounds__(P2G_THREADS) k_p2g(Dev d, Pass p, const slosh_particle_t* __restrict__ particles, uint32_t n) {
+__global__ void __launch_bounds__(P2G_THREADS, P2GTile<P2G_PER_THREAD>::MINB) k_p2g(Dev d, Pass p, const slosh_particle_t* __restrict__ particles,
+                                                                                 uint32_t n) {
     constexpr int P2G_CHUNK = P2G_THREADS * P2G_PER_THREAD;
+    constexpr int P2G_TILE_NODES = P2GTile<P2G_PER_THREAD>::NODES;
+    constexpr int P2G_TILE_CELLS = P2GTile<P2G_PER_THREAD>::CELLS;
     extern __shared__ int smem[];
     int* tile = smem;                          // [6][P2G_TILE_NODES]
     int* ctile = smem + 6 * P2G_TILE_NODES;    // [P2G_TILE_CELLS]
@@ -428,26 +442,151 @@ __device__ __forceinline__ float3 sample_displacement(const Dev& d, float3 xp, c
 
 constexpr int G2P_THREADS = 256;
 
+// ---- the CTA's face-velocity tile (APIC G2P) --------------------------------------------------------------
+// The CTA's particles are spatially sorted, so their cells span a small box. Before gathering, the CTA copies
+// the three face-velocity components of that box plus a margin of G2P_MARGIN cells (clamped to the grid) from
+// the brick pool into shared memory; the gathers at the particle (nodes within one cell of its cell) and at the
+// RK2 midpoint (less than two cells away: nodes within three cells) then read the tile with plain index
+// arithmetic instead of brick-table lookups. A particle whose stencil falls outside the tile, the midpoint
+// samples that test face flags, the density displacement and FLIP read the pool as before; a CTA whose box does
+// not fit reads the pool throughout. The values are the pool's, so results are identical.
+constexpr int G2P_TILE_NODES = 2048;  // per component: 24 KB for the three
+constexpr int G2P_MARGIN = 3;
+struct VelTile {
+    int ox, oy, oz;  // tile origin (cells, clamped into the grid)
+    int tx, ty, tz;  // tile extent
+    const float* s;  // [3][G2P_TILE_NODES] in shared memory
+};
+// Clamped node coordinates of a stencil (the values stencil_indices addresses).
+struct NodeBox {
+    int x0, x1, y0, y1, z0, z1;
+};
+__device__ __forceinline__ NodeBox stencil_nodes(const Dev& d, const Stencil& s) {
+    NodeBox b;
+    b.x0 = clampi(s.base.x, 0, d.grid.x - 1);
+    b.x1 = clampi(s.base.x + 1, 0, d.grid.x - 1);
+    b.y0 = clampi(s.base.y, 0, d.grid.y - 1);
+    b.y1 = clampi(s.base.y + 1, 0, d.grid.y - 1);
+    b.z0 = clampi(s.base.z, 0, d.grid.z - 1);
+    b.z1 = clampi(s.base.z + 1, 0, d.grid.z - 1);
+    return b;
+}
+// The 8 stencil values of one component from the tile; false (nothing read) if any node lies outside it.
+__device__ __forceinline__ bool tile_vals(const VelTile& T, int axis, const NodeBox& b, float (&u)[8]) {
+    const int x0 = b.x0 - T.ox, x1 = b.x1 - T.ox, y0 = b.y0 - T.oy, y1 = b.y1 - T.oy, z0 = b.z0 - T.oz, z1 = b.z1 - T.oz;
+    if (unsigned(x0) >= unsigned(T.tx) || unsigned(x1) >= unsigned(T.tx) || unsigned(y0) >= unsigned(T.ty) ||
+        unsigned(y1) >= unsigned(T.ty) || unsigned(z0) >= unsigned(T.tz) || unsigned(z1) >= unsigned(T.tz))
+        return false;
+    const float* c = T.s + axis * G2P_TILE_NODES;
+    const int sy = T.tx, sz = T.tx * T.ty;
+    const int r00 = y0 * sy + z0 * sz, r10 = y1 * sy + z0 * sz, r01 = y0 * sy + z1 * sz, r11 = y1 * sy + z1 * sz;
+    u[0] = c[r00 + x0]; u[1] = c[r00 + x1];
+    u[2] = c[r10 + x0]; u[3] = c[r10 + x1];
+    u[4] = c[r01 + x0]; u[5] = c[r01 + x1];
+    u[6] = c[r11 + x0]; u[7] = c[r11 + x1];
+    return true;
+}
+// GatherComponent (APIC) from the tile, the pool where the tile does not cover the stencil.
+__device__ __forceinline__ void gather_apic_tile(const Dev& d, const VelTile& T, int axis, float3 xp, const float* __restrict__ vel,
+                                                 float& unew, float3& grad) {
+    const Stencil s = stencil_of(d, xp, axis);
+    float u[8];
+    if (!tile_vals(T, axis, stencil_nodes(d, s), u)) {
+        uint32_t idx[8];
+        stencil_indices(d, s, axis, idx);
+#pragma unroll
+        for (int o = 0; o < 8; ++o) u[o] = vel[idx[o]];
+    }
+    unew = lerp3(u, s.fx, s.fy, s.fz, d.inv_h, true, &grad);
+}
+// SampleVelocityComponent without the known-face test, from the tile where it covers the stencil.
+__device__ __forceinline__ float sample_tile(const Dev& d, const VelTile& T, int axis, float3 xp, const float* __restrict__ vel) {
+    const Stencil s = stencil_of(d, xp, axis);
+    float u[8];
+    if (!tile_vals(T, axis, stencil_nodes(d, s), u)) {
+        uint32_t idx[8];
+        stencil_indices(d, s, axis, idx);
+#pragma unroll
+        for (int o = 0; o < 8; ++o) u[o] = vel[idx[o]];
+    }
+    return lerp3(u, s.fx, s.fy, s.fz, d.inv_h, false, nullptr);
+}
+
 // AdvectParticle + G2PAdvectCS (Slosh.usf:1452-1678).
-__global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p(Dev d, Pass p, slosh_particle_t* __restrict__ particles, uint32_t n,
+template <int MINB>
+__global__ void __launch_bounds__(G2P_THREADS, MINB) k_g2p(Dev d, Pass p, slosh_particle_t* __restrict__ particles, uint32_t n,
                                                      const float* __restrict__ vel, const float* __restrict__ disp,
                                                      uint32_t apply_density) {
     const uint32_t i = blockIdx.x * G2P_THREADS + threadIdx.x;
     uint32_t brick = NO_BRICK;
     uint32_t speed_bits = 0u;
+    __shared__ float s_vel[3 * G2P_TILE_NODES];
+    __shared__ int s_box[6];
+    float4 ra = make_float4(0.0f, 0.0f, 0.0f, -1.0f), rb = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    uint4 rc = make_uint4(0u, 0u, 0u, 0u);
+    if (i < n) load_particle_raw(particles, i, ra, rb, rc);
+    // The tile (APIC only): the box of the CTA's live particles' cells plus the margin, clamped to the grid.
+    VelTile T{0, 0, 0, 0, 0, 0, s_vel};
+    if (p.use_apic) {
+        if (threadIdx.x < 3) { s_box[threadIdx.x] = 0x7FFFFFFF; s_box[3 + threadIdx.x] = -0x7FFFFFFF; }
+        __syncthreads();
+        const int big = 0x7FFFFFFF;
+        int3 mn = make_int3(big, big, big), mx = make_int3(-big, -big, -big);
+        if (i < n && !is_dead_age(ra.w)) {
+            const int3 c = make_int3(clampi(int(floorf(ra.x * d.inv_h)), 0, d.grid.x - 1), clampi(int(floorf(ra.y * d.inv_h)), 0, d.grid.y - 1),
+                                     clampi(int(floorf(ra.z * d.inv_h)), 0, d.grid.z - 1));
+            mn = c;
+            mx = c;
+        }
+        mn.x = __reduce_min_sync(0xFFFFFFFFu, mn.x); mn.y = __reduce_min_sync(0xFFFFFFFFu, mn.y); mn.z = __reduce_min_sync(0xFFFFFFFFu, mn.z);
+        mx.x = __reduce_max_sync(0xFFFFFFFFu, mx.x); mx.y = __reduce_max_sync(0xFFFFFFFFu, mx.y); mx.z = __reduce_max_sync(0xFFFFFFFFu, mx.z);
+        if ((threadIdx.x & 31) == 0) {
+            atomicMin(s_box + 0, mn.x); atomicMin(s_box + 1, mn.y); atomicMin(s_box + 2, mn.z);
+            atomicMax(s_box + 3, mx.x); atomicMax(s_box + 4, mx.y); atomicMax(s_box + 5, mx.z);
+        }
+        __syncthreads();
+        if (s_box[0] != big) {
+            T.ox = max(s_box[0] - G2P_MARGIN, 0);
+            T.oy = max(s_box[1] - G2P_MARGIN, 0);
+            T.oz = max(s_box[2] - G2P_MARGIN, 0);
+            T.tx = min(s_box[3] + G2P_MARGIN, d.grid.x - 1) - T.ox + 1;
+            T.ty = min(s_box[4] + G2P_MARGIN, d.grid.y - 1) - T.oy + 1;
+            T.tz = min(s_box[5] + G2P_MARGIN, d.grid.z - 1) - T.oz + 1;
+            const long long nodes = (long long)T.tx * T.ty * T.tz;
+            if (nodes > G2P_TILE_NODES) {
+                T.tx = T.ty = T.tz = 0;  // does not fit: every stencil reads the pool
+            } else {
+                // fill: node t = (x, y, z) of the tile, its brick's slot, the three components
+                const int sy = T.tx, sz = T.tx * T.ty;
+                for (int t = threadIdx.x; t < int(nodes); t += G2P_THREADS) {
+                    const int lz = t / sz, r = t - lz * sz, ly = r / sy, lx = r - ly * sy;
+                    const int3 c = make_int3(T.ox + lx, T.oy + ly, T.oz + lz);
+                    const uint32_t ci = cell_index(d, c);
+                    const float v0 = vel[ci], v1 = vel[d.pool_cells + ci], v2 = vel[2u * d.pool_cells + ci];
+                    s_vel[t] = v0;
+                    s_vel[G2P_TILE_NODES + t] = v1;
+                    s_vel[2 * G2P_TILE_NODES + t] = v2;
+                }
+            }
+        }
+        __syncthreads();
+    }
     if (i < n) {
-        float4 ra, rb;
-        uint4 rc;
-        load_particle_raw(particles, i, ra, rb, rc);
         ParticleF P = unpack_particle(ra, rb, rc);
         if (!is_dead_age(P.age)) {
             const float h = d.h, inv_h = d.inv_h, dt = p.dt;
             const float lo = h * 1.01f;
             const float3 hi = make_float3((float(d.grid.x) - 1.01f) * h, (float(d.grid.y) - 1.01f) * h, (float(d.grid.z) - 1.01f) * h);
-            float3 pic, delta, dw, gx, gy, gz;
-            gather_component(d, p, 0, P.pos, vel, pic.x, delta.x, dw.x, gx);
-            gather_component(d, p, 1, P.pos, vel, pic.y, delta.y, dw.y, gy);
-            gather_component(d, p, 2, P.pos, vel, pic.z, delta.z, dw.z, gz);
+            float3 pic, delta = make_float3(0.0f, 0.0f, 0.0f), dw = make_float3(0.0f, 0.0f, 0.0f), gx, gy, gz;
+            if (p.use_apic) {
+                gather_apic_tile(d, T, 0, P.pos, vel, pic.x, gx);
+                gather_apic_tile(d, T, 1, P.pos, vel, pic.y, gy);
+                gather_apic_tile(d, T, 2, P.pos, vel, pic.z, gz);
+            } else {
+                gather_component(d, p, 0, P.pos, vel, pic.x, delta.x, dw.x, gx);
+                gather_component(d, p, 1, P.pos, vel, pic.y, delta.y, dw.y, gy);
+                gather_component(d, p, 2, P.pos, vel, pic.z, delta.z, dw.z, gz);
+            }
             float3 nv;
             if (p.use_apic) {
                 nv = pic;
@@ -470,8 +609,13 @@ __global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p(Dev d, Pass p, slosh_par
             float3 v2 = v1;
             if (mid_cells < 2.0f) {
                 const bool check = mid_cells > 1.0f;
-                const float3 sv = make_float3(sample_component(d, 0, mid, v1.x, check, vel), sample_component(d, 1, mid, v1.y, check, vel),
-                                              sample_component(d, 2, mid, v1.z, check, vel));
+                float3 sv;
+                if (check || !p.use_apic) {
+                    sv = make_float3(sample_component(d, 0, mid, v1.x, check, vel), sample_component(d, 1, mid, v1.y, check, vel),
+                                     sample_component(d, 2, mid, v1.z, check, vel));
+                } else {
+                    sv = make_float3(sample_tile(d, T, 0, mid, vel), sample_tile(d, T, 1, mid, vel), sample_tile(d, T, 2, mid, vel));
+                }
                 const float t = saturatef(mid_cells - 1.0f);
                 v2 = make_float3(sv.x + t * (v1.x - sv.x), sv.y + t * (v1.y - sv.y), sv.z + t * (v1.z - sv.z));
             }
@@ -616,7 +760,7 @@ int launch_touch_particles(const Dev& d, const slosh_particle_t* particles, uint
 template <int PER>
 void launch_p2g_per(const Dev& d, const Pass& p, const slosh_particle_t* particles, uint32_t n, cudaStream_t s) {
     static bool configured = false;
-    const int smem = (6 * P2G_TILE_NODES + P2G_TILE_CELLS) * int(sizeof(int));
+    const int smem = (6 * P2GTile<PER>::NODES + P2GTile<PER>::CELLS) * int(sizeof(int));
     if (!configured) {
         cudaFuncSetAttribute(k_p2g<PER>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         configured = true;
@@ -639,7 +783,8 @@ int launch_p2g(const Dev& d, const Pass& p, const slosh_particle_t* particles, u
 int launch_g2p(const Dev& d, const Pass& p, slosh_particle_t* particles, uint32_t n, const float* vel, const float* disp,
                bool apply_density, cudaStream_t s) {
     if (n == 0) return 0;
-    k_g2p<<<(n + G2P_THREADS - 1u) / G2P_THREADS, G2P_THREADS, 0, s>>>(d, p, particles, n, vel, disp, apply_density ? 1u : 0u);
+    // 4 CTAs per SM (64 registers): 5 (48 registers, spills) and 6 (40) measured no faster
+    k_g2p<4><<<(n + G2P_THREADS - 1u) / G2P_THREADS, G2P_THREADS, 0, s>>>(d, p, particles, n, vel, disp, apply_density ? 1u : 0u);
     return 1;
 }
 
