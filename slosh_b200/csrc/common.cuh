@@ -192,6 +192,16 @@ __device__ __forceinline__ void store_dead(slosh_particle_t* out, uint32_t i) { 
 }
 __device__ __forceinline__ bool is_dead_age(float age) { return !(age >= 0.0f); }
 
+// Programmatic dependent launch. A kernel launched with programmatic stream serialisation (launch_k) may be
+// scheduled while its predecessor in the stream is still draining; pdl_entry() first waits until that
+// predecessor has completed and its writes are visible (griddepcontrol.wait), then lets the kernel's own
+// successor be scheduled (griddepcontrol.launch_dependents), so a successor's CTAs take the SMs this kernel's
+// CTAs release while it finishes. Both instructions are no-ops in a kernel launched without the attribute.
+__device__ __forceinline__ void pdl_entry() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // ---- hashing (SloshCommon.ush:255-265) ----------------------------------------------------------------
 __device__ __forceinline__ uint32_t pcg_hash(uint32_t v) {
     const uint32_t state = v * 747796405u + 2891336453u;

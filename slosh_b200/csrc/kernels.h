@@ -18,6 +18,25 @@ struct Shape {
     int num_sms;
 };
 
+// Launches kernel k on stream s, with programmatic stream serialisation unless SLOSH_PDL=0: the kernel may be
+// scheduled before its predecessor in the stream completes, and must call pdl_entry() before anything else.
+// The attribute survives stream capture as a programmatic edge of the graph.
+bool pdl_enabled();
+template <typename... P, typename... A>
+inline cudaError_t launch_k(void (*k)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, A&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl_enabled() ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, k, static_cast<A&&>(args)...);
+}
+
 // ---- brick pool (Slosh.usf:1719-1831) ----
 int launch_pool_update(const Dev& d, cudaStream_t s);
 int launch_clear_new_slots(const Dev& d, const Shape& sh, cudaStream_t s);

@@ -43,6 +43,17 @@ __device__ __forceinline__ float lv_ld(const float* a, uint32_t i, uint32_t prec
     const uint16_t h = reinterpret_cast<const uint16_t*>(a)[i];
     return prec == SLOSH_PRECISION_FP16_STORAGE ? __half2float(__ushort_as_half(h)) : __uint_as_float(uint32_t(h) << 16);
 }
+// The same load through L2 only (ld.global.cg): for values another CTA of the cluster wrote earlier in the
+// same kernel, ordered by a cluster barrier.
+__device__ __forceinline__ float lv_ldcg(const float* a, uint32_t i, uint32_t prec) {
+    if (prec == SLOSH_PRECISION_FP32) return __ldcg(a + i);
+    const uint16_t h = __ldcg(reinterpret_cast<const unsigned short*>(a) + i);
+    return prec == SLOSH_PRECISION_FP16_STORAGE ? __half2float(__ushort_as_half(h)) : __uint_as_float(uint32_t(h) << 16);
+}
+template <bool CG>
+__device__ __forceinline__ float lvx(const float* a, uint32_t i, uint32_t prec) {
+    return CG ? lv_ldcg(a, i, prec) : lv_ld(a, i, prec);
+}
 __device__ __forceinline__ uint16_t to_storage16(float v, uint32_t prec) {
     return prec == SLOSH_PRECISION_FP16_STORAGE ? __half_as_ushort(__float2half_rn(v)) : __bfloat16_as_ushort(__float2bfloat16_rn(v));
 }
@@ -392,6 +403,7 @@ __device__ __forceinline__ float ratio_f(double num, double den) { return fabs(d
 
 // ---- solve setup: iteration state in ctl[] --------------------------------------------------------------
 __global__ void k_solve_setup(MGState m, uint32_t limit, uint32_t tol_mode, double tol) {
+    pdl_entry();
     m.ctl[0] = 0u;        // completed iterations
     m.ctl[1] = limit;     // iteration limit
     m.ctl[2] = tol_mode;  // 1: stop at ||r|| <= tol ||b||
@@ -401,6 +413,7 @@ __global__ void k_solve_setup(MGState m, uint32_t limit, uint32_t tol_mode, doub
 
 // ---- MGBuildTypeCS: coarse cell = air if any child is air, else fluid if any child is fluid ---------------
 __global__ void k_build_type(Dev d, MGLevel fine, MGLevel coarse, int fine_is_pool) {
+    pdl_entry();
     const uint32_t ci = blockIdx.x * blockDim.x + threadIdx.x;
     if (ci >= coarse.cells) return;
     const int3 c = coord3(ci, coarse.dim);
@@ -420,6 +433,7 @@ __global__ void k_build_type(Dev d, MGLevel fine, MGLevel coarse, int fine_is_po
 constexpr uint32_t CW_FLUID = 1u << 6, CW_RED = 1u << 7, CW_NONSOLID_SHIFT = 8u;
 
 __global__ void k_level_words(MGLevel L) {
+    pdl_entry();
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= L.cells) return;
     const int3 c = coord3(i, L.dim);
@@ -446,12 +460,13 @@ __device__ __forceinline__ float word_diag(uint32_t w) {
 // Sum of x over the fluid neighbours of a dense global level, in neighbour order. All six values are
 // loaded unconditionally (indices clamped into the level, so a missing neighbour reads some cell of
 // the level) and then selected by the word, so the loads overlap the word's.
+template <bool CG = false>
 __device__ __forceinline__ float word_sum_g(const float* x, uint32_t prec, uint32_t w, uint32_t i, uint32_t dx, uint32_t dxy,
                                             uint32_t last) {
     const uint32_t off[6] = {i - 1u, i + 1u, i - dx, i + dx, i - dxy, i + dxy};
     float v[6];
 #pragma unroll
-    for (int n = 0; n < 6; ++n) v[n] = lv_ld(x, min(off[n], last), prec);
+    for (int n = 0; n < 6; ++n) v[n] = lvx<CG>(x, min(off[n], last), prec);
     float sum = 0.0f;
 #pragma unroll
     for (int n = 0; n < 6; ++n)
@@ -475,6 +490,7 @@ __device__ __forceinline__ float word_sum(const float* x, uint32_t w, uint32_t i
 // First stores the solve's stencil words and each active brick's neighbour and own slots; the residual
 // pass itself reads the cell types directly (its neighbours' words may not be written yet).
 __global__ void __launch_bounds__(GRID_THREADS) k_pcg_words(Dev d, MGState m) {
+    pdl_entry();
     const uint32_t active = d.active_bricks[0];
     const uint32_t lane = threadIdx.x & 31u, wpb = blockDim.x >> 5;
     for (uint32_t e = blockIdx.x * wpb + (threadIdx.x >> 5); e < active; e += gridDim.x * wpb) {
@@ -511,6 +527,7 @@ __global__ void __launch_bounds__(GRID_THREADS) k_pcg_words(Dev d, MGState m) {
 }
 __global__ void __launch_bounds__(GRID_THREADS) k_pcg_init(Dev d, MGState m, const float* __restrict__ p, const float* __restrict__ div,
                                                            unsigned long long handle) {
+    pdl_entry();
     struct V {
         Q6 p;
         float4 dv, dg;
@@ -575,6 +592,7 @@ __device__ __forceinline__ Nb6 load_black(const Dev& d, const MGState& m, uint32
 // brick).
 template <bool DOT>
 __global__ void __launch_bounds__(GRID_THREADS, 3) k_smooth0(Dev d, MGState m) {
+    pdl_entry();
     w4_pass<DOT ? 1 : 0, 1>(d, m, 1,
         [&](const Geo& g, const uint32_t* ns) { return load_sweep(d, m, g, ns); },
         [&](const Geo& g, const SweepQ& v, double* v0, double*) {
@@ -603,6 +621,7 @@ __global__ void __launch_bounds__(GRID_THREADS, 3) k_smooth0(Dev d, MGState m) {
 
 // Black sweep (no dot product).
 __global__ void __launch_bounds__(GRID_THREADS) k_smooth0_black(Dev d, MGState m) {
+    pdl_entry();
     w0_black<4>(d, m, [](uint32_t, uint32_t) {},
         [&](uint32_t i, uint32_t l, const uint32_t* ns) { return load_black(d, m, i, l, ns); },
         [&](uint32_t i, uint32_t, const Nb6& v) {
@@ -619,6 +638,7 @@ __global__ void __launch_bounds__(GRID_THREADS) k_smooth0_black(Dev d, MGState m
 // x_c where the parent is fluid and 0 elsewhere) in shared memory. Adding +0 instead of skipping the
 // addition changes at most the sign of a zero z_n, which the neighbour sum (started at +0) absorbs.
 __global__ void __launch_bounds__(GRID_THREADS) k_prolong_smooth0(Dev d, MGState m) {
+    pdl_entry();
     constexpr int WARPS = GRID_THREADS / 32;
     __shared__ float s_cx[WARPS][216];
     const MGLevel C = m.lv[1];
@@ -665,16 +685,18 @@ __global__ void __launch_bounds__(GRID_THREADS) k_prolong_smooth0(Dev d, MGState
 // Levels 1..3 through the active-brick footprints, with the per-solve stencil words; each pass is a
 // per-cell body and a grid-wide kernel over the level's footprint.
 // Sweep of one colour (want = CW_RED: red cells, 0: black cells) at cell i of level L.
+template <bool CG = false>
 __device__ __forceinline__ void smooth_fp_cell(const MGLevel& L, uint32_t i, uint32_t want) {
     const uint32_t dx = uint32_t(L.dim.x), dxy = uint32_t(L.dim.x * L.dim.y);
     const uint32_t w = L.word[i];
-    const float b = lv_ld(L.b, i, L.prec);
-    const float sum = word_sum_g(L.x, L.prec, w, i, dx, dxy, L.cells - 1u);
+    const float b = lvx<CG>(L.b, i, L.prec);
+    const float sum = word_sum_g<CG>(L.x, L.prec, w, i, dx, dxy, L.cells - 1u);
     if (!(w & CW_FLUID) || (w & CW_RED) != want) return;
     lv_st(L.x, i, L.prec, (b + sum) / word_diag(w));
 }
 // Restriction F -> C at coarse cell ci: b_c = scale x (sum of the fluid children's residuals), scale = 1/4 in
 // the reference (times mg_correction_scale).
+template <bool CG = false>
 __device__ __forceinline__ void restrict_fp_cell(const MGLevel& F, const MGLevel& C, uint32_t ci, int3 c, float scale) {
     const uint32_t fdx = uint32_t(F.dim.x), fdxy = uint32_t(F.dim.x * F.dim.y);
     const uint32_t flast = F.cells - 1u;
@@ -688,7 +710,7 @@ __device__ __forceinline__ void restrict_fp_cell(const MGLevel& F, const MGLevel
         const bool in = inside3(f, F.dim);
         const uint32_t fi = in ? lin3(f, F.dim) : 0u;
         const uint32_t w = F.word[fi];
-        const float r = lv_ld(F.b, fi, F.prec) - (word_diag(w) * lv_ld(F.x, fi, F.prec) - word_sum_g(F.x, F.prec, w, fi, fdx, fdxy, flast));
+        const float r = lvx<CG>(F.b, fi, F.prec) - (word_diag(w) * lvx<CG>(F.x, fi, F.prec) - word_sum_g<CG>(F.x, F.prec, w, fi, fdx, fdxy, flast));
         res[o] = 0.0f;
         if (in && (w & CW_FLUID)) {
             fl |= 1u << o;
@@ -705,22 +727,23 @@ __device__ __forceinline__ void restrict_fp_cell(const MGLevel& F, const MGLevel
     lv_st(C.x, ci, C.prec, (cw & CW_RED) ? bb / word_diag(cw) : 0.0f);
 }
 // Prolongation C -> F fused with the black sweep of F (see k_prolong_smooth0) at fine cell i.
+template <bool CG = false>
 __device__ __forceinline__ void prolong_smooth_fp_cell(const MGLevel& F, const MGLevel& C, uint32_t i, int3 c) {
     const uint32_t dx = uint32_t(F.dim.x), dxy = uint32_t(F.dim.x * F.dim.y);
     const uint32_t last = F.cells - 1u, clast = C.cells - 1u;
     // The neighbours' x and their parents' words and x are loaded before the word is tested
     // (indices clamped into the levels; values of non-fluid neighbours are not used).
     const uint32_t w = F.word[i];
-    const float b = lv_ld(F.b, i, F.prec);
+    const float b = lvx<CG>(F.b, i, F.prec);
     const uint32_t off[6] = {i - 1u, i + 1u, i - dx, i + dx, i - dxy, i + dxy};
     float v[6];
 #pragma unroll
     for (int n = 0; n < 6; ++n) {
         const int3 nb = add3(c, nbr_off(n));
         const uint32_t pi = min(lin3(make_int3(nb.x / 2, nb.y / 2, nb.z / 2), C.dim), clast);
-        const float xn = lv_ld(F.x, min(off[n], last), F.prec);
+        const float xn = lvx<CG>(F.x, min(off[n], last), F.prec);
         const uint32_t pw = C.word[pi];
-        const float px = lv_ld(C.x, pi, C.prec);
+        const float px = lvx<CG>(C.x, pi, C.prec);
         v[n] = (pw & CW_FLUID) ? q_prec(xn + px, F.prec) : xn;  // the prolonged value as it would be stored
     }
     if (!(w & CW_FLUID) || (w & CW_RED)) return;
@@ -732,17 +755,20 @@ __device__ __forceinline__ void prolong_smooth_fp_cell(const MGLevel& F, const M
 }
 
 __global__ void k_smooth_fp(Dev d, MGState m, int l, uint32_t parity) {
+    pdl_entry();
     const MGLevel L = m.lv[l];
     const uint32_t want = parity == 0u ? CW_RED : 0u;
     for_footprint(d, L, l, [&](uint32_t i, int3) { smooth_fp_cell(L, i, want); });
 }
 // Restriction l -> l + 1 over level l + 1's footprint.
 __global__ void k_restrict_fp(Dev d, MGState m, int l) {
+    pdl_entry();
     const MGLevel F = m.lv[l], C = m.lv[l + 1];
     for_footprint(d, C, l + 1, [&](uint32_t ci, int3 c) { restrict_fp_cell(F, C, ci, c, m.restrict_scale); });
 }
 // Prolongation l + 1 -> l fused with the black sweep of level l.
 __global__ void k_prolong_smooth_fp(Dev d, MGState m, int l) {
+    pdl_entry();
     const MGLevel F = m.lv[l], C = m.lv[l + 1];
     for_footprint(d, F, l, [&](uint32_t i, int3 c) { prolong_smooth_fp_cell(F, C, i, c); });
 }
@@ -752,6 +778,7 @@ __global__ void k_prolong_smooth_fp(Dev d, MGState m, int l) {
 // memory, then sum each of the 64 coarse cells' fluid children in child order (x fastest), as the
 // per-coarse-cell loop does.
 __global__ void __launch_bounds__(GRID_THREADS) k_restrict0(Dev d, MGState m) {
+    pdl_entry();
     constexpr int WARPS = GRID_THREADS / 32;
     __shared__ float s_res[WARPS][BRICK_CELLS];
     __shared__ uint8_t s_fluid[WARPS][BRICK_CELLS];
@@ -1086,6 +1113,7 @@ constexpr size_t st_smem_bytes() {
 // k_smooth0 from a stage: z (face), r and the diagonal (bodies).
 template <bool DOT>
 __global__ void __launch_bounds__(ST_WARPS * 32) k_smooth0_st(Dev d, MGState m) {
+    pdl_entry();
     const float* fa[1] = {m.z};
     const float* ba[2] = {m.r, d.cell_diag};
     st_pass<1, 2, DOT ? 1 : 0>(d, m, 1, fa, ba,
@@ -1117,6 +1145,7 @@ __global__ void __launch_bounds__(ST_WARPS * 32) k_smooth0_st(Dev d, MGState m) 
 }
 // Black sweep from a stage.
 __global__ void __launch_bounds__(ST_WARPS * 32) k_smooth0_black_st(Dev d, MGState m) {
+    pdl_entry();
     const float* fa[1] = {m.z};
     const float* ba[2] = {m.r, d.cell_diag};
     st_black<1, 2>(d, m, fa, ba, [](WarpStage<1, 2>&, uint32_t, uint32_t) {},
@@ -1131,6 +1160,7 @@ __global__ void __launch_bounds__(ST_WARPS * 32) k_smooth0_black_st(Dev d, MGSta
 }
 // k_prolong_smooth0 from a stage (the level-1 6^3 block is staged by plain loads as before).
 __global__ void __launch_bounds__(ST_WARPS * 32) k_prolong_smooth0_st(Dev d, MGState m) {
+    pdl_entry();
     __shared__ float s_cx[ST_WARPS][216];
     const MGLevel C = m.lv[1];
     const float ivs = 1.0f / coarse_scale(m);  // a power of two: exact
@@ -1175,6 +1205,7 @@ __global__ void __launch_bounds__(ST_WARPS * 32) k_prolong_smooth0_st(Dev d, MGS
 }
 // k_restrict0 from a stage: the brick's fine residuals into the warp's s_res, then the 64 coarse cells.
 __global__ void __launch_bounds__(ST_WARPS * 32) k_restrict0_st(Dev d, MGState m) {
+    pdl_entry();
     __shared__ float s_res[ST_WARPS][BRICK_CELLS];
     const MGLevel C = m.lv[1];
     const uint32_t warp = threadIdx.x >> 5;
@@ -1244,6 +1275,7 @@ __global__ void __launch_bounds__(ST_WARPS * 32) k_restrict0_st(Dev d, MGState m
 }
 // k_apply_a from a stage: z and the previous direction (faces), the diagonal (body).
 __global__ void __launch_bounds__(ST_WARPS * 32) k_apply_a_st(Dev d, MGState m) {
+    pdl_entry();
     const uint32_t it = m.ctl[0];
     const bool first = it == 0u;
     const float beta = first ? 0.0f : ratio_f(m.flexible ? m.scalars[0] - m.scalars[9] : m.scalars[0], m.scalars[3]);
@@ -1287,6 +1319,7 @@ __global__ void __launch_bounds__(ST_WARPS * 32) k_apply_a_st(Dev d, MGState m) 
 // V-cycle's z) as bodies.
 template <bool FLEX>
 __global__ void __launch_bounds__(ST_WARPS * 32) k_update_pr_st(Dev d, MGState m, float* __restrict__ p, unsigned long long handle) {
+    pdl_entry();
     constexpr int NB = FLEX ? 6 : 5;
     const float alpha = ratio_f(m.scalars[0], m.scalars[2]);
     const float* dcur = dir_buf_c(m, (m.ctl[0] + 1u) & 1u);
@@ -1338,6 +1371,7 @@ __global__ void __launch_bounds__(ST_WARPS * 32) k_update_pr_st(Dev d, MGState m
 // cells of its colour -- and writes level tail's x back. On entry level `tail` holds b and the
 // red-initialised x from the restriction that produced it.
 __global__ void __launch_bounds__(1024) k_tail_lists(MGState m, int tail) {
+    pdl_entry();
     __shared__ uint32_t s_warp[33];
     uint32_t off = 0;
     for (int l = tail; l < m.num_levels; ++l) {
@@ -1436,8 +1470,10 @@ __device__ __forceinline__ void s_coarse_solve(const SLevel L, int iterations) {
     }
     __syncthreads();
 }
-__global__ void __launch_bounds__(1024) k_vcycle_tail(MGState m, int tail, int iterations) {
-    extern __shared__ __align__(16) unsigned char s_tail[];
+// The tail's V-cycle on one CTA of 1024 threads (s_tail: mg_tail_smem bytes of shared memory). CG: level tail's x
+// and b were written earlier in the same kernel by other CTAs of the cluster, so they are read through L2.
+template <bool CG>
+__device__ __forceinline__ void vcycle_tail_body(const MGState& m, int tail, int iterations, unsigned char* s_tail) {
     const int nl = m.num_levels;
     SLevel S[SLOSH_MAX_MG_LEVELS];
     uint32_t total = 0;
@@ -1478,10 +1514,13 @@ __global__ void __launch_bounds__(1024) k_vcycle_tail(MGState m, int tail, int i
                         const float* src = k < c16 ? m.lv[tail].x : m.lv[tail].b;
                         const uint32_t e = 4u * (k < c16 ? k : k - c16);
                         const uint32_t pr = m.lv[tail].prec;
-                        v[r] = make_uint4(__float_as_uint(lv_ld(src, e, pr)), __float_as_uint(lv_ld(src, e + 1u, pr)),
-                                          __float_as_uint(lv_ld(src, e + 2u, pr)), __float_as_uint(lv_ld(src, e + 3u, pr)));
+                        v[r] = make_uint4(__float_as_uint(lvx<CG>(src, e, pr)), __float_as_uint(lvx<CG>(src, e + 1u, pr)),
+                                          __float_as_uint(lvx<CG>(src, e + 2u, pr)), __float_as_uint(lvx<CG>(src, e + 3u, pr)));
+                    } else if (k < 2u * c16) {
+                        const uint4* g = k < c16 ? gx + k : gb + (k - c16);
+                        v[r] = CG ? __ldcg(g) : *g;
                     } else {
-                        v[r] = k < c16 ? gx[k] : (k < 2u * c16 ? gb[k - c16] : img[k]);
+                        v[r] = img[k];
                     }
                 }
             }
@@ -1562,9 +1601,69 @@ __global__ void __launch_bounds__(1024) k_vcycle_tail(MGState m, int tail, int i
         }
     }
 }
+__global__ void __launch_bounds__(1024) k_vcycle_tail(MGState m, int tail, int iterations) {
+    pdl_entry();
+    extern __shared__ __align__(16) unsigned char s_tail[];
+    vcycle_tail_body<false>(m, tail, iterations, s_tail);
+}
+
+// ---- the middle levels in one thread-block cluster ------------------------------------------------------
+// Levels c0..tail-1 of the V-cycle are small (at 256^3 level 2 has 8 and level 3 one cell per active brick),
+// so as separate grid-wide passes each costs a launch and a chain of dependent loads, not bandwidth. One
+// cluster of MID_CLUSTER CTAs (one per SM) runs them instead, from the restriction c0 - 1 -> c0 to the
+// post-smoothing of level c0, each pass over the level's footprint split across the cluster's threads and
+// followed by a cluster barrier (release / acquire); values written by other CTAs are read through L2. Between
+// the descent and the ascent CTA 0 runs the tail's V-cycle in its shared memory. The passes are the per-cell
+// bodies of k_restrict_fp, k_smooth_fp and k_prolong_smooth_fp, so the results are those of the separate
+// launches. Measured slower on B200 and therefore opt-in (SLOSH_MG_CLUSTER=2 or 3): a 256^3 substep's pressure
+// solve takes 3.66 ms with the cluster from level 2 and 3.07 ms from level 3, against 2.76 ms with the separate
+// launches -- on 16 SMs each pass's chain of dependent L2 loads takes longer than a launch across all 148.
+constexpr int MID_CLUSTER = 16;
+__device__ __forceinline__ void cluster_barrier() {
+    asm volatile("barrier.cluster.arrive.release;\n\tbarrier.cluster.wait.acquire;" ::: "memory");
+}
+__global__ void __launch_bounds__(1024) k_vcycle_mid(Dev d, MGState m, int c0, int tail, int iterations) {
+    pdl_entry();
+    extern __shared__ __align__(16) unsigned char s_tail[];
+    uint32_t rank;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(rank));
+    const uint32_t t0 = rank * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;  // the grid is one cluster
+    const int sweeps = max(m.sweeps, 1);
+    auto sweep = [&](int l, uint32_t parity) {
+        const MGLevel L = m.lv[l];
+        const uint32_t want = parity == 0u ? CW_RED : 0u;
+        for_footprint_span(d, L, l, t0, stride, [&](uint32_t i, int3) { smooth_fp_cell<true>(L, i, want); });
+        cluster_barrier();
+    };
+    for (int l = c0 - 1; l < tail; ++l) {
+        const MGLevel F = m.lv[l], C = m.lv[l + 1];
+        for_footprint_span(d, C, l + 1, t0, stride, [&](uint32_t ci, int3 c) { restrict_fp_cell<true>(F, C, ci, c, m.restrict_scale); });
+        cluster_barrier();
+        if (l + 1 < tail) {
+            sweep(l + 1, 1u);
+            for (int k = 1; k < sweeps; ++k) {
+                sweep(l + 1, 0u);
+                sweep(l + 1, 1u);
+            }
+        }
+    }
+    if (rank == 0u) vcycle_tail_body<true>(m, tail, iterations, s_tail);
+    cluster_barrier();
+    for (int l = tail - 1; l >= c0; --l) {
+        const MGLevel F = m.lv[l], C = m.lv[l + 1];
+        for_footprint_span(d, F, l, t0, stride, [&](uint32_t i, int3 c) { prolong_smooth_fp_cell<true>(F, C, i, c); });
+        cluster_barrier();
+        for (int k = 1; k < sweeps; ++k) {
+            sweep(l, 0u);
+            sweep(l, 1u);
+        }
+        sweep(l, 0u);
+    }
+}
 
 // ---- the coarse solve directly on level 0 (grids of <= 512 cells have a single level) --------------------
 __global__ void __launch_bounds__(1024) k_coarse_solve0(Dev d, MGState m, int iterations) {
+    pdl_entry();
     const MGLevel L = m.lv[0];
     for (int it = 0; it < iterations; ++it) {
         for (uint32_t colour = 0; colour < 2u; ++colour) {
@@ -1588,6 +1687,7 @@ __global__ void __launch_bounds__(1024) k_coarse_solve0(Dev d, MGState m, int it
 // neighbour's new direction z_n + beta d_n itself (bit-identical to what that neighbour writes).
 
 __global__ void __launch_bounds__(GRID_THREADS, 3) k_apply_a(Dev d, MGState m) {
+    pdl_entry();
     const uint32_t it = m.ctl[0];
     const bool first = it == 0u;
     // flexible PCG: beta = (rho_k - r_k.z_{k-1}) / rho_{k-1}, the numerator formed in FP64
@@ -1640,6 +1740,7 @@ __global__ void __launch_bounds__(GRID_THREADS, 3) k_apply_a(Dev d, MGState m) {
 // FLEX (flexible PCG) also reduces r_{k+1}.z_k with the z of the finished V-cycle, before it is overwritten.
 template <bool FLEX>
 __global__ void __launch_bounds__(GRID_THREADS, 3) k_update_pr(Dev d, MGState m, float* __restrict__ p, unsigned long long handle) {
+    pdl_entry();
     const float alpha = ratio_f(m.scalars[0], m.scalars[2]);
     const float* dcur = dir_buf(m, (m.ctl[0] + 1u) & 1u);
     struct V {
@@ -1696,6 +1797,7 @@ __global__ void __launch_bounds__(GRID_THREADS, 3) k_update_pr(Dev d, MGState m,
 // ---- ||b - A p||^2 (FP64 evaluation) and ||b||^2 of a finished solve (diagnostic) -------------------------
 __global__ void __launch_bounds__(GRID_THREADS) k_true_residual(Dev d, MGState m, const float* __restrict__ p,
                                                                 const float* __restrict__ div) {
+    pdl_entry();
     struct V {
         Q6 p;
         float4 dv, dg;
@@ -1773,10 +1875,55 @@ inline int st_grid_cap(const Dev& d) { return std::max(1, int((d.num_pool_bricks
 
 }  // namespace
 
+// Programmatic dependent launch of the solve's kernels (launch_k): on unless SLOSH_PDL=0.
+bool pdl_enabled() {
+    static const int v = [] {
+        const char* e = std::getenv("SLOSH_PDL");
+        return (e && e[0] == '0') ? 0 : 1;
+    }();
+    return v != 0;
+}
+
 int mg_tail_level(const MGState& m) {
     int t = m.num_levels - 1;
     while (t - 1 >= 1 && m.lv[t - 1].cells <= 4096u) --t;
     return t;
+}
+
+// First level of the cluster segment (k_vcycle_mid) for this hierarchy, 0 when the separate passes run (the
+// default): SLOSH_MG_CLUSTER=2 or =3 starts it at that level, when the tail is at or below it and the GPU can
+// place a cluster of MID_CLUSTER CTAs with the tail's shared memory.
+int mid_level(const MGState& m, int tail) {
+    static const int from = [] {
+        const char* e = std::getenv("SLOSH_MG_CLUSTER");
+        return e ? std::atoi(e) : 0;
+    }();
+    if (from < 2 || tail < from) return 0;
+    static int ok = -1;
+    static size_t checked_smem = 0;
+    const size_t smem = mg_tail_smem(m);
+    if (ok < 0 || smem > checked_smem) {
+        ok = 0;
+        if (cudaFuncSetAttribute(k_vcycle_mid, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess &&
+            cudaFuncSetAttribute(k_vcycle_mid, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) == cudaSuccess) {
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(MID_CLUSTER);
+            cfg.blockDim = dim3(1024);
+            cfg.dynamicSmemBytes = smem;
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeClusterDimension;
+            attr[0].val.clusterDim.x = MID_CLUSTER;
+            attr[0].val.clusterDim.y = 1;
+            attr[0].val.clusterDim.z = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            int clusters = 0;
+            if (cudaOccupancyMaxActiveClusters(&clusters, k_vcycle_mid, &cfg) == cudaSuccess && clusters > 0) ok = 1;
+        }
+        cudaGetLastError();
+        checked_smem = smem;
+    }
+    return ok ? from : 0;
 }
 
 int launch_mg_setup(const MGState& m, uint32_t limit, bool tol_mode, double tol, cudaStream_t s) {
@@ -1786,18 +1933,19 @@ int launch_mg_setup(const MGState& m, uint32_t limit, bool tol_mode, double tol,
         cudaFuncSetAttribute(k_vcycle_tail, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         configured = smem;
     }
-    k_solve_setup<<<1, 1, 0, s>>>(m, limit, tol_mode ? 1u : 0u, tol);
+    mid_level(m, mg_tail_level(m));
+    launch_k(k_solve_setup, 1, 1, 0, s, m, limit, tol_mode ? 1u : 0u, tol);
     return 1;
 }
 int launch_mg_build_type(const Dev& d, const MGState& m, int l, cudaStream_t s) {
     const MGLevel& C = m.lv[l + 1];
-    k_build_type<<<blocks_for(C.cells, 256), 256, 0, s>>>(d, m.lv[l], C, l == 0 ? 1 : 0);
+    launch_k(k_build_type, blocks_for(C.cells, 256), 256, 0, s, d, m.lv[l], C, l == 0 ? 1 : 0);
     return 1;
 }
 int launch_pcg_init(const Dev& d, const MGState& m, const float* p, const float* div, unsigned long long handle, const Shape& sh,
                     cudaStream_t s) {
-    k_pcg_words<<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m);
-    k_pcg_init<<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m, p, div, handle);
+    launch_k(k_pcg_words, sh.mg_ctas, GRID_THREADS, 0, s, d, m);
+    launch_k(k_pcg_init, sh.mg_ctas, GRID_THREADS, 0, s, d, m, p, div, handle);
     return 2;
 }
 
@@ -1807,12 +1955,12 @@ size_t mg_tail_smem(const MGState& m) {
     return total;
 }
 int launch_mg_words(const MGState& m, int l, cudaStream_t s) {
-    k_level_words<<<blocks_for(m.lv[l].cells, 256), 256, 0, s>>>(m.lv[l]);
+    launch_k(k_level_words, blocks_for(m.lv[l].cells, 256), 256, 0, s, m.lv[l]);
     return 1;
 }
 int launch_mg_tail_lists(const MGState& m, cudaStream_t s) {
     if (m.num_levels < 2) return 0;
-    k_tail_lists<<<1, 1024, 0, s>>>(m, mg_tail_level(m));
+    launch_k(k_tail_lists, 1, 1024, 0, s, m, mg_tail_level(m));
     return 1;
 }
 
@@ -1825,16 +1973,16 @@ int launch_vcycle(const Dev& d, const MGState& m, int coarse_iterations, const S
             if (dot) ST_LAUNCH(k_smooth0_st<true>, 1, 2, d, m, sh, s);
             else ST_LAUNCH(k_smooth0_st<false>, 1, 2, d, m, sh, s);
         } else {
-            if (dot) k_smooth0<true><<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m);
-            else k_smooth0<false><<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m);
+            if (dot) launch_k(k_smooth0<true>, sh.mg_ctas, GRID_THREADS, 0, s, d, m);
+            else launch_k(k_smooth0<false>, sh.mg_ctas, GRID_THREADS, 0, s, d, m);
         }
     };
     auto smooth0_black = [&]() {
         if (staged) ST_LAUNCH(k_smooth0_black_st, 1, 2, d, m, sh, s);
-        else k_smooth0_black<<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m);
+        else launch_k(k_smooth0_black, sh.mg_ctas, GRID_THREADS, 0, s, d, m);
     };
     if (nl == 1) {
-        k_coarse_solve0<<<1, 1024, 0, s>>>(d, m, coarse_iterations);
+        launch_k(k_coarse_solve0, 1, 1024, 0, s, d, m, coarse_iterations);
         smooth0_red(true);
         return 2;
     }
@@ -1857,30 +2005,48 @@ int launch_vcycle(const Dev& d, const MGState& m, int coarse_iterations, const S
         smooth0_black();
         n += 2;
     }
-    for (int l = 0; l < tail; ++l) {
+    const int mid = mid_level(m, tail);  // levels mid..tail-1 and the tail in one cluster (0: separate passes)
+    const int down_end = mid > 0 ? mid - 1 : tail;
+    for (int l = 0; l < down_end; ++l) {
         if (l == 0) {
             if (staged) ST_LAUNCH(k_restrict0_st, 1, 2, d, m, sh, s);
-            else k_restrict0<<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m);
+            else launch_k(k_restrict0, sh.mg_ctas, GRID_THREADS, 0, s, d, m);
         } else {
-            k_restrict_fp<<<fp_blocks(l + 1), 256, 0, s>>>(d, m, l);
+            launch_k(k_restrict_fp, fp_blocks(l + 1), 256, 0, s, d, m, l);
         }
         ++n;
         if (l + 1 < tail) {  // the tail kernel does its own pre-smoothing
-            k_smooth_fp<<<fp_blocks(l + 1), 256, 0, s>>>(d, m, l + 1, 1u);
+            launch_k(k_smooth_fp, fp_blocks(l + 1), 256, 0, s, d, m, l + 1, 1u);
             ++n;
             for (int k = 1; k < sweeps; ++k) {
-                k_smooth_fp<<<fp_blocks(l + 1), 256, 0, s>>>(d, m, l + 1, 0u);
-                k_smooth_fp<<<fp_blocks(l + 1), 256, 0, s>>>(d, m, l + 1, 1u);
+                launch_k(k_smooth_fp, fp_blocks(l + 1), 256, 0, s, d, m, l + 1, 0u);
+                launch_k(k_smooth_fp, fp_blocks(l + 1), 256, 0, s, d, m, l + 1, 1u);
                 n += 2;
             }
         }
     }
-    k_vcycle_tail<<<1, 1024, mg_tail_smem(m), s>>>(m, tail, coarse_iterations);
+    if (mid > 0) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(MID_CLUSTER);
+        cfg.blockDim = dim3(1024);
+        cfg.dynamicSmemBytes = mg_tail_smem(m);
+        cfg.stream = s;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = MID_CLUSTER;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        cudaLaunchKernelEx(&cfg, k_vcycle_mid, d, m, mid, tail, coarse_iterations);
+    } else {
+        launch_k(k_vcycle_tail, 1, 1024, mg_tail_smem(m), s, m, tail, coarse_iterations);
+    }
     ++n;
-    for (int l = tail - 1; l >= 0; --l) {
+    for (int l = (mid > 0 ? mid - 1 : tail - 1); l >= 0; --l) {
         if (l == 0) {
             if (staged) ST_LAUNCH(k_prolong_smooth0_st, 1, 2, d, m, sh, s);
-            else k_prolong_smooth0<<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m);
+            else launch_k(k_prolong_smooth0, sh.mg_ctas, GRID_THREADS, 0, s, d, m);
             for (int k = 1; k < sweeps; ++k) {
                 smooth0_red(false);
                 smooth0_black();
@@ -1888,13 +2054,13 @@ int launch_vcycle(const Dev& d, const MGState& m, int coarse_iterations, const S
             }
             smooth0_red(true);
         } else {
-            k_prolong_smooth_fp<<<fp_blocks(l), 256, 0, s>>>(d, m, l);
+            launch_k(k_prolong_smooth_fp, fp_blocks(l), 256, 0, s, d, m, l);
             for (int k = 1; k < sweeps; ++k) {
-                k_smooth_fp<<<fp_blocks(l), 256, 0, s>>>(d, m, l, 0u);
-                k_smooth_fp<<<fp_blocks(l), 256, 0, s>>>(d, m, l, 1u);
+                launch_k(k_smooth_fp, fp_blocks(l), 256, 0, s, d, m, l, 0u);
+                launch_k(k_smooth_fp, fp_blocks(l), 256, 0, s, d, m, l, 1u);
                 n += 2;
             }
-            k_smooth_fp<<<fp_blocks(l), 256, 0, s>>>(d, m, l, 0u);
+            launch_k(k_smooth_fp, fp_blocks(l), 256, 0, s, d, m, l, 0u);
         }
         n += 2;
     }
@@ -1902,7 +2068,7 @@ int launch_vcycle(const Dev& d, const MGState& m, int coarse_iterations, const S
 }
 int launch_pcg_apply_a(const Dev& d, const MGState& m, const Shape& sh, cudaStream_t s) {
     if (mg_staged()) ST_LAUNCH(k_apply_a_st, 2, 1, d, m, sh, s);
-    else k_apply_a<<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m);
+    else launch_k(k_apply_a, sh.mg_ctas, GRID_THREADS, 0, s, d, m);
     return 1;
 }
 int launch_pcg_update_pr(const Dev& d, const MGState& m, float* p, unsigned long long handle, const Shape& sh, cudaStream_t s) {
@@ -1910,15 +2076,15 @@ int launch_pcg_update_pr(const Dev& d, const MGState& m, float* p, unsigned long
         if (m.flexible) ST_LAUNCH_ARGS(k_update_pr_st<true>, 0, 6, d, sh, s, d, m, p, handle);
         else ST_LAUNCH_ARGS(k_update_pr_st<false>, 0, 5, d, sh, s, d, m, p, handle);
     } else if (m.flexible) {
-        k_update_pr<true><<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m, p, handle);
+        launch_k(k_update_pr<true>, sh.mg_ctas, GRID_THREADS, 0, s, d, m, p, handle);
     } else {
-        k_update_pr<false><<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m, p, handle);
+        launch_k(k_update_pr<false>, sh.mg_ctas, GRID_THREADS, 0, s, d, m, p, handle);
     }
     return 1;
 }
 int launch_pcg_update_d(const Dev&, const MGState&, const Shape&, cudaStream_t) { return 0; }  // fused into ApplyA
 int launch_true_residual(const Dev& d, const MGState& m, const float* p, const float* div, const Shape& sh, cudaStream_t s) {
-    k_true_residual<<<sh.mg_ctas, GRID_THREADS, 0, s>>>(d, m, p, div);
+    launch_k(k_true_residual, sh.mg_ctas, GRID_THREADS, 0, s, d, m, p, div);
     return 1;
 }
 

@@ -220,10 +220,14 @@ def test_preconditioner_options(slosh, oracle_mod, scale, sweeps, flexible, mode
     assert g.results().last_solve_rel_residual <= 1e-6
 
 
-def test_staged_level0_passes_give_identical_results(slosh):
-    """The level-0 MGPCG passes can read their bricks from shared-memory stages filled by bulk async copies
-    (SLOSH_MG_STAGED=1, read once per process) instead of straight from global memory: a 96^3 scene stepped in a
-    child process with the staged passes must end bit-identical to the default passes here."""
+@pytest.mark.parametrize("env", [{"SLOSH_MG_STAGED": "1"}, {"SLOSH_MG_CLUSTER": "2"}, {"SLOSH_PDL": "0"}],
+                         ids=["staged_level0", "cluster_levels", "no_pdl"])
+def test_alternative_solver_paths_give_identical_results(slosh, env):
+    """The MGPCG solve has measured alternatives, each read once per process from the environment: level-0 passes
+    that read their bricks from shared-memory stages filled by bulk async copies (SLOSH_MG_STAGED=1), levels 2 to
+    the tail in one thread-block cluster (SLOSH_MG_CLUSTER=2) and plain stream order instead of programmatic
+    dependent launch (SLOSH_PDL=0). A 96^3 scene (levels 2 and 3 below the tail) stepped in a child process with
+    the alternative must end bit-identical to the default path here."""
     import subprocess
     import sys
     code = (
@@ -240,11 +244,11 @@ def test_staged_level0_passes_give_identical_results(slosh):
     ) % (os.path.dirname(os.path.dirname(os.path.abspath(__file__))),)
     import tempfile
     with tempfile.TemporaryDirectory() as tmp:
-        out = os.path.join(tmp, "staged.npy")
-        env = dict(os.environ, SLOSH_MG_STAGED="1")
-        r = subprocess.run([sys.executable, "-c", code, out], env=env, capture_output=True, text=True, timeout=600)
+        out = os.path.join(tmp, "alt.npy")
+        r = subprocess.run([sys.executable, "-c", code, out], env=dict(os.environ, **env), capture_output=True, text=True,
+                           timeout=600)
         assert r.returncode == 0, r.stderr[-2000:]
-        staged = np.load(out)
+        alt = np.load(out)
     sc = scenes.dam_break_sphere(slosh.settings_default, n=96)
     s = sc["settings"]
     s.max_substeps = 16
@@ -257,4 +261,4 @@ def test_staged_level0_passes_give_identical_results(slosh):
         sim.step_frame(A.frame_input(s))
     plain = np.concatenate([sim.particles().view(np.uint32).ravel(), sim.read("PRESSURE").view(np.uint32)])
     sim.close()
-    assert np.array_equal(staged, plain)
+    assert np.array_equal(alt, plain)
