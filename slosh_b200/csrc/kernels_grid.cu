@@ -285,6 +285,8 @@ __global__ void k_clear_new_slots(Dev d) {  // ClearNewSlotsCS
 __global__ void __launch_bounds__(GRID_THREADS) k_mark_cells(Dev d, Pass p) {
     uint32_t fluid = 0;
     for_active_cells<false>(d, [&](uint32_t index, int3 c) {
+        const int count = d.cell_count[index];  // loaded before the collider tests, like the pressure
+        const float pressure = d.pressure[index];
         uint32_t packed = CELL_AIR;
         if (c.x == 0 || c.y == 0 || c.z == 0 || c.x == d.grid.x - 1 || c.y == d.grid.y - 1 || c.z == d.grid.z - 1) {
             packed = CELL_SOLID;
@@ -297,13 +299,12 @@ __global__ void __launch_bounds__(GRID_THREADS) k_mark_cells(Dev d, Pass p) {
             }
         }
         if (type_of(packed) != CELL_SOLID) {
-            const int count = d.cell_count[index];
             packed = count > 0 ? CELL_FLUID : CELL_AIR;
             if (float(count) >= 0.5f * p.target_ppc) packed |= CELL_DENSE_FLAG;
         }
         d.cell_type[index] = packed;
         if (type_of(packed) == CELL_FLUID) {
-            d.pressure[index] = d.pressure[index] * p.warm_start_scale;
+            d.pressure[index] = pressure * p.warm_start_scale;
             ++fluid;
         } else {
             d.pressure[index] = 0.0f;
@@ -317,17 +318,27 @@ __global__ void __launch_bounds__(GRID_THREADS) k_mark_cells(Dev d, Pass p) {
 __global__ void __launch_bounds__(GRID_THREADS) k_normalize(Dev d, Pass p, float* __restrict__ vel) {
     const uint32_t tf = d.total_faces;
     for_active_cells<true>(d, [&](uint32_t index, int3 c) {
+        // the cell's and the three lower neighbours' types and the three faces' sums, before any store
         const uint32_t b = d.cell_type[index];
+        int moms[3], wts[3];
+        uint32_t tas[3];
 #pragma unroll
         for (int axis = 0; axis < 3; ++axis) {
             const uint32_t f = uint32_t(axis) * d.pool_cells + index;
-            const int mom = d.accum[f], wt = d.accum[tf + f];
+            moms[axis] = d.accum[f];
+            wts[axis] = d.accum[tf + f];
+            tas[axis] = d.cell_type[nidx(d, index, c, 2 * axis)];
+        }
+#pragma unroll
+        for (int axis = 0; axis < 3; ++axis) {
+            const uint32_t f = uint32_t(axis) * d.pool_cells + index;
+            const int mom = moms[axis], wt = wts[axis];
             if (mom != 0 || wt != 0) { d.accum[f] = 0; d.accum[tf + f] = 0; }
             float u = wt > 0 ? float(mom) / float(wt) : 0.0f;
             d.face_weight[f] = float(wt) * P2G_FIXED_INV;
             uint32_t flags = wt > 0 ? FACE_HAS_WEIGHT : 0u;
             if (p.use_apic == 0u) d.vel_old[f] = u;
-            const uint32_t a = ntype(d, index, c, 2 * axis);
+            const uint32_t a = in_grid(d, add3(c, nbr_off(2 * axis))) ? tas[axis] : CELL_SOLID;
             if (type_of(a) == CELL_SOLID || type_of(b) == CELL_SOLID) {
                 const uint32_t solid = type_of(b) == CELL_SOLID ? b : a;
                 const uint32_t id = collider_of(solid);
@@ -382,23 +393,36 @@ __global__ void __launch_bounds__(GRID_THREADS) k_viscosity(Dev d, Pass p, const
 // ---- DivergenceCS --------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(GRID_THREADS) k_divergence(Dev d, Pass p, const float* __restrict__ vel) {
     for_active_cells<true>(d, [&](uint32_t index, int3 c) {
+        // one round of loads: the cell's type, its six faces' velocities and weights and its neighbours' types
+        // (a neighbour outside the grid reads the null brick and counts as solid); only cells beside air load
+        // more (the air cells' densities)
+        const uint32_t type = d.cell_type[index];
+        uint32_t nbr[6], nts[6];
+        float vlo[3], vhi[3], wlo[3], whi[3];
+#pragma unroll
+        for (int n = 0; n < 6; ++n) {
+            nbr[n] = nidx(d, index, c, n);
+            nts[n] = d.cell_type[nbr[n]];
+        }
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            vlo[a] = vel[uint32_t(a) * d.pool_cells + index];
+            vhi[a] = vel[uint32_t(a) * d.pool_cells + nbr[2 * a + 1]];
+            wlo[a] = d.face_weight[uint32_t(a) * d.pool_cells + index];
+            whi[a] = d.face_weight[uint32_t(a) * d.pool_cells + nbr[2 * a + 1]];
+        }
         d.cell_count[index] = 0;
-        if (type_of(d.cell_type[index]) != CELL_FLUID) {
+        if (type_of(type) != CELL_FLUID) {
             d.divergence[index] = 0.0f;
             d.cell_diag[index] = 0.0f;
             return;
         }
         float div = 0.0f;
         float ws = 0.0f;
-        uint32_t plus[3];
 #pragma unroll
-        for (int a = 0; a < 3; ++a) plus[a] = nidx(d, index, c, 2 * a + 1);
+        for (int a = 0; a < 3; ++a) div = div + (vhi[a] - vlo[a]);
 #pragma unroll
-        for (int a = 0; a < 3; ++a)
-            div = div + (vel[uint32_t(a) * d.pool_cells + plus[a]] - vel[uint32_t(a) * d.pool_cells + index]);
-#pragma unroll
-        for (int a = 0; a < 3; ++a)
-            ws = ws + (d.face_weight[uint32_t(a) * d.pool_cells + index] + d.face_weight[uint32_t(a) * d.pool_cells + plus[a]]);
+        for (int a = 0; a < 3; ++a) ws = ws + (wlo[a] + whi[a]);
         const float rho = ws / (6.0f * p.target_ppc);
         const float excess = fmaxf(rho - (1.0f + p.density_deadband), 0.0f);
         const float target = fminf(p.density_correction * excess, 0.5f) * d.h / p.dt;
@@ -406,8 +430,9 @@ __global__ void __launch_bounds__(GRID_THREADS) k_divergence(Dev d, Pass p, cons
         float diag = 0.0f;
 #pragma unroll
         for (int n = 0; n < 6; ++n) {
-            const uint32_t nt = type_of(ntype(d, index, c, n));
-            diag = diag + (nt == CELL_FLUID ? 1.0f : (nt == CELL_AIR ? air_face_weight(d, p, rho, add3(c, nbr_off(n))) : 0.0f));
+            const int3 nc = add3(c, nbr_off(n));
+            const uint32_t nt = in_grid(d, nc) ? type_of(nts[n]) : CELL_SOLID;
+            diag = diag + (nt == CELL_FLUID ? 1.0f : (nt == CELL_AIR ? air_face_weight(d, p, rho, nc) : 0.0f));
         }
         d.cell_diag[index] = diag;
     });
@@ -437,31 +462,47 @@ __global__ void __launch_bounds__(GRID_THREADS) k_rbgs(Dev d, float* __restrict_
 }
 
 // ---- ProjectFace (its two-way coupling terms are accumulated by k_coupling_faces after the pass) ---------
+// Every value a face may need (the neighbour's type and pressure, the cell's pressure, the face's velocity
+// and flags) is loaded before the types are tested, so a cell costs one round of loads; a neighbour outside
+// the grid reads the null brick and counts as solid. Only faces between fluid and air load more (the
+// densities of the ghost-fluid weight).
 __global__ void __launch_bounds__(GRID_THREADS) k_project(Dev d, Pass p, float* __restrict__ vel) {
     for_active_cells<true>(d, [&](uint32_t index, int3 c) {
         const uint32_t b = d.cell_type[index];
+        const float pc = d.pressure[index];
+        uint32_t ta[3], fl[3];
+        float pn[3], vf[3];
 #pragma unroll
         for (int axis = 0; axis < 3; ++axis) {
             const uint32_t f = uint32_t(axis) * d.pool_cells + index;
-            const uint32_t a = ntype(d, index, c, 2 * axis);
-            uint32_t flags = d.face_flags[f] & FACE_HAS_WEIGHT;
+            const uint32_t ni = nidx(d, index, c, 2 * axis);
+            ta[axis] = d.cell_type[ni];
+            pn[axis] = d.pressure[ni];
+            fl[axis] = d.face_flags[f];
+            vf[axis] = vel[f];
+        }
+#pragma unroll
+        for (int axis = 0; axis < 3; ++axis) {
+            const uint32_t f = uint32_t(axis) * d.pool_cells + index;
+            const int3 ca = add3(c, nbr_off(2 * axis));
+            const uint32_t a = in_grid(d, ca) ? ta[axis] : CELL_SOLID;
+            uint32_t flags = fl[axis] & FACE_HAS_WEIGHT;
             if (type_of(a) == CELL_SOLID && type_of(b) == CELL_SOLID) {
             } else if (type_of(a) == CELL_SOLID || type_of(b) == CELL_SOLID) {
                 flags |= FACE_VALID | FACE_SOLID;
             } else if (type_of(a) == CELL_FLUID || type_of(b) == CELL_FLUID) {
-                const int3 ca = add3(c, nbr_off(2 * axis));
                 float pa, pb;
                 if (type_of(a) == CELL_FLUID && type_of(b) == CELL_FLUID) {
-                    pa = d.pressure[nbr_index_cta(index, c, 2 * axis)];
-                    pb = d.pressure[index];
+                    pa = pn[axis];
+                    pb = pc;
                 } else if (type_of(a) == CELL_FLUID) {
-                    pa = d.pressure[nbr_index_cta(index, c, 2 * axis)];
+                    pa = pn[axis];
                     pb = pa - pa * air_face_weight(d, p, cell_density(d, p, ca), c);
                 } else {
-                    pb = d.pressure[index];
+                    pb = pc;
                     pa = pb - pb * air_face_weight(d, p, cell_density(d, p, c), ca);
                 }
-                vel[f] = vel[f] - (pb - pa);
+                vel[f] = vf[axis] - (pb - pa);
                 flags |= FACE_VALID;
             }
             d.face_flags[f] = flags;
@@ -740,11 +781,19 @@ __global__ void __launch_bounds__(GRID_THREADS) k_extrapolate(Dev d, const float
     for (uint32_t it = 0; it < iteration; ++it) known |= 1u << (FACE_EXTRAP_SHIFT + it);
     const uint32_t new_bit = 1u << (FACE_EXTRAP_SHIFT + iteration);
     for_active_cells<true>(d, [&](uint32_t index, int3 c) {
+        // the three faces' flags and values first (one round), the neighbours only for faces still unknown
+        uint32_t fls[3];
+        float cen[3];
+#pragma unroll
+        for (int axis = 0; axis < 3; ++axis) {
+            fls[axis] = d.face_flags[uint32_t(axis) * d.pool_cells + index];
+            cen[axis] = src[uint32_t(axis) * d.pool_cells + index];
+        }
 #pragma unroll
         for (int axis = 0; axis < 3; ++axis) {
             const uint32_t f = uint32_t(axis) * d.pool_cells + index;
-            const uint32_t flags = d.face_flags[f];
-            const float center = src[f];
+            const uint32_t flags = fls[axis];
+            const float center = cen[axis];
             if ((flags & known) != 0u) { dst[f] = center; continue; }
             // all six neighbours' flags and values are loaded before any is tested (an out-of-grid
             // neighbour reads the null slot and is then skipped)
