@@ -159,56 +159,133 @@ __device__ uint32_t block_scan_1024(uint32_t v, uint32_t* s_warp, uint32_t* tota
 // timing. Here the same stack discipline runs in ascending brick order through block scans: freed
 // slots are pushed in brick order, the j-th brick needing storage pops entry (free count - j), and
 // the active and new-slot lists come out in brick order. This is the serial (canonical) result.
-// Shared-memory budget of the separable dilation: two byte planes of num_bricks.
+// Shared-memory budget of pool_update_smem: two byte planes and a bit plane of num_bricks.
 constexpr uint32_t POOL_SMEM_BRICKS = 100000u;
+
+// The pool update with its flags in shared memory (num_bricks <= POOL_SMEM_BRICKS): the wanted flags from the
+// separable dilation (one byte per brick) and whether each brick holds a slot (one bit per brick, from one
+// coalesced pass over the brick table), so the three ordered scans below read shared memory only and go to global
+// memory just for the bricks that change (freed slots, popped slots). Each thread owns the same contiguous run of
+// bricks in every phase, so the order is that of the reference-order loop over bricks.
+__device__ __forceinline__ void pool_update_smem(const Dev& d, uint8_t* s_flags, uint32_t* s_warp, uint32_t b0, uint32_t b1, int f0) {
+    const uint32_t nb = d.num_bricks;
+    const int bx = d.brick_dim.x, by = d.brick_dim.y, bz = d.brick_dim.z;
+    uint8_t* a = s_flags;
+    uint8_t* t = s_flags + nb;
+    uint32_t* has = reinterpret_cast<uint32_t*>(s_flags + ((2u * nb + 3u) & ~3u));
+    const uint32_t nwords = (nb + 31u) / 32u;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    // Phase 1: wanted = touched within one brick (3x3x3 dilation); which bricks hold a slot.
+    for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) a[b] = d.brick_touch[b] != 0u ? 1 : 0;
+    for (uint32_t w = warp; w < nwords; w += blockDim.x / 32u) {
+        const uint32_t b = w * 32u + lane;
+        const uint32_t bits = __ballot_sync(0xFFFFFFFFu, b < nb && d.brick_table_w[b] != 0u);
+        if (lane == 0u) has[w] = bits;
+    }
+    __syncthreads();
+    for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) {  // x
+        const int x = int(b % uint32_t(bx));
+        t[b] = a[b] | (x > 0 ? a[b - 1] : 0) | (x + 1 < bx ? a[b + 1] : 0);
+    }
+    __syncthreads();
+    for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) {  // y
+        const int y = int((b / uint32_t(bx)) % uint32_t(by));
+        a[b] = t[b] | (y > 0 ? t[b - bx] : 0) | (y + 1 < by ? t[b + bx] : 0);
+    }
+    __syncthreads();
+    const uint32_t plane = uint32_t(bx * by);
+    for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) {  // z
+        const int z = int(b / plane);
+        const uint8_t w = a[b] | (z > 0 ? a[b - plane] : 0) | (z + 1 < bz ? a[b + plane] : 0);
+        t[b] = w;
+        d.brick_want[b] = w;
+    }
+    __syncthreads();
+    auto want = [&](uint32_t b) -> bool { return t[b] != 0; };
+    auto holds = [&](uint32_t b) -> bool { return ((has[b >> 5] >> (b & 31u)) & 1u) != 0u; };
+    // unwanted bricks free their slot, pushed in brick order
+    uint32_t nfree = 0;
+    for (uint32_t b = b0; b < b1; ++b)
+        if (!want(b) && holds(b)) ++nfree;
+    uint32_t total_free;
+    uint32_t k = block_scan_1024(nfree, s_warp, &total_free);
+    for (uint32_t b = b0; b < b1; ++b) {
+        if (!want(b) && holds(b)) {
+            const uint32_t slot = d.brick_table_w[b];
+            d.free_slots[1u + uint32_t(f0) + k] = slot;
+            ++k;
+            d.slot_brick[slot] = NO_BRICK;
+            d.brick_table_w[b] = 0u;
+            atomicAnd(has + (b >> 5), ~(1u << (b & 31u)));
+        }
+    }
+    const int f = f0 + int(total_free);
+    __syncthreads();
+    // Phase 2: wanted bricks without storage pop slots in brick order.
+    uint32_t nneed = 0;
+    for (uint32_t b = b0; b < b1; ++b)
+        if (want(b) && !holds(b)) ++nneed;
+    uint32_t total_need;
+    uint32_t j = block_scan_1024(nneed, s_warp, &total_need);
+    for (uint32_t b = b0; b < b1; ++b) {
+        if (want(b) && !holds(b)) {
+            const int count = f - int(j);
+            if (count > 0) {
+                const uint32_t slot = d.free_slots[count];
+                d.brick_table_w[b] = slot;
+                d.slot_brick[slot] = b;
+                d.new_slots[1u + j] = slot;
+                atomicOr(has + (b >> 5), 1u << (b & 31u));
+            }
+            ++j;
+        }
+    }
+    __syncthreads();
+    // Phase 3: active list in brick order; touch flags consumed.
+    uint32_t nact = 0;
+    for (uint32_t b = b0; b < b1; ++b)
+        if (want(b) && holds(b)) ++nact;
+    uint32_t total_act;
+    uint32_t act = block_scan_1024(nact, s_warp, &total_act);
+    for (uint32_t b = b0; b < b1; ++b)
+        if (want(b) && holds(b)) d.active_bricks[1u + act++] = b;
+    for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) d.brick_touch[b] = 0u;
+    if (threadIdx.x == 0) {
+        const uint32_t ok = uint32_t(min(int(total_need), max(f, 0)));
+        d.new_slots[0] = ok;
+        d.free_slots[0] = uint32_t(max(f - int(total_need), 0));
+        d.active_bricks[0] = total_act;
+        d.stats[8] += total_need - ok;
+        d.stats[7] = max(d.stats[7], total_act);
+    }
+}
 
 __global__ void __launch_bounds__(1024) k_pool_update(Dev d) {
     __shared__ uint32_t s_warp[33];
-    extern __shared__ uint8_t s_flags[];  // [0, nb): touch / z pass, [nb, 2 nb): scratch
+    extern __shared__ uint8_t s_flags[];  // pool_update_smem's flags (num_bricks <= POOL_SMEM_BRICKS), else unused
     const uint32_t nb = d.num_bricks;
     const uint32_t per = (nb + blockDim.x - 1u) / blockDim.x;
     const uint32_t b0 = min(threadIdx.x * per, nb);
     const uint32_t b1 = min(b0 + per, nb);
     const int f0 = int(d.free_slots[0]);
+    if (nb <= POOL_SMEM_BRICKS) {  // uniform
+        pool_update_smem(d, s_flags, s_warp, b0, b1, f0);
+        return;
+    }
     const int bx = d.brick_dim.x, by = d.brick_dim.y, bz = d.brick_dim.z;
 
     // Phase 1: wanted = touched within one brick (3x3x3 dilation); unwanted bricks free their slot.
-    if (nb <= POOL_SMEM_BRICKS) {
-        uint8_t* a = s_flags;
-        uint8_t* t = s_flags + nb;
-        for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) a[b] = d.brick_touch[b] != 0u ? 1 : 0;
-        __syncthreads();
-        for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) {  // x
-            const int x = int(b % uint32_t(bx));
-            t[b] = a[b] | (x > 0 ? a[b - 1] : 0) | (x + 1 < bx ? a[b + 1] : 0);
-        }
-        __syncthreads();
-        for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) {  // y
-            const int y = int((b / uint32_t(bx)) % uint32_t(by));
-            a[b] = t[b] | (y > 0 ? t[b - bx] : 0) | (y + 1 < by ? t[b + bx] : 0);
-        }
-        __syncthreads();
-        const uint32_t plane = uint32_t(bx * by);
-        for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) {  // z
-            const int z = int(b / plane);
-            const uint8_t w = a[b] | (z > 0 ? a[b - plane] : 0) | (z + 1 < bz ? a[b + plane] : 0);
-            t[b] = w;
-            d.brick_want[b] = w;
-        }
-        __syncthreads();
-    } else {
-        for (uint32_t b = b0; b < b1; ++b) {
-            const int3 c = brick_coord_of(d, b);
-            bool wanted = false;
-            for (int z = max(c.z - 1, 0); z <= min(c.z + 1, bz - 1) && !wanted; ++z)
-                for (int y = max(c.y - 1, 0); y <= min(c.y + 1, by - 1) && !wanted; ++y)
-                    for (int x = max(c.x - 1, 0); x <= min(c.x + 1, bx - 1); ++x)
-                        if (d.brick_touch[uint32_t(x + bx * (y + by * z))] != 0u) { wanted = true; break; }
-            d.brick_want[b] = wanted ? 1u : 0u;
-        }
-        __syncthreads();
+    for (uint32_t b = b0; b < b1; ++b) {
+        const int3 c = brick_coord_of(d, b);
+        bool wanted = false;
+        for (int z = max(c.z - 1, 0); z <= min(c.z + 1, bz - 1) && !wanted; ++z)
+            for (int y = max(c.y - 1, 0); y <= min(c.y + 1, by - 1) && !wanted; ++y)
+                for (int x = max(c.x - 1, 0); x <= min(c.x + 1, bx - 1); ++x)
+                    if (d.brick_touch[uint32_t(x + bx * (y + by * z))] != 0u) { wanted = true; break; }
+        d.brick_want[b] = wanted ? 1u : 0u;
     }
-    auto want = [&](uint32_t b) -> bool { return nb <= POOL_SMEM_BRICKS ? s_flags[nb + b] != 0 : d.brick_want[b] != 0u; };
+    __syncthreads();
+    auto want = [&](uint32_t b) -> bool { return d.brick_want[b] != 0u; };
     uint32_t nfree = 0;
     for (uint32_t b = b0; b < b1; ++b)
         if (!want(b) && d.brick_table_w[b] != 0u) ++nfree;
@@ -824,7 +901,7 @@ __global__ void __launch_bounds__(GRID_THREADS) k_extrapolate(Dev d, const float
 }  // namespace
 
 int launch_pool_update(const Dev& d, cudaStream_t s) {
-    const uint32_t smem = d.num_bricks <= POOL_SMEM_BRICKS ? 2u * d.num_bricks : 0u;
+    const uint32_t smem = d.num_bricks <= POOL_SMEM_BRICKS ? ((2u * d.num_bricks + 3u) & ~3u) + 4u * ((d.num_bricks + 31u) / 32u) : 0u;
     static uint32_t configured = 0;
     if (smem > 48u * 1024u && smem > configured) {
         cudaFuncSetAttribute(k_pool_update, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
