@@ -36,9 +36,11 @@ HBM_FALLBACK_GBS = 6650.0
 # The preconditioner the GPU arm runs by default: the reference's MGPCG (same V-cycle structure, same stopping
 # test) with each coarse-grid correction scaled by 1.9, which makes up for the piecewise-constant prolongation,
 # two red-black sweep pairs per smoothing and 4 coarsest-level iterations (the coarsest solve's accuracy does
-# not change the iteration count). `--mg-correction 1 --mg-sweeps 1 --mg-coarse-iterations 16` runs the
-# reference's V-cycle exactly; the line's "reference_vcycle" object times it on the same box.
-PRECOND = {"mg_correction_scale": 1.9, "mg_smoothing_sweeps": 2, "pcg_flexible": 0, "mg_coarse_iterations": 4}
+# not change the iteration count) and the finest level's sweeps over-relaxed by 1.15.
+# `--mg-correction 1 --mg-sweeps 1 --mg-coarse-iterations 16 --mg-smoother-weight 1` runs the reference's V-cycle
+# exactly; the line's "reference_vcycle" object times it on the same box.
+PRECOND = {"mg_correction_scale": 1.9, "mg_smoothing_sweeps": 2, "pcg_flexible": 0, "mg_coarse_iterations": 4,
+           "mg_smoother_weight": 1.15}
 
 
 def apply_precond(settings, args):
@@ -46,8 +48,10 @@ def apply_precond(settings, args):
     settings.mg_smoothing_sweeps = args.mg_sweeps
     settings.pcg_flexible = args.pcg_flexible
     settings.mg_coarse_iterations = args.mg_coarse_iterations
+    settings.mg_smoother_weight = args.mg_smoother_weight
     return {"mg_correction_scale": args.mg_correction, "mg_smoothing_sweeps": args.mg_sweeps,
-            "pcg_flexible": bool(args.pcg_flexible), "mg_coarse_iterations": args.mg_coarse_iterations}
+            "pcg_flexible": bool(args.pcg_flexible), "mg_coarse_iterations": args.mg_coarse_iterations,
+            "mg_smoother_weight": args.mg_smoother_weight}
 
 
 def parse():
@@ -84,6 +88,7 @@ def parse():
     ap.add_argument("--mg-sweeps", type=int, default=PRECOND["mg_smoothing_sweeps"])
     ap.add_argument("--pcg-flexible", type=int, default=PRECOND["pcg_flexible"])
     ap.add_argument("--mg-coarse-iterations", type=int, default=PRECOND["mg_coarse_iterations"])
+    ap.add_argument("--mg-smoother-weight", type=float, default=PRECOND["mg_smoother_weight"])
     return ap.parse_args()
 
 
@@ -251,7 +256,7 @@ def run_reference(args):
                    "step": "one substep (the GPU arm's step is one frame; both report substeps/s)",
                    "window": f"frames 1-{warm_frames + 1} untimed, then {args.steps} substeps from frame {warm_frames + 2}",
                    "preconditioner": {"mg_correction_scale": 1.0, "mg_smoothing_sweeps": 1, "pcg_flexible": False,
-                                      "mg_coarse_iterations": 16}},
+                                      "mg_coarse_iterations": 16, "mg_smoother_weight": 1.0}},
         "pressure_iterations_mean": statistics.mean(iters) if iters else None,
         "cpu_baseline": {"value": value, "unit": "substeps/s", "cores": cores, "kind": "port",
                          "sample": f"{args.steps} substeps of {sc['name']} from frame {warm_frames + 2}, C++ oracle with OpenMP"},
@@ -352,6 +357,7 @@ def run_slosh(args):
     if args.solver == "mgpcg" and not args.no_reference_vcycle:
         def ref_settings(st, _):
             st.mg_correction_scale, st.mg_smoothing_sweeps, st.pcg_flexible, st.mg_coarse_iterations = 1.0, 1, 0, 16
+            st.mg_smoother_weight = 1.0
             return None
         _, sim2, stream2, fi2, _ = _scene_sim(args, S, A, local, ref_settings)
         for _ in range(max(args.warmup, 3) - 1):
@@ -368,7 +374,7 @@ def run_slosh(args):
                   "pressure_iterations_mean": statistics.mean(run2["iters"]) if run2["iters"] else None,
                   "pressure_rel_residual_max": max(run2["rels"]) if run2["rels"] else None,
                   "preconditioner": {"mg_correction_scale": 1.0, "mg_smoothing_sweeps": 1, "pcg_flexible": False,
-                                     "mg_coarse_iterations": 16}}
+                                     "mg_coarse_iterations": 16, "mg_smoother_weight": 1.0}}
     if rank != 0:
         if dist:
             dist.barrier()

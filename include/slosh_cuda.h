@@ -38,7 +38,7 @@ extern "C" {
 #define SLOSH_API __attribute__((visibility("default")))
 #endif
 
-#define SLOSH_ABI_VERSION 2u
+#define SLOSH_ABI_VERSION 3u
 
 /* Limits, SloshTypes.h:93-110. The particle cap is raised above the reference's 16,777,216. */
 #define SLOSH_MAX_COLLIDERS 64u
@@ -128,6 +128,11 @@ typedef struct slosh_settings_t {
     uint32_t pcg_flexible;       /* 1: flexible PCG, beta = r_k.(z_k - z_{k-1}) / rho_{k-1} (Polak-Ribiere),
                                     robust to a preconditioner that is not exactly linear (FP16/BF16
                                     storage); 0: beta = rho_k / rho_{k-1} (the reference) */
+    float mg_smoother_weight;    /* over-relaxation of the finest level's red-black sweeps: each sweep sets
+                                    x + w (x_GS - x) instead of the Gauss-Seidel value x_GS, and the red
+                                    initialisation of the preconditioned residual is w r / diag; coarser
+                                    levels are unchanged. 1 = the reference; 1.15 saves about one PCG
+                                    iteration in ten on 256^3 grids. Clamped to [0.5, 1.9]. */
 } slosh_settings_t;
 
 /* FSloshParticleGPU (SloshTypes.h:84-91): Pos, Age (negative or NaN = dead), Vel,

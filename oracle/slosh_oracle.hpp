@@ -325,6 +325,7 @@ inline void settings_default(slosh_settings_t* s) {  // SloshTypes.h:113-160
     s->mg_correction_scale = 1.0f;
     s->mg_smoothing_sweeps = 1;
     s->pcg_flexible = 0u;
+    s->mg_smoother_weight = 1.0f;
 }
 
 // Step_RenderThread's clamps (SloshProxy.cpp:344-347). The grid and particle caps are raised above
@@ -437,6 +438,7 @@ struct PassParams {
     float restrict_scale = 0.25f;  // factor of the restriction's fluid-child sum: 0.25 x mg_correction_scale
     int mg_sweeps = 1;             // red-black sweep pairs per pre- and post-smoothing (mg_smoothing_sweeps)
     uint32_t pcg_flexible = 0;     // flexible (Polak-Ribiere) beta
+    float smooth_weight = 1.0f;    // over-relaxation of level 0's red-black sweeps (mg_smoother_weight)
     uint32_t frame_seed = 0;
 };
 
@@ -1321,7 +1323,9 @@ public:
                     R diag, sum;
                     stencil(l, xf, c, i, &cell_diag, diag, sum);
                     R b = bf[i];
-                    R x = store_q(l, (b + sum) / diag);
+                    const R gs = (b + sum) / diag;
+                    // level 0 over-relaxed by mg_smoother_weight: x + w (x_GS - x); 1 = the reference
+                    R x = store_q(l, (l == 0 && P.smooth_weight != 1.0f) ? xf[i] + R(P.smooth_weight) * (gs - xf[i]) : gs);
                     xf[i] = x;
                     dv = double(b * x);
                 } else if (dot) {
@@ -1466,6 +1470,10 @@ public:
         return rho;
     }
 
+    // The preconditioner's red initialisation of level 0 (one red half-sweep from zero): w (r / diag) with the
+    // smoother weight w, r / diag for the reference.
+    R red_init(R v) const { return P.smooth_weight != 1.0f ? R(P.smooth_weight) * v : v; }
+
     static float ratio_f(double num, double den) {  // alpha / beta: FP64 ratio rounded to FP32
         return std::fabs(den) > 1e-30 ? float(num / den) : 0.0f;
     }
@@ -1484,7 +1492,7 @@ public:
             stencil(0, p, c, i, &cell_diag, diag, sum);
             R ri = -div[i] - (diag * p[i] - sum);
             pcg_r[i] = ri;
-            pcg_z[i] = is_red(c) ? ri / diag : R(0);
+            pcg_z[i] = is_red(c) ? red_init(ri / diag) : R(0);
             return double(ri * ri);
         });
         bb_local = level0_dot([&](uint32_t i, I3) -> double {
@@ -1534,7 +1542,7 @@ public:
                 R ri = pcg_r[i] - alpha * pcg_q[i];
                 pcg_r[i] = ri;
                 R diag = cell_diag[i] + R(DIAG_EPSILON);
-                pcg_z[i] = is_red(c) ? ri / diag : R(0);
+                pcg_z[i] = is_red(c) ? red_init(ri / diag) : R(0);
                 return double(ri * ri);
             });
             done = it + 1;
@@ -2199,6 +2207,7 @@ public:
         P.restrict_scale = 0.25f * clampr(s.mg_correction_scale, 0.5f, 1.95f);
         P.mg_sweeps = clampi(s.mg_smoothing_sweeps, 1, 4);
         P.pcg_flexible = s.pcg_flexible ? 1u : 0u;
+        P.smooth_weight = clampr(s.mg_smoother_weight, 0.5f, 1.9f);
         P.ghost_fluid = s.ghost_fluid ? 1u : 0u;
         const int interval = clampi(s.density_projection_interval, 1, 8);
         P.density_relaxation = 1.0f - std::pow(1.0f - clampr(s.density_relaxation, 0.0f, 1.0f), float(interval));

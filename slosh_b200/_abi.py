@@ -74,7 +74,7 @@ class Settings(C.Structure):
         ("max_frame_dt", C.c_float), ("cfl", C.c_float), ("max_speed", C.c_float),
         ("tolerance", C.c_float), ("max_iterations", C.c_int32), ("precision_mode", C.c_uint32),
         ("warm_start", C.c_uint32), ("mg_correction_scale", C.c_float), ("mg_smoothing_sweeps", C.c_int32),
-        ("pcg_flexible", C.c_uint32),
+        ("pcg_flexible", C.c_uint32), ("mg_smoother_weight", C.c_float),
     ]
 
 

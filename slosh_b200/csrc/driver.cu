@@ -103,6 +103,7 @@ slosh_settings_t defaults() {
     s.mg_correction_scale = 1.0f;
     s.mg_smoothing_sweeps = 1;
     s.pcg_flexible = 0u;
+    s.mg_smoother_weight = 1.0f;
     return s;
 }
 
@@ -734,12 +735,15 @@ struct Ctx {
             const float restrict_scale = 0.25f * clampf_h(s.mg_correction_scale, 0.5f, 1.95f);
             const int sweeps = clampi_h(s.mg_smoothing_sweeps, 1, 4);
             const uint32_t flexible = s.pcg_flexible ? 1u : 0u;
-            if (restrict_scale != mg.restrict_scale || sweeps != mg.sweeps || flexible != mg.flexible) {
+            const float smooth_weight = clampf_h(s.mg_smoother_weight, 0.5f, 1.9f);
+            if (restrict_scale != mg.restrict_scale || sweeps != mg.sweeps || flexible != mg.flexible ||
+                smooth_weight != mg.smooth_weight) {
                 CK(cudaStreamSynchronize(stream));
                 destroy_graphs();
                 mg.restrict_scale = restrict_scale;
                 mg.sweeps = sweeps;
                 mg.flexible = flexible;
+                mg.smooth_weight = smooth_weight;
             }
         }
         ++sim_frame;

@@ -119,6 +119,7 @@ struct MGState {
     float restrict_scale;       // factor of the restriction's fluid-child sum: 0.25 x mg_correction_scale
     int sweeps;                 // red-black sweep pairs per pre- and post-smoothing (mg_smoothing_sweeps)
     uint32_t flexible;          // flexible PCG: UpdatePR also reduces r_{k+1}.z_k into scalars[9]
+    float smooth_weight;        // over-relaxation of level 0's red-black sweeps (mg_smoother_weight; 1 = reference)
 };
 int launch_mg_words(const MGState& m, int l, cudaStream_t s);
 int launch_mg_tail_lists(const MGState& m, cudaStream_t s);

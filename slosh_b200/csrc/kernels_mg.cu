@@ -73,6 +73,14 @@ __device__ __forceinline__ float coarse_scale(const MGState& m) {
     e = max(-60, min(60, e));
     return ldexpf(1.0f, e);
 }
+// Coarse-level stencil word bits (k_level_words): bits 0-5 fluid neighbour, 6 fluid, 7 red, 8-13 non-solid neighbour.
+constexpr uint32_t CW_FLUID = 1u << 6, CW_RED = 1u << 7, CW_NONSOLID_SHIFT = 8u;
+// Level 0's over-relaxed sweep value x + w (x_GS - x) with w = mg_smoother_weight, and its red initialisation (one
+// red half-sweep from zero) w x_GS; w == 1 leaves the reference's Gauss-Seidel value x_GS.
+__device__ __forceinline__ float relax0(const MGState& m, float x_old, float gs) {
+    return m.smooth_weight != 1.0f ? x_old + m.smooth_weight * (gs - x_old) : gs;
+}
+__device__ __forceinline__ float red_init0(const MGState& m, float gs) { return m.smooth_weight != 1.0f ? m.smooth_weight * gs : gs; }
 __device__ __forceinline__ uint32_t lin3(int3 c, int3 dim) { return uint32_t(c.x + dim.x * (c.y + dim.y * c.z)); }
 __device__ __forceinline__ int3 coord3(uint32_t i, int3 dim) {
     return make_int3(int(i % uint32_t(dim.x)), int((i / uint32_t(dim.x)) % uint32_t(dim.y)), int(i / uint32_t(dim.x * dim.y)));
@@ -229,9 +237,11 @@ __device__ __forceinline__ uint32_t l0_nbr(uint32_t i, uint32_t l, int n, const 
 // round by round, x ascending, starting from 0.0, and the lanes fold with shfl_down 16..1.
 struct Geo {
     uint32_t i, l, h, y, z;  // pool and local index of the quad's first cell; half, row, plane
+    uint32_t b;              // the brick (w4_pass only)
 };
-__device__ __forceinline__ Geo geo_of(uint32_t base, uint32_t lane, uint32_t k) {
+__device__ __forceinline__ Geo geo_of(uint32_t base, uint32_t lane, uint32_t k, uint32_t brick = 0u) {
     Geo g;
+    g.b = brick;
     g.h = lane & 1u;
     g.y = (lane >> 1) & 7u;
     g.z = 2u * k + (lane >> 4);
@@ -298,11 +308,11 @@ __device__ __forceinline__ void w4_pass(const Dev& d, const MGState& m, uint32_t
         for (uint32_t k0 = 0; k0 < 4u; k0 += uint32_t(B)) {
             decltype(load(Geo{}, ns)) vals[B];
 #pragma unroll
-            for (int b = 0; b < B; ++b) vals[b] = load(geo_of(base, lane, k0 + uint32_t(b)), ns);
+            for (int b = 0; b < B; ++b) vals[b] = load(geo_of(base, lane, k0 + uint32_t(b), s1.w), ns);
 #pragma unroll
             for (int b = 0; b < B; ++b) {
                 double v0[4] = {0.0, 0.0, 0.0, 0.0}, v1[4] = {0.0, 0.0, 0.0, 0.0};
-                apply(geo_of(base, lane, k0 + uint32_t(b)), vals[b], v0, v1);
+                apply(geo_of(base, lane, k0 + uint32_t(b), s1.w), vals[b], v0, v1);
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
                     acc0 = acc0 + v0[j];
@@ -389,13 +399,37 @@ struct SweepQ {
     Q6 z;
     float4 r, dg;
     uint32_t w;
+    float pa, pb;  // PROLONGED: the prolongation terms of cells 0-1 and 2-3 (their level-1 parents)
 };
+// PROLONGED (the first red sweep after k_prolong_smooth0 with an over-relaxed smoother): the red cells' stored
+// z lacks the prolongation, which the fused kernel adds only to the values it reads, so the sweep rebuilds each
+// red cell's prolonged value z + x_parent / coarse scale (fluid parents) from level 1, as k_prolong_smooth0 does.
+template <bool PROLONGED = false>
 __device__ __forceinline__ SweepQ load_sweep(const Dev& d, const MGState& m, const Geo& g, const uint32_t* ns) {
     SweepQ v;
     v.z = load_q6(m.z, g, ns);
     v.r = ld4(m.r + g.i);
     v.dg = ld4(d.cell_diag + g.i);
     v.w = quad_words(m, g);
+    v.pa = v.pb = 0.0f;
+    if (PROLONGED) {
+        const MGLevel C = m.lv[1];
+        const float ivs = 1.0f / coarse_scale(m);  // a power of two: exact
+        const int3 bc = brick_coord_of(d, g.b);
+        float pv[2];
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const int3 c = make_int3(bc.x * 4 + 2 * int(g.h) + k, bc.y * 4 + int(g.y >> 1), bc.z * 4 + int(g.z >> 1));
+            pv[k] = 0.0f;
+            if (inside3(c, C.dim)) {
+                const uint32_t ci = lin3(c, C.dim);
+                const float x = lv_ld(C.x, ci, C.prec);
+                pv[k] = (C.word[ci] & CW_FLUID) ? x * ivs : 0.0f;
+            }
+        }
+        v.pa = pv[0];
+        v.pb = pv[1];
+    }
     return v;
 }
 
@@ -430,7 +464,6 @@ __global__ void k_build_type(Dev d, MGLevel fine, MGLevel coarse, int fine_is_po
 }
 
 // ---- coarse-level stencil words (once per solve, after the coarse types) -----------------------------------
-constexpr uint32_t CW_FLUID = 1u << 6, CW_RED = 1u << 7, CW_NONSOLID_SHIFT = 8u;
 
 __global__ void k_level_words(MGLevel L) {
     pdl_entry();
@@ -557,7 +590,7 @@ __global__ void __launch_bounds__(GRID_THREADS) k_pcg_init(Dev d, MGState m, con
                 const float b = -comp(v.dv, j);
                 const float ri = b - (diag * comp(v.p.c, j) - nb_sum(n, w));
                 r[j] = ri;
-                z[j] = (w & W_RED) ? ri / diag : 0.0f;
+                z[j] = (w & W_RED) ? red_init0(m, ri / diag) : 0.0f;
                 v0[j] = double(ri * ri);
                 v1[j] = double(b * b);
             }
@@ -580,7 +613,7 @@ __device__ __forceinline__ Nb6 load_black(const Dev& d, const MGState& m, uint32
     Nb6 v;
     v.w = m.word[i];
     v.c0 = m.r[i];
-    v.c1 = 0.0f;
+    v.c1 = m.smooth_weight != 1.0f ? m.z[i] : 0.0f;  // the cell's own value, for the over-relaxed update
     v.c2 = d.cell_diag[i];
 #pragma unroll
     for (int n = 0; n < 6; ++n) v.n[n] = m.z[l0_nbr(i, l, n, ns)];
@@ -590,11 +623,11 @@ __device__ __forceinline__ Nb6 load_black(const Dev& d, const MGState& m, uint32
 // Red sweep; with DOT also rho = r . z over all cells (red: the new value, black: the current z), which
 // shifts rho. Cells the sweep does not update are stored back unchanged (each cell belongs to one warp's
 // brick).
-template <bool DOT>
+template <bool DOT, bool PROLONGED = false>
 __global__ void __launch_bounds__(GRID_THREADS, 3) k_smooth0(Dev d, MGState m) {
     pdl_entry();
     w4_pass<DOT ? 1 : 0, 1>(d, m, 1,
-        [&](const Geo& g, const uint32_t* ns) { return load_sweep(d, m, g, ns); },
+        [&](const Geo& g, const uint32_t* ns) { return load_sweep<PROLONGED>(d, m, g, ns); },
         [&](const Geo& g, const SweepQ& v, double* v0, double*) {
             const X2 x = partner(v.z);
             float out[4];
@@ -608,8 +641,8 @@ __global__ void __launch_bounds__(GRID_THREADS, 3) k_smooth0(Dev d, MGState m) {
                     float n[6];
                     nbrs6(v.z, x, g.h, j, n);
                     const float val = (rj + nb_sum(n, w)) / (comp(v.dg, j) + DIAG_EPSILON);
-                    out[j] = val;
-                    v0[j] = double(rj * val);
+                    out[j] = relax0(m, PROLONGED ? zj + (j < 2 ? v.pa : v.pb) : zj, val);
+                    v0[j] = double(rj * out[j]);
                 } else {
                     v0[j] = double(rj * zj);
                 }
@@ -626,7 +659,7 @@ __global__ void __launch_bounds__(GRID_THREADS) k_smooth0_black(Dev d, MGState m
         [&](uint32_t i, uint32_t l, const uint32_t* ns) { return load_black(d, m, i, l, ns); },
         [&](uint32_t i, uint32_t, const Nb6& v) {
             if (!(v.w & W_FLUID)) return;
-            m.z[i] = (v.c0 + nb_sum(v.n, v.w)) / (v.c2 + DIAG_EPSILON);
+            m.z[i] = relax0(m, v.c1, (v.c0 + nb_sum(v.n, v.w)) / (v.c2 + DIAG_EPSILON));
         });
 }
 
@@ -678,7 +711,7 @@ __global__ void __launch_bounds__(GRID_THREADS) k_prolong_smooth0(Dev d, MGState
 #pragma unroll
             for (int n = 0; n < 6; ++n)
                 if ((v.w >> n) & 1u) sum = sum + (v.n[n] + cx[po[n]]);
-            m.z[i] = (v.c0 + sum) / (v.c2 + DIAG_EPSILON);
+            m.z[i] = relax0(m, v.c1 + cx[p], (v.c0 + sum) / (v.c2 + DIAG_EPSILON));
         });
 }
 
@@ -1341,7 +1374,7 @@ __global__ void __launch_bounds__(ST_WARPS * 32) k_update_pr_st(Dev d, MGState m
                 po[j] = comp(vp, j) + alpha * comp(vd, j);
                 const float ri = comp(vr, j) - alpha * comp(vq, j);
                 ro[j] = ri;
-                zo[j] = (w & W_RED) ? ri / (comp(dg, j) + DIAG_EPSILON) : 0.0f;
+                zo[j] = (w & W_RED) ? red_init0(m, ri / (comp(dg, j) + DIAG_EPSILON)) : 0.0f;
                 v0[j] = double(ri * ri);
                 if (FLEX) v1[j] = double(ri * comp(vz, j));
             }
@@ -1771,7 +1804,7 @@ __global__ void __launch_bounds__(GRID_THREADS, 3) k_update_pr(Dev d, MGState m,
                 po[j] = comp(v.p, j) + alpha * comp(v.d, j);
                 const float ri = comp(v.r, j) - alpha * comp(v.q, j);
                 ro[j] = ri;
-                zo[j] = (w & W_RED) ? ri / (comp(v.dg, j) + DIAG_EPSILON) : 0.0f;
+                zo[j] = (w & W_RED) ? red_init0(m, ri / (comp(v.dg, j) + DIAG_EPSILON)) : 0.0f;
                 v0[j] = double(ri * ri);
                 if (FLEX) v1[j] = double(ri * comp(v.z, j));
             }
@@ -1967,11 +2000,17 @@ int launch_mg_tail_lists(const MGState& m, cudaStream_t s) {
 // One V-cycle (SloshProxy.cpp:904-959), leaving rho = r.z in scalars[0] (previous rho in scalars[3]).
 int launch_vcycle(const Dev& d, const MGState& m, int coarse_iterations, const Shape& sh, cudaStream_t s) {
     const int nl = m.num_levels;
-    const bool staged = mg_staged();
-    auto smooth0_red = [&](bool dot) {
+    const bool relaxed = m.smooth_weight != 1.0f;  // over-relaxed level 0: the global-memory passes only
+    const bool staged = mg_staged() && !relaxed;
+    // prolonged: the first red sweep after k_prolong_smooth0, which with the over-relaxed smoother rebuilds the red
+    // cells' prolonged values (the Gauss-Seidel value does not depend on them)
+    auto smooth0_red = [&](bool dot, bool prolonged = false) {
         if (staged) {
             if (dot) ST_LAUNCH(k_smooth0_st<true>, 1, 2, d, m, sh, s);
             else ST_LAUNCH(k_smooth0_st<false>, 1, 2, d, m, sh, s);
+        } else if (prolonged && relaxed) {
+            if (dot) launch_k(k_smooth0<true, true>, sh.mg_ctas, GRID_THREADS, 0, s, d, m);
+            else launch_k(k_smooth0<false, true>, sh.mg_ctas, GRID_THREADS, 0, s, d, m);
         } else {
             if (dot) launch_k(k_smooth0<true>, sh.mg_ctas, GRID_THREADS, 0, s, d, m);
             else launch_k(k_smooth0<false>, sh.mg_ctas, GRID_THREADS, 0, s, d, m);
@@ -2048,11 +2087,11 @@ int launch_vcycle(const Dev& d, const MGState& m, int coarse_iterations, const S
             if (staged) ST_LAUNCH(k_prolong_smooth0_st, 1, 2, d, m, sh, s);
             else launch_k(k_prolong_smooth0, sh.mg_ctas, GRID_THREADS, 0, s, d, m);
             for (int k = 1; k < sweeps; ++k) {
-                smooth0_red(false);
+                smooth0_red(false, k == 1);
                 smooth0_black();
                 n += 2;
             }
-            smooth0_red(true);
+            smooth0_red(true, sweeps == 1);
         } else {
             launch_k(k_prolong_smooth_fp, fp_blocks(l), 256, 0, s, d, m, l);
             for (int k = 1; k < sweeps; ++k) {

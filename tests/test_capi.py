@@ -38,7 +38,7 @@ def test_library_exports_every_declared_symbol(slosh):
 
 def test_abi_version_and_struct_sizes(slosh):
     lib = slosh.load_library()
-    assert lib.slosh_abi_version() == 2
+    assert lib.slosh_abi_version() == 3
     assert C.sizeof(A.Particle) == 48
     assert C.sizeof(A.Collider) == 80
     assert C.sizeof(A.Manipulator) == 80

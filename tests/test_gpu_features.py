@@ -197,17 +197,22 @@ def test_launch_shape_does_not_change_results(slosh):
     assert np.array_equal(runs[0][1], runs[1][1])
 
 
-@pytest.mark.parametrize("scale,sweeps,flexible,mode", [
-    (1.7, 1, 0, A.PRECISION_FP32),
-    (1.7, 2, 1, A.PRECISION_FP32),
-    (1.0, 3, 1, A.PRECISION_FP32),
-    (1.9, 1, 1, A.PRECISION_BF16_STORAGE),
+@pytest.mark.parametrize("scale,sweeps,flexible,mode,weight", [
+    (1.7, 1, 0, A.PRECISION_FP32, 1.0),
+    (1.7, 2, 1, A.PRECISION_FP32, 1.0),
+    (1.0, 3, 1, A.PRECISION_FP32, 1.0),
+    (1.9, 1, 1, A.PRECISION_BF16_STORAGE, 1.0),
+    (1.9, 2, 0, A.PRECISION_FP32, 1.15),
+    (1.9, 1, 0, A.PRECISION_FP32, 1.3),
+    (1.7, 3, 1, A.PRECISION_FP16_STORAGE, 1.15),
 ])
-def test_preconditioner_options(slosh, oracle_mod, scale, sweeps, flexible, mode):
+def test_preconditioner_options(slosh, oracle_mod, scale, sweeps, flexible, mode, weight):
     """The multigrid preconditioner's options (coarse-grid correction scale, red-black sweep pairs per
-    smoothing, flexible PCG, with FP32 and BF16 coarse storage) on a 96^3 sparse scene whose hierarchy uses
-    footprint levels, the shared-memory tail and the coarsest solve: bit-exact against the oracle run with
-    the same options, every solve to its tolerance."""
+    smoothing, flexible PCG, over-relaxation of the finest level's sweeps, with FP32, BF16 and FP16 coarse
+    storage) on a 96^3 sparse scene whose hierarchy uses footprint levels, the shared-memory tail and the
+    coarsest solve: bit-exact against the oracle run with the same options, every solve to its tolerance. One
+    sweep pair with over-relaxation makes the first red sweep after the prolongation the one that also forms
+    rho."""
     sc = scenes.dam_break_sphere(slosh.settings_default, n=96)
     s = sc["settings"]
     s.max_substeps = 16
@@ -215,6 +220,7 @@ def test_preconditioner_options(slosh, oracle_mod, scale, sweeps, flexible, mode
     s.mg_smoothing_sweeps = sweeps
     s.pcg_flexible = flexible
     s.precision_mode = mode
+    s.mg_smoother_weight = weight
     g, o = pair(slosh, oracle_mod, sc)
     run_frames(g, o, sc, frames=2)
     assert g.results().last_solve_rel_residual <= 1e-6

@@ -390,17 +390,19 @@ def test_overcorrected_vcycle_needs_fewer_iterations(oracle_mod):
     assert all(abs(a - b) <= 1 for a, b in zip(counts["flex"], counts["scaled"])), counts
 
 
-@pytest.mark.parametrize("scale,sweeps,flexible", [(1.0, 1, 0), (1.9, 2, 1)])
-def test_mgpcg_matches_direct_solve_sparse_64(oracle_mod, scale, sweeps, flexible):
+@pytest.mark.parametrize("scale,sweeps,flexible,weight", [(1.0, 1, 0, 1.0), (1.9, 2, 1, 1.0), (1.9, 2, 0, 1.15)])
+def test_mgpcg_matches_direct_solve_sparse_64(oracle_mod, scale, sweeps, flexible, weight):
     """The solve's mathematics pinned independently of any reduction order: the FP64 oracle's MGPCG on the sparse
     64^3 dam break + falling sphere (ghost-fluid diagonals at the free surface, several MG levels through the
-    footprints and the shared tail), with the reference's V-cycle and with the tuned options, against scipy's
-    direct sparse solve of the same assembled system (diag_f + 1e-4 on the fluid cells, -1 per fluid neighbour)."""
+    footprints and the shared tail), with the reference's V-cycle and with the tuned options (over-relaxed finest
+    sweeps included), against scipy's direct sparse solve of the same assembled system (diag_f + 1e-4 on the
+    fluid cells, -1 per fluid neighbour)."""
     import scipy.sparse.linalg as spla
     sc = scenes.dam_break_sphere(oracle_mod.settings_default, n=64)
     s = sc["settings"]
     s.max_substeps = 16
     s.mg_correction_scale, s.mg_smoothing_sweeps, s.pcg_flexible = scale, sweeps, flexible
+    s.mg_smoother_weight = weight
     o = oracle_mod.Oracle(s, fp64=True)
     o.set_emit_seed(sc["seed"])
     fi = A.frame_input(s, emits=sc["emits"])
