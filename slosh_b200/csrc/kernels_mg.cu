@@ -203,6 +203,26 @@ __device__ __forceinline__ void for_footprint_span(const Dev& d, const MGLevel& 
         if (inside3(c, L.dim)) fn(lin3(c, L.dim), c);
     }
 }
+// The footprint cells of one colour (parity 0: red, (x + y + z) even; 1: black) of level l = 1 or 2, whose brick
+// footprints have an even side, so a cell's colour is that of its position inside the footprint: item j of a brick
+// is (2 (j mod s/2) + ((y + z + parity) & 1), y, z) with y = (j / (s/2)) mod s, z = j / (s^2/2). A sweep then
+// visits only the cells it updates: half the threads of the all-cell walk.
+template <class Fn>
+__device__ __forceinline__ void for_footprint_colour(const Dev& d, const MGLevel& L, int l, uint32_t parity, Fn fn) {
+    const uint32_t side = uint32_t(8 >> l), half = side / 2u;
+    const uint32_t per = side * side * half;
+    const uint32_t count = d.active_bricks[0];
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;; t += gridDim.x * blockDim.x) {
+        const uint32_t e = t / per, j = t % per;
+        const uint32_t brick = d.active_bricks[1u + min(e, d.num_bricks - 1u)];
+        if (e >= count) break;
+        const int3 bc = brick_coord_of(d, brick);
+        const uint32_t y = (j / half) % side, z = j / (half * side);
+        const uint32_t x = 2u * (j % half) + ((y + z + parity) & 1u);
+        const int3 c = make_int3(bc.x * int(side) + int(x), bc.y * int(side) + int(y), bc.z * int(side) + int(z));
+        if (inside3(c, L.dim)) fn(lin3(c, L.dim), c);
+    }
+}
 template <class Fn>
 __device__ __forceinline__ void for_footprint(const Dev& d, const MGLevel& L, int l, Fn fn) {
     for_footprint_span(d, L, l, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x, fn);
@@ -791,7 +811,8 @@ __global__ void k_smooth_fp(Dev d, MGState m, int l, uint32_t parity) {
     pdl_entry();
     const MGLevel L = m.lv[l];
     const uint32_t want = parity == 0u ? CW_RED : 0u;
-    for_footprint(d, L, l, [&](uint32_t i, int3) { smooth_fp_cell(L, i, want); });
+    if (l <= 2) for_footprint_colour(d, L, l, parity, [&](uint32_t i, int3) { smooth_fp_cell(L, i, want); });
+    else for_footprint(d, L, l, [&](uint32_t i, int3) { smooth_fp_cell(L, i, want); });
 }
 // Restriction l -> l + 1 over level l + 1's footprint.
 __global__ void k_restrict_fp(Dev d, MGState m, int l) {
@@ -803,7 +824,8 @@ __global__ void k_restrict_fp(Dev d, MGState m, int l) {
 __global__ void k_prolong_smooth_fp(Dev d, MGState m, int l) {
     pdl_entry();
     const MGLevel F = m.lv[l], C = m.lv[l + 1];
-    for_footprint(d, F, l, [&](uint32_t i, int3 c) { prolong_smooth_fp_cell(F, C, i, c); });
+    if (l <= 2) for_footprint_colour(d, F, l, 1u, [&](uint32_t i, int3 c) { prolong_smooth_fp_cell(F, C, i, c); });
+    else for_footprint(d, F, l, [&](uint32_t i, int3 c) { prolong_smooth_fp_cell(F, C, i, c); });
 }
 
 // ---- MGRestrictCS level 0 -> 1 over the 4^3 level-1 cells of every active brick (SparseCoarse) -----------
@@ -2032,6 +2054,13 @@ int launch_vcycle(const Dev& d, const MGState& m, int coarse_iterations, const S
         const uint64_t cells = l <= 3 ? uint64_t(d.num_pool_bricks - 1u) * side * side * side : uint64_t(m.lv[l].cells);
         return int(std::max<uint64_t>(1, std::min<uint64_t>(uint64_t(sh.brick_ctas), (cells + 255u) / 256u)));
     };
+    // the one-colour passes (k_smooth_fp, k_prolong_smooth_fp) of levels 1 and 2 visit half the footprint
+    auto fp_blocks_sweep = [&](int l) {
+        if (l > 2) return fp_blocks(l);
+        const uint32_t side = uint32_t(8 >> l);
+        const uint64_t cells = uint64_t(d.num_pool_bricks - 1u) * side * side * side / 2u;
+        return int(std::max<uint64_t>(1, std::min<uint64_t>(uint64_t(sh.brick_ctas), (cells + 255u) / 256u)));
+    };
     // Pre-smoothing: the black half of the first pair (the red half is the red initialisation written by
     // UpdatePR or the restriction), then sweeps - 1 red-black pairs. Post-smoothing: sweeps black-red pairs,
     // the first black half fused with the prolongation, the last red half of level 0 with rho = r.z.
@@ -2055,11 +2084,11 @@ int launch_vcycle(const Dev& d, const MGState& m, int coarse_iterations, const S
         }
         ++n;
         if (l + 1 < tail) {  // the tail kernel does its own pre-smoothing
-            launch_k(k_smooth_fp, fp_blocks(l + 1), 256, 0, s, d, m, l + 1, 1u);
+            launch_k(k_smooth_fp, fp_blocks_sweep(l + 1), 256, 0, s, d, m, l + 1, 1u);
             ++n;
             for (int k = 1; k < sweeps; ++k) {
-                launch_k(k_smooth_fp, fp_blocks(l + 1), 256, 0, s, d, m, l + 1, 0u);
-                launch_k(k_smooth_fp, fp_blocks(l + 1), 256, 0, s, d, m, l + 1, 1u);
+                launch_k(k_smooth_fp, fp_blocks_sweep(l + 1), 256, 0, s, d, m, l + 1, 0u);
+                launch_k(k_smooth_fp, fp_blocks_sweep(l + 1), 256, 0, s, d, m, l + 1, 1u);
                 n += 2;
             }
         }
@@ -2093,13 +2122,13 @@ int launch_vcycle(const Dev& d, const MGState& m, int coarse_iterations, const S
             }
             smooth0_red(true, sweeps == 1);
         } else {
-            launch_k(k_prolong_smooth_fp, fp_blocks(l), 256, 0, s, d, m, l);
+            launch_k(k_prolong_smooth_fp, fp_blocks_sweep(l), 256, 0, s, d, m, l);
             for (int k = 1; k < sweeps; ++k) {
-                launch_k(k_smooth_fp, fp_blocks(l), 256, 0, s, d, m, l, 0u);
-                launch_k(k_smooth_fp, fp_blocks(l), 256, 0, s, d, m, l, 1u);
+                launch_k(k_smooth_fp, fp_blocks_sweep(l), 256, 0, s, d, m, l, 0u);
+                launch_k(k_smooth_fp, fp_blocks_sweep(l), 256, 0, s, d, m, l, 1u);
                 n += 2;
             }
-            launch_k(k_smooth_fp, fp_blocks(l), 256, 0, s, d, m, l, 0u);
+            launch_k(k_smooth_fp, fp_blocks_sweep(l), 256, 0, s, d, m, l, 0u);
         }
         n += 2;
     }
