@@ -199,6 +199,7 @@ struct Ctx {
         bool tol_mode;
         float tol;
         int coarse;
+        bool setup;
         cudaGraph_t graph;
         cudaGraphExec_t exec;
         int pre_nodes, body_nodes;
@@ -615,13 +616,17 @@ struct Ctx {
     // Sequence of one solve: setup, coarse cell types, PCGInit, then while the device says so:
     // V-cycle, UpdateD, ApplyA, UpdatePR. This is the reference's order (init, V-cycle, UpdateD(first),
     // then per iteration ApplyA, UpdatePR and -- unless it was the last -- V-cycle, UpdateD).
+    // setup: build the per-solve structure (coarse types, stencil words, tail lists) from the cell types; the
+    // density solve of the frame's last substep runs on the types its pressure solve just used and skips it.
     int enqueue_pre(const Dev& d, float* p, const float* div, uint32_t limit, bool tol_mode, float tol, unsigned long long handle,
-                    cudaStream_t s) {
+                    cudaStream_t s, bool setup) {
         int n = launch_mg_setup(mg, limit, tol_mode, double(tol), s);
-        for (int l = 0; l < num_levels - 1; ++l) n += launch_mg_build_type(d, mg, l, s);
-        for (int l = 1; l < num_levels; ++l) n += launch_mg_words(mg, l, s);
-        n += launch_mg_tail_lists(mg, s);
-        n += launch_pcg_init(d, mg, p, div, handle, shape, s);
+        if (setup) {
+            for (int l = 0; l < num_levels - 1; ++l) n += launch_mg_build_type(d, mg, l, s);
+            for (int l = 1; l < num_levels; ++l) n += launch_mg_words(mg, l, s);
+            n += launch_mg_tail_lists(mg, s);
+        }
+        n += launch_pcg_init(d, mg, p, div, handle, shape, s, setup);
         return n;
     }
     int enqueue_body(const Dev& d, float* p, int coarse, unsigned long long handle, cudaStream_t s) {
@@ -631,11 +636,12 @@ struct Ctx {
         n += launch_pcg_update_pr(d, mg, p, handle, shape, s);
         return n;
     }
-    SolveGraph* solve_graph(float* p, const float* div, uint32_t limit, bool tol_mode, float tol, int coarse) {
+    SolveGraph* solve_graph(float* p, const float* div, uint32_t limit, bool tol_mode, float tol, int coarse, bool setup) {
         for (auto& g : graphs)
-            if (g.p == p && g.div == div && g.limit == limit && g.tol_mode == tol_mode && g.tol == tol && g.coarse == coarse) return &g;
+            if (g.p == p && g.div == div && g.limit == limit && g.tol_mode == tol_mode && g.tol == tol && g.coarse == coarse && g.setup == setup)
+                return &g;
         const Dev d = dev();
-        SolveGraph G{p, div, limit, tol_mode, tol, coarse, nullptr, nullptr, 0, 0};
+        SolveGraph G{p, div, limit, tol_mode, tol, coarse, setup, nullptr, nullptr, 0, 0};
         CK(cudaStreamBeginCapture(cap_stream, cudaStreamCaptureModeThreadLocal));
         cudaGraph_t cg = nullptr;
         try {
@@ -645,7 +651,7 @@ struct Ctx {
             CK(cudaStreamGetCaptureInfo(cap_stream, &st, nullptr, &cg, &deps, &nd));
             cudaGraphConditionalHandle h;
             CK(cudaGraphConditionalHandleCreate(&h, cg, 0, cudaGraphCondAssignDefault));
-            G.pre_nodes = enqueue_pre(d, p, div, limit, tol_mode, tol, h, cap_stream);
+            G.pre_nodes = enqueue_pre(d, p, div, limit, tol_mode, tol, h, cap_stream, setup);
             CK(cudaStreamGetCaptureInfo(cap_stream, &st, nullptr, &cg, &deps, &nd));
             cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
             cp.conditional.handle = h;
@@ -674,7 +680,8 @@ struct Ctx {
         graphs.push_back(G);
         return &graphs.back();
     }
-    // slot 0: the pressure solve's statistics are read back at the end of the frame; slot 1: density.
+    // slot 0: the pressure solve, whose statistics are read back at the end of the frame; slot 1: the density
+    // solve, which follows slot 0's solve in the same substep on the same cell types and reuses its setup.
     void mgpcg(float* p, const float* div, int fixed_iterations, float tolerance, int max_iterations, int coarse_iterations,
                int slot) {
         const bool tol_mode = fixed_iterations <= 0;
@@ -683,7 +690,7 @@ struct Ctx {
         SolveGraph* G = nullptr;
         if (use_graphs) {
             try {
-                G = solve_graph(p, div, limit, tol_mode, tolerance, coarse_iterations);
+                G = solve_graph(p, div, limit, tol_mode, tolerance, coarse_iterations, slot == 0);
             } catch (const CudaError& e) {
                 std::fprintf(stderr, "slosh: CUDA graph capture of the solve failed (%s: %s); issuing kernels directly\n", e.what,
                              cudaGetErrorString(e.code));
@@ -695,7 +702,7 @@ struct Ctx {
             CK(cudaGraphLaunch(G->exec, stream));
             frame_solves.push_back({G->pre_nodes, G->body_nodes, slot});
         } else {
-            int pre = enqueue_pre(d, p, div, limit, tol_mode, tolerance, 0ull, stream);
+            int pre = enqueue_pre(d, p, div, limit, tol_mode, tolerance, 0ull, stream, slot == 0);
             int body = 0;
             for (uint32_t it = 0; it < limit; ++it) {
                 CK(cudaMemcpyAsync(h_ctl + 4 * slot, mg.ctl, 16, cudaMemcpyDeviceToHost, stream));

@@ -130,7 +130,7 @@ int launch_mg_setup(const MGState& m, uint32_t limit, bool tol_mode, double tol,
 int launch_mg_build_type(const Dev& d, const MGState& m, int l, cudaStream_t s);
 // handle: the WHILE node's condition when the solve runs as a CUDA graph, 0 otherwise.
 int launch_pcg_init(const Dev& d, const MGState& m, const float* p, const float* div, unsigned long long handle, const Shape& sh,
-                    cudaStream_t s);
+                    cudaStream_t s, bool words = true);
 int launch_vcycle(const Dev& d, const MGState& m, int coarse_iterations, const Shape& sh, cudaStream_t s);
 int launch_pcg_apply_a(const Dev& d, const MGState& m, const Shape& sh, cudaStream_t s);
 int launch_pcg_update_pr(const Dev& d, const MGState& m, float* p, unsigned long long handle, const Shape& sh, cudaStream_t s);

@@ -550,31 +550,52 @@ __global__ void __launch_bounds__(GRID_THREADS) k_pcg_words(Dev d, MGState m) {
         const uint32_t brick = d.active_bricks[1u + e];
         const uint32_t slot = __ldg(d.brick_table + brick);
         const int3 bc = brick_coord_of(d, brick);
+        uint32_t mine = 0u;  // lanes 0-5: the slot of face neighbour `lane` (0 = outside the grid or unallocated)
         if (lane < 6) {
             const int3 nb = add3(bc, nbr_off(int(lane)));
             const bool in = nb.x >= 0 && nb.y >= 0 && nb.z >= 0 && nb.x < d.brick_dim.x && nb.y < d.brick_dim.y && nb.z < d.brick_dim.z;
-            m.nbr_slots[8u * e + lane] = in ? __ldg(d.brick_table + brick_index_of(d, nb)) : 0u;
+            mine = in ? __ldg(d.brick_table + brick_index_of(d, nb)) : 0u;
+            m.nbr_slots[8u * e + lane] = mine;
         } else if (lane == 6) {
             m.nbr_slots[8u * e + 6u] = slot;
         } else if (lane == 7) {
             m.nbr_slots[8u * e + 7u] = brick;
         }
-        for (uint32_t k = 0; k < 16u; ++k) {
-            const uint32_t l = lane + 32u * k;
-            const int3 lc = local_coord_of(l);
-            const int3 c = make_int3(bc.x * 8 + lc.x, bc.y * 8 + lc.y, bc.z * 8 + lc.z);
-            uint32_t w = 0u;
-            if (in_grid(d, c)) {
-                const uint32_t i = slot * BRICK_CELLS + l;
-                if ((d.cell_type[i] & CELL_TYPE_MASK) == CELL_FLUID) w |= W_FLUID;
-                if (is_red(c)) w |= W_RED;
+        uint32_t ns[6];
 #pragma unroll
-                for (int n = 0; n < 6; ++n) {
-                    if (!in_grid(d, add3(c, nbr_off(n)))) continue;
-                    if ((d.cell_type[nbr_index(d, i, c, n)] & CELL_TYPE_MASK) == CELL_FLUID) w |= 1u << n;
-                }
+        for (int n = 0; n < 6; ++n) ns[n] = __shfl_sync(0xFFFFFFFFu, mine, n);
+        // 16 cells per lane in groups of 4: the types of a group's cells and their 6 neighbours are all loaded
+        // before its words are stored (a neighbour across a face through the face neighbour's slot; an
+        // unallocated brick is the all-zero null slot, whose cells are air)
+        for (uint32_t g = 0; g < 4u; ++g) {
+            uint32_t t[4][7];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const uint32_t l = lane + 32u * (4u * g + uint32_t(q));
+                const int3 lc = local_coord_of(l);
+                const int3 c = make_int3(bc.x * 8 + lc.x, bc.y * 8 + lc.y, bc.z * 8 + lc.z);
+                const uint32_t i = slot * BRICK_CELLS + l;
+                const bool in = in_grid(d, c);
+                t[q][6] = in ? d.cell_type[i] : 0u;
+#pragma unroll
+                for (int n = 0; n < 6; ++n)
+                    t[q][n] = (in && in_grid(d, add3(c, nbr_off(n)))) ? d.cell_type[l0_nbr(i, l, n, ns)] : 0u;
             }
-            m.word[slot * BRICK_CELLS + l] = uint8_t(w);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const uint32_t l = lane + 32u * (4u * g + uint32_t(q));
+                const int3 lc = local_coord_of(l);
+                const int3 c = make_int3(bc.x * 8 + lc.x, bc.y * 8 + lc.y, bc.z * 8 + lc.z);
+                uint32_t w = 0u;
+                if (in_grid(d, c)) {
+                    if ((t[q][6] & CELL_TYPE_MASK) == CELL_FLUID) w |= W_FLUID;
+                    if (is_red(c)) w |= W_RED;
+#pragma unroll
+                    for (int n = 0; n < 6; ++n)
+                        if ((t[q][n] & CELL_TYPE_MASK) == CELL_FLUID) w |= 1u << n;
+                }
+                m.word[slot * BRICK_CELLS + l] = uint8_t(w);
+            }
         }
     }
 }
@@ -1998,10 +2019,10 @@ int launch_mg_build_type(const Dev& d, const MGState& m, int l, cudaStream_t s) 
     return 1;
 }
 int launch_pcg_init(const Dev& d, const MGState& m, const float* p, const float* div, unsigned long long handle, const Shape& sh,
-                    cudaStream_t s) {
-    launch_k(k_pcg_words, sh.mg_ctas, GRID_THREADS, 0, s, d, m);
+                    cudaStream_t s, bool words) {
+    if (words) launch_k(k_pcg_words, sh.mg_ctas, GRID_THREADS, 0, s, d, m);
     launch_k(k_pcg_init, sh.mg_ctas, GRID_THREADS, 0, s, d, m, p, div, handle);
-    return 2;
+    return words ? 2 : 1;
 }
 
 size_t mg_tail_smem(const MGState& m) {
