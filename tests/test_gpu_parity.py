@@ -63,13 +63,27 @@ def test_tiny_dam_break_substeps(slosh, oracle_mod, solver):
     _run_frames(g, o, sc, frames=6)
 
 
-@pytest.mark.parametrize("n", [64, 96])
-def test_sparse_sphere_coarse_levels(slosh, oracle_mod, n):
+def test_tiny_over_relaxed_smoother(slosh, oracle_mod):
+    """The over-relaxed finest smoother on a hierarchy of only a few small levels (the tail and the coarsest
+    solve right below level 0), one sweep pair: bit-exact against the oracle."""
+    sc = scenes.tiny(slosh.settings_default, n=16)
+    sc["settings"].mg_smoother_weight = 1.3
+    g, o = _pair(slosh, oracle_mod, sc)
+    _run_frames(g, o, sc, frames=4)
+
+
+@pytest.mark.parametrize("n,tuned", [(64, False), (96, False), (100, True)])
+def test_sparse_sphere_coarse_levels(slosh, oracle_mod, n, tuned):
     """Sparse dam break + falling sphere large enough that MGPCG visits coarse levels through the
     active bricks' footprints (64^3: levels 1 and the single-CTA tail from level 2; 96^3: levels 1-2,
-    tail from level 3), bit-exact substep by substep."""
+    tail from level 3; 100^3: bricks cut by the grid's faces, so the footprint walks meet cells outside the
+    grid), bit-exact substep by substep; 100^3 with the benchmark's preconditioner (correction scale 1.9, two
+    sweep pairs, 4 coarsest iterations, finest sweeps over-relaxed by 1.15)."""
     sc = scenes.dam_break_sphere(slosh.settings_default, n=n)
     sc["settings"].max_substeps = 16
+    if tuned:
+        s = sc["settings"]
+        s.mg_correction_scale, s.mg_smoothing_sweeps, s.mg_coarse_iterations, s.mg_smoother_weight = 1.9, 2, 4, 1.15
     g, o = _pair(slosh, oracle_mod, sc)
     assert g.layout().num_mg_levels >= 4
     _run_frames(g, o, sc, frames=2)
