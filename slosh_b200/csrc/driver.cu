@@ -173,6 +173,7 @@ struct Ctx {
 
     // simulation state on the host
     uint32_t num_particles = 0;
+    uint64_t placed_since_sort = 0;  // particles emitted or uploaded since the last sort (in placement order)
     uint64_t total_emitted = 0, sim_frame = 0;
     uint32_t emit_seed = 1;
     float prev_dt = 0.0f, last_max_speed = 0.0f;
@@ -358,6 +359,7 @@ struct Ctx {
         compute_layout(s);
         alloc_particles(s.particle_capacity);
         num_particles = 0;
+        placed_since_sort = 0;
         const size_t tf = total_faces, pc = pool_cells;
         for (int i = 0; i < 3; ++i) vel[i] = dalloc<float>(tf, false);
         vmap[0] = 0; vmap[1] = 1; vmap[2] = 2;
@@ -604,12 +606,14 @@ struct Ctx {
         count(launch_emit(d, particles[pbuf], particle_count, em, uint32_t(cnt), bound, capacity, emit_seed++, stream));
         total_emitted += cnt;
         num_particles += uint32_t(cnt);
+        placed_since_sort += cnt;
     }
 
     void sort_particles() {
         PhaseScope ps(this, 0);
         count(launch_sort(dev(), sortb, particles[pbuf], particles[pbuf ^ 1], num_particles, num_sort_keys, sort_dim, stream));
         pbuf ^= 1;
+        placed_since_sort = 0;
     }
 
     // ---- MGPCG driver (AddPressureSolveMGPCG, SloshProxy.cpp:807-1020) ----
@@ -803,7 +807,8 @@ struct Ctx {
         float* V[3] = {vel[vmap[0]], vel[vmap[1]], vel[vmap[2]]};
         {
             PhaseScope ps(this, 2);
-            count(launch_p2g(d, P, particles[pbuf], num_particles, stream));
+            // more than an eighth of the particles in placement order: the wider P2G tile
+            count(launch_p2g(d, P, particles[pbuf], num_particles, placed_since_sort * 8u > num_particles, stream));
         }
         int c = 0;
         {
@@ -1413,6 +1418,7 @@ SLOSH_API slosh_status slosh_upload_particles(void* ctx, const slosh_particle_t*
         if (count)
             CK(cudaMemcpyAsync(c->particles[c->pbuf], particles, sizeof(slosh_particle_t) * count, cudaMemcpyHostToDevice, c->stream));
         c->num_particles = count;
+        c->placed_since_sort = count;
         uint32_t pcv[2] = {count, 0u};
         CK(cudaMemcpyAsync(c->particle_count, pcv, 8, cudaMemcpyHostToDevice, c->stream));
         c->h2d_bytes += sizeof(slosh_particle_t) * count + 8;
@@ -1548,6 +1554,7 @@ SLOSH_API slosh_status slosh_write_buffer(void* ctx, int32_t buffer_id, const vo
             if (n > c->capacity) throw StatusError{SLOSH_ERR_CAPACITY, "more particles than particle_capacity"};
             if (n) CK(cudaMemcpy(c->particles[c->pbuf], host_src, n * sizeof(slosh_particle_t), cudaMemcpyHostToDevice));
             c->num_particles = uint32_t(n);
+            c->placed_since_sort = n;
             return SLOSH_OK;
         }
         const BufView v = buffer_view(*c, buffer_id);

@@ -62,7 +62,8 @@ int launch_emit_reserve(uint32_t* particle_count, uint32_t count, cudaStream_t s
 int launch_emit(const Dev& d, slosh_particle_t* particles, const uint32_t* particle_count, const slosh_emit_request_t& em,
                 uint32_t count, uint32_t bound, uint32_t capacity, uint32_t seed, cudaStream_t s);
 int launch_touch_particles(const Dev& d, const slosh_particle_t* particles, uint32_t n, cudaStream_t s);
-int launch_p2g(const Dev& d, const Pass& p, const slosh_particle_t* particles, uint32_t n, cudaStream_t s);
+// unsorted: many particles were placed since the last sort (their order is emission order): the wider tile.
+int launch_p2g(const Dev& d, const Pass& p, const slosh_particle_t* particles, uint32_t n, bool unsorted, cudaStream_t s);
 int launch_g2p(const Dev& d, const Pass& p, slosh_particle_t* particles, uint32_t n, const float* vel, const float* disp,
                bool apply_density, cudaStream_t s);
 

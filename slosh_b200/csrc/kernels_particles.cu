@@ -121,8 +121,9 @@ __global__ void k_touch(Dev d, const slosh_particle_t* __restrict__ particles, u
 // Measured per 256^3 launch (sorted frames): 2 particles per thread with a 1,024-node tile (28 KB) and 48
 // registers (5 CTAs per SM) 0.769 ms (0.820 before the unchecked interior path and the merged flush; 0.975 with
 // the 2,048-node tile at 4 CTAs per SM), 0.857 with 4 particles per thread; 1 per thread at 6 CTAs per SM was
-// slower. In the three frames between a bulk emission and the first sort the particles are in emission order
-// and most CTA and warp boxes exceed the tile, so those launches take 1.2-1.4 ms on the direct path.
+// slower. In the frames between a bulk emission and the first sort the particles are in emission order and most
+// boxes exceed the 1,024-node tile (1.2-1.4 ms per launch on the direct path); the driver then launches the
+// 2,048-node tile, which fits them: 0.78-0.80 ms.
 constexpr int P2G_THREADS = 256;
 constexpr int P2G_WARPS = P2G_THREADS / 32;
 #ifndef P2G_MINB_ONE
@@ -133,10 +134,12 @@ constexpr int P2G_WARPS = P2G_THREADS / 32;
 #endif
 constexpr int P2G_PER_THREAD_DEFAULT = 2;
 // Tile capacity per CTA in nodes: a CTA of 2 particles per thread (512 particles, one 4^3 sort key of 8 per
-// cell) covers about 64 to 180 cells once sorted.
-template <int PER> struct P2GTile {
-    static constexpr int NODES = PER >= 4 ? 2048 : (PER == 2 ? 1024 : 512);
-    static constexpr int MINB = PER >= 4 ? 1 : (PER == 2 ? P2G_MINB_SMALL : P2G_MINB_ONE);
+// cell) covers about 64 to 180 cells once sorted. WIDE: the 2,048-node tile (56 KB, 4 CTAs per SM) for the frames
+// between a bulk emission and the next sort, whose emission-ordered runs of 512 particles span two or three rows
+// of cells (at 192^3, frame 2: 98.6 % of the CTA boxes fit 2,048 nodes, 10 % fit 1,024).
+template <int PER, bool WIDE = false> struct P2GTile {
+    static constexpr int NODES = (WIDE || PER >= 4) ? 2048 : (PER == 2 ? 1024 : 512);
+    static constexpr int MINB = WIDE ? 4 : (PER >= 4 ? 1 : (PER == 2 ? P2G_MINB_SMALL : P2G_MINB_ONE));
     static constexpr int SMEM = NODES * 7 * 4;  // momentum and weight of the 3 components + counts
 };
 
@@ -310,11 +313,11 @@ __device__ __forceinline__ void p2g_flush(const Dev& d, const P2GBox& b, const i
     }
 }
 
-template <int P2G_PER_THREAD>
-__global__ void __launch_bounds__(P2G_THREADS, P2GTile<P2G_PER_THREAD>::MINB) k_p2g(Dev d, Pass p, const slosh_particle_t* __restrict__ particles,
+template <int P2G_PER_THREAD, bool WIDE = false>
+__global__ void __launch_bounds__(P2G_THREADS, P2GTile<P2G_PER_THREAD, WIDE>::MINB) k_p2g(Dev d, Pass p, const slosh_particle_t* __restrict__ particles,
                                                                                  uint32_t n) {
     constexpr int CHUNK = P2G_THREADS * P2G_PER_THREAD;
-    constexpr int NODES = P2GTile<P2G_PER_THREAD>::NODES;
+    constexpr int NODES = P2GTile<P2G_PER_THREAD, WIDE>::NODES;
     constexpr int WARP_NODES = NODES / P2G_WARPS;
     extern __shared__ int p2g_smem[];  // [7][NODES]: momentum, weight of the 3 components, then counts
     __shared__ int s_box[6];
@@ -693,24 +696,25 @@ int launch_touch_particles(const Dev& d, const slosh_particle_t* particles, uint
     k_touch<<<(n + 255u) / 256u, 256, 0, s>>>(d, particles, n);
     return 1;
 }
-template <int PER>
+template <int PER, bool WIDE = false>
 void launch_p2g_per(const Dev& d, const Pass& p, const slosh_particle_t* particles, uint32_t n, cudaStream_t s) {
     static bool configured = false;
-    const int smem = P2GTile<PER>::SMEM;
+    const int smem = P2GTile<PER, WIDE>::SMEM;
     if (!configured) {
-        cudaFuncSetAttribute(k_p2g<PER>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaFuncSetAttribute(k_p2g<PER, WIDE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         configured = true;
     }
     const uint32_t chunk = uint32_t(P2G_THREADS * PER);
-    k_p2g<PER><<<(n + chunk - 1u) / chunk, P2G_THREADS, smem, s>>>(d, p, particles, n);
+    k_p2g<PER, WIDE><<<(n + chunk - 1u) / chunk, P2G_THREADS, smem, s>>>(d, p, particles, n);
 }
-int launch_p2g(const Dev& d, const Pass& p, const slosh_particle_t* particles, uint32_t n, cudaStream_t s) {
+int launch_p2g(const Dev& d, const Pass& p, const slosh_particle_t* particles, uint32_t n, bool unsorted, cudaStream_t s) {
     if (n == 0) return 0;
     static const int per = [] {
         const char* e = std::getenv("SLOSH_P2G_PER_THREAD");
         return e ? std::atoi(e) : P2G_PER_THREAD_DEFAULT;
     }();
-    if (per == 8) launch_p2g_per<8>(d, p, particles, n, s);
+    if (per == 2 && unsorted) launch_p2g_per<2, true>(d, p, particles, n, s);
+    else if (per == 8) launch_p2g_per<8>(d, p, particles, n, s);
     else if (per == 4) launch_p2g_per<4>(d, p, particles, n, s);
     else if (per == 1) launch_p2g_per<1>(d, p, particles, n, s);
     else launch_p2g_per<2>(d, p, particles, n, s);
