@@ -184,6 +184,14 @@ __device__ __forceinline__ void store_particle(slosh_particle_t* out, uint32_t i
     v[1] = make_float4(p.vel.x, p.vel.y, p.vel.z, __uint_as_float(c0));
     reinterpret_cast<uint4*>(v)[2] = make_uint4(c1, c2, c3, c4);
 }
+// The same record with the APIC rows already packed (c[0..4] as store_particle forms them).
+__device__ __forceinline__ void store_particle_packed(slosh_particle_t* out, uint32_t i, float3 pos, float age, float3 vel,
+                                                      const uint32_t (&c)[5]) {
+    float4* v = reinterpret_cast<float4*>(out + i);
+    v[0] = make_float4(pos.x, pos.y, pos.z, age);
+    v[1] = make_float4(vel.x, vel.y, vel.z, __uint_as_float(c[0]));
+    reinterpret_cast<uint4*>(v)[2] = make_uint4(c[1], c[2], c[3], c[4]);
+}
 __device__ __forceinline__ void store_dead(slosh_particle_t* out, uint32_t i) {  // DeadParticlePacked
     ParticleF p;
     p.pos = p.vel = p.cx = p.cy = p.cz = make_float3(0.0f, 0.0f, 0.0f);
