@@ -159,46 +159,42 @@ __device__ uint32_t block_scan_1024(uint32_t v, uint32_t* s_warp, uint32_t* tota
 // timing. Here the same stack discipline runs in ascending brick order through block scans: freed
 // slots are pushed in brick order, the j-th brick needing storage pops entry (free count - j), and
 // the active and new-slot lists come out in brick order. This is the serial (canonical) result.
-// Shared-memory budget of pool_update_smem: two byte planes and a bit plane of num_bricks.
+// Shared-memory budget of pool_update_smem: a byte plane and a bit plane of num_bricks.
 constexpr uint32_t POOL_SMEM_BRICKS = 100000u;
 
-// The pool update with its flags in shared memory (num_bricks <= POOL_SMEM_BRICKS): the wanted flags from the
-// separable dilation (one byte per brick) and whether each brick holds a slot (one bit per brick, from one
-// coalesced pass over the brick table), so the three ordered scans below read shared memory only and go to global
-// memory just for the bricks that change (freed slots, popped slots). Each thread owns the same contiguous run of
-// bricks in every phase, so the order is that of the reference-order loop over bricks.
+// Per brick (all CTAs, one thread each): bit 0 = wanted (touched within one brick: BrickAllocCS's 3x3x3 dilation),
+// bit 1 = holds a slot, into brick_want, for pool_update_smem's one CTA.
+__global__ void k_pool_flags(Dev d) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= d.num_bricks) return;
+    const int3 c = brick_coord_of(d, b);
+    const int bx = d.brick_dim.x, by = d.brick_dim.y, bz = d.brick_dim.z;
+    uint32_t touched = 0u;
+    for (int z = max(c.z - 1, 0); z <= min(c.z + 1, bz - 1); ++z)
+        for (int y = max(c.y - 1, 0); y <= min(c.y + 1, by - 1); ++y)
+            for (int x = max(c.x - 1, 0); x <= min(c.x + 1, bx - 1); ++x) touched |= d.brick_touch[uint32_t(x + bx * (y + by * z))];
+    d.brick_want[b] = (touched != 0u ? 1u : 0u) | (d.brick_table_w[b] != 0u ? 2u : 0u);
+}
+
+// The pool update with its flags in shared memory (num_bricks <= POOL_SMEM_BRICKS): the wanted flags (one byte per
+// brick) and whether each brick holds a slot (one bit per brick), both from k_pool_flags, so the three ordered scans
+// below read shared memory only and go to global memory just for the bricks that change (freed slots, popped
+// slots). Each thread owns the same contiguous run of bricks in every phase, so the order is that of the
+// reference-order loop over bricks.
 __device__ __forceinline__ void pool_update_smem(const Dev& d, uint8_t* s_flags, uint32_t* s_warp, uint32_t b0, uint32_t b1, int f0) {
     const uint32_t nb = d.num_bricks;
-    const int bx = d.brick_dim.x, by = d.brick_dim.y, bz = d.brick_dim.z;
-    uint8_t* a = s_flags;
-    uint8_t* t = s_flags + nb;
-    uint32_t* has = reinterpret_cast<uint32_t*>(s_flags + ((2u * nb + 3u) & ~3u));
+    uint8_t* t = s_flags;
+    uint32_t* has = reinterpret_cast<uint32_t*>(s_flags + ((nb + 3u) & ~3u));
     const uint32_t nwords = (nb + 31u) / 32u;
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    // Phase 1: wanted = touched within one brick (3x3x3 dilation); which bricks hold a slot.
-    for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) a[b] = d.brick_touch[b] != 0u ? 1 : 0;
+    // Phase 1: the wanted flags (touched within one brick, k_pool_flags' 3x3x3 dilation, bit 0 of brick_want) into
+    // bytes, and which bricks hold a slot (bit 1) into bits.
     for (uint32_t w = warp; w < nwords; w += blockDim.x / 32u) {
         const uint32_t b = w * 32u + lane;
-        const uint32_t bits = __ballot_sync(0xFFFFFFFFu, b < nb && d.brick_table_w[b] != 0u);
+        const uint32_t f = b < nb ? d.brick_want[b] : 0u;
+        if (b < nb) t[b] = uint8_t(f & 1u);
+        const uint32_t bits = __ballot_sync(0xFFFFFFFFu, (f & 2u) != 0u);
         if (lane == 0u) has[w] = bits;
-    }
-    __syncthreads();
-    for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) {  // x
-        const int x = int(b % uint32_t(bx));
-        t[b] = a[b] | (x > 0 ? a[b - 1] : 0) | (x + 1 < bx ? a[b + 1] : 0);
-    }
-    __syncthreads();
-    for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) {  // y
-        const int y = int((b / uint32_t(bx)) % uint32_t(by));
-        a[b] = t[b] | (y > 0 ? t[b - bx] : 0) | (y + 1 < by ? t[b + bx] : 0);
-    }
-    __syncthreads();
-    const uint32_t plane = uint32_t(bx * by);
-    for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) {  // z
-        const int z = int(b / plane);
-        const uint8_t w = a[b] | (z > 0 ? a[b - plane] : 0) | (z + 1 < bz ? a[b + plane] : 0);
-        t[b] = w;
-        d.brick_want[b] = w;
     }
     __syncthreads();
     auto want = [&](uint32_t b) -> bool { return t[b] != 0; };
@@ -919,11 +915,16 @@ __global__ void __launch_bounds__(GRID_THREADS) k_extrapolate(Dev d, const float
 }  // namespace
 
 int launch_pool_update(const Dev& d, cudaStream_t s) {
-    const uint32_t smem = d.num_bricks <= POOL_SMEM_BRICKS ? ((2u * d.num_bricks + 3u) & ~3u) + 4u * ((d.num_bricks + 31u) / 32u) : 0u;
+    const uint32_t smem = d.num_bricks <= POOL_SMEM_BRICKS ? ((d.num_bricks + 3u) & ~3u) + 4u * ((d.num_bricks + 31u) / 32u) : 0u;
     static uint32_t configured = 0;
     if (smem > 48u * 1024u && smem > configured) {
         cudaFuncSetAttribute(k_pool_update, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         configured = smem;
+    }
+    if (d.num_bricks <= POOL_SMEM_BRICKS) {
+        k_pool_flags<<<(d.num_bricks + 255u) / 256u, 256, 0, s>>>(d);
+        k_pool_update<<<1, 1024, smem, s>>>(d);
+        return 2;
     }
     k_pool_update<<<1, 1024, smem, s>>>(d);
     return 1;
