@@ -122,13 +122,13 @@ struct MGState {
     uint32_t flexible;          // flexible PCG: UpdatePR also reduces r_{k+1}.z_k into scalars[9]
     float smooth_weight;        // over-relaxation of level 0's red-black sweeps (mg_smoother_weight; 1 = reference)
 };
-int launch_mg_words(const MGState& m, int l, cudaStream_t s);
+int launch_mg_words(const Dev& d, const MGState& m, int l, const Shape& sh, cudaStream_t s);
 int launch_mg_tail_lists(const MGState& m, cudaStream_t s);
 size_t mg_tail_smem(const MGState& m);
 // First level handled by the single-CTA tail kernel of the V-cycle.
 int mg_tail_level(const MGState& m);
 int launch_mg_setup(const MGState& m, uint32_t limit, bool tol_mode, double tol, cudaStream_t s);
-int launch_mg_build_type(const Dev& d, const MGState& m, int l, cudaStream_t s);
+int launch_mg_build_type(const Dev& d, const MGState& m, int l, const Shape& sh, cudaStream_t s);
 // handle: the WHILE node's condition when the solve runs as a CUDA graph, 0 otherwise.
 int launch_pcg_init(const Dev& d, const MGState& m, const float* p, const float* div, unsigned long long handle, const Shape& sh,
                     cudaStream_t s, bool words = true);

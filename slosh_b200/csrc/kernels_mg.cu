@@ -466,11 +466,8 @@ __global__ void k_solve_setup(MGState m, uint32_t limit, uint32_t tol_mode, doub
 }
 
 // ---- MGBuildTypeCS: coarse cell = air if any child is air, else fluid if any child is fluid ---------------
-__global__ void k_build_type(Dev d, MGLevel fine, MGLevel coarse, int fine_is_pool) {
-    pdl_entry();
-    const uint32_t ci = blockIdx.x * blockDim.x + threadIdx.x;
-    if (ci >= coarse.cells) return;
-    const int3 c = coord3(ci, coarse.dim);
+__device__ __forceinline__ void build_type_cell(const Dev& d, const MGLevel& fine, const MGLevel& coarse, int fine_is_pool, uint32_t ci,
+                                                int3 c) {
     bool any_air = false, any_fluid = false;
 #pragma unroll
     for (int o = 0; o < 8; ++o) {
@@ -482,14 +479,22 @@ __global__ void k_build_type(Dev d, MGLevel fine, MGLevel coarse, int fine_is_po
     }
     coarse.type[ci] = any_air ? CELL_AIR : (any_fluid ? CELL_FLUID : CELL_SOLID);
 }
+__global__ void k_build_type(Dev d, MGLevel fine, MGLevel coarse, int fine_is_pool) {
+    pdl_entry();
+    const uint32_t ci = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ci >= coarse.cells) return;
+    build_type_cell(d, fine, coarse, fine_is_pool, ci, coord3(ci, coarse.dim));
+}
+// Levels 1-3 over the active bricks' footprints only; the rest of the level was cleared to air (0) before, which is
+// what the dense build gives cells over unallocated bricks (their fine cells are the null brick's air).
+__global__ void k_build_type_fp(Dev d, MGLevel fine, MGLevel coarse, int lc) {
+    pdl_entry();
+    for_footprint(d, coarse, lc, [&](uint32_t ci, int3 c) { build_type_cell(d, fine, coarse, lc == 1 ? 1 : 0, ci, c); });
+}
 
 // ---- coarse-level stencil words (once per solve, after the coarse types) -----------------------------------
 
-__global__ void k_level_words(MGLevel L) {
-    pdl_entry();
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= L.cells) return;
-    const int3 c = coord3(i, L.dim);
+__device__ __forceinline__ void level_word_cell(const MGLevel& L, uint32_t i, int3 c) {
     uint32_t w = (L.type[i] & CELL_TYPE_MASK) == CELL_FLUID ? CW_FLUID : 0u;
     if (is_red(c)) w |= CW_RED;
 #pragma unroll
@@ -501,6 +506,17 @@ __global__ void k_level_words(MGLevel L) {
         if (t != CELL_SOLID) w |= 1u << (CW_NONSOLID_SHIFT + n);
     }
     L.word[i] = uint16_t(w);
+}
+__global__ void k_level_words(MGLevel L) {
+    pdl_entry();
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= L.cells) return;
+    level_word_cell(L, i, coord3(i, L.dim));
+}
+// Levels 1-3: only the footprint cells' words are read (by the footprint passes and their neighbours' sums).
+__global__ void k_level_words_fp(Dev d, MGLevel L, int l) {
+    pdl_entry();
+    for_footprint(d, L, l, [&](uint32_t i, int3 c) { level_word_cell(L, i, c); });
 }
 // DiagEpsilon plus one per non-solid neighbour, added in neighbour order like FINE_STENCIL.
 __device__ __forceinline__ float word_diag(uint32_t w) {
@@ -2013,8 +2029,20 @@ int launch_mg_setup(const MGState& m, uint32_t limit, bool tol_mode, double tol,
     launch_k(k_solve_setup, 1, 1, 0, s, m, limit, tol_mode ? 1u : 0u, tol);
     return 1;
 }
-int launch_mg_build_type(const Dev& d, const MGState& m, int l, cudaStream_t s) {
+// Grid of a footprint walk over level l (1-3): one thread per footprint cell of the pool's capacity, capped at the
+// brick passes' width (a grid-stride loop).
+static int fp_grid(const Dev& d, const Shape& sh, int l) {
+    const uint64_t side = uint64_t(8 >> l);
+    const uint64_t cells = uint64_t(d.num_pool_bricks - 1u) * side * side * side;
+    return int(std::max<uint64_t>(1, std::min<uint64_t>(uint64_t(sh.brick_ctas), (cells + 255u) / 256u)));
+}
+int launch_mg_build_type(const Dev& d, const MGState& m, int l, const Shape& sh, cudaStream_t s) {
     const MGLevel& C = m.lv[l + 1];
+    if (l + 1 <= 3) {
+        cudaMemsetAsync(C.type, 0, size_t(C.cells) * sizeof(uint32_t), s);
+        launch_k(k_build_type_fp, fp_grid(d, sh, l + 1), 256, 0, s, d, m.lv[l], C, l + 1);
+        return 1;
+    }
     launch_k(k_build_type, blocks_for(C.cells, 256), 256, 0, s, d, m.lv[l], C, l == 0 ? 1 : 0);
     return 1;
 }
@@ -2030,8 +2058,9 @@ size_t mg_tail_smem(const MGState& m) {
     tail_offsets(m, mg_tail_level(m), -1, &total);
     return total;
 }
-int launch_mg_words(const MGState& m, int l, cudaStream_t s) {
-    launch_k(k_level_words, blocks_for(m.lv[l].cells, 256), 256, 0, s, m.lv[l]);
+int launch_mg_words(const Dev& d, const MGState& m, int l, const Shape& sh, cudaStream_t s) {
+    if (l <= 3) launch_k(k_level_words_fp, fp_grid(d, sh, l), 256, 0, s, d, m.lv[l], l);
+    else launch_k(k_level_words, blocks_for(m.lv[l].cells, 256), 256, 0, s, m.lv[l]);
     return 1;
 }
 int launch_mg_tail_lists(const MGState& m, cudaStream_t s) {
