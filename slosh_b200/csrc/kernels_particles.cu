@@ -118,10 +118,11 @@ __global__ void k_touch(Dev d, const slosh_particle_t* __restrict__ particles, u
 // measured 2.3 times slower than two 32-bit ones.) A particle whose 2x2x2 stencils all lie inside the grid (every particle the clamped
 // advection leaves, all but freshly placed ones at the walls) adds its 24 pairs without per-node tests: a zero
 // weight adds (0, 0).
-// Measured per 256^3 launch (sorted frames): 2 particles per thread with a 1,024-node tile (28 KB) and 48
-// registers (5 CTAs per SM) 0.769 ms (0.820 before the unchecked interior path and the merged flush; 0.975 with
-// the 2,048-node tile at 4 CTAs per SM), 0.857 with 4 particles per thread; 1 per thread at 6 CTAs per SM was
-// slower. In the frames between a bulk emission and the first sort the particles are in emission order and most
+// Measured per 256^3 launch (sorted frames): 2 particles per thread with a 1,024-node tile (28 KB), both records
+// loaded before the box reduction and held in registers (64 registers, 4 CTAs per SM) 0.739 ms; the same at 48
+// registers and 5 CTAs per SM (68 bytes of spills) 0.748, and reading the records again after the barrier at 5
+// CTAs per SM 0.767 (0.820 before the unchecked interior path and the merged flush; 0.975 with the 2,048-node
+// tile at 4 CTAs per SM); 0.857 with 4 particles per thread; 1 per thread at 6 CTAs per SM was slower. In the frames between a bulk emission and the first sort the particles are in emission order and most
 // boxes exceed the 1,024-node tile (1.2-1.4 ms per launch on the direct path); the driver then launches the
 // 2,048-node tile, which fits them: 0.78-0.80 ms.
 constexpr int P2G_THREADS = 256;
@@ -130,7 +131,7 @@ constexpr int P2G_WARPS = P2G_THREADS / 32;
 #define P2G_MINB_ONE 6
 #endif
 #ifndef P2G_MINB_SMALL
-#define P2G_MINB_SMALL 5  // 48 registers, 5 CTAs per SM with the small tile
+#define P2G_MINB_SMALL 4  // 64 registers, 4 CTAs per SM with the small tile
 #endif
 constexpr int P2G_PER_THREAD_DEFAULT = 2;
 // Tile capacity per CTA in nodes: a CTA of 2 particles per thread (512 particles, one 4^3 sort key of 8 per
@@ -313,6 +314,19 @@ __device__ __forceinline__ void p2g_flush(const Dev& d, const P2GBox& b, const i
     }
 }
 
+// f(k) for k = 0 .. N - 1 until it returns false; unrolled where per-k registers are indexed by k.
+template <bool UNROLL, int N, class F>
+__device__ __forceinline__ void for_each_k(F f) {
+    if constexpr (UNROLL) {
+#pragma unroll
+        for (int k = 0; k < N; ++k)
+            if (!f(k)) break;
+    } else {
+        for (int k = 0; k < N; ++k)
+            if (!f(k)) break;
+    }
+}
+
 template <int P2G_PER_THREAD, bool WIDE = false>
 __global__ void __launch_bounds__(P2G_THREADS, P2GTile<P2G_PER_THREAD, WIDE>::MINB) k_p2g(Dev d, Pass p, const slosh_particle_t* __restrict__ particles,
                                                                                  uint32_t n) {
@@ -327,15 +341,28 @@ __global__ void __launch_bounds__(P2G_THREADS, P2GTile<P2G_PER_THREAD, WIDE>::MI
     if (threadIdx.x < 3) { s_box[threadIdx.x] = big; s_box[3 + threadIdx.x] = -big; }
     __syncthreads();
     int3 wmn = make_int3(big, big, big), wmx = make_int3(-big, -big, -big);  // this warp's cell box
-    for (int k = 0; k < P2G_PER_THREAD; ++k) {
+    // HOLD: the whole records are loaded here and kept in registers across the barrier, so their latency
+    // overlaps the box reduction; otherwise only the positions, and the records are read again below.
+    constexpr bool HOLD = P2G_PER_THREAD <= 2;
+    constexpr int NH = HOLD ? P2G_PER_THREAD : 1;
+    float4 ha[NH], hb[NH];
+    uint4 hc[NH];
+    for_each_k<HOLD, P2G_PER_THREAD>([&](int k) {
         const uint32_t i = first + uint32_t(k);
-        if (i >= n) break;
-        const float4 a = __ldg(reinterpret_cast<const float4*>(particles + i));
-        if (is_dead_age(a.w)) continue;
+        if (i >= n) return false;
+        float4 a;
+        if constexpr (HOLD) {
+            load_particle_raw(particles, i, ha[k], hb[k], hc[k]);
+            a = ha[k];
+        } else {
+            a = __ldg(reinterpret_cast<const float4*>(particles + i));
+        }
+        if (is_dead_age(a.w)) return true;
         const int3 c = p2g_cell(d, make_float3(a.x, a.y, a.z));
         wmn = make_int3(min(wmn.x, c.x), min(wmn.y, c.y), min(wmn.z, c.z));
         wmx = make_int3(max(wmx.x, c.x), max(wmx.y, c.y), max(wmx.z, c.z));
-    }
+        return true;
+    });
     wmn.x = __reduce_min_sync(0xFFFFFFFFu, wmn.x); wmn.y = __reduce_min_sync(0xFFFFFFFFu, wmn.y); wmn.z = __reduce_min_sync(0xFFFFFFFFu, wmn.z);
     wmx.x = __reduce_max_sync(0xFFFFFFFFu, wmx.x); wmx.y = __reduce_max_sync(0xFFFFFFFFu, wmx.y); wmx.z = __reduce_max_sync(0xFFFFFFFFu, wmx.z);
     if (lane == 0 && wmn.x <= wmx.x) {
@@ -348,16 +375,23 @@ __global__ void __launch_bounds__(P2G_THREADS, P2GTile<P2G_PER_THREAD, WIDE>::MI
     // The CTA's box in the whole tile (block-uniform), else this warp's box in its eighth (warp-uniform).
     P2GBox b;
     const bool cta = p2g_box(make_int3(s_box[0], s_box[1], s_box[2]), make_int3(s_box[3], s_box[4], s_box[5]), NODES, b);
+    auto record = [&](int k, uint32_t i, float4& ra, float4& rb, uint4& rc) {
+        if constexpr (HOLD) {
+            ra = ha[k]; rb = hb[k]; rc = hc[k];
+        } else {
+            load_particle_raw(particles, i, ra, rb, rc);
+        }
+    };
     if (!cta && !p2g_box(wmn, wmx, WARP_NODES, b)) {
-        for (int k = 0; k < P2G_PER_THREAD; ++k) {
+        for_each_k<HOLD, P2G_PER_THREAD>([&](int k) {
             const uint32_t i = first + uint32_t(k);
-            if (i >= n) break;
+            if (i >= n) return false;
             float4 ra, rb;
             uint4 rc;
-            load_particle_raw(particles, i, ra, rb, rc);
-            if (is_dead_age(ra.w)) continue;
-            p2g_particle_global(d, apic, unpack_particle(ra, rb, rc));
-        }
+            record(k, i, ra, rb, rc);
+            if (!is_dead_age(ra.w)) p2g_particle_global(d, apic, unpack_particle(ra, rb, rc));
+            return true;
+        });
         return;
     }
     int* tile = p2g_smem + (cta ? 0 : warp * WARP_NODES);  // this CTA's or warp's tile
@@ -368,15 +402,15 @@ __global__ void __launch_bounds__(P2G_THREADS, P2GTile<P2G_PER_THREAD, WIDE>::MI
     if (cta) __syncthreads();
     else __syncwarp();
     const uint32_t tile_s = uint32_t(__cvta_generic_to_shared(tile));
-    for (int k = 0; k < P2G_PER_THREAD; ++k) {
+    for_each_k<HOLD, P2G_PER_THREAD>([&](int k) {
         const uint32_t i = first + uint32_t(k);
-        if (i >= n) break;
+        if (i >= n) return false;
         float4 ra, rb;
         uint4 rc;
-        load_particle_raw(particles, i, ra, rb, rc);
-        if (is_dead_age(ra.w)) continue;
-        p2g_particle_tile(d, apic, unpack_particle(ra, rb, rc), b, tile_s, NODES);
-    }
+        record(k, i, ra, rb, rc);
+        if (!is_dead_age(ra.w)) p2g_particle_tile(d, apic, unpack_particle(ra, rb, rc), b, tile_s, NODES);
+        return true;
+    });
     if (cta) __syncthreads();
     else __syncwarp();
     p2g_flush(d, b, tile, NODES, cta ? int(threadIdx.x) : lane, cta ? P2G_THREADS : 32);
