@@ -542,8 +542,8 @@ __device__ __forceinline__ float3 sample_displacement(const Dev& d, float3 xp, c
 constexpr int G2P_THREADS = 256;
 // The new particle record is written once and read again only by the next substep's passes, after the grid
 // passes in between: cache-streaming (evict-first) stores keep it from displacing the face velocities the
-// gathers reuse (0.993 -> 0.982 ms per 256^3 launch; cache-streaming loads of the record measured 0.996, and
-// in P2G, whose records are read once too, 0.741 against 0.739).
+// gathers reuse (0.993 -> 0.982 ms per 256^3 launch). Loading the record without an L1 allocation or evict-first
+// in L2 was slower, here (0.996-0.998 ms) and in P2G (0.741-0.774 against 0.740 ms).
 __device__ __forceinline__ void g2p_store(slosh_particle_t* out, uint32_t i, float3 pos, float age, float3 vel, const uint32_t (&c)[5]) {
     float4* v = reinterpret_cast<float4*>(out + i);
     __stcs(v, make_float4(pos.x, pos.y, pos.z, age));
