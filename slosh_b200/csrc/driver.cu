@@ -38,6 +38,14 @@ int warm_start(Net* net, const Dev& d, const float* divergence, float* pressure,
 
 namespace slosh {
 namespace {
+// P2G as a per-brick gather instead of the shared-memory scatter (SLOSH_P2G_GATHER=1; read once per process).
+bool p2g_gather_enabled() {
+    static const bool on = [] {
+        const char* e = std::getenv("SLOSH_P2G_GATHER");
+        return e != nullptr && std::atoi(e) != 0;
+    }();
+    return on;
+}
 
 thread_local std::string g_error;
 
@@ -162,6 +170,7 @@ struct Ctx {
     slosh_manipulator_t* manipulators_d = nullptr;
     uint32_t* particle_count = nullptr;
     SortBuffers sortb{};
+    P2GGather gather{};  // the per-cell particle index of the gather P2G (allocated only when it is on)
     MGState mg{};
 
     // pinned host staging
@@ -349,6 +358,11 @@ struct Ctx {
         sortb.tile_hist = dalloc<uint32_t>(sortb.tile_hist_capacity, true);
         sortb.scan_tmp_capacity = sort_scan_tmp_size(cap, num_sort_keys);
         sortb.scan_tmp = dalloc<uint32_t>(sortb.scan_tmp_capacity, true);
+        if (p2g_gather_enabled()) {
+            gather.rank = dalloc<uint32_t>(cap, true);
+            gather.index = dalloc<uint32_t>(cap, true);
+            gather.overflow = dalloc<uint32_t>(size_t(cap) + 1u, true);
+        }
         pbuf = 0;
     }
 
@@ -370,6 +384,10 @@ struct Ctx {
         face_weight = dalloc<float>(tf, false);
         cell_type = dalloc<uint32_t>(pc, false);
         cell_count = dalloc<int32_t>(pc, false);
+        if (p2g_gather_enabled()) {
+            gather.offsets = dalloc<uint32_t>(pc, false);
+            gather.scan_tmp = dalloc<uint32_t>(exclusive_scan_tmp_size(pc), false);
+        }
         pressure = dalloc<float>(pc, false);
         divergence = dalloc<float>(pc, false);
         cell_diag = dalloc<float>(pc, false);
@@ -807,8 +825,12 @@ struct Ctx {
         float* V[3] = {vel[vmap[0]], vel[vmap[1]], vel[vmap[2]]};
         {
             PhaseScope ps(this, 2);
-            // more than an eighth of the particles in placement order: the wider P2G tile
-            count(launch_p2g(d, P, particles[pbuf], num_particles, placed_since_sort * 8u > num_particles, stream));
+            if (p2g_gather_enabled()) {
+                count(launch_p2g_gather(d, P, gather, particles[pbuf], num_particles, stream));
+            } else {
+                // more than an eighth of the particles in placement order: the wider P2G tile
+                count(launch_p2g(d, P, particles[pbuf], num_particles, placed_since_sort * 8u > num_particles, stream));
+            }
         }
         int c = 0;
         {

@@ -66,6 +66,20 @@ int launch_touch_particles(const Dev& d, const slosh_particle_t* particles, uint
 int launch_p2g(const Dev& d, const Pass& p, const slosh_particle_t* particles, uint32_t n, bool unsorted, cudaStream_t s);
 int launch_g2p(const Dev& d, const Pass& p, slosh_particle_t* particles, uint32_t n, const float* vel, const float* disp,
                bool apply_density, cudaStream_t s);
+// P2G as a per-brick gather (opt-in, SLOSH_P2G_GATHER=1): a per-cell particle index rebuilt every launch (counts
+// into cell_count with the rank of each particle in its cell, an exclusive scan, a scatter of particle ids), then
+// one CTA per active brick that visits the particles of the brick's cells and of the one-cell layer around it and
+// writes the brick's 512 nodes x 6 sums with plain stores. Particles in cells of unallocated bricks (pool
+// overflow) are added by a last pass with global adds.
+struct P2GGather {
+    uint32_t* rank;      // capacity: rank of the particle within its cell (~0u: dead or in an unallocated brick)
+    uint32_t* index;     // capacity: particle ids in pool-cell order
+    uint32_t* offsets;   // pool cells: exclusive scan of the counts
+    uint32_t* overflow;  // capacity + 1: [0] count, then the ids of live particles in unallocated bricks
+    uint32_t* scan_tmp;  // exclusive_scan_tmp_size(pool cells)
+};
+int launch_p2g_gather(const Dev& d, const Pass& p, const P2GGather& g, const slosh_particle_t* particles, uint32_t n,
+                      cudaStream_t s);
 
 // ---- spatial sort (SloshSort.usf) ----
 struct SortBuffers {

@@ -416,6 +416,145 @@ __global__ void __launch_bounds__(P2G_THREADS, P2GTile<P2G_PER_THREAD, WIDE>::MI
     p2g_flush(d, b, tile, NODES, cta ? int(threadIdx.x) : lane, cta ? P2G_THREADS : 32);
 }
 
+// ---- P2G as a per-brick gather (opt-in) -------------------------------------------------------------------
+// The index: each live particle's rank in its cell from warp-aggregated adds into cell_count (which are P2G's
+// particle counts themselves), an exclusive scan of the counts over the pool cells, and a scatter of the particle
+// ids into pool-cell order. Particles in cells of unallocated bricks go to the overflow list instead.
+__global__ void __launch_bounds__(256) k_gather_count(Dev d, const slosh_particle_t* __restrict__ particles, uint32_t n, P2GGather g) {
+    const uint32_t i = blockIdx.x * 256u + threadIdx.x;
+    uint32_t ci = 0xFFFFFFFFu;  // no cell: out of range, dead, or in an unallocated brick
+    if (i < n) {
+        const float4 a = __ldg(reinterpret_cast<const float4*>(particles + i));
+        if (!is_dead_age(a.w)) {
+            const uint32_t c = cell_index(d, p2g_cell(d, make_float3(a.x, a.y, a.z)));
+            if (is_null_cell(c)) {
+                const uint32_t k = atomicAdd(g.overflow, 1u);
+                g.overflow[1u + k] = i;
+            } else {
+                ci = c;
+            }
+        }
+    }
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t peers = __match_any_sync(0xFFFFFFFFu, ci);
+    const uint32_t leader = uint32_t(__ffs(int(peers))) - 1u;
+    uint32_t base = 0u;
+    if (ci != 0xFFFFFFFFu && lane == leader) base = uint32_t(atomicAdd(d.cell_count + ci, __popc(peers)));
+    base = __shfl_sync(0xFFFFFFFFu, base, int(leader));
+    if (i < n) g.rank[i] = ci != 0xFFFFFFFFu ? base + uint32_t(__popc(peers & ((1u << lane) - 1u))) : 0xFFFFFFFFu;
+}
+__global__ void __launch_bounds__(256) k_gather_scatter(Dev d, const slosh_particle_t* __restrict__ particles, uint32_t n, P2GGather g) {
+    const uint32_t i = blockIdx.x * 256u + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t r = g.rank[i];
+    if (r == 0xFFFFFFFFu) return;
+    const float4 a = __ldg(reinterpret_cast<const float4*>(particles + i));
+    const uint32_t ci = cell_index(d, p2g_cell(d, make_float3(a.x, a.y, a.z)));
+    g.index[g.offsets[ci] + r] = i;
+}
+
+// The contributions of one particle to the nodes of brick bc only (node coordinates in [8 bc, 8 bc + 7] and inside
+// the grid), added to a 6 x 512 tile: the momentum of component a at local node l is the word at shared address
+// tile + 4 (2 a 512 + l), its weight the word at tile + 4 ((2 a + 1) 512 + l). The factors and roundings are
+// p2g_particle_tile's, so each node receives the same integers as from the scatter (integer sums: any order).
+__device__ __forceinline__ void p2g_particle_brick(const Dev& d, bool apic, const ParticleF& part, int3 bc, uint32_t tile) {
+    const float inv_h = d.inv_h, h = d.h;
+#pragma unroll
+    for (int axis = 0; axis < 3; ++axis) {
+        const float3 cp = apic ? (axis == 0 ? part.cx : (axis == 1 ? part.cy : part.cz)) : make_float3(0.0f, 0.0f, 0.0f);
+        const float up = compf(part.vel, axis);
+        const float ox = axis == 0 ? 0.0f : 0.5f, oy = axis == 1 ? 0.0f : 0.5f, oz = axis == 2 ? 0.0f : 0.5f;
+        const float gx = part.pos.x * inv_h - ox, gy = part.pos.y * inv_h - oy, gz = part.pos.z * inv_h - oz;
+        const int3 base = make_int3(int(floorf(gx)), int(floorf(gy)), int(floorf(gz)));
+        const float fx = gx - float(base.x), fy = gy - float(base.y), fz = gz - float(base.z);
+        const float wx[2] = {1.0f - fx, fx}, wy[2] = {1.0f - fy, fy}, wz[2] = {1.0f - fz, fz};
+        float px[2], py[2], pz[2];
+        bool inx[2], iny[2], inz[2];
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            px[j] = cp.x * ((float(base.x + j) + ox) * h - part.pos.x);
+            py[j] = cp.y * ((float(base.y + j) + oy) * h - part.pos.y);
+            pz[j] = cp.z * ((float(base.z + j) + oz) * h - part.pos.z);
+            inx[j] = ((base.x + j) >> 3) == bc.x && base.x + j < d.grid.x;
+            iny[j] = ((base.y + j) >> 3) == bc.y && base.y + j < d.grid.y;
+            inz[j] = ((base.z + j) >> 3) == bc.z && base.z + j < d.grid.z;
+        }
+        const float upx[2] = {up + px[0], up + px[1]};
+        const uint32_t t = tile + 4u * uint32_t(2 * axis * BRICK_CELLS);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int oiy = q & 1, oiz = q >> 1;
+            if (!(iny[oiy] && inz[oiz])) continue;
+            const float wyzs = (wy[oiy] * wz[oiz]) * P2G_FIXED_SCALE;
+            const float pyz = py[oiy] + pz[oiz];
+#pragma unroll
+            for (int oix = 0; oix < 2; ++oix) {
+                if (!inx[oix]) continue;
+                const float ws = wx[oix] * wyzs;
+                const uint32_t l = uint32_t(((base.x + oix) & 7) + 8 * ((base.y + oiy) & 7) + 64 * ((base.z + oiz) & 7));
+                red_shared_add_u32(t + 4u * l, uint32_t(__float2int_rn(ws * (upx[oix] + pyz))));
+                red_shared_add_u32(t + 4u * (uint32_t(BRICK_CELLS) + l), uint32_t(__float2int_rn(ws)));
+            }
+        }
+    }
+}
+
+// One CTA per active brick at a time (grid-stride): the particles of the 10 x 10 x 10 cells around the brick (its
+// own 8^3 and the one-cell layer of its neighbours; a row of cells in one brick is one contiguous index range)
+// add into a shared tile, which is then stored over the brick's nodes. No global atomics.
+constexpr int P2GG_THREADS = 256;
+__global__ void __launch_bounds__(P2GG_THREADS) k_p2g_gather(Dev d, Pass p, const slosh_particle_t* __restrict__ particles, P2GGather g) {
+    __shared__ int tile[6 * BRICK_CELLS];
+    const uint32_t tile_s = uint32_t(__cvta_generic_to_shared(tile));
+    const bool apic = p.use_apic != 0;
+    const uint32_t active = d.active_bricks[0];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    for (uint32_t e = blockIdx.x; e < active; e += gridDim.x) {
+        const uint32_t brick = d.active_bricks[1u + e];
+        const uint32_t slot = __ldg(d.brick_table + brick);
+        const int3 bc = brick_coord_of(d, brick);
+        for (uint32_t t = threadIdx.x; t < 6u * BRICK_CELLS; t += P2GG_THREADS) tile[t] = 0;
+        __syncthreads();
+        for (uint32_t row = warp; row < 100u; row += P2GG_THREADS / 32) {
+            const int y = bc.y * 8 - 1 + int(row % 10u), z = bc.z * 8 - 1 + int(row / 10u);
+            if (y < 0 || z < 0 || y >= d.grid.y || z >= d.grid.z) continue;
+            for (int sg = 0; sg < 3; ++sg) {
+                const int x0 = sg == 0 ? bc.x * 8 - 1 : (sg == 1 ? bc.x * 8 : bc.x * 8 + 8);
+                const int x1 = sg == 1 ? min(bc.x * 8 + 7, d.grid.x - 1) : x0;
+                if (x0 < 0 || x0 >= d.grid.x) continue;
+                const uint32_t s2 = __ldg(d.brick_table + brick_index_of(d, make_int3(x0 >> 3, y >> 3, z >> 3)));
+                if (s2 == 0u) continue;  // an unallocated brick: its particles are in the overflow list
+                const uint32_t c0 = s2 * BRICK_CELLS + local_index_of(make_int3(x0, y, z));
+                const uint32_t c1 = c0 + uint32_t(x1 - x0);
+                const uint32_t start = g.offsets[c0], end = g.offsets[c1] + uint32_t(d.cell_count[c1]);
+                for (uint32_t j = start + lane; j < end; j += 32u) {
+                    float4 ra, rb;
+                    uint4 rc;
+                    load_particle_raw(particles, g.index[j], ra, rb, rc);
+                    p2g_particle_brick(d, apic, unpack_particle(ra, rb, rc), bc, tile_s);
+                }
+            }
+        }
+        __syncthreads();
+        for (uint32_t t = threadIdx.x; t < 6u * BRICK_CELLS; t += P2GG_THREADS) {
+            const uint32_t q = t / uint32_t(BRICK_CELLS), l = t % uint32_t(BRICK_CELLS);
+            d.accum[(q & 1u) * d.total_faces + (q >> 1) * d.pool_cells + slot * BRICK_CELLS + l] = tile[t];
+        }
+        __syncthreads();
+    }
+}
+// Particles in cells of unallocated bricks (pool overflow): their contributions to allocated bricks by global adds.
+__global__ void __launch_bounds__(256) k_p2g_overflow(Dev d, Pass p, const slosh_particle_t* __restrict__ particles, P2GGather g) {
+    const uint32_t count = g.overflow[0];
+    const bool apic = p.use_apic != 0;
+    for (uint32_t k = blockIdx.x * 256u + threadIdx.x; k < count; k += gridDim.x * 256u) {
+        float4 ra, rb;
+        uint4 rc;
+        load_particle_raw(particles, g.overflow[1u + k], ra, rb, rc);
+        p2g_particle_global(d, apic, unpack_particle(ra, rb, rc));
+    }
+}
+
 // ---- G2P + advection ---------------------------------------------------------------------------------
 struct Stencil {
     int3 base;
@@ -767,6 +906,24 @@ int launch_p2g(const Dev& d, const Pass& p, const slosh_particle_t* particles, u
     else if (per == 1) launch_p2g_per<1>(d, p, particles, n, s);
     else launch_p2g_per<2>(d, p, particles, n, s);
     return 1;
+}
+int launch_p2g_gather(const Dev& d, const Pass& p, const P2GGather& g, const slosh_particle_t* particles, uint32_t n,
+                      cudaStream_t s) {
+    if (n == 0) return 0;
+    static const int sms = [] {
+        int dev = 0, v = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+        return v;
+    }();
+    cudaMemsetAsync(g.overflow, 0, 4, s);
+    const uint32_t blocks = (n + 255u) / 256u;
+    k_gather_count<<<blocks, 256, 0, s>>>(d, particles, n, g);
+    const int scans = launch_exclusive_scan(reinterpret_cast<const uint32_t*>(d.cell_count), g.offsets, d.pool_cells, g.scan_tmp, s);
+    k_gather_scatter<<<blocks, 256, 0, s>>>(d, particles, n, g);
+    k_p2g_gather<<<sms * 8, P2GG_THREADS, 0, s>>>(d, p, particles, g);  // 8 CTAs of 12 KB per SM
+    k_p2g_overflow<<<sms, 256, 0, s>>>(d, p, particles, g);
+    return 4 + scans;
 }
 int launch_g2p(const Dev& d, const Pass& p, slosh_particle_t* particles, uint32_t n, const float* vel, const float* disp,
                bool apply_density, cudaStream_t s) {

@@ -226,6 +226,23 @@ def test_preconditioner_options(slosh, oracle_mod, scale, sweeps, flexible, mode
     assert g.results().last_solve_rel_residual <= 1e-6
 
 
+def test_gather_p2g_matches_oracle():
+    """P2G as a per-brick gather (SLOSH_P2G_GATHER=1, read once per process: a per-cell particle index, then one CTA
+    per brick over the particles of its cells and of the one-cell layer around it, no global atomics): the parity
+    tests that reach P2G's edge cases run in a child process on the gather path, bit-exact against the oracle --
+    bricks cut by the grid's faces (100^3), particles left in unallocated bricks (pool overflow), colliders, the
+    64^3 dam break, the RBGS and MGPCG tiny scenes."""
+    import subprocess
+    import sys
+    here = os.path.dirname(os.path.abspath(__file__))
+    sel = "tiny_dam_break or sparse_sphere or pool_overflow or collider or dam_break_64 or emission"
+    r = subprocess.run([sys.executable, "-m", "pytest", "-x", "-q", "-m", "gpu", "-p", "no:cacheprovider",
+                        os.path.join(here, "test_gpu_parity.py"), "-k", sel],
+                       env=dict(os.environ, SLOSH_P2G_GATHER="1"), capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-2000:]
+    assert " passed" in r.stdout and " failed" not in r.stdout, r.stdout[-2000:]
+
+
 @pytest.mark.parametrize("env", [{"SLOSH_MG_STAGED": "1"}, {"SLOSH_MG_CLUSTER": "2"}, {"SLOSH_PDL": "0"}],
                          ids=["staged_level0", "cluster_levels", "no_pdl"])
 def test_alternative_solver_paths_give_identical_results(slosh, env):
