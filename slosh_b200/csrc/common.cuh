@@ -44,6 +44,7 @@ struct Dev {
     uint32_t* free_slots;
     uint32_t* brick_touch;
     uint32_t* brick_want;
+    uint32_t* pool_scratch;  // the pool update's per-CTA counts and offsets (pool_scratch_words(num_bricks))
     uint32_t* new_slots;
     uint32_t* active_bricks;
     // cells

@@ -163,7 +163,7 @@ struct Ctx {
     int32_t* cell_count = nullptr;
     float *pressure = nullptr, *divergence = nullptr, *cell_diag = nullptr, *density_q = nullptr, *density_rhs = nullptr;
     uint32_t *brick_table = nullptr, *slot_brick = nullptr, *free_slots = nullptr, *brick_touch = nullptr;
-    uint32_t *brick_want = nullptr, *new_slots = nullptr, *active_bricks = nullptr;
+    uint32_t *brick_want = nullptr, *new_slots = nullptr, *active_bricks = nullptr, *pool_scratch = nullptr;
     uint32_t* stats = nullptr;
     int32_t* coupling = nullptr;
     slosh_collider_t* colliders_d = nullptr;
@@ -400,6 +400,7 @@ struct Ctx {
         brick_table = dalloc<uint32_t>(num_bricks, false);
         brick_touch = dalloc<uint32_t>(num_bricks, false);
         brick_want = dalloc<uint32_t>(num_bricks, false);
+        pool_scratch = dalloc<uint32_t>(pool_scratch_words(num_bricks), false);
         new_slots = dalloc<uint32_t>(num_pool_bricks + 1u, false);
         slot_brick = dalloc<uint32_t>(num_pool_bricks, false);
         free_slots = dalloc<uint32_t>(num_pool_bricks, false);
@@ -525,6 +526,7 @@ struct Ctx {
         d.free_slots = free_slots;
         d.brick_touch = brick_touch;
         d.brick_want = brick_want;
+        d.pool_scratch = pool_scratch;
         d.new_slots = new_slots;
         d.active_bricks = active_bricks;
         d.cell_type = cell_type;

@@ -39,6 +39,7 @@ inline cudaError_t launch_k(void (*k)(P...), dim3 grid, dim3 block, size_t smem,
 
 // ---- brick pool (Slosh.usf:1719-1831) ----
 int launch_pool_update(const Dev& d, cudaStream_t s);
+size_t pool_scratch_words(uint32_t num_bricks);
 int launch_clear_new_slots(const Dev& d, const Shape& sh, cudaStream_t s);
 
 // ---- grid passes ----

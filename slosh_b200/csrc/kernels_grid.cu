@@ -154,183 +154,81 @@ __device__ uint32_t block_scan_1024(uint32_t v, uint32_t* s_warp, uint32_t* tota
     return excl;
 }
 
-// ---- brick pool: BrickFreeCS + BrickAllocCS + PoolArgsCS in one CTA ------------------------------
-// The reference pushes and pops the free stack with atomics, so slot assignment depends on thread
-// timing. Here the same stack discipline runs in ascending brick order through block scans: freed
-// slots are pushed in brick order, the j-th brick needing storage pops entry (free count - j), and
-// the active and new-slot lists come out in brick order. This is the serial (canonical) result.
-// Shared-memory budget of pool_update_smem: a byte plane and a bit plane of num_bricks.
-constexpr uint32_t POOL_SMEM_BRICKS = 100000u;
+// ---- brick pool: BrickFreeCS + BrickAllocCS + PoolArgsCS -------------------------------------------------
+// The reference pushes and pops the free stack with atomics, so slot assignment depends on thread timing. Here
+// the same stack discipline runs in ascending brick order through scans: freed slots are pushed in brick order,
+// the j-th brick needing storage pops entry (free count - j), and the active and new-slot lists come out in brick
+// order. This is the serial (canonical) result. Four launches, one thread per brick in CTAs of 1,024 bricks:
+//   k_pool_flags  wanted (touched within one brick: BrickAllocCS's 3x3x3 dilation) and held flags per brick, and
+//                 each CTA's counts of bricks that free, need and keep a slot;
+//   k_pool_plan   one CTA: the CTAs' exclusive offsets of the three counts, the stack's new top, the lists'
+//                 lengths and the statistics;
+//   k_pool_free   freed slots pushed at their offsets;
+//   k_pool_alloc  slots popped in brick order (the pushes are complete), the active list, touch flags consumed.
+// pool_scratch: [c] frees, [n + c] needs, [2n + c] keeps of CTA c (n CTAs), then the three offsets the same way,
+// then the stack's old and new top.
+constexpr uint32_t POOL_CTA = 1024u;
+__device__ __forceinline__ uint32_t pool_ctas(uint32_t nb) { return (nb + POOL_CTA - 1u) / POOL_CTA; }
 
-// Per brick (all CTAs, one thread each): bit 0 = wanted (touched within one brick: BrickAllocCS's 3x3x3 dilation),
-// bit 1 = holds a slot, into brick_want, for pool_update_smem's one CTA.
-__global__ void k_pool_flags(Dev d) {
-    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= d.num_bricks) return;
-    const int3 c = brick_coord_of(d, b);
-    const int bx = d.brick_dim.x, by = d.brick_dim.y, bz = d.brick_dim.z;
-    uint32_t touched = 0u;
-    for (int z = max(c.z - 1, 0); z <= min(c.z + 1, bz - 1); ++z)
-        for (int y = max(c.y - 1, 0); y <= min(c.y + 1, by - 1); ++y)
-            for (int x = max(c.x - 1, 0); x <= min(c.x + 1, bx - 1); ++x) touched |= d.brick_touch[uint32_t(x + bx * (y + by * z))];
-    d.brick_want[b] = (touched != 0u ? 1u : 0u) | (d.brick_table_w[b] != 0u ? 2u : 0u);
-}
-
-// The pool update with its flags in shared memory (num_bricks <= POOL_SMEM_BRICKS): the wanted flags (one byte per
-// brick) and whether each brick holds a slot (one bit per brick), both from k_pool_flags, so the three ordered scans
-// below read shared memory only and go to global memory just for the bricks that change (freed slots, popped
-// slots). Each thread owns the same contiguous run of bricks in every phase, so the order is that of the
-// reference-order loop over bricks.
-__device__ __forceinline__ void pool_update_smem(const Dev& d, uint8_t* s_flags, uint32_t* s_warp, uint32_t b0, uint32_t b1, int f0) {
-    const uint32_t nb = d.num_bricks;
-    uint8_t* t = s_flags;
-    uint32_t* has = reinterpret_cast<uint32_t*>(s_flags + ((nb + 3u) & ~3u));
-    const uint32_t nwords = (nb + 31u) / 32u;
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    // Phase 1: the wanted flags (touched within one brick, k_pool_flags' 3x3x3 dilation, bit 0 of brick_want) into
-    // bytes, and which bricks hold a slot (bit 1) into bits.
-    for (uint32_t w = warp; w < nwords; w += blockDim.x / 32u) {
-        const uint32_t b = w * 32u + lane;
-        const uint32_t f = b < nb ? d.brick_want[b] : 0u;
-        if (b < nb) t[b] = uint8_t(f & 1u);
-        const uint32_t bits = __ballot_sync(0xFFFFFFFFu, (f & 2u) != 0u);
-        if (lane == 0u) has[w] = bits;
-    }
-    __syncthreads();
-    auto want = [&](uint32_t b) -> bool { return t[b] != 0; };
-    auto holds = [&](uint32_t b) -> bool { return ((has[b >> 5] >> (b & 31u)) & 1u) != 0u; };
-    // unwanted bricks free their slot, pushed in brick order
-    uint32_t nfree = 0;
-    for (uint32_t b = b0; b < b1; ++b)
-        if (!want(b) && holds(b)) ++nfree;
-    uint32_t total_free;
-    uint32_t k = block_scan_1024(nfree, s_warp, &total_free);
-    for (uint32_t b = b0; b < b1; ++b) {
-        if (!want(b) && holds(b)) {
-            const uint32_t slot = d.brick_table_w[b];
-            d.free_slots[1u + uint32_t(f0) + k] = slot;
-            ++k;
-            d.slot_brick[slot] = NO_BRICK;
-            d.brick_table_w[b] = 0u;
-            atomicAnd(has + (b >> 5), ~(1u << (b & 31u)));
-        }
-    }
-    const int f = f0 + int(total_free);
-    __syncthreads();
-    // Phase 2: wanted bricks without storage pop slots in brick order.
-    uint32_t nneed = 0;
-    for (uint32_t b = b0; b < b1; ++b)
-        if (want(b) && !holds(b)) ++nneed;
-    uint32_t total_need;
-    uint32_t j = block_scan_1024(nneed, s_warp, &total_need);
-    for (uint32_t b = b0; b < b1; ++b) {
-        if (want(b) && !holds(b)) {
-            const int count = f - int(j);
-            if (count > 0) {
-                const uint32_t slot = d.free_slots[count];
-                d.brick_table_w[b] = slot;
-                d.slot_brick[slot] = b;
-                d.new_slots[1u + j] = slot;
-                atomicOr(has + (b >> 5), 1u << (b & 31u));
-            }
-            ++j;
-        }
-    }
-    __syncthreads();
-    // Phase 3: active list in brick order; touch flags consumed.
-    uint32_t nact = 0;
-    for (uint32_t b = b0; b < b1; ++b)
-        if (want(b) && holds(b)) ++nact;
-    uint32_t total_act;
-    uint32_t act = block_scan_1024(nact, s_warp, &total_act);
-    for (uint32_t b = b0; b < b1; ++b)
-        if (want(b) && holds(b)) d.active_bricks[1u + act++] = b;
-    for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) d.brick_touch[b] = 0u;
-    if (threadIdx.x == 0) {
-        const uint32_t ok = uint32_t(min(int(total_need), max(f, 0)));
-        d.new_slots[0] = ok;
-        d.free_slots[0] = uint32_t(max(f - int(total_need), 0));
-        d.active_bricks[0] = total_act;
-        d.stats[8] += total_need - ok;
-        d.stats[7] = max(d.stats[7], total_act);
-    }
-}
-
-__global__ void __launch_bounds__(1024) k_pool_update(Dev d) {
+__global__ void __launch_bounds__(POOL_CTA) k_pool_flags(Dev d) {
     __shared__ uint32_t s_warp[33];
-    extern __shared__ uint8_t s_flags[];  // pool_update_smem's flags (num_bricks <= POOL_SMEM_BRICKS), else unused
-    const uint32_t nb = d.num_bricks;
-    const uint32_t per = (nb + blockDim.x - 1u) / blockDim.x;
-    const uint32_t b0 = min(threadIdx.x * per, nb);
-    const uint32_t b1 = min(b0 + per, nb);
-    const int f0 = int(d.free_slots[0]);
-    if (nb <= POOL_SMEM_BRICKS) {  // uniform
-        pool_update_smem(d, s_flags, s_warp, b0, b1, f0);
-        return;
-    }
-    const int bx = d.brick_dim.x, by = d.brick_dim.y, bz = d.brick_dim.z;
-
-    // Phase 1: wanted = touched within one brick (3x3x3 dilation); unwanted bricks free their slot.
-    for (uint32_t b = b0; b < b1; ++b) {
+    const uint32_t b = blockIdx.x * POOL_CTA + threadIdx.x;
+    const uint32_t nc = pool_ctas(d.num_bricks);
+    uint32_t f = 0u;
+    if (b < d.num_bricks) {
         const int3 c = brick_coord_of(d, b);
-        bool wanted = false;
-        for (int z = max(c.z - 1, 0); z <= min(c.z + 1, bz - 1) && !wanted; ++z)
-            for (int y = max(c.y - 1, 0); y <= min(c.y + 1, by - 1) && !wanted; ++y)
-                for (int x = max(c.x - 1, 0); x <= min(c.x + 1, bx - 1); ++x)
-                    if (d.brick_touch[uint32_t(x + bx * (y + by * z))] != 0u) { wanted = true; break; }
-        d.brick_want[b] = wanted ? 1u : 0u;
+        const int bx = d.brick_dim.x, by = d.brick_dim.y, bz = d.brick_dim.z;
+        uint32_t touched = 0u;
+        for (int z = max(c.z - 1, 0); z <= min(c.z + 1, bz - 1); ++z)
+            for (int y = max(c.y - 1, 0); y <= min(c.y + 1, by - 1); ++y)
+                for (int x = max(c.x - 1, 0); x <= min(c.x + 1, bx - 1); ++x) touched |= d.brick_touch[uint32_t(x + bx * (y + by * z))];
+        f = (touched != 0u ? 1u : 0u) | (d.brick_table_w[b] != 0u ? 2u : 0u);
+        d.brick_want[b] = f;
+    }
+    uint32_t total;
+    block_scan_1024(f == 2u ? 1u : 0u, s_warp, &total);  // held, not wanted: frees
+    if (threadIdx.x == 0) d.pool_scratch[blockIdx.x] = total;
+    block_scan_1024(f == 1u ? 1u : 0u, s_warp, &total);  // wanted, not held: needs
+    if (threadIdx.x == 0) d.pool_scratch[nc + blockIdx.x] = total;
+    block_scan_1024(f == 3u ? 1u : 0u, s_warp, &total);  // wanted and held: keeps
+    if (threadIdx.x == 0) d.pool_scratch[2u * nc + blockIdx.x] = total;
+}
+
+// Exclusive scan of n per-CTA counts in place (1,024 threads, each over a contiguous run); returns the sum.
+__device__ uint32_t pool_scan_runs(uint32_t* v, uint32_t* out, uint32_t n, uint32_t* s_warp) {
+    const uint32_t per = (n + blockDim.x - 1u) / blockDim.x;
+    const uint32_t c0 = min(threadIdx.x * per, n), c1 = min(c0 + per, n);
+    uint32_t sum = 0u;
+    for (uint32_t c = c0; c < c1; ++c) sum += v[c];
+    uint32_t total;
+    uint32_t run = block_scan_1024(sum, s_warp, &total);
+    for (uint32_t c = c0; c < c1; ++c) {
+        const uint32_t t = v[c];
+        out[c] = run;
+        run += t;
     }
     __syncthreads();
-    auto want = [&](uint32_t b) -> bool { return d.brick_want[b] != 0u; };
-    uint32_t nfree = 0;
-    for (uint32_t b = b0; b < b1; ++b)
-        if (!want(b) && d.brick_table_w[b] != 0u) ++nfree;
-    uint32_t total_free;
-    uint32_t k = block_scan_1024(nfree, s_warp, &total_free);
-    for (uint32_t b = b0; b < b1; ++b) {
-        if (!want(b)) {
-            const uint32_t slot = d.brick_table_w[b];
-            if (slot != 0u) {
-                d.free_slots[1u + uint32_t(f0) + k] = slot;
-                ++k;
-                d.slot_brick[slot] = NO_BRICK;
-                d.brick_table_w[b] = 0u;
-            }
-        }
-    }
+    return total;
+}
+__global__ void __launch_bounds__(1024) k_pool_plan(Dev d) {
+    __shared__ uint32_t s_warp[33];
+    const uint32_t nc = pool_ctas(d.num_bricks);
+    uint32_t* cnt = d.pool_scratch;
+    uint32_t* off = d.pool_scratch + 3u * nc;
+    const int f0 = int(d.free_slots[0]);
+    const uint32_t total_free = pool_scan_runs(cnt, off, nc, s_warp);
+    const uint32_t total_need = pool_scan_runs(cnt + nc, off + nc, nc, s_warp);
     const int f = f0 + int(total_free);
-    __syncthreads();
-
-    // Phase 2: wanted bricks without storage pop slots in brick order.
-    uint32_t nneed = 0;
-    for (uint32_t b = b0; b < b1; ++b)
-        if (want(b) && d.brick_table_w[b] == 0u) ++nneed;
-    uint32_t total_need;
-    uint32_t j = block_scan_1024(nneed, s_warp, &total_need);
-    for (uint32_t b = b0; b < b1; ++b) {
-        if (want(b) && d.brick_table_w[b] == 0u) {
-            const int count = f - int(j);
-            if (count > 0) {
-                const uint32_t slot = d.free_slots[count];
-                d.brick_table_w[b] = slot;
-                d.slot_brick[slot] = b;
-                d.new_slots[1u + j] = slot;
-            }
-            ++j;
-        }
+    // a CTA's active bricks: those keeping their slot and those of its needs whose pop finds a slot (rank < f)
+    for (uint32_t c = threadIdx.x; c < nc; c += blockDim.x) {
+        const int got = min(max(f - int(off[nc + c]), 0), int(cnt[nc + c]));
+        cnt[2u * nc + c] += uint32_t(got);
     }
     __syncthreads();
-
-    // Phase 3: active list in brick order; touch flags consumed.
-    uint32_t nact = 0;
-    for (uint32_t b = b0; b < b1; ++b)
-        if (want(b) && d.brick_table_w[b] != 0u) ++nact;
-    uint32_t total_act;
-    uint32_t a = block_scan_1024(nact, s_warp, &total_act);
-    for (uint32_t b = b0; b < b1; ++b)
-        if (want(b) && d.brick_table_w[b] != 0u) d.active_bricks[1u + a++] = b;
-    for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) d.brick_touch[b] = 0u;
+    const uint32_t total_act = pool_scan_runs(cnt + 2u * nc, off + 2u * nc, nc, s_warp);
     if (threadIdx.x == 0) {
+        d.pool_scratch[6u * nc] = uint32_t(f0);
+        d.pool_scratch[6u * nc + 1u] = uint32_t(f);
         const uint32_t ok = uint32_t(min(int(total_need), max(f, 0)));
         d.new_slots[0] = ok;
         d.free_slots[0] = uint32_t(max(f - int(total_need), 0));
@@ -338,6 +236,43 @@ __global__ void __launch_bounds__(1024) k_pool_update(Dev d) {
         d.stats[8] += total_need - ok;
         d.stats[7] = max(d.stats[7], total_act);
     }
+}
+__global__ void __launch_bounds__(POOL_CTA) k_pool_free(Dev d) {
+    __shared__ uint32_t s_warp[33];
+    const uint32_t b = blockIdx.x * POOL_CTA + threadIdx.x;
+    const uint32_t nc = pool_ctas(d.num_bricks);
+    const uint32_t f = b < d.num_bricks ? d.brick_want[b] : 0u;
+    uint32_t total;
+    const uint32_t k = block_scan_1024(f == 2u ? 1u : 0u, s_warp, &total) + d.pool_scratch[3u * nc + blockIdx.x];
+    if (f == 2u) {
+        const uint32_t f0 = d.pool_scratch[6u * nc];
+        const uint32_t slot = d.brick_table_w[b];
+        d.free_slots[1u + f0 + k] = slot;
+        d.slot_brick[slot] = NO_BRICK;
+        d.brick_table_w[b] = 0u;
+    }
+}
+__global__ void __launch_bounds__(POOL_CTA) k_pool_alloc(Dev d) {
+    __shared__ uint32_t s_warp[33];
+    const uint32_t b = blockIdx.x * POOL_CTA + threadIdx.x;
+    const uint32_t nc = pool_ctas(d.num_bricks);
+    const uint32_t f = b < d.num_bricks ? d.brick_want[b] : 0u;
+    uint32_t total;
+    const uint32_t j = block_scan_1024(f == 1u ? 1u : 0u, s_warp, &total) + d.pool_scratch[4u * nc + blockIdx.x];
+    bool act = f == 3u;
+    if (f == 1u) {
+        const int count = int(d.pool_scratch[6u * nc + 1u]) - int(j);
+        if (count > 0) {
+            const uint32_t slot = d.free_slots[count];
+            d.brick_table_w[b] = slot;
+            d.slot_brick[slot] = b;
+            d.new_slots[1u + j] = slot;
+            act = true;
+        }
+    }
+    const uint32_t a = block_scan_1024(act ? 1u : 0u, s_warp, &total) + d.pool_scratch[5u * nc + blockIdx.x];
+    if (act) d.active_bricks[1u + a] = b;
+    if (b < d.num_bricks) d.brick_touch[b] = 0u;
 }
 
 __global__ void k_clear_new_slots(Dev d) {  // ClearNewSlotsCS
@@ -915,20 +850,14 @@ __global__ void __launch_bounds__(GRID_THREADS) k_extrapolate(Dev d, const float
 }  // namespace
 
 int launch_pool_update(const Dev& d, cudaStream_t s) {
-    const uint32_t smem = d.num_bricks <= POOL_SMEM_BRICKS ? ((d.num_bricks + 3u) & ~3u) + 4u * ((d.num_bricks + 31u) / 32u) : 0u;
-    static uint32_t configured = 0;
-    if (smem > 48u * 1024u && smem > configured) {
-        cudaFuncSetAttribute(k_pool_update, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-        configured = smem;
-    }
-    if (d.num_bricks <= POOL_SMEM_BRICKS) {
-        k_pool_flags<<<(d.num_bricks + 255u) / 256u, 256, 0, s>>>(d);
-        k_pool_update<<<1, 1024, smem, s>>>(d);
-        return 2;
-    }
-    k_pool_update<<<1, 1024, smem, s>>>(d);
-    return 1;
+    const uint32_t nc = (d.num_bricks + POOL_CTA - 1u) / POOL_CTA;
+    k_pool_flags<<<nc, POOL_CTA, 0, s>>>(d);
+    k_pool_plan<<<1, 1024, 0, s>>>(d);
+    k_pool_free<<<nc, POOL_CTA, 0, s>>>(d);
+    k_pool_alloc<<<nc, POOL_CTA, 0, s>>>(d);
+    return 4;
 }
+size_t pool_scratch_words(uint32_t num_bricks) { return 6u * size_t((num_bricks + POOL_CTA - 1u) / POOL_CTA) + 2u; }
 int launch_clear_new_slots(const Dev& d, const Shape& sh, cudaStream_t s) {
     k_clear_new_slots<<<sh.brick_ctas, 256, 0, s>>>(d);
     return 1;
