@@ -646,8 +646,7 @@ struct Ctx {
                     cudaStream_t s, bool setup) {
         int n = launch_mg_setup(mg, limit, tol_mode, double(tol), s);
         if (setup) {
-            for (int l = 0; l < num_levels - 1; ++l) n += launch_mg_build_type(d, mg, l, shape, s);
-            for (int l = 1; l < num_levels; ++l) n += launch_mg_words(d, mg, l, shape, s);
+            n += launch_mg_coarse_setup(d, mg, shape, s);
             n += launch_mg_tail_lists(mg, s);
         }
         n += launch_pcg_init(d, mg, p, div, handle, shape, s, setup);

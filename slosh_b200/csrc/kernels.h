@@ -144,6 +144,8 @@ size_t mg_tail_smem(const MGState& m);
 int mg_tail_level(const MGState& m);
 int launch_mg_setup(const MGState& m, uint32_t limit, bool tol_mode, double tol, cudaStream_t s);
 int launch_mg_build_type(const Dev& d, const MGState& m, int l, const Shape& sh, cudaStream_t s);
+// Every coarse level's types and words (levels 1-3 fused: one launch for the types, one for the words).
+int launch_mg_coarse_setup(const Dev& d, const MGState& m, const Shape& sh, cudaStream_t s);
 // handle: the WHILE node's condition when the solve runs as a CUDA graph, 0 otherwise.
 int launch_pcg_init(const Dev& d, const MGState& m, const float* p, const float* div, unsigned long long handle, const Shape& sh,
                     cudaStream_t s, bool words = true);

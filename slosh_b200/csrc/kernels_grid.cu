@@ -69,26 +69,40 @@ __device__ float cell_density(const Dev& d, const Pass& p, int3 c) {
 __device__ __forceinline__ float air_face_weight(const Dev& d, const Pass& p, float rho_fluid, int3 air) {
     return p.ghost_fluid != 0u ? 1.0f / ghost_theta(rho_fluid, cell_density(d, p, air)) : 1.0f;
 }
-// CellDensityInterior (Slosh.usf:753-773).
-__device__ float cell_density_interior(const Dev& d, const Pass& p, uint32_t index, int3 c) {
+// CellDensityInterior (Slosh.usf:753-773) and whether a cell touches air, from one round of loads: the six
+// neighbours' types (outside the grid: solid) and the weights of the cell's six faces (-x, +x, -y, +y, -z, +z), all
+// issued before any is tested; the sums keep CellDensityInterior's order.
+struct DensityNbrs {
+    uint32_t nt[6];
+    float w[6];
+};
+template <bool kSlots = true>
+__device__ __forceinline__ DensityNbrs load_density_nbrs(const Dev& d, uint32_t index, int3 c) {
+    DensityNbrs q;
+#pragma unroll
+    for (int n = 0; n < 6; ++n) {
+        const uint32_t ni = nidx<kSlots>(d, index, c, n);
+        q.nt[n] = in_grid(d, add3(c, nbr_off(n))) ? d.cell_type[ni] : CELL_SOLID;
+        const uint32_t a = uint32_t(n >> 1);
+        q.w[n] = d.face_weight[a * d.pool_cells + ((n & 1) ? ni : index)];
+    }
+    return q;
+}
+__device__ __forceinline__ float density_interior_of(const Pass& p, const DensityNbrs& q) {
     float ws = 0.0f, faces = 0.0f;
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        if (type_of(ntype(d, index, c, 2 * a)) != CELL_SOLID) {
-            ws = ws + d.face_weight[uint32_t(a) * d.pool_cells + index];
-            faces = faces + 1.0f;
-        }
-        if (type_of(ntype(d, index, c, 2 * a + 1)) != CELL_SOLID) {
-            ws = ws + d.face_weight[uint32_t(a) * d.pool_cells + nidx(d, index, c, 2 * a + 1)];
+    for (int n = 0; n < 6; ++n) {
+        if (type_of(q.nt[n]) != CELL_SOLID) {
+            ws = ws + q.w[n];
             faces = faces + 1.0f;
         }
     }
     return faces > 0.0f ? ws / (faces * p.target_ppc) : 1.0f;
 }
-__device__ __forceinline__ bool touches_air(const Dev& d, uint32_t index, int3 c) {
+__device__ __forceinline__ bool touches_air_of(const DensityNbrs& q) {
     bool t = false;
 #pragma unroll
-    for (int n = 0; n < 6; ++n) t = t || type_of(ntype(d, index, c, n)) == CELL_AIR;
+    for (int n = 0; n < 6; ++n) t = t || type_of(q.nt[n]) == CELL_AIR;
     return t;
 }
 
@@ -736,16 +750,23 @@ __global__ void __launch_bounds__(GRID_THREADS) k_residual(Dev d, Pass p, const 
     uint32_t max_bits = 0u, rate_sum = 0u, cells = 0u, dens_sum = 0u, interior = 0u;
     for_active_cells<true>(d, [&](uint32_t index, int3 c) {
         if (type_of(d.cell_type[index]) != CELL_FLUID) return;
+        // one round of loads: the faces' velocities, the neighbours' types and the face weights
+        float vlo[3], vhi[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            vhi[a] = vel[uint32_t(a) * d.pool_cells + nidx(d, index, c, 2 * a + 1)];
+            vlo[a] = vel[uint32_t(a) * d.pool_cells + index];
+        }
+        const DensityNbrs q = load_density_nbrs(d, index, c);
         float div = 0.0f;
 #pragma unroll
-        for (int a = 0; a < 3; ++a)
-            div = div + (vel[uint32_t(a) * d.pool_cells + nidx(d, index, c, 2 * a + 1)] - vel[uint32_t(a) * d.pool_cells + index]);
+        for (int a = 0; a < 3; ++a) div = div + (vhi[a] - vlo[a]);
         const float rate = fabsf(div) * d.inv_h;
         max_bits = max(max_bits, __float_as_uint(rate));
         rate_sum += __float2uint_rz(fminf(rate, 1.0e5f) * 1000.0f);
         ++cells;
-        if (!touches_air(d, index, c)) {
-            const float dens = clampf(cell_density_interior(d, p, index, c), 0.0f, 4.0f);
+        if (!touches_air_of(q)) {
+            const float dens = clampf(density_interior_of(p, q), 0.0f, 4.0f);
             dens_sum += uint32_t(__float2int_rn((dens - 1.0f) * 10000.0f));
             ++interior;
         }
@@ -771,8 +792,9 @@ __global__ void __launch_bounds__(GRID_THREADS) k_density_rhs(Dev d, Pass p) {
     for_active_cells<true>(d, [&](uint32_t index, int3 c) {
         d.density_q[index] = 0.0f;
         if (type_of(d.cell_type[index]) != CELL_FLUID) { d.density_rhs[index] = 0.0f; return; }
-        float dev = cell_density_interior(d, p, index, c) - 1.0f;
-        if (touches_air(d, index, c)) dev = fmaxf(dev, 0.0f);
+        const DensityNbrs q = load_density_nbrs(d, index, c);
+        float dev = density_interior_of(p, q) - 1.0f;
+        if (touches_air_of(q)) dev = fmaxf(dev, 0.0f);
         d.density_rhs[index] = -p.density_relaxation * clampf(dev, -0.5f, 0.5f);
     });
 }

@@ -492,6 +492,69 @@ __global__ void k_build_type_fp(Dev d, MGLevel fine, MGLevel coarse, int lc) {
     for_footprint(d, coarse, lc, [&](uint32_t ci, int3 c) { build_type_cell(d, fine, coarse, lc == 1 ? 1 : 0, ci, c); });
 }
 
+// Levels 1 to top (top <= 3) in one launch, one warp per active brick: a coarse type is air when any of its level-0
+// descendants inside the grid is air, else fluid when any is fluid, else solid -- the rule above applied level by
+// level gives the same (every cell inside a level has a child inside the level below), and the descendants of a
+// brick's footprint cells at levels 1-3 are the brick's own 512 cells. Lane t holds cells l = t + 32 k (k = 0..15):
+// x = t & 7, y = (t >> 3) + 4 (k & 1), z = k >> 1, so the children of one coarse cell are combined across lanes
+// t ^ 1, t ^ 2, t ^ 4 (x), t ^ 8, t ^ 16 and k ^ 1 (y), k ^ 2, k ^ 4, k ^ 8 (z).
+__device__ __forceinline__ uint32_t type_of_flags(uint32_t f) { return (f & 1u) ? CELL_AIR : ((f & 2u) ? CELL_FLUID : CELL_SOLID); }
+__global__ void __launch_bounds__(256) k_build_types_fp13(Dev d, MGState m, int top) {
+    pdl_entry();
+    const uint32_t active = d.active_bricks[0];
+    const uint32_t lane = threadIdx.x & 31u, wpb = blockDim.x >> 5;
+    for (uint32_t e = blockIdx.x * wpb + (threadIdx.x >> 5); e < active; e += gridDim.x * wpb) {
+        const uint32_t brick = d.active_bricks[1u + e];
+        const uint32_t slot = __ldg(d.brick_table + brick);
+        const int3 bc = brick_coord_of(d, brick);
+        uint32_t g[16];  // bit 0: some descendant is air, bit 1: some is fluid
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            const uint32_t l = lane + 32u * uint32_t(k);
+            const int3 lc = local_coord_of(l);
+            const int3 c = make_int3(bc.x * 8 + lc.x, bc.y * 8 + lc.y, bc.z * 8 + lc.z);
+            const uint32_t t = in_grid(d, c) ? (d.cell_type[slot * BRICK_CELLS + l] & CELL_TYPE_MASK) : CELL_SOLID;
+            g[k] = (t == CELL_AIR ? 1u : 0u) | (t == CELL_FLUID ? 2u : 0u);
+        }
+        const uint32_t x = lane & 7u, ylo = lane >> 3;
+        // level 1: x pairs (t ^ 1), y pairs (t ^ 8), z pairs (k ^ 2)
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            if (k & 2) continue;
+            uint32_t v = g[k] | g[k ^ 2];
+            v |= __shfl_xor_sync(0xFFFFFFFFu, v, 1);
+            v |= __shfl_xor_sync(0xFFFFFFFFu, v, 8);
+            g[k] = v;
+            const MGLevel& L = m.lv[1];
+            const uint32_t y = ylo + 4u * uint32_t(k & 1), z = uint32_t(k) >> 1;
+            const int3 c = make_int3(bc.x * 4 + int(x >> 1), bc.y * 4 + int(y >> 1), bc.z * 4 + int(z >> 1));
+            if ((lane & 9u) == 0u && inside3(c, L.dim)) L.type[lin3(c, L.dim)] = type_of_flags(v);
+        }
+        if (top < 2) continue;
+        // level 2: with the above, x quads (t ^ 2), y quads (t ^ 16), z quads (k ^ 4)
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            if (k & 6) continue;
+            uint32_t v = g[k] | g[k ^ 4];
+            v |= __shfl_xor_sync(0xFFFFFFFFu, v, 2);
+            v |= __shfl_xor_sync(0xFFFFFFFFu, v, 16);
+            g[k] = v;
+            const MGLevel& L = m.lv[2];
+            const uint32_t y = ylo + 4u * uint32_t(k & 1), z = uint32_t(k) >> 1;
+            const int3 c = make_int3(bc.x * 2 + int(x >> 2), bc.y * 2 + int(y >> 2), bc.z * 2 + int(z >> 2));
+            if ((lane & 27u) == 0u && inside3(c, L.dim)) L.type[lin3(c, L.dim)] = type_of_flags(v);
+        }
+        if (top < 3) continue;
+        // level 3: the whole brick
+        uint32_t v = g[0] | g[1] | g[8] | g[9];
+        v = __reduce_or_sync(0xFFFFFFFFu, v);
+        const MGLevel& L = m.lv[3];
+        if (lane == 0u && inside3(bc, L.dim)) L.type[lin3(bc, L.dim)] = type_of_flags(v);
+    }
+}
+// The words of levels 1 to top (top <= 3) in one launch: each thread walks the three footprints in turn.
+__global__ void k_level_words_fp13(Dev d, MGState m, int top);
+
 // ---- coarse-level stencil words (once per solve, after the coarse types) -----------------------------------
 
 __device__ __forceinline__ void level_word_cell(const MGLevel& L, uint32_t i, int3 c) {
@@ -517,6 +580,14 @@ __global__ void k_level_words(MGLevel L) {
 __global__ void k_level_words_fp(Dev d, MGLevel L, int l) {
     pdl_entry();
     for_footprint(d, L, l, [&](uint32_t i, int3 c) { level_word_cell(L, i, c); });
+}
+__global__ void k_level_words_fp13(Dev d, MGState m, int top) {
+    pdl_entry();
+    const uint32_t t0 = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+    for (int l = 1; l <= top; ++l) {
+        const MGLevel& L = m.lv[l];
+        for_footprint_span(d, L, l, t0, stride, [&](uint32_t i, int3 c) { level_word_cell(L, i, c); });
+    }
 }
 // DiagEpsilon plus one per non-solid neighbour, added in neighbour order like FINE_STENCIL.
 __device__ __forceinline__ float word_diag(uint32_t w) {
@@ -2045,6 +2116,22 @@ int launch_mg_build_type(const Dev& d, const MGState& m, int l, const Shape& sh,
     }
     launch_k(k_build_type, blocks_for(C.cells, 256), 256, 0, s, d, m.lv[l], C, l == 0 ? 1 : 0);
     return 1;
+}
+// The coarse types and stencil words of every level: levels 1-3 (those walked through the active bricks'
+// footprints) by one launch each for the types and the words, the dense levels below them level by level.
+int launch_mg_coarse_setup(const Dev& d, const MGState& m, const Shape& sh, cudaStream_t s) {
+    const int nl = m.num_levels;
+    if (nl < 2) return 0;
+    const int top = std::min(3, nl - 1);
+    int n = 0;
+    for (int l = 1; l <= top; ++l) cudaMemsetAsync(m.lv[l].type, 0, size_t(m.lv[l].cells) * sizeof(uint32_t), s);
+    launch_k(k_build_types_fp13, sh.mg_ctas, 256, 0, s, d, m, top);
+    ++n;
+    for (int l = top; l < nl - 1; ++l) n += launch_mg_build_type(d, m, l, sh, s);
+    launch_k(k_level_words_fp13, fp_grid(d, sh, 1), 256, 0, s, d, m, top);
+    ++n;
+    for (int l = top + 1; l < nl; ++l) n += launch_mg_words(d, m, l, sh, s);
+    return n;
 }
 int launch_pcg_init(const Dev& d, const MGState& m, const float* p, const float* div, unsigned long long handle, const Shape& sh,
                     cudaStream_t s, bool words) {
