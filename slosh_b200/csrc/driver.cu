@@ -887,11 +887,8 @@ struct Ctx {
         }
         {
             PhaseScope ps(this, 7);
-            for (int it = 0; it < S.extrapolation_layers; ++it) {
-                const int dst = (c + 1) % 3;
-                count(launch_extrapolate(d, V[c], V[dst], uint32_t(it), shape, stream));
-                c = dst;
-            }
+            // in place (the reference passes the field from buffer to buffer; the values are the same)
+            for (int it = 0; it < S.extrapolation_layers; ++it) count(launch_extrapolate(d, V[c], uint32_t(it), shape, stream));
             if (density) count(launch_density_displacement(d, V[(c + 2) % 3], shape, stream));
         }
         {

@@ -56,7 +56,8 @@ int launch_coupling(const Dev& d, const Pass& p, const float* vel, const Shape& 
 int launch_submerged(const Dev& d, const Shape& sh, cudaStream_t s);
 int launch_density_rhs(const Dev& d, const Pass& p, const Shape& sh, cudaStream_t s);
 int launch_density_displacement(const Dev& d, float* dst, const Shape& sh, cudaStream_t s);
-int launch_extrapolate(const Dev& d, const float* src, float* dst, uint32_t iteration, const Shape& sh, cudaStream_t s);
+// One layer of ExtrapolateFace, in place.
+int launch_extrapolate(const Dev& d, float* vel, uint32_t iteration, const Shape& sh, cudaStream_t s);
 
 // ---- particles ----
 int launch_emit_reserve(uint32_t* particle_count, uint32_t count, cudaStream_t s);

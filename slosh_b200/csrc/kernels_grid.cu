@@ -820,38 +820,35 @@ __global__ void __launch_bounds__(GRID_THREADS) k_density_displacement(Dev d, fl
     });
 }
 
-// ---- ExtrapolateFace ---------------------------------------------------------------------------------------
-// A face's own new bit is written while neighbours read its flags; readers only test bits set by
-// earlier layers, so the result does not depend on the interleaving.
-__global__ void __launch_bounds__(GRID_THREADS) k_extrapolate(Dev d, const float* __restrict__ src, float* __restrict__ dst,
-                                                              uint32_t iteration) {
+// ---- ExtrapolateFace -------------------------------------------------------------------------------------------
+// In place: a layer writes only faces unknown so far (the average of their known neighbours, with the layer's bit,
+// or zero), and every reader uses only faces known from earlier layers, which no layer writes, so the result equals
+// the reference's pass from one buffer into another. A face's own new bit is written while neighbours read its
+// flags; readers only test bits set by earlier layers, so the result does not depend on the interleaving. Known
+// faces cost one flag load (the two-buffer form copies their values).
+__global__ void __launch_bounds__(GRID_THREADS) k_extrapolate(Dev d, float* vel, uint32_t iteration) {
     uint32_t known = FACE_VALID;
     for (uint32_t it = 0; it < iteration; ++it) known |= 1u << (FACE_EXTRAP_SHIFT + it);
     const uint32_t new_bit = 1u << (FACE_EXTRAP_SHIFT + iteration);
     for_active_cells<true>(d, [&](uint32_t index, int3 c) {
-        // the three faces' flags and values first (one round), the neighbours only for faces still unknown
         uint32_t fls[3];
-        float cen[3];
+#pragma unroll
+        for (int axis = 0; axis < 3; ++axis) fls[axis] = d.face_flags[uint32_t(axis) * d.pool_cells + index];
 #pragma unroll
         for (int axis = 0; axis < 3; ++axis) {
-            fls[axis] = d.face_flags[uint32_t(axis) * d.pool_cells + index];
-            cen[axis] = src[uint32_t(axis) * d.pool_cells + index];
-        }
-#pragma unroll
-        for (int axis = 0; axis < 3; ++axis) {
-            const uint32_t f = uint32_t(axis) * d.pool_cells + index;
             const uint32_t flags = fls[axis];
-            const float center = cen[axis];
-            if ((flags & known) != 0u) { dst[f] = center; continue; }
-            // all six neighbours' flags and values are loaded before any is tested (an out-of-grid
-            // neighbour reads the null slot and is then skipped)
+            if ((flags & known) != 0u) continue;
+            const uint32_t f = uint32_t(axis) * d.pool_cells + index;
+            // the face's value and all six neighbours' flags and values are loaded before any is tested (an
+            // out-of-grid neighbour reads the null slot and is then skipped)
+            const float center = vel[f];
             uint32_t nf[6];
             float nv[6];
 #pragma unroll
             for (int n = 0; n < 6; ++n) {
                 const uint32_t ni = uint32_t(axis) * d.pool_cells + nbr_index_cta(index, c, n);
                 nf[n] = d.face_flags[ni];
-                nv[n] = src[ni];
+                nv[n] = vel[ni];
             }
             float sum = 0.0f, count = 0.0f;
 #pragma unroll
@@ -860,10 +857,10 @@ __global__ void __launch_bounds__(GRID_THREADS) k_extrapolate(Dev d, const float
                 if ((nf[n] & known) != 0u && (nf[n] & FACE_SOLID) == 0u) { sum = sum + nv[n]; count = count + 1.0f; }
             }
             if (count > 0.0f) {
-                dst[f] = sum / count;
+                vel[f] = sum / count;
                 d.face_flags[f] = flags | new_bit;
-            } else {
-                dst[f] = 0.0f;
+            } else if (__float_as_uint(center) != 0u) {
+                vel[f] = 0.0f;
             }
         }
     });
@@ -931,8 +928,8 @@ int launch_density_displacement(const Dev& d, float* dst, const Shape& sh, cudaS
     k_density_displacement<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, dst);
     return 1;
 }
-int launch_extrapolate(const Dev& d, const float* src, float* dst, uint32_t iteration, const Shape& sh, cudaStream_t s) {
-    k_extrapolate<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, src, dst, iteration);
+int launch_extrapolate(const Dev& d, float* vel, uint32_t iteration, const Shape& sh, cudaStream_t s) {
+    k_extrapolate<<<sh.brick_ctas, GRID_THREADS, 0, s>>>(d, vel, iteration);
     return 1;
 }
 
