@@ -651,38 +651,34 @@ __global__ void __launch_bounds__(GRID_THREADS) k_pcg_words(Dev d, MGState m) {
         uint32_t ns[6];
 #pragma unroll
         for (int n = 0; n < 6; ++n) ns[n] = __shfl_sync(0xFFFFFFFFu, mine, n);
-        // 16 cells per lane in groups of 4: the types of a group's cells and their 6 neighbours are all loaded
-        // before its words are stored (a neighbour across a face through the face neighbour's slot; an
-        // unallocated brick is the all-zero null slot, whose cells are air)
-        for (uint32_t g = 0; g < 4u; ++g) {
-            uint32_t t[4][7];
+        // the half-row quads of the level-0 passes: per round the types of the lane's 4 cells and of the adjacent
+        // rows' 4 (16-byte loads; across a face through the face neighbour's slot, an unallocated brick being the
+        // null slot of air cells), the +-x neighbours inside the row from the partner lane; the 4 words go out as
+        // one 32-bit store
+        const float* types = reinterpret_cast<const float*>(d.cell_type);  // loaded and shuffled as bits only
+        const uint32_t base = slot * BRICK_CELLS;
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const uint32_t l = lane + 32u * (4u * g + uint32_t(q));
-                const int3 lc = local_coord_of(l);
-                const int3 c = make_int3(bc.x * 8 + lc.x, bc.y * 8 + lc.y, bc.z * 8 + lc.z);
-                const uint32_t i = slot * BRICK_CELLS + l;
-                const bool in = in_grid(d, c);
-                t[q][6] = in ? d.cell_type[i] : 0u;
+        for (uint32_t k = 0; k < 4u; ++k) {
+            const Geo g = geo_of(base, lane, k);
+            const Q6 q = load_q6(types, g, ns);
+            const X2 x = partner(q);
+            uint32_t packed = 0u;
 #pragma unroll
-                for (int n = 0; n < 6; ++n)
-                    t[q][n] = (in && in_grid(d, add3(c, nbr_off(n)))) ? d.cell_type[l0_nbr(i, l, n, ns)] : 0u;
-            }
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const uint32_t l = lane + 32u * (4u * g + uint32_t(q));
-                const int3 lc = local_coord_of(l);
-                const int3 c = make_int3(bc.x * 8 + lc.x, bc.y * 8 + lc.y, bc.z * 8 + lc.z);
+            for (int j = 0; j < 4; ++j) {
+                const int3 c = make_int3(bc.x * 8 + int(4u * g.h) + j, bc.y * 8 + int(g.y), bc.z * 8 + int(g.z));
                 uint32_t w = 0u;
                 if (in_grid(d, c)) {
-                    if ((t[q][6] & CELL_TYPE_MASK) == CELL_FLUID) w |= W_FLUID;
+                    float n[6];
+                    nbrs6(q, x, g.h, j, n);
+                    if ((__float_as_uint(comp(q.c, j)) & CELL_TYPE_MASK) == CELL_FLUID) w |= W_FLUID;
                     if (is_red(c)) w |= W_RED;
 #pragma unroll
-                    for (int n = 0; n < 6; ++n)
-                        if ((t[q][n] & CELL_TYPE_MASK) == CELL_FLUID) w |= 1u << n;
+                    for (int m6 = 0; m6 < 6; ++m6)
+                        if (in_grid(d, add3(c, nbr_off(m6))) && (__float_as_uint(n[m6]) & CELL_TYPE_MASK) == CELL_FLUID) w |= 1u << m6;
                 }
-                m.word[slot * BRICK_CELLS + l] = uint8_t(w);
+                packed |= w << (8 * j);
             }
+            *reinterpret_cast<uint32_t*>(m.word + g.i) = packed;
         }
     }
 }
