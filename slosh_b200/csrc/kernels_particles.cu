@@ -121,8 +121,9 @@ __global__ void k_touch(Dev d, const slosh_particle_t* __restrict__ particles, u
 // Measured per 256^3 launch (sorted frames): 2 particles per thread with a 1,024-node tile (28 KB), both records
 // loaded before the box reduction and held in registers (64 registers, 4 CTAs per SM) 0.739 ms; the same at 48
 // registers and 5 CTAs per SM (68 bytes of spills) 0.748, and reading the records again after the barrier at 5
-// CTAs per SM 0.767 (0.820 before the unchecked interior path and the merged flush; 0.975 with the 2,048-node
-// tile at 4 CTAs per SM); 0.857 with 4 particles per thread; 1 per thread at 6 CTAs per SM was slower. In the frames between a bulk emission and the first sort the particles are in emission order and most
+// CTAs per SM 0.767 (0.820 before the unchecked interior path and the merged flush); the 2,048-node tile on sorted
+// frames too, also at 4 CTAs per SM, 0.772; 0.857 with 4 particles per thread; 1 per thread at 6 CTAs per SM was
+// slower. In the frames between a bulk emission and the first sort the particles are in emission order and most
 // boxes exceed the 1,024-node tile (1.2-1.4 ms per launch on the direct path); the driver then launches the
 // 2,048-node tile, which fits them: 0.78-0.80 ms.
 constexpr int P2G_THREADS = 256;
